@@ -1,0 +1,640 @@
+// C ABI of the B200 kriging engine: contexts, device buffers, parameter
+// checks and the fit / predict / cross-validate pipelines.
+//
+// Host-side math here is the one-off frame set-up of a call (3x3 matrices);
+// every per-sample and per-target step runs in the CUDA kernels. There is no
+// CPU path for the kriging itself.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "btk_internal.h"
+
+namespace {
+
+using namespace btk;
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr, n = 0;
+  }
+  cudaError_t grow(size_t want) {
+    if (want <= n) return cudaSuccess;
+    release();
+    cudaError_t e = cudaMalloc(&p, sizeof(T) * (want > 0 ? want : 1));
+    if (e == cudaSuccess) n = want;
+    return e;
+  }
+};
+
+// ---- 3x3 frames (crates/core/src/rotation.rs:8-43, aniso.rs:88-94) ----
+// Products accumulate column by column as nalgebra's gemv does, so the
+// search frame is the reference's to the last bit.
+struct M3 {
+  double m[3][3];
+};
+
+M3 eye() {
+  M3 r{};
+  r.m[0][0] = r.m[1][1] = r.m[2][2] = 1.0;
+  return r;
+}
+
+M3 mul(const M3& a, const M3& b) {
+  M3 r{};
+  for (int j = 0; j < 3; ++j)
+    for (int i = 0; i < 3; ++i) {
+      double y = a.m[i][0] * b.m[0][j];
+      y = a.m[i][1] * b.m[1][j] + y;
+      y = a.m[i][2] * b.m[2][j] + y;
+      r.m[i][j] = y;
+    }
+  return r;
+}
+
+M3 rows(double a, double b, double c, double d, double e, double f, double g, double h, double i) {
+  M3 r;
+  r.m[0][0] = a, r.m[0][1] = b, r.m[0][2] = c, r.m[1][0] = d, r.m[1][1] = e, r.m[1][2] = f;
+  r.m[2][0] = g, r.m[2][1] = h, r.m[2][2] = i;
+  return r;
+}
+
+M3 rotation(double az, double dip, double rake) {
+  const double k = 3.14159265358979323846 / 180.0;  // f64::to_radians
+  double sa = std::sin(az * k), ca = std::cos(az * k), sd = std::sin(dip * k), cd = std::cos(dip * k);
+  double sr = std::sin(rake * k), cr = std::cos(rake * k);
+  M3 r1 = rows(sa, ca, 0.0, -ca, sa, 0.0, 0.0, 0.0, 1.0);
+  M3 r2 = rows(cd, 0.0, -sd, 0.0, 1.0, 0.0, sd, 0.0, cd);
+  M3 r3 = rows(1.0, 0.0, 0.0, 0.0, cr, sr, 0.0, -sr, cr);
+  return mul(mul(r3, r2), r1);
+}
+
+M3 block_frame(double az, double dip, double rake) {
+  M3 r = rotation(az, dip, rake);
+  return rows(-r.m[1][0], -r.m[1][1], -r.m[1][2], r.m[0][0], r.m[0][1], r.m[0][2], r.m[2][0], r.m[2][1], r.m[2][2]);
+}
+
+M3 aniso_matrix(const btk_aniso& a) {
+  M3 d{};
+  d.m[0][0] = 1.0 / a.major, d.m[1][1] = 1.0 / a.semi, d.m[2][2] = 1.0 / a.minor;
+  return mul(d, rotation(a.azimuth, a.dip, a.rake));
+}
+
+void put9(const M3& m, double* out) {
+  for (int i = 0; i < 9; ++i) out[i] = m.m[i / 3][i % 3];
+}
+
+}  // namespace
+
+struct btk_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sm_count = 0;
+  int64_t launches = 0;
+  std::string err;
+  double ppc = 2.0;  // samples per grid cell
+
+  bool fitted = false;
+  int64_t n = 0;
+  bool has_err = false, planar = false;
+  btk_search search{};
+  btk_variogram vg{};
+  VgDev vgd{};
+  SearchDev spd{};
+  GridDev gd{};
+  std::vector<double> host_z;  // sample elevations, for the planar test
+
+  DevBuf<double> x, y, z, v, e, px, py, pz, spx, spy, spz, swx, swy, swz, bpart, b6, frame9, origin3;
+  DevBuf<uint32_t> sidx, start, cell_count, cell_of;
+  DevBuf<uint8_t> twin;
+  DevBuf<int64_t> loo_perm;
+
+  // per-call scratch, grown on demand
+  DevBuf<double> txyz, aos, ft9;
+  DevBuf<int64_t> perm, lists, lens, redo, redo_len;
+  DevBuf<uint32_t> nbr;
+  DevBuf<int32_t> cnt, o_nused;
+  DevBuf<int8_t> sst, o_status;
+  DevBuf<double> o_value, o_var, o_lag;
+
+  Launch launch(cudaStream_t s) { return Launch{s ? s : stream, sm_count, &launches}; }
+};
+
+namespace {
+
+int fail(btk_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess) return fail(ctx, BTK_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+bool fin(double v) { return std::isfinite(v); }
+
+// crates/variogram/src/{composite,model,aniso}.rs validate(); power has no
+// sill and goes to the reference's LU path, which this engine does not run.
+int check_vg(btk_ctx* ctx, const btk_variogram* vg) {
+  if (!vg) return fail(ctx, BTK_EINVAL, "variogram is required");
+  if (!(vg->nugget >= 0.0 && fin(vg->nugget))) return fail(ctx, BTK_EINVAL, "nugget must be finite and >= 0");
+  if (vg->nstruct < 0 || vg->nstruct > BTK_MAX_STRUCT)
+    return fail(ctx, BTK_EUNSUPPORTED, "at most 4 nested structures");
+  for (int k = 0; k < vg->nstruct; ++k) {
+    const btk_structure& s = vg->s[k];
+    if (!(s.sill >= 0.0 && fin(s.sill) && s.range > 0.0 && fin(s.range)))
+      return fail(ctx, BTK_EINVAL, "structure sill must be finite and >= 0, range finite and > 0");
+    if (s.model < BTK_SPHERICAL || s.model > BTK_POWER) return fail(ctx, BTK_EINVAL, "unknown variogram model");
+    if (s.model == BTK_POWER)
+      return fail(ctx, BTK_EUNSUPPORTED, "the power model has no sill (the reference solves it by LU)");
+  }
+  const btk_aniso& a = vg->aniso;
+  if (a.on && (!(a.major > 0 && a.semi > 0 && a.minor > 0) || !fin(a.major) || !fin(a.semi) ||
+               !fin(a.minor) || !fin(a.azimuth) || !fin(a.dip) || !fin(a.rake)))
+    return fail(ctx, BTK_EINVAL, "anisotropy ranges must be finite and > 0, angles finite");
+  return BTK_OK;
+}
+
+// crates/estimation/src/search.rs:214-264, plus the options not run here.
+int check_search(btk_ctx* ctx, const btk_search* s) {
+  if (!s) return fail(ctx, BTK_EINVAL, "search is required");
+  if (std::isnan(s->radius) || s->radius <= 0.0 || s->max_samples <= 0 || s->min_samples < 0 ||
+      s->min_samples > s->max_samples)
+    return fail(ctx, BTK_EINVAL, "need radius > 0 and 1 <= min_samples <= max_samples");
+  if (s->sectors > 0 && s->octant) return fail(ctx, BTK_EINVAL, "give octant or sectors, not both");
+  if (s->max_per_octant >= 0 && !s->octant) return fail(ctx, BTK_EINVAL, "max_per_octant needs octant");
+  if (s->max_per_octant == 0) return fail(ctx, BTK_EINVAL, "max_per_sector must be >= 1");
+  if (s->max_samples > kMaxN)
+    return fail(ctx, BTK_EUNSUPPORTED, "more than 64 samples per system (the reference solves these by LU)");
+  if (s->max_per_hole >= 0) return fail(ctx, BTK_EUNSUPPORTED, "max_per_hole is not run on the GPU");
+  if (s->sectors > 0) return fail(ctx, BTK_EUNSUPPORTED, "plane sectors are not run on the GPU");
+  if (s->min_sectors >= 0 || s->max_empty_sectors >= 0 || s->min_holes >= 0)
+    return fail(ctx, BTK_EUNSUPPORTED, "min_sectors, max_empty_sectors and min_holes are not run on the GPU");
+  const btk_aniso& a = s->aniso;
+  if (a.on && (!(a.major > 0 && a.semi > 0 && a.minor > 0) || !fin(a.azimuth) || !fin(a.dip) ||
+               !fin(a.rake)))
+    return fail(ctx, BTK_EINVAL, "search anisotropy ranges must be finite and > 0, angles finite");
+  return BTK_OK;
+}
+
+void make_vgdev(const btk_variogram& vg, VgDev& d) {
+  d = VgDev{};
+  d.nugget = vg.nugget;
+  double sum = 0.0;
+  for (int k = 0; k < vg.nstruct; ++k) sum += vg.s[k].sill;  // composite.rs:50-52
+  d.c0 = vg.nugget + sum;
+  d.nstruct = vg.nstruct;
+  for (int k = 0; k < vg.nstruct; ++k) {
+    d.model[k] = vg.s[k].model;
+    d.param[k] = vg.s[k].param;
+    d.sill[k] = vg.s[k].sill;
+    d.inv_range[k] = 1.0 / std::fmax(vg.s[k].range, 2.2250738585072014e-308);
+  }
+  d.has_frame = vg.aniso.on ? 1 : 0;
+  put9(vg.aniso.on ? aniso_matrix(vg.aniso) : eye(), d.frame);
+}
+
+// Search frame and sector set-up (search.rs:343-348, 395-425, 488-512).
+void make_searchdev(btk_ctx* ctx) {
+  const btk_search& s = ctx->search;
+  SearchDev& d = ctx->spd;
+  const btk_aniso* metric = s.aniso.on ? &s.aniso : (ctx->vg.aniso.on ? &ctx->vg.aniso : nullptr);
+  d.radius2 = s.radius * s.radius;
+  d.min_samples = int(s.min_samples);
+  d.max_samples = int(s.max_samples);
+  d.planar = ctx->planar ? 1 : 0;
+  d.nsec = s.octant ? (ctx->planar ? 4 : 8) : 1;
+  int64_t cap = s.octant ? (s.max_per_octant >= 0 ? s.max_per_octant : (s.max_samples + d.nsec - 1) / d.nsec)
+                         : s.max_samples;
+  if (cap > s.max_samples) cap = s.max_samples;
+  d.cap = int(cap);
+  put9(metric ? block_frame(metric->azimuth, metric->dip, metric->rake) : eye(), d.axes);
+  put9(metric ? aniso_matrix(*metric) : eye(), d.frame);
+}
+
+double frobenius(const double* m) {
+  double s = 0.0;
+  for (int i = 0; i < 9; ++i) s += m[i] * m[i];
+  return std::sqrt(s);
+}
+
+// Projection and grid over the fitted samples for the current search.
+int index_samples(btk_ctx* ctx) {
+  const int64_t n = ctx->n;
+  make_searchdev(ctx);
+  Launch L = ctx->launch(nullptr);
+  CK(ctx->frame9.grow(9));
+  CK(ctx->origin3.grow(3));
+  CK(cudaMemcpyAsync(ctx->frame9.p, ctx->spd.frame, 9 * sizeof(double), cudaMemcpyHostToDevice, L.stream));
+  CK(cudaMemcpyAsync(ctx->origin3.p, ctx->spd.origin, 3 * sizeof(double), cudaMemcpyHostToDevice, L.stream));
+  CK(ctx->px.grow(n));
+  CK(ctx->py.grow(n));
+  CK(ctx->pz.grow(n));
+  CK(launch_project(L, n, ctx->x.p, ctx->y.p, ctx->z.p, ctx->frame9.p, ctx->origin3.p, ctx->px.p, ctx->py.p,
+                    ctx->pz.p));
+  CK(ctx->bpart.grow(6 * 1024));
+  CK(ctx->b6.grow(6));
+  CK(launch_bounds(L, n, ctx->px.p, ctx->py.p, ctx->pz.p, ctx->bpart.p, ctx->b6.p));
+  double b[6];
+  CK(cudaMemcpyAsync(b, ctx->b6.p, sizeof b, cudaMemcpyDeviceToHost, L.stream));
+  CK(cudaStreamSynchronize(L.stream));
+
+  GridDev& g = ctx->gd;
+  double ext[3], longest = 0.0, prod = 1.0;
+  int spanned = 0;
+  for (int d = 0; d < 3; ++d) ext[d] = b[3 + d] - b[d], longest = std::fmax(longest, ext[d]);
+  for (int d = 0; d < 3; ++d)
+    if (ext[d] > longest * 1e-9) prod *= ext[d], ++spanned;
+  const double target_cells = std::fmax(double(n) / ctx->ppc, 1.0);
+  double h = longest > 0.0 ? std::pow(prod / target_cells, 1.0 / spanned) : 1.0;
+  auto cells = [&](double hh) {
+    double c = 1.0;
+    for (double e : ext) c *= std::floor(e / hh) + 1.0;
+    return c;
+  };
+  while (cells(h) > 4.0 * target_cells + 64.0) h *= 2.0;
+  g.h = h;
+  double scale = 0.0;
+  for (int d = 0; d < 3; ++d) {
+    g.lo[d] = b[d];
+    g.dims[d] = int(std::floor(ext[d] / h)) + 1;
+    scale = std::fmax(scale, std::fmax(std::fabs(b[d]), std::fabs(b[3 + d])));
+  }
+  g.slack = 1e-9 * (scale + h);
+  g.ncells = int64_t(g.dims[0]) * g.dims[1] * g.dims[2];
+  CK(ctx->cell_count.grow(g.ncells));
+  CK(ctx->start.grow(g.ncells + 1));
+  CK(ctx->cell_of.grow(n));
+  CK(ctx->spx.grow(n));
+  CK(ctx->spy.grow(n));
+  CK(ctx->spz.grow(n));
+  CK(ctx->swx.grow(n));
+  CK(ctx->swy.grow(n));
+  CK(ctx->swz.grow(n));
+  CK(ctx->sidx.grow(n));
+  CK(launch_grid_build(L, n, ctx->x.p, ctx->y.p, ctx->z.p, ctx->px.p, ctx->py.p, ctx->pz.p, g, ctx->cell_count.p,
+                       ctx->start.p, ctx->cell_of.p, ctx->spx.p, ctx->spy.p, ctx->spz.p, ctx->swx.p, ctx->swy.p,
+                       ctx->swz.p, ctx->sidx.p));
+  g.start = ctx->start.p;
+  g.px = ctx->spx.p, g.py = ctx->spy.p, g.pz = ctx->spz.p;
+  g.wx = ctx->swx.p, g.wy = ctx->swy.p, g.wz = ctx->swz.p;
+  g.idx = ctx->sidx.p;
+  const int reach = 1 + int(std::ceil(kEps * frobenius(ctx->spd.frame) / h));
+  CK(ctx->twin.grow(n));
+  CK(launch_twins(L, n, g, reach, ctx->x.p, ctx->y.p, ctx->z.p, ctx->twin.p));
+  // Leave-one-out walks the samples in cell order, so a tile's targets are near.
+  std::vector<uint32_t> order(n);
+  CK(cudaMemcpyAsync(order.data(), ctx->sidx.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, L.stream));
+  CK(cudaStreamSynchronize(L.stream));
+  std::vector<int64_t> perm(order.begin(), order.end());
+  CK(ctx->loo_perm.grow(n));
+  CK(cudaMemcpy(ctx->loo_perm.p, perm.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice));
+  return BTK_OK;
+}
+
+int ensure_scratch(btk_ctx* ctx, int64_t m) {
+  const size_t mm = size_t(m > 0 ? m : 1);
+  CK(ctx->nbr.grow(mm * size_t(ctx->search.max_samples)));
+  CK(ctx->cnt.grow(mm));
+  CK(ctx->sst.grow(mm));
+  CK(ctx->lists.grow(2 * mm));
+  CK(ctx->lens.grow(2));
+  CK(ctx->redo.grow(2 * mm));
+  CK(ctx->redo_len.grow(2));
+  return BTK_OK;
+}
+
+// Search then solve for m targets whose coordinates are device SoA arrays.
+int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const double* ty, const double* tz,
+             const int64_t* perm, int64_t nwork, int loo, int32_t kind, double kparam, int32_t precision,
+             const btk_outputs* o) {
+  if (kind < BTK_ORDINARY || kind > BTK_INDICATOR) return fail(ctx, BTK_EINVAL, "unknown kriging kind");
+  if (precision != BTK_FP64 && precision != BTK_MIXED) return fail(ctx, BTK_EINVAL, "unknown precision");
+  if (kind == BTK_SIMPLE && !std::isfinite(kparam)) return fail(ctx, BTK_EINVAL, "simple kriging needs a finite mean");
+  if (!o || !o->value) return fail(ctx, BTK_EINVAL, "outputs need a value array");
+  int rc = ensure_scratch(ctx, m);
+  if (rc) return rc;
+  Launch L = ctx->launch(s);
+  CK(launch_search(L, ctx->spd, ctx->gd, tx, ty, tz, perm, nwork, loo, ctx->nbr.p, ctx->cnt.p, ctx->sst.p));
+  SolveDev a{};
+  a.vg = ctx->vgd;
+  a.kind = kind;
+  a.kparam = kparam;
+  a.max_samples = int(ctx->search.max_samples);
+  a.sx = ctx->x.p, a.sy = ctx->y.p, a.sz = ctx->z.p, a.sv = ctx->v.p, a.se = ctx->has_err ? ctx->e.p : nullptr;
+  a.twin = ctx->twin.p;
+  a.tx = tx, a.ty = ty, a.tz = tz;
+  a.nbr = ctx->nbr.p, a.count = ctx->cnt.p, a.sstatus = ctx->sst.p;
+  a.m = m;
+  a.value = o->value, a.variance = o->variance, a.lagrange = o->lagrange, a.n_used = o->n_used, a.status = o->status;
+  const bool two = ctx->search.max_samples > 32;
+  if (two) CK(launch_bucket(L, m, ctx->cnt.p, ctx->sst.p, ctx->lists.p, ctx->lens.p));
+  for (int b = 0; b < (two ? 2 : 1); ++b) {
+    SolveDev ab = a;
+    if (two) ab.list = ctx->lists.p + b * m, ab.list_len = ctx->lens.p + b;
+    const int rows = b == 0 ? 32 : 64;
+    if (precision == BTK_FP64) {
+      CK(launch_solve(L, ab, rows));
+    } else {
+      int64_t* redo = ctx->redo.p + b * m;
+      int64_t* redo_len = ctx->redo_len.p + b;
+      CK(cudaMemsetAsync(redo_len, 0, sizeof(int64_t), L.stream));
+      CK(launch_solve_mixed(L, ab, rows, redo, redo_len));
+      SolveDev ar = a;
+      ar.list = redo, ar.list_len = redo_len;
+      CK(launch_solve_redo(L, ar, rows));
+    }
+  }
+  return BTK_OK;
+}
+
+int need_fit(btk_ctx* ctx) {
+  if (!ctx) return BTK_EINVAL;
+  if (!ctx->fitted) return fail(ctx, BTK_ENOTFITTED, "estimator is not fitted; call fit first");
+  return BTK_OK;
+}
+
+// Device outputs for a host call: value (+ optional arrays).
+int host_outputs(btk_ctx* ctx, int64_t m, const btk_outputs* out, btk_outputs* d) {
+  const size_t mm = size_t(m > 0 ? m : 1);
+  CK(ctx->o_value.grow(mm));
+  CK(ctx->o_var.grow(mm));
+  CK(ctx->o_lag.grow(mm));
+  CK(ctx->o_nused.grow(mm));
+  CK(ctx->o_status.grow(mm));
+  d->value = ctx->o_value.p;
+  d->variance = ctx->o_var.p;
+  d->lagrange = ctx->o_lag.p;
+  d->n_used = ctx->o_nused.p;
+  d->status = ctx->o_status.p;
+  (void)out;
+  return BTK_OK;
+}
+
+int copy_out(btk_ctx* ctx, int64_t m, const btk_outputs* d, const btk_outputs* out) {
+  cudaStream_t s = ctx->stream;
+  const size_t mm = size_t(m);
+  if (m > 0) {
+    CK(cudaMemcpyAsync(out->value, d->value, mm * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (out->variance) CK(cudaMemcpyAsync(out->variance, d->variance, mm * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (out->lagrange) CK(cudaMemcpyAsync(out->lagrange, d->lagrange, mm * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (out->n_used) CK(cudaMemcpyAsync(out->n_used, d->n_used, mm * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    if (out->status) CK(cudaMemcpyAsync(out->status, d->status, mm * sizeof(int8_t), cudaMemcpyDeviceToHost, s));
+  }
+  CK(cudaStreamSynchronize(s));
+  return BTK_OK;
+}
+
+__global__ void k_split_xyz(int64_t m, const double* aos, double* x, double* y, double* z) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < m; i += int64_t(gridDim.x) * blockDim.x) {
+    x[i] = aos[3 * i], y[i] = aos[3 * i + 1], z[i] = aos[3 * i + 2];
+  }
+}
+
+// Host m x 3 row-major coordinates to device x, y, z arrays in ctx->txyz.
+int upload_targets(btk_ctx* ctx, int64_t m, const double* xyz) {
+  const size_t mm = size_t(m > 0 ? m : 1);
+  CK(ctx->aos.grow(3 * mm));
+  CK(ctx->txyz.grow(3 * mm));
+  if (m == 0) return BTK_OK;
+  CK(cudaMemcpyAsync(ctx->aos.p, xyz, 3 * size_t(m) * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  int64_t b = (m + 255) / 256;
+  if (b > int64_t(ctx->sm_count) * 8) b = int64_t(ctx->sm_count) * 8;
+  k_split_xyz<<<int(b), 256, 0, ctx->stream>>>(m, ctx->aos.p, ctx->txyz.p, ctx->txyz.p + m, ctx->txyz.p + 2 * m);
+  ++ctx->launches;
+  CK(cudaGetLastError());
+  return BTK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* btk_version(void) { return "boitata_b200 0.1.0 (sm_100a)"; }
+
+btk_ctx* btk_create(int device, char* err, size_t errlen) {
+  auto say = [&](const std::string& m) {
+    if (err && errlen) std::snprintf(err, errlen, "%s", m.c_str());
+  };
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    say(std::string("no CUDA device: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "count is 0"));
+    return nullptr;
+  }
+  if (device < 0 || device >= count) {
+    say("device index out of range");
+    return nullptr;
+  }
+  if ((e = cudaSetDevice(device)) != cudaSuccess) {
+    say(std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    return nullptr;
+  }
+  btk_ctx* c = new btk_ctx;
+  c->device = device;
+  if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) {
+    say(std::string("stream/attribute: ") + cudaGetErrorString(e));
+    delete c;
+    return nullptr;
+  }
+  if (const char* p = std::getenv("BTK_SAMPLES_PER_CELL")) {
+    double v = std::atof(p);
+    if (v > 0.0) c->ppc = v;
+  }
+  return c;
+}
+
+void btk_destroy(btk_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream), cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* btk_last_error(const btk_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int64_t btk_launch_count(const btk_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int btk_fit(btk_ctx* ctx, int64_t n, const double* xyz, const double* values, const double* err_var,
+            const int64_t* holes, const btk_search* search, const btk_variogram* vg) {
+  if (!ctx) return BTK_EINVAL;
+  (void)holes;  // per-hole rules are refused by check_search
+  ctx->fitted = false;
+  if (n <= 0 || !xyz || !values) return fail(ctx, BTK_EINVAL, "fit needs at least one sample with coordinates and values");
+  if (n >= int64_t(0xffffffffu)) return fail(ctx, BTK_EINVAL, "too many samples");
+  int rc = check_vg(ctx, vg);
+  if (rc) return rc;
+  if ((rc = check_search(ctx, search))) return rc;
+  std::vector<double> hx(n), hy(n), hz(n);
+  for (int64_t i = 0; i < n; ++i) {
+    hx[i] = xyz[3 * i], hy[i] = xyz[3 * i + 1], hz[i] = xyz[3 * i + 2];
+    if (!fin(hx[i]) || !fin(hy[i]) || !fin(hz[i])) return fail(ctx, BTK_EINVAL, "coordinates must be finite");
+    if (!fin(values[i])) return fail(ctx, BTK_EINVAL, "values must be finite; drop missing values first");
+    if (err_var && (!fin(err_var[i]) || err_var[i] < 0.0))
+      return fail(ctx, BTK_EINVAL, "error_variance must be finite and >= 0");
+  }
+  CK(cudaSetDevice(ctx->device));
+  ctx->n = n;
+  ctx->search = *search;
+  ctx->vg = *vg;
+  ctx->has_err = err_var != nullptr;
+  bool planar = true;  // search.rs:470-473
+  for (int64_t i = 1; i < n && planar; ++i) planar = hz[i] == hz[0];
+  ctx->planar = planar;
+  ctx->spd.origin[0] = hx[0], ctx->spd.origin[1] = hy[0], ctx->spd.origin[2] = hz[0];
+  make_vgdev(*vg, ctx->vgd);
+  for (auto* b : {&ctx->x, &ctx->y, &ctx->z, &ctx->v, &ctx->e}) CK(b->grow(n));
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemcpyAsync(ctx->x.p, hx.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(ctx->y.p, hy.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(ctx->z.p, hz.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(ctx->v.p, values, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (err_var) CK(cudaMemcpyAsync(ctx->e.p, err_var, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  if ((rc = index_samples(ctx))) return rc;
+  CK(cudaStreamSynchronize(s));
+  ctx->fitted = true;
+  return BTK_OK;
+}
+
+int btk_set_search(btk_ctx* ctx, const btk_search* search) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if ((rc = check_search(ctx, search))) return rc;
+  CK(cudaSetDevice(ctx->device));
+  ctx->search = *search;
+  if ((rc = index_samples(ctx))) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return BTK_OK;
+}
+
+int btk_predict_device(btk_ctx* ctx, int64_t m, const double* d_xyz, int32_t kind, double kparam, int32_t precision,
+                       const btk_outputs* d_out, void* stream) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if (m < 0 || (m > 0 && !d_xyz)) return fail(ctx, BTK_EINVAL, "targets are required");
+  if (m == 0) return BTK_OK;
+  CK(cudaSetDevice(ctx->device));
+  return run_path(ctx, static_cast<cudaStream_t>(stream), m, d_xyz, d_xyz + m, d_xyz + 2 * m, nullptr, m, 0, kind,
+                  kparam, precision, d_out);
+}
+
+int btk_predict(btk_ctx* ctx, int64_t m, const double* xyz, int32_t kind, double kparam, int32_t precision,
+                const btk_outputs* out) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if (!out || !out->value) return fail(ctx, BTK_EINVAL, "outputs need a value array");
+  if (m < 0 || (m > 0 && !xyz)) return fail(ctx, BTK_EINVAL, "targets are required");
+  if (m == 0) return BTK_OK;
+  CK(cudaSetDevice(ctx->device));
+  if ((rc = upload_targets(ctx, m, xyz))) return rc;
+  btk_outputs d{};
+  if ((rc = host_outputs(ctx, m, out, &d))) return rc;
+  const double* t = ctx->txyz.p;
+  if ((rc = run_path(ctx, nullptr, m, t, t + m, t + 2 * m, nullptr, m, 0, kind, kparam, precision, &d))) return rc;
+  return copy_out(ctx, m, &d, out);
+}
+
+int btk_predict_geometry_device(btk_ctx* ctx, const btk_geometry* g, int32_t kind, double kparam, int32_t precision,
+                                const btk_outputs* d_out, void* stream) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if (!g) return fail(ctx, BTK_EINVAL, "geometry is required");
+  for (int a = 0; a < 3; ++a) {
+    if (!(g->size[a] > 0.0 && fin(g->size[a]))) return fail(ctx, BTK_EINVAL, "cell sizes must be positive");
+    if (g->count[a] <= 0) return fail(ctx, BTK_EINVAL, "cell counts must be positive");
+    if (!fin(g->origin[a]) || !fin(g->rotation[a])) return fail(ctx, BTK_EINVAL, "origin and rotation must be finite");
+  }
+  CK(cudaSetDevice(ctx->device));
+  const int64_t m = g->count[0] * g->count[1] * g->count[2];
+  const int64_t tiles = ((g->count[0] + 3) / 4) * ((g->count[1] + 3) / 4) * ((g->count[2] + 1) / 2);
+  const int64_t nwork = tiles * 32;
+  CK(ctx->txyz.grow(3 * size_t(m)));
+  CK(ctx->perm.grow(size_t(nwork)));
+  CK(ctx->ft9.grow(9));
+  M3 f = block_frame(g->rotation[0], g->rotation[1], g->rotation[2]);
+  double ft[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) ft[3 * i + j] = f.m[j][i];
+  Launch L = ctx->launch(static_cast<cudaStream_t>(stream));
+  CK(cudaMemcpyAsync(ctx->ft9.p, ft, sizeof ft, cudaMemcpyHostToDevice, L.stream));
+  double* t = ctx->txyz.p;
+  CK(launch_centroids(L, *g, ctx->ft9.p, 0, nwork, t, t + m, t + 2 * m, ctx->perm.p));
+  return run_path(ctx, L.stream, m, t, t + m, t + 2 * m, ctx->perm.p, nwork, 0, kind, kparam, precision, d_out);
+}
+
+int btk_cross_validate(btk_ctx* ctx, int32_t kind, double kparam, int32_t precision, const btk_outputs* out) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if (!out || !out->value) return fail(ctx, BTK_EINVAL, "outputs need a value array");
+  CK(cudaSetDevice(ctx->device));
+  btk_outputs d{};
+  if ((rc = host_outputs(ctx, ctx->n, out, &d))) return rc;
+  if ((rc = run_path(ctx, nullptr, ctx->n, ctx->x.p, ctx->y.p, ctx->z.p, ctx->loo_perm.p, ctx->n, 1, kind, kparam,
+                     precision, &d)))
+    return rc;
+  return copy_out(ctx, ctx->n, &d, out);
+}
+
+int btk_neighbors(btk_ctx* ctx, int64_t m, const double* xyz, int32_t loo, int64_t* idx, int32_t* count, int8_t* ok) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  const double* t;
+  const int64_t* perm = nullptr;
+  if (loo) {
+    m = ctx->n;
+    t = ctx->x.p;
+    perm = ctx->loo_perm.p;
+  } else {
+    if (m <= 0 || !xyz) return fail(ctx, BTK_EINVAL, "targets are required");
+    if ((rc = upload_targets(ctx, m, xyz))) return rc;
+    t = ctx->txyz.p;
+  }
+  if ((rc = ensure_scratch(ctx, m))) return rc;
+  Launch L = ctx->launch(nullptr);
+  const double *tx = loo ? ctx->x.p : t, *ty = loo ? ctx->y.p : t + m, *tz = loo ? ctx->z.p : t + 2 * m;
+  CK(launch_search(L, ctx->spd, ctx->gd, tx, ty, tz, perm, m, loo ? 1 : 0, ctx->nbr.p, ctx->cnt.p, ctx->sst.p));
+  const size_t k = size_t(ctx->search.max_samples);
+  std::vector<uint32_t> nb(size_t(m) * k);
+  std::vector<int8_t> st(m);
+  CK(cudaMemcpyAsync(nb.data(), ctx->nbr.p, nb.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, L.stream));
+  CK(cudaMemcpyAsync(count, ctx->cnt.p, size_t(m) * sizeof(int32_t), cudaMemcpyDeviceToHost, L.stream));
+  CK(cudaMemcpyAsync(st.data(), ctx->sst.p, size_t(m) * sizeof(int8_t), cudaMemcpyDeviceToHost, L.stream));
+  CK(cudaStreamSynchronize(L.stream));
+  for (size_t i = 0; i < nb.size(); ++i) idx[i] = nb[i] == 0xffffffffu ? -1 : int64_t(nb[i]);
+  for (int64_t i = 0; i < m; ++i) ok[i] = st[i] == BTK_ST_OK ? 1 : 0;
+  return BTK_OK;
+}
+
+int btk_centroids(btk_ctx* ctx, const btk_geometry* g, int64_t first, int64_t m, double* xyz) {
+  if (!ctx || !g || m < 0) return fail(ctx, BTK_EINVAL, "geometry and a non-negative count are required");
+  if (m == 0) return BTK_OK;
+  CK(cudaSetDevice(ctx->device));
+  M3 f = block_frame(g->rotation[0], g->rotation[1], g->rotation[2]);
+  double ft[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) ft[3 * i + j] = f.m[j][i];
+  CK(ctx->ft9.grow(9));
+  CK(ctx->txyz.grow(3 * size_t(m)));
+  Launch L = ctx->launch(nullptr);
+  CK(cudaMemcpyAsync(ctx->ft9.p, ft, sizeof ft, cudaMemcpyHostToDevice, L.stream));
+  double* t = ctx->txyz.p;
+  CK(launch_centroids(L, *g, ctx->ft9.p, first, m, t, t + m, t + 2 * m, nullptr));
+  std::vector<double> a(3 * size_t(m));
+  CK(cudaMemcpyAsync(a.data(), t, a.size() * sizeof(double), cudaMemcpyDeviceToHost, L.stream));
+  CK(cudaStreamSynchronize(L.stream));
+  for (int64_t i = 0; i < m; ++i) xyz[3 * i] = a[i], xyz[3 * i + 1] = a[m + i], xyz[3 * i + 2] = a[2 * m + i];
+  return BTK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,238 @@
+// Fit-time kernels: projection of the samples into the search frame, their
+// bounding box, the uniform grid (counting sort by cell), the coincident-
+// sample flags, and block-model centroids.
+//
+// The projection p = frame * (s - origin) with the origin at the first
+// sample follows crates/estimation/src/search.rs:704-745 bit for bit
+// (exact-order FP64, no FMA), since the search ranks samples by distances
+// between these points. The grid itself is this engine's own: any grid
+// gives the same (d2, index)-ordered candidates as search/grid.rs.
+#include <cfloat>
+
+#include "btk_device.cuh"
+
+namespace btk {
+namespace {
+
+__global__ void k_project(int64_t n, const double* __restrict__ x, const double* __restrict__ y,
+                          const double* __restrict__ z, const double* __restrict__ frame,
+                          const double* __restrict__ origin, double* px, double* py, double* pz) {
+  double M[9], o[3];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) M[k] = frame[k];
+  o[0] = origin[0], o[1] = origin[1], o[2] = origin[2];
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    double d[3] = {xsub(x[i], o[0]), xsub(y[i], o[1]), xsub(z[i], o[2])}, p[3];
+    mulv_exact(M, d, p);
+    px[i] = p[0], py[i] = p[1], pz[i] = p[2];
+  }
+}
+
+// Per-block min/max of the three coordinates, then one block folds them.
+__global__ void k_bounds_partial(int64_t n, const double* px, const double* py, const double* pz, double* partial) {
+  __shared__ double s[6][256];
+  double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    double p[3] = {px[i], py[i], pz[i]};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) lo[d] = fmin(lo[d], p[d]), hi[d] = fmax(hi[d], p[d]);
+  }
+  for (int d = 0; d < 3; ++d) s[d][threadIdx.x] = lo[d], s[3 + d][threadIdx.x] = hi[d];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int d = 0; d < 3; ++d) {
+        s[d][threadIdx.x] = fmin(s[d][threadIdx.x], s[d][threadIdx.x + w]);
+        s[3 + d][threadIdx.x] = fmax(s[3 + d][threadIdx.x], s[3 + d][threadIdx.x + w]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x < 6) partial[blockIdx.x * 6 + threadIdx.x] = s[threadIdx.x][0];
+}
+
+__global__ void k_bounds_final(int nblocks, const double* partial, double* out6) {
+  if (threadIdx.x != 0) return;
+  double r[6] = {DBL_MAX, DBL_MAX, DBL_MAX, -DBL_MAX, -DBL_MAX, -DBL_MAX};
+  for (int b = 0; b < nblocks; ++b)
+    for (int d = 0; d < 3; ++d) r[d] = fmin(r[d], partial[6 * b + d]), r[3 + d] = fmax(r[3 + d], partial[6 * b + 3 + d]);
+  for (int k = 0; k < 6; ++k) out6[k] = r[k];
+}
+
+__device__ __forceinline__ int cell_axis(double p, double lo, double h, int dim) {
+  double u = floor((p - lo) / h);
+  u = fmin(fmax(u, 0.0), double(dim - 1));  // fmax maps NaN to 0
+  return int(u);
+}
+
+__global__ void k_cell_count(int64_t n, const double* px, const double* py, const double* pz, GridDev g,
+                             uint32_t* count, uint32_t* cell_of) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    int cx = cell_axis(px[i], g.lo[0], g.h, g.dims[0]);
+    int cy = cell_axis(py[i], g.lo[1], g.h, g.dims[1]);
+    int cz = cell_axis(pz[i], g.lo[2], g.h, g.dims[2]);
+    int64_t id = cx + int64_t(g.dims[0]) * (cy + int64_t(g.dims[1]) * cz);
+    cell_of[i] = uint32_t(id);
+    atomicAdd(&count[id], 1u);
+  }
+}
+
+// Exclusive scan of `count` into `start` (ncells + 1 entries) by one block:
+// each thread sums a contiguous chunk, the block scans the chunk sums.
+__global__ void k_scan(int64_t ncells, const uint32_t* count, uint32_t* start) {
+  __shared__ uint32_t sums[1024];
+  int64_t chunk = (ncells + blockDim.x - 1) / blockDim.x;
+  int64_t a = threadIdx.x * chunk, b = min(ncells, a + chunk);
+  uint32_t s = 0;
+  for (int64_t c = a; c < b; ++c) s += count[c];
+  sums[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 1; w < blockDim.x; w <<= 1) {
+    uint32_t v = threadIdx.x >= w ? sums[threadIdx.x - w] : 0;
+    __syncthreads();
+    sums[threadIdx.x] += v;
+    __syncthreads();
+  }
+  uint32_t run = sums[threadIdx.x] - s;
+  for (int64_t c = a; c < b; ++c) {
+    start[c] = run;
+    run += count[c];
+  }
+  if (threadIdx.x == blockDim.x - 1) start[ncells] = sums[threadIdx.x];
+}
+
+__global__ void k_scatter(int64_t n, const double* x, const double* y, const double* z, const double* px,
+                          const double* py, const double* pz, const uint32_t* cell_of, const uint32_t* start,
+                          uint32_t* fill, double* spx, double* spy, double* spz, double* swx, double* swy,
+                          double* swz, uint32_t* sidx) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    uint32_t c = cell_of[i];
+    uint32_t pos = start[c] + atomicAdd(&fill[c], 1u);
+    spx[pos] = px[i], spy[pos] = py[i], spz[pos] = pz[i];
+    swx[pos] = x[i], swy[pos] = y[i], swz[pos] = z[i];
+    sidx[pos] = uint32_t(i);
+  }
+}
+
+// twin[i] = 1 when another sample lies within 1e-6 m of sample i, by the
+// test of crates/estimation/src/coincident.rs:13-15 (exact order). Pairs
+// that close are in the same or adjacent cells (`reach` covers the frame's
+// stretch); a system needs the coincident guard only if it holds a twin.
+__global__ void k_twins(int64_t n, GridDev g, int reach, const double* x, const double* y, const double* z,
+                        uint8_t* twin) {
+  const double eps2 = kEps * kEps;
+  for (int64_t s = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; s < n; s += int64_t(gridDim.x) * blockDim.x) {
+    int c[3] = {cell_axis(g.px[s], g.lo[0], g.h, g.dims[0]), cell_axis(g.py[s], g.lo[1], g.h, g.dims[1]),
+                cell_axis(g.pz[s], g.lo[2], g.h, g.dims[2])};
+    uint32_t me = g.idx[s];
+    double w[3] = {g.wx[s], g.wy[s], g.wz[s]};
+    bool found = false;
+    for (int dz = -reach; dz <= reach && !found; ++dz)
+      for (int dy = -reach; dy <= reach && !found; ++dy) {
+        int cy = c[1] + dy, cz = c[2] + dz;
+        if (cy < 0 || cy >= g.dims[1] || cz < 0 || cz >= g.dims[2]) continue;
+        int x0 = max(c[0] - reach, 0), x1 = min(c[0] + reach, g.dims[0] - 1);
+        int64_t row = int64_t(g.dims[0]) * (cy + int64_t(g.dims[1]) * cz);
+        for (uint32_t e = g.start[row + x0]; e < g.start[row + x1 + 1]; ++e) {
+          if (g.idx[e] == me) continue;
+          if (d2_exact(w[0], w[1], w[2], g.wx[e], g.wy[e], g.wz[e]) <= eps2) { found = true; break; }
+        }
+      }
+    twin[me] = found ? 1 : 0;
+  }
+}
+
+// Centroids of block-model cells (crates/core/src/block_model.rs:76-86):
+// origin + block_frame^T * ((ijk + 0.5) * size), exact order. With
+// `perm_tiles` the work items are 4 x 4 x 2 tiles of cells (32 per tile, one
+// per search lane) and perm_tiles[k] is the cell of work item k, or -1.
+__global__ void k_centroids(btk_geometry geo, const double* __restrict__ ft, int64_t first, int64_t m, double* tx,
+                            double* ty, double* tz, int64_t* perm_tiles) {
+  double F[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) F[k] = ft[k];
+  const int64_t nx = geo.count[0], ny = geo.count[1], nz = geo.count[2];
+  const int64_t tx_n = (nx + 3) / 4, ty_n = (ny + 3) / 4;
+  for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < m; k += int64_t(gridDim.x) * blockDim.x) {
+    int64_t i, j, l, cell;
+    if (perm_tiles) {
+      int64_t tile = k >> 5, lane = k & 31;
+      int64_t a = tile % tx_n, b = tile / tx_n % ty_n, c = tile / (tx_n * ty_n);
+      i = 4 * a + (lane & 3), j = 4 * b + ((lane >> 2) & 3), l = 2 * c + (lane >> 4);
+      if (i >= nx || j >= ny || l >= nz) {
+        perm_tiles[k] = -1;
+        continue;
+      }
+      cell = i + nx * (j + ny * l);
+      perm_tiles[k] = cell;
+    } else {
+      cell = first + k;
+      i = cell % nx, j = cell / nx % ny, l = cell / (nx * ny);
+    }
+    double local[3] = {xmul(xadd(double(i), 0.5), geo.size[0]), xmul(xadd(double(j), 0.5), geo.size[1]),
+                       xmul(xadd(double(l), 0.5), geo.size[2])};
+    double w[3];
+    mulv_exact(F, local, w);
+    int64_t out = perm_tiles ? cell : k;
+    tx[out] = xadd(geo.origin[0], w[0]);
+    ty[out] = xadd(geo.origin[1], w[1]);
+    tz[out] = xadd(geo.origin[2], w[2]);
+  }
+}
+
+int grid_blocks(const Launch& L, int64_t n, int threads) {
+  int64_t b = (n + threads - 1) / threads;
+  int64_t cap = int64_t(L.sm_count) * 8;
+  return int(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+}  // namespace
+
+cudaError_t launch_project(const Launch& L, int64_t n, const double* x, const double* y, const double* z,
+                           const double* frame, const double* origin, double* px, double* py, double* pz) {
+  k_project<<<grid_blocks(L, n, 256), 256, 0, L.stream>>>(n, x, y, z, frame, origin, px, py, pz);
+  ++*L.counter;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bounds(const Launch& L, int64_t n, const double* px, const double* py, const double* pz,
+                          double* partial, double* out6) {
+  int nb = grid_blocks(L, n, 256);
+  if (nb > 1024) nb = 1024;
+  k_bounds_partial<<<nb, 256, 0, L.stream>>>(n, px, py, pz, partial);
+  k_bounds_final<<<1, 32, 0, L.stream>>>(nb, partial, out6);
+  *L.counter += 2;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grid_build(const Launch& L, int64_t n, const double* x, const double* y, const double* z,
+                              const double* px, const double* py, const double* pz, GridDev g, uint32_t* count,
+                              uint32_t* start, uint32_t* cell_of, double* spx, double* spy, double* spz,
+                              double* swx, double* swy, double* swz, uint32_t* sidx) {
+  cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t) * size_t(g.ncells), L.stream);
+  if (e != cudaSuccess) return e;
+  int nb = grid_blocks(L, n, 256);
+  k_cell_count<<<nb, 256, 0, L.stream>>>(n, px, py, pz, g, count, cell_of);
+  k_scan<<<1, 1024, 0, L.stream>>>(g.ncells, count, start);
+  e = cudaMemsetAsync(count, 0, sizeof(uint32_t) * size_t(g.ncells), L.stream);
+  if (e != cudaSuccess) return e;
+  k_scatter<<<nb, 256, 0, L.stream>>>(n, x, y, z, px, py, pz, cell_of, start, count, spx, spy, spz, swx, swy, swz,
+                                      sidx);
+  *L.counter += 3;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_twins(const Launch& L, int64_t n, GridDev g, int reach, const double* x, const double* y,
+                         const double* z, uint8_t* twin) {
+  k_twins<<<grid_blocks(L, n, 128), 128, 0, L.stream>>>(n, g, reach, x, y, z, twin);
+  ++*L.counter;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_centroids(const Launch& L, btk_geometry g, const double* frame_t, int64_t first, int64_t m,
+                             double* tx, double* ty, double* tz, int64_t* perm_tiles) {
+  k_centroids<<<grid_blocks(L, m, 256), 256, 0, L.stream>>>(g, frame_t, first, m, tx, ty, tz, perm_tiles);
+  ++*L.counter;
+  return cudaGetLastError();
+}
+
+}  // namespace btk

@@ -1,0 +1,102 @@
+// Internal host/device interface of the B200 kriging engine: the parameter
+// blocks the kernels take by value and the launchers the C ABI calls.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "boitata_b200.h"
+
+namespace btk {
+
+constexpr int kMaxN = 64;       // most samples per system (kernel.rs:11)
+constexpr int kMaxSlots = 64;   // most list entries per search lane
+constexpr double kPivot = 1e-12;  // kernel.rs:17
+constexpr double kEps = 1e-6;     // coincident.rs:11
+
+// Variogram with everything the kernels need precomputed on the host.
+struct VgDev {
+  double nugget, c0;
+  int nstruct;
+  int model[BTK_MAX_STRUCT];
+  double param[BTK_MAX_STRUCT], sill[BTK_MAX_STRUCT], inv_range[BTK_MAX_STRUCT];
+  int has_frame;
+  double frame[9];  // diag(1/major, 1/semi, 1/minor) * rotation (aniso.rs:88-94)
+};
+
+// Search parameters in the form the search kernel uses.
+struct SearchDev {
+  double radius2;
+  int min_samples, max_samples;
+  int nsec;  // 1 without balancing, 4 quadrants, 8 octants
+  int cap;   // per-sector list length: min(sector cap, max_samples)
+  int planar;
+  double axes[9];   // block_frame of the search ellipsoid (octant signs)
+  double frame[9];  // projection into the search space
+  double origin[3];  // first sample (search.rs:704-745)
+};
+
+// Uniform grid over the projected samples, which are stored sorted by cell.
+struct GridDev {
+  double lo[3];
+  double h;
+  int dims[3];
+  int64_t ncells;
+  double slack;  // absolute margin on cell-face distances
+  const uint32_t* start;  // ncells + 1
+  const double *px, *py, *pz;  // projected, cell order
+  const double *wx, *wy, *wz;  // world, cell order
+  const uint32_t* idx;         // original sample index, cell order
+};
+
+// Everything a solve launch reads and writes.
+struct SolveDev {
+  VgDev vg;
+  int kind;
+  double kparam;
+  int max_samples;
+  const double *sx, *sy, *sz, *sv, *se;  // samples, original order; se may be null
+  const uint8_t* twin;                    // 1 where another sample lies within 1e-6 m
+  const double *tx, *ty, *tz;            // targets, by target index
+  const uint32_t* nbr;                   // [target][max_samples]
+  const int32_t* count;
+  const int8_t* sstatus;
+  const int64_t* list;      // systems of this bucket (target indices), or null for 0..m-1
+  const int64_t* list_len;  // device count of `list`
+  int64_t m;
+  double *value, *variance, *lagrange;
+  int32_t* n_used;
+  int8_t* status;
+};
+
+// ---- launchers (each returns the launch's error, if any) ----
+struct Launch {
+  cudaStream_t stream;
+  int sm_count;
+  int64_t* counter;  // launches issued, for btk_launch_count
+};
+
+cudaError_t launch_project(const Launch& L, int64_t n, const double* x, const double* y, const double* z,
+                           const double* frame, const double* origin, double* px, double* py, double* pz);
+cudaError_t launch_bounds(const Launch& L, int64_t n, const double* px, const double* py, const double* pz,
+                          double* partial /* 6 * 1024 */, double* out6);
+cudaError_t launch_grid_build(const Launch& L, int64_t n, const double* x, const double* y, const double* z,
+                              const double* px, const double* py, const double* pz, GridDev g, uint32_t* count,
+                              uint32_t* start, uint32_t* cell_of, double* spx, double* spy, double* spz,
+                              double* swx, double* swy, double* swz, uint32_t* sidx);
+cudaError_t launch_twins(const Launch& L, int64_t n, GridDev g, int reach, const double* x, const double* y,
+                         const double* z, uint8_t* twin);
+cudaError_t launch_centroids(const Launch& L, btk_geometry g, const double* frame_t, int64_t first, int64_t m,
+                             double* tx, double* ty, double* tz, int64_t* perm_tiles);
+cudaError_t launch_search(const Launch& L, const SearchDev& sp, const GridDev& g, const double* tx,
+                          const double* ty, const double* tz, const int64_t* perm, int64_t m, int loo,
+                          uint32_t* nbr, int32_t* count, int8_t* status);
+cudaError_t launch_bucket(const Launch& L, int64_t m, const int32_t* count, const int8_t* sstatus, int64_t* lists,
+                          int64_t* lens);
+// FP64 form; rows 32 (a warp per system) or 64 (a warp pair).
+cudaError_t launch_solve(const Launch& L, const SolveDev& a, int rows);
+// Mixed form; systems it leaves to FP64 are appended to redo / *redo_len.
+cudaError_t launch_solve_mixed(const Launch& L, const SolveDev& a, int rows, int64_t* redo, int64_t* redo_len);
+// FP64 re-solve of the redo list (a.list / a.list_len point at it).
+cudaError_t launch_solve_redo(const Launch& L, const SolveDev& a, int rows);
+
+}  // namespace btk

@@ -1,0 +1,492 @@
+// Per-system kriging solve (K2 assembly, K3 factor-and-solve, K4 epilogue),
+// one system per warp (n <= 32) or per warp pair (n <= 64).
+//
+// Reference: crates/estimation/src/kernel.rs:24-123 (and the coincident
+// guard of crates/estimation/src/coincident.rs:27-111 via krige.rs:83-95).
+// The reference factors C = L L^T (packed Cholesky), solves C a = c and
+// C b = 1, and forms mu = (sum a - 1) / sum b, w = a - mu b, value = w . z,
+// sigma^2 = max(C0 - w . c - mu, 0), with a singular system where a pivot is
+// NaN or <= 1e-12 C0.
+//
+// B200 form: the estimate, variance and Lagrange multiplier only need the
+// quadratic forms u^T C^-1 v for u, v in {c, 1, f(z)}. With C = L D L^T (L
+// unit lower) and y_v = L^-1 v they are sum_i y_u,i y_v,i / D_i, so one
+// right-looking LDL^T pass, with the three forward substitutions fused into
+// it, replaces the factorisation and both triangular solves: no back
+// substitution and no square roots. D_k is the Schur-complement pivot, the
+// same quantity the reference tests against 1e-12 C0.
+//
+// Layout: row i of the lower triangle lives in registers of lane i (A[R],
+// compile-time indexed); step k broadcasts the unscaled column k and the
+// three y_k through a double-buffered shared-memory line, one group barrier
+// per step. Assembly is balanced: the n(n-1)/2 covariances are spread over
+// all lanes into a packed shared-memory triangle, then each lane loads its
+// row (conflict-free: row offsets i(i-1)/2 cover every bank pair twice).
+//
+// Mixed form: the same assembly (FP64), an FP32 LDL^T with fused forward
+// substitution and an FP32 back substitution give approximate solutions
+// x_v; FP64 residuals r_v = v - C x_v (C from the FP64 triangle) correct the
+// forms to u^T x_v + x_u^T r_v, whose error is second order in the
+// residuals. The Lagrange multiplier and the variance are then formed in
+// FP64. A system whose FP32 pivots fall below 1e-5 C0 or whose residual is
+// large goes to an FP64 re-solve list (status flag BTK_ST_FP64_FALLBACK).
+#include "btk_device.cuh"
+
+namespace btk {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+template <int NW>
+struct SolveSmem {
+  static constexpr int R = 32 * NW;
+  double P[R][3];
+  double T[R * (R - 1) / 2];
+  double col[2][R];
+  double rhs[2][4];
+  double red[NW][8];
+  int ired[NW];
+  double mz[R], me[R];
+  int cof[R], cfirst[R], csize[R];
+};
+
+template <int NW>
+struct MixedSmem {
+  static constexpr int R = 32 * NW;
+  SolveSmem<NW> base;
+  float colf[2][R];
+  float rhsf[2][4];
+  float L[R][R + 1];
+  double xs[3][R];
+};
+
+template <int NW>
+__device__ __forceinline__ void gsync(int gid) {
+  if (NW == 1)
+    __syncwarp();
+  else
+    asm volatile("bar.sync %0, %1;" ::"r"(gid + 1), "r"(NW * 32) : "memory");
+}
+
+template <int NW>
+__device__ __forceinline__ bool group_any(SolveSmem<NW>& S, int gid, int wig, bool pred) {
+  int v = __any_sync(kFull, pred);
+  if (NW == 1) return v != 0;
+  if ((threadIdx.x & 31) == 0) S.ired[wig] = v;
+  gsync<NW>(gid);
+  int all = 0;
+#pragma unroll
+  for (int w = 0; w < NW; ++w) all |= S.ired[w];
+  gsync<NW>(gid);
+  return all != 0;
+}
+
+// Sums of five values over the group, returned on every lane.
+template <int NW>
+__device__ __forceinline__ void group_sum5(SolveSmem<NW>& S, int gid, int wig, double v[5]) {
+#pragma unroll
+  for (int q = 0; q < 5; ++q)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(kFull, v[q], o);
+  if (NW == 1) return;
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int q = 0; q < 5; ++q) S.red[wig][q] = v[q];
+  gsync<NW>(gid);
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) s += S.red[w][q];
+    v[q] = s;
+  }
+  gsync<NW>(gid);
+}
+
+__device__ __forceinline__ double kind_f(int kind, double kparam, double z) {
+  return kind == BTK_SIMPLE ? z - kparam : (kind == BTK_INDICATOR ? (z <= kparam ? 1.0 : 0.0) : z);
+}
+
+__device__ __forceinline__ double lag64(const VgDev& vg, const double* a, const double* b) {
+  double d[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+  if (vg.has_frame) {
+    double r[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r[k] = vg.frame[3 * k] * d[0] + vg.frame[3 * k + 1] * d[1] + vg.frame[3 * k + 2] * d[2];
+    d[0] = r[0], d[1] = r[1], d[2] = r[2];
+  }
+  return sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+}
+
+// Coincident guard on one lane (coincident.rs:27-82): samples within 1e-6 m
+// of a cluster's first member join it; each cluster becomes one datum at the
+// first member with the mean of f(z) (the value the spread weights give,
+// krige.rs:89-92) and error variance sum_ij C / k^2 - C0 + sum err / k^2.
+// World coordinates in P, errors in me, f(z) in mz; rewritten in place.
+template <int NW>
+__device__ void merge_clusters(SolveSmem<NW>& S, int n, const VgDev& vg, int* nn_out) {
+  const double eps2 = kEps * kEps;
+  int* of = S.cof;
+  int* first = S.cfirst;
+  int* size = S.csize;
+  int nc = 0;
+  for (int i = 0; i < n; ++i) {
+    int c = -1;
+    for (int q = 0; q < nc && c < 0; ++q) {
+      const double* a = S.P[first[q]];
+      if (d2_exact(a[0], a[1], a[2], S.P[i][0], S.P[i][1], S.P[i][2]) <= eps2) c = q;
+    }
+    if (c < 0) c = nc, first[nc] = i, size[nc] = 0, ++nc;
+    of[i] = c;
+    size[c] += 1;
+  }
+  // Cluster c is written to slot c <= first[c]; every sample it reads has an
+  // index >= first[c], and no later cluster reads a slot below its own first
+  // member, so the rewrite can run in place in cluster order.
+  for (int c = 0; c < nc; ++c) {
+    const int f = first[c];
+    double loc0 = S.P[f][0], loc1 = S.P[f][1], loc2 = S.P[f][2], err = S.me[f], zb = S.mz[f];
+    if (size[c] > 1) {
+      const double k = double(size[c]);
+      double var = 0.0, zs = 0.0;
+      for (int i = f; i < n; ++i) {
+        if (of[i] != c) continue;
+        var += S.me[i];
+        zs += S.mz[i];
+        for (int j = f; j < n; ++j)
+          if (of[j] == c) var += cov64(vg, lag64(vg, S.P[i], S.P[j]));
+      }
+      err = var / (k * k) - vg.c0;
+      zb = zs / k;
+    }
+    S.P[c][0] = loc0, S.P[c][1] = loc1, S.P[c][2] = loc2;
+    S.me[c] = err, S.mz[c] = zb;
+  }
+  *nn_out = nc;
+}
+
+__device__ __forceinline__ void tri_index(int e, int& i, int& j) {
+  int r = int((1.0f + sqrtf(8.0f * float(e) + 1.0f)) * 0.5f);
+  while (r * (r - 1) / 2 > e) --r;
+  while ((r + 1) * r / 2 <= e) ++r;
+  i = r, j = e - r * (r - 1) / 2;
+}
+
+__device__ __forceinline__ void write_fail(const SolveDev& a, int64_t ti, int8_t st, int n_used) {
+  a.value[ti] = NAN;
+  if (a.variance) a.variance[ti] = NAN;
+  if (a.lagrange) a.lagrange[ti] = NAN;
+  if (a.n_used) a.n_used[ti] = n_used;
+  if (a.status) a.status[ti] = st;
+}
+
+// Everything up to the packed covariance triangle: loads the system of
+// target ti, applies the coincident guard, projects into the variogram
+// frame, assembles T (strictly lower, packed) and returns this row's data.
+// Returns false (outputs written) when there is nothing to solve.
+template <int NW>
+__device__ __forceinline__ bool assemble(const SolveDev& a, SolveSmem<NW>& S, int gid, int wig, int row, int64_t ti,
+                                         int& n, int& nn, bool& have, double& c, double& err, double& zf) {
+  constexpr int R = 32 * NW;
+  n = a.count[ti];
+  const int8_t st = a.sstatus[ti];
+  if (st != BTK_ST_OK || n <= 0 || n > R) {
+    if (row == 0) write_fail(a, ti, st != BTK_ST_OK ? st : (n > R ? BTK_ST_UNSUPPORTED : BTK_ST_SEARCH_FAILED), 0);
+    return false;
+  }
+  const double t[3] = {a.tx[ti], a.ty[ti], a.tz[ti]};
+  have = row < n;
+  double w[3] = {0, 0, 0};
+  double z = 0.0;
+  err = 0.0;
+  int tw = 0;
+  if (have) {
+    const uint32_t j = a.nbr[ti * a.max_samples + row];
+    w[0] = a.sx[j], w[1] = a.sy[j], w[2] = a.sz[j];
+    z = a.sv[j];
+    if (a.se) err = a.se[j];
+    tw = a.twin[j];
+  }
+  zf = kind_f(a.kind, a.kparam, z);
+  nn = n;
+  if (group_any<NW>(S, gid, wig, tw != 0)) {
+    if (have) S.P[row][0] = w[0], S.P[row][1] = w[1], S.P[row][2] = w[2], S.me[row] = err, S.mz[row] = zf;
+    gsync<NW>(gid);
+    if (row == 0) merge_clusters<NW>(S, n, a.vg, &S.ired[0]);
+    gsync<NW>(gid);
+    nn = S.ired[0];
+    have = row < nn;
+    if (have) w[0] = S.P[row][0], w[1] = S.P[row][1], w[2] = S.P[row][2], err = S.me[row], zf = S.mz[row];
+    gsync<NW>(gid);
+  }
+  // Samples relative to the target, in the variogram's frame (kernel.rs:34-42).
+  double p[3] = {w[0] - t[0], w[1] - t[1], w[2] - t[2]};
+  if (a.vg.has_frame) {
+    const double* M = a.vg.frame;
+    double r[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r[k] = M[3 * k] * p[0] + M[3 * k + 1] * p[1] + M[3 * k + 2] * p[2];
+    p[0] = r[0], p[1] = r[1], p[2] = r[2];
+  }
+  if (have) S.P[row][0] = p[0], S.P[row][1] = p[1], S.P[row][2] = p[2];
+  gsync<NW>(gid);
+  const int E = nn * (nn - 1) / 2;
+  for (int e = row; e < E; e += R) {
+    int i, j;
+    tri_index(e, i, j);
+    const double dx = S.P[i][0] - S.P[j][0], dy = S.P[i][1] - S.P[j][1], dz = S.P[i][2] - S.P[j][2];
+    S.T[e] = cov64(a.vg, sqrt(dx * dx + dy * dy + dz * dz));
+  }
+  c = have ? cov64(a.vg, sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2])) : 0.0;
+  gsync<NW>(gid);
+  return true;
+}
+
+// Estimate, variance and Lagrange multiplier from the five forms
+// s[0] = 1'C^-1 c, s[1] = 1'C^-1 1, s[2] = f'C^-1 c, s[3] = f'C^-1 1,
+// s[4] = c'C^-1 c (kernel.rs:86-122).
+__device__ __forceinline__ void epilogue(const SolveDev& a, int64_t ti, const double s[5], int n_used, int8_t flag) {
+  const double c0 = a.vg.c0;
+  double mu, value, swc;
+  if (a.kind == BTK_SIMPLE) {
+    mu = 0.0;
+    value = a.kparam + s[2];
+    swc = s[4];
+  } else {
+    mu = (s[0] - 1.0) / s[1];
+    value = s[2] - mu * s[3];
+    if (a.kind == BTK_INDICATOR) value = value < 0.0 ? 0.0 : (value > 1.0 ? 1.0 : value);
+    swc = s[4] - mu * s[0];
+  }
+  a.value[ti] = value;
+  if (a.variance) a.variance[ti] = fmax(c0 - swc - mu, 0.0);
+  if (a.lagrange) a.lagrange[ti] = mu;
+  if (a.n_used) a.n_used[ti] = n_used;
+  if (a.status) a.status[ti] = int8_t(BTK_ST_OK | flag);
+}
+
+template <int NW>
+__global__ void __launch_bounds__(128) k_solve64(SolveDev a, int8_t flag) {
+  constexpr int R = 32 * NW;
+  constexpr int GROUPS = 128 / R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int gid = threadIdx.x / R, row = threadIdx.x % R, wig = row >> 5;
+  SolveSmem<NW>& S = reinterpret_cast<SolveSmem<NW>*>(smem_raw)[gid];
+  const int64_t nitems = a.list ? *a.list_len : a.m;
+  const double c0 = a.vg.c0;
+  for (int64_t item = int64_t(blockIdx.x) * GROUPS + gid; item < nitems; item += int64_t(gridDim.x) * GROUPS) {
+    const int64_t ti = a.list ? a.list[item] : item;
+    gsync<NW>(gid);
+    int n, nn;
+    bool have;
+    double c, err, zf;
+    if (!assemble<NW>(a, S, gid, wig, row, ti, n, nn, have, c, err, zf)) continue;
+
+    double A[R];
+    const int tri = row * (row - 1) / 2;
+#pragma unroll
+    for (int q = 0; q < R; ++q)
+      A[q] = q < row ? (have ? S.T[tri + q] : 0.0) : (q == row ? (have ? c0 + err : 1.0) : 0.0);
+    double y0 = have ? c : 0.0, y1 = have ? 1.0 : 0.0, y2 = have ? zf : 0.0;
+    double dme = 1.0;
+    bool sing = false;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      if (k >= nn) break;
+      const int b = k & 1;
+      S.col[b][row] = A[k];
+      if (row == k) S.rhs[b][0] = y0, S.rhs[b][1] = y1, S.rhs[b][2] = y2;
+      gsync<NW>(gid);
+      const double d = S.col[b][k];
+      if (!(d > kPivot * c0)) {  // NaN or at most 1e-12 C0 (kernel.rs:61)
+        sing = true;
+        break;
+      }
+      if (row == k) dme = d;
+      if (row > k) {
+        const double f = A[k] * (1.0 / d);
+#pragma unroll
+        for (int q = k + 1; q < R; ++q) A[q] = fma(-f, S.col[b][q], A[q]);
+        y0 = fma(-f, S.rhs[b][0], y0);
+        y1 = fma(-f, S.rhs[b][1], y1);
+        y2 = fma(-f, S.rhs[b][2], y2);
+        A[k] = f;
+      }
+    }
+    if (sing) {
+      if (row == 0) write_fail(a, ti, BTK_ST_SINGULAR, 0);
+      continue;
+    }
+    const double wt = have ? 1.0 / dme : 0.0;
+    double s[5] = {y1 * y0 * wt, y1 * y1 * wt, y2 * y0 * wt, y2 * y1 * wt, y0 * y0 * wt};
+    group_sum5<NW>(S, gid, wig, s);
+    if (row == 0) epilogue(a, ti, s, n, flag);
+  }
+}
+
+template <int NW>
+__global__ void __launch_bounds__(128) k_solve_mixed(SolveDev a, int64_t* redo, int64_t* redo_len) {
+  constexpr int R = 32 * NW;
+  constexpr int GROUPS = 128 / R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int gid = threadIdx.x / R, row = threadIdx.x % R, wig = row >> 5;
+  MixedSmem<NW>& X = reinterpret_cast<MixedSmem<NW>*>(smem_raw)[gid];
+  SolveSmem<NW>& S = X.base;
+  const int64_t nitems = a.list ? *a.list_len : a.m;
+  const double c0 = a.vg.c0;
+  const float c0f = float(c0);
+  for (int64_t item = int64_t(blockIdx.x) * GROUPS + gid; item < nitems; item += int64_t(gridDim.x) * GROUPS) {
+    const int64_t ti = a.list ? a.list[item] : item;
+    gsync<NW>(gid);
+    int n, nn;
+    bool have;
+    double c, err, zf;
+    if (!assemble<NW>(a, S, gid, wig, row, ti, n, nn, have, c, err, zf)) continue;
+
+    // FP32 LDL^T with the forward substitution of (c, 1, f) fused in.
+    float A[R];
+    const int tri = row * (row - 1) / 2;
+    const double diag = have ? c0 + err : 1.0;
+#pragma unroll
+    for (int q = 0; q < R; ++q)
+      A[q] = q < row ? (have ? float(S.T[tri + q]) : 0.f) : (q == row ? float(diag) : 0.f);
+    float y0 = have ? float(c) : 0.f, y1 = have ? 1.f : 0.f, y2 = have ? float(zf) : 0.f;
+    float dme = 1.f;
+    bool weak = false;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      if (k >= nn) break;
+      const int b = k & 1;
+      X.colf[b][row] = A[k];
+      if (row == k) X.rhsf[b][0] = y0, X.rhsf[b][1] = y1, X.rhsf[b][2] = y2;
+      gsync<NW>(gid);
+      const float d = X.colf[b][k];
+      if (!(d > 1e-5f * c0f)) {
+        weak = true;
+        break;
+      }
+      if (row == k) dme = d;
+      if (row > k) {
+        const float f = A[k] * __frcp_rn(d);
+#pragma unroll
+        for (int q = k + 1; q < R; ++q) A[q] = fmaf(-f, X.colf[b][q], A[q]);
+        y0 = fmaf(-f, X.rhsf[b][0], y0);
+        y1 = fmaf(-f, X.rhsf[b][1], y1);
+        y2 = fmaf(-f, X.rhsf[b][2], y2);
+        A[k] = f;
+      }
+    }
+    if (weak) {  // leave it to the FP64 form, which also takes the singular decision
+      if (row == 0) redo[atomicAdd(reinterpret_cast<unsigned long long*>(redo_len), 1ull)] = ti;
+      continue;
+    }
+    // Back substitution L^T x = D^-1 y, column by column from the last row.
+#pragma unroll
+    for (int q = 0; q < R; ++q) X.L[row][q] = A[q];
+    float u0 = y0 / dme, u1 = y1 / dme, u2 = y2 / dme;
+    gsync<NW>(gid);
+    for (int k = nn - 1; k >= 0; --k) {
+      const int b = k & 1;
+      if (row == k) X.rhsf[b][0] = u0, X.rhsf[b][1] = u1, X.rhsf[b][2] = u2;
+      gsync<NW>(gid);
+      if (row < k) {
+        const float l = X.L[k][row];
+        u0 = fmaf(-l, X.rhsf[b][0], u0);
+        u1 = fmaf(-l, X.rhsf[b][1], u1);
+        u2 = fmaf(-l, X.rhsf[b][2], u2);
+      }
+    }
+    // FP64 residuals r_v = v - C x_v with C from the FP64 triangle.
+    const double x0 = have ? double(u0) : 0.0, x1 = have ? double(u1) : 0.0, x2 = have ? double(u2) : 0.0;
+    X.xs[0][row] = x0, X.xs[1][row] = x1, X.xs[2][row] = x2;
+    gsync<NW>(gid);
+    double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+    if (have) {
+      double a0 = diag * x0, a1 = diag * x1, a2 = diag * x2;
+      for (int j = 0; j < nn; ++j) {
+        if (j == row) continue;
+        const double cij = j < row ? S.T[tri + j] : S.T[j * (j - 1) / 2 + row];
+        a0 = fma(cij, X.xs[0][j], a0);
+        a1 = fma(cij, X.xs[1][j], a1);
+        a2 = fma(cij, X.xs[2][j], a2);
+      }
+      r0 = c - a0, r1 = 1.0 - a1, r2 = zf - a2;
+    }
+    // Corrected forms u'x_v + x_u'r_v (error second order in the residuals).
+    double s[5] = {x0 + x1 * r0, x1 + x1 * r1, zf * x0 + x2 * r0, zf * x1 + x2 * r1, c * x0 + x0 * r0};
+    if (!have) s[0] = s[1] = s[2] = s[3] = s[4] = 0.0;
+    group_sum5<NW>(S, gid, wig, s);
+    if (!(s[1] > 0.0) || !(fabs(s[0]) < 1e30)) {
+      if (row == 0) redo[atomicAdd(reinterpret_cast<unsigned long long*>(redo_len), 1ull)] = ti;
+      continue;
+    }
+    if (row == 0) epilogue(a, ti, s, n, 0);
+  }
+}
+
+__global__ void k_bucket(int64_t m, const int32_t* count, const int8_t* sstatus, int64_t* small, int64_t* large,
+                         int64_t* lens) {
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < m; t += int64_t(gridDim.x) * blockDim.x) {
+    const bool big = sstatus[t] == BTK_ST_OK && count[t] > 32;
+    unsigned long long* len = reinterpret_cast<unsigned long long*>(lens + (big ? 1 : 0));
+    (big ? large : small)[atomicAdd(len, 1ull)] = t;
+  }
+}
+
+template <class K>
+int blocks_for(const Launch& L, K kern, size_t smem) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+  return L.sm_count * per_sm;
+}
+
+template <int NW>
+cudaError_t run_fp64(const Launch& L, const SolveDev& a, int8_t flag) {
+  const size_t smem = sizeof(SolveSmem<NW>) * (128 / (32 * NW));
+  auto kern = k_solve64<NW>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  kern<<<blocks_for(L, kern, smem), 128, smem, L.stream>>>(a, flag);
+  ++*L.counter;
+  return cudaGetLastError();
+}
+
+template <int NW>
+cudaError_t run_mixed(const Launch& L, const SolveDev& a, int64_t* redo, int64_t* redo_len) {
+  const size_t smem = sizeof(MixedSmem<NW>) * (128 / (32 * NW));
+  auto kern = k_solve_mixed<NW>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  kern<<<blocks_for(L, kern, smem), 128, smem, L.stream>>>(a, redo, redo_len);
+  ++*L.counter;
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_bucket(const Launch& L, int64_t m, const int32_t* count, const int8_t* sstatus, int64_t* lists,
+                          int64_t* lens) {
+  cudaError_t e = cudaMemsetAsync(lens, 0, 2 * sizeof(int64_t), L.stream);
+  if (e != cudaSuccess) return e;
+  int64_t b = (m + 255) / 256;
+  if (b > int64_t(L.sm_count) * 8) b = int64_t(L.sm_count) * 8;
+  if (b < 1) b = 1;
+  k_bucket<<<int(b), 256, 0, L.stream>>>(m, count, sstatus, lists, lists + m, lens);
+  ++*L.counter;
+  return cudaGetLastError();
+}
+
+// rows: 32 (one warp per system) or 64 (a warp pair).
+cudaError_t launch_solve(const Launch& L, const SolveDev& a, int rows) {
+  return rows > 32 ? run_fp64<2>(L, a, 0) : run_fp64<1>(L, a, 0);
+}
+
+cudaError_t launch_solve_mixed(const Launch& L, const SolveDev& a, int rows, int64_t* redo, int64_t* redo_len) {
+  return rows > 32 ? run_mixed<2>(L, a, redo, redo_len) : run_mixed<1>(L, a, redo, redo_len);
+}
+
+cudaError_t launch_solve_redo(const Launch& L, const SolveDev& a, int rows) {
+  return rows > 32 ? run_fp64<2>(L, a, BTK_ST_FP64_FALLBACK) : run_fp64<1>(L, a, BTK_ST_FP64_FALLBACK);
+}
+
+}  // namespace btk

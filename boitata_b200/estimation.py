@@ -1,0 +1,331 @@
+"""Estimators with the reference's call surface: fit on samples, predict at targets.
+
+Mirrors python/boitata/estimation.py:209-423 (`_Base.fit/predict/
+cross_validate`, `OrdinaryKriging`, `SimpleKriging`, `IndicatorKriging`) and
+the pyo3 engine behind it (crates/py/src/estimation.rs:1213-1868): samples
+sharing a location keep the first one with a warning (args.rs:318-376),
+targets a search cannot fill are NaN, several searches run as passes on the
+targets earlier passes left (batch.rs:132-147). The kriging itself runs in
+the CUDA engine through its C ABI; `precision` selects the FP64 form
+(default, the reference's arithmetic) or the mixed FP32/FP64 form.
+"""
+
+import ctypes
+import math
+import warnings
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from .errors import InvalidInput, Unsupported
+from .geometry import BlockModel, Geometry
+from .search import Search
+from .variogram import Variogram
+
+PRECISIONS = {"fp64": N.FP64, "mixed": N.MIXED}
+
+
+def points(coords):
+    """(n, 2) or (n, 3) finite coordinates as an (n, 3) float64 array (containers.rs:15-54)."""
+    a = np.asarray(coords, dtype=np.float64)
+    if a.ndim != 2 or a.shape[1] not in (2, 3):
+        raise InvalidInput("coordinates must be a 2-D array of shape (n, 2) or (n, 3)")
+    if not np.all(np.isfinite(a)):
+        raise InvalidInput("coordinates must be finite")
+    if a.shape[1] == 2:
+        a = np.column_stack([a, np.zeros(len(a))])
+    return np.ascontiguousarray(a)
+
+
+def finite(values, what, n=None):
+    v = np.ascontiguousarray(np.asarray(values, dtype=np.float64))
+    if v.ndim != 1:
+        raise InvalidInput(f"{what} must be a 1-D numeric array")
+    if not np.all(np.isfinite(v)):
+        raise InvalidInput(f"{what} must be finite; drop missing values first")
+    if n is not None and len(v) != n:
+        raise InvalidInput(f"{what}: expected {n} values, got {len(v)}")
+    return v
+
+
+def distinct(locs, holes=None):
+    """Rows to keep so no two samples share a location: the first of each group,
+    with a UserWarning naming the dropped groups (args.rs:318-376 over
+    eda::duplicates with tolerance 0, which treats -0 as 0)."""
+    key = np.ascontiguousarray(locs + 0.0)
+    _, first, inverse, counts = np.unique(key, axis=0, return_index=True, return_inverse=True, return_counts=True)
+    inverse = inverse.ravel()
+    if np.all(counts == 1):
+        return np.arange(len(locs))
+    keep = np.sort(first)
+    groups = []
+    for g in np.nonzero(counts > 1)[0]:
+        rows = np.nonzero(inverse == g)[0]
+        groups.append(rows)
+    groups.sort(key=lambda r: r[0])
+    lines = []
+    for rows in groups[:20]:
+        who = (f"holes {', '.join(str(holes[i]) for i in rows)}" if holes is not None
+               else f"rows {', '.join(str(i) for i in rows)}")
+        x, y, z = locs[rows[0]]
+        lines.append(f"{who} at ({x}, {y}, {z})")
+    if len(groups) > 20:
+        lines.append(f"and {len(groups) - 20} more")
+    warnings.warn(f"{len(groups)} locations hold several samples; kept the first of each: {'; '.join(lines)}",
+                  UserWarning, stacklevel=3)
+    return keep
+
+
+@dataclass(frozen=True)
+class CrossValidation:
+    """Cross-validation results; NaN where a sample had too few neighbours (estimation.py:112-170)."""
+
+    actual: np.ndarray
+    estimate: np.ndarray
+    variance: np.ndarray
+
+    @property
+    def error(self):
+        return self.estimate - self.actual
+
+    @property
+    def mean_error(self):
+        return float(np.nanmean(self.error))
+
+    @property
+    def mean_squared_error(self):
+        return float(np.nanmean(self.error ** 2))
+
+    @property
+    def standardized_squared_error(self):
+        return float(np.nanmean(self.error ** 2 / self.variance))
+
+    @property
+    def correlation(self):
+        ok = np.isfinite(self.estimate)
+        return float(np.corrcoef(self.actual[ok], self.estimate[ok])[0, 1])
+
+
+class _Base:
+    _kind = N.ORDINARY
+
+    def __init__(self, variogram, search, *, kparam=0.0, precision="fp64", device=0):
+        if variogram is None:
+            raise InvalidInput("kriging needs a variogram")
+        if not isinstance(variogram, Variogram):
+            raise InvalidInput("variogram must be a Variogram")
+        searches = list(search) if isinstance(search, (list, tuple)) else [search]
+        if not searches or not all(isinstance(s, Search) for s in searches):
+            raise InvalidInput("search must be a Search or a sequence of Search (passes)")
+        if self._kind == N.SIMPLE and not variogram.is_stationary():
+            raise InvalidInput("simple kriging needs a variogram with a sill: every structure must be stationary "
+                               "(not power); use ordinary kriging")
+        if precision not in PRECISIONS:
+            raise InvalidInput(f"precision must be one of {sorted(PRECISIONS)}")
+        self.variogram = variogram
+        self.searches = searches
+        self._kparam = float(kparam)
+        self.precision = precision
+        self._device = device
+        self._ctx = None
+        self._pass = None
+        self._samples = None
+
+    # -- fit --------------------------------------------------------------
+    def fit(self, coords, values, *, holes=None, error_variance=None):
+        """Stores the samples; samples sharing a location keep the first one, with a warning."""
+        locs = points(coords)
+        n = len(locs)
+        vals = finite(values, "values", n)
+        err = None
+        if error_variance is not None:
+            err = finite(error_variance, "error_variance", n)
+            if np.any(err < 0):
+                raise InvalidInput("error_variance must be >= 0")
+        if holes is not None:
+            holes = list(holes)
+            if len(holes) != n:
+                raise InvalidInput(f"holes: expected {n} values, got {len(holes)}")
+        keep = distinct(locs, holes)
+        locs, vals = np.ascontiguousarray(locs[keep]), np.ascontiguousarray(vals[keep])
+        err = None if err is None else np.ascontiguousarray(err[keep])
+        self._samples = (locs, vals, err)
+        if self._ctx is None:
+            self._ctx = N.Context(self._device)
+        self._pass = None
+        self._use_pass(0)
+        return self
+
+    def _use_pass(self, p):
+        if self._pass == p:
+            return
+        ctx = self._ctx
+        s = self.searches[p].to_c()
+        if self._pass is None:
+            locs, vals, err = self._samples
+            vg = self.variogram.to_c()
+            rc = ctx._lib.btk_fit(ctx.handle, len(locs), locs.ctypes.data, vals.ctypes.data,
+                                  None if err is None else err.ctypes.data, None, ctypes.byref(s), ctypes.byref(vg))
+            ctx.check(rc, "fit")
+        else:
+            ctx.check(ctx._lib.btk_set_search(ctx.handle, ctypes.byref(s)), "search")
+        self._pass = p
+
+    def _fitted(self):
+        if self._samples is None:
+            raise InvalidInput("estimator is not fitted; call fit first")
+
+    @property
+    def values(self):
+        self._fitted()
+        return self._samples[1].copy()
+
+    # -- predict ------------------------------------------------------------
+    def _run(self, xyz, precision):
+        m = len(xyz)
+        out = {k: np.full(m, np.nan) for k in ("value", "variance", "lagrange")}
+        out["n_used"] = np.zeros(m, dtype=np.int32)
+        out["status"] = np.zeros(m, dtype=np.int8)
+        if m == 0:
+            return out
+        o = N.OutputsC(out["value"].ctypes.data, out["variance"].ctypes.data, out["lagrange"].ctypes.data,
+                       out["n_used"].ctypes.data, out["status"].ctypes.data)
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        ctx = self._ctx
+        rc = ctx._lib.btk_predict(ctx.handle, m, xyz.ctypes.data, self._kind, self._kparam, PRECISIONS[precision],
+                                  ctypes.byref(o))
+        ctx.check(rc, "predict")
+        return out
+
+    def _level(self, targets):
+        """Centroids of a single-layer model turned only in azimuth take the
+        elevation of 2-D data (crates/py/src/estimation.rs:960-992)."""
+        g = targets.geometry
+        locs = self._samples[0]
+        if g.count[2] != 1 or g.rotation[1] != 0.0 or g.rotation[2] != 0.0:
+            return None
+        z = locs[0, 2]
+        return z if math.isfinite(z) and np.all(locs[:, 2] == z) else None
+
+    def predict_full(self, targets, *, precision=None):
+        """Every output of the engine: value, variance, lagrange, n_used, status and pass (1-based, 0 unfilled)."""
+        self._fitted()
+        precision = precision or self.precision
+        if precision not in PRECISIONS:
+            raise InvalidInput(f"precision must be one of {sorted(PRECISIONS)}")
+        if isinstance(targets, Geometry):
+            targets = BlockModel(targets)
+        if isinstance(targets, BlockModel):
+            xyz = targets.centroids(self._ctx)
+            z = self._level(targets)
+            if z is not None:
+                xyz[:, 2] = z
+        else:
+            xyz = points(targets)
+        m = len(xyz)
+        res = None
+        remaining = np.arange(m)
+        for p in range(len(self.searches)):
+            if len(remaining) == 0:
+                break
+            self._use_pass(p)
+            out = self._run(xyz[remaining], precision)
+            if res is None:
+                res = {k: v.copy() for k, v in out.items()}
+                res["pass"] = np.where(np.isfinite(out["value"]), 1, 0).astype(np.int32)
+            else:
+                got = np.isfinite(out["value"])
+                for k in out:
+                    res[k][remaining[got]] = out[k][got]
+                res["pass"][remaining[got]] = p + 1
+                st = out["status"]
+                res["status"][remaining[~got]] = st[~got]
+            remaining = np.nonzero(~np.isfinite(res["value"]))[0]
+        return res
+
+    def predict(self, targets, *, return_variance=False, diagnostics=False, precision=None):
+        """Estimates at targets; NaN where the search found too few samples (estimation.py:273-335).
+
+        targets : (n, 2|3) array, Geometry or BlockModel (centroids made on the device).
+        """
+        if diagnostics:
+            raise Unsupported("diagnostics tables are not produced by this engine; use predict_full")
+        res = self.predict_full(targets, precision=precision)
+        if return_variance:
+            return res["value"], res["variance"]
+        return res["value"]
+
+    def cross_validate(self, *, folds=None, precision=None):
+        """Re-estimates every sample from the others, through the same passes (estimation.py:337-355)."""
+        self._fitted()
+        if folds is not None:
+            raise Unsupported("k-fold cross-validation is not run by this engine; use folds=None (leave-one-out)")
+        precision = precision or self.precision
+        n = len(self._samples[0])
+        est = np.full(n, np.nan)
+        var = np.full(n, np.nan)
+        for p in range(len(self.searches)):
+            self._use_pass(p)
+            value, variance = np.full(n, np.nan), np.full(n, np.nan)
+            o = N.OutputsC(value.ctypes.data, variance.ctypes.data, None, None, None)
+            ctx = self._ctx
+            ctx.check(ctx._lib.btk_cross_validate(ctx.handle, self._kind, self._kparam, PRECISIONS[precision],
+                                                  ctypes.byref(o)), "cross_validate")
+            fill = ~np.isfinite(est) & np.isfinite(value)
+            est[fill], var[fill] = value[fill], variance[fill]
+            if np.all(np.isfinite(est)):
+                break
+        return CrossValidation(self._samples[1].copy(), est, var)
+
+    def neighbors(self, targets, *, loo=False, search_pass=0):
+        """Neighbour lists (selection order, -1 padded), counts and success flags of the search."""
+        self._fitted()
+        self._use_pass(search_pass)
+        k = self.searches[search_pass].max_samples
+        if loo:
+            m = len(self._samples[0])
+            xyz = None
+        else:
+            xyz = points(targets)
+            m = len(xyz)
+        idx = np.empty((m, k), dtype=np.int64)
+        cnt = np.empty(m, dtype=np.int32)
+        ok = np.empty(m, dtype=np.int8)
+        ctx = self._ctx
+        rc = ctx._lib.btk_neighbors(ctx.handle, m, None if xyz is None else xyz.ctypes.data, 1 if loo else 0,
+                                    idx.ctypes.data, cnt.ctypes.data, ok.ctypes.data)
+        ctx.check(rc, "neighbors")
+        return idx, cnt, ok.astype(bool)
+
+
+class OrdinaryKriging(_Base):
+    """Kriging with an unknown, locally constant mean (weights sum to 1)."""
+
+    _kind = N.ORDINARY
+
+    def __init__(self, variogram, search, *, precision="fp64", device=0):
+        super().__init__(variogram, search, precision=precision, device=device)
+
+
+class SimpleKriging(_Base):
+    """Kriging with a known global `mean`."""
+
+    _kind = N.SIMPLE
+
+    def __init__(self, variogram, search, *, mean=0.0, precision="fp64", device=0):
+        mean = float(mean)
+        if not math.isfinite(mean):
+            raise InvalidInput("mean must be finite")
+        super().__init__(variogram, search, kparam=mean, precision=precision, device=device)
+        self.mean = mean
+
+
+class IndicatorKriging(_Base):
+    """Ordinary kriging of the indicator `value <= threshold`; estimates are probabilities."""
+
+    _kind = N.INDICATOR
+
+    def __init__(self, variogram, search, threshold, *, precision="fp64", device=0):
+        super().__init__(variogram, search, kparam=float(threshold), precision=precision, device=device)
+        self.threshold = float(threshold)

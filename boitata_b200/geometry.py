@@ -1,0 +1,70 @@
+"""Block-model geometry as kriging targets.
+
+Mirrors crates/core/src/block_model.rs:19-86 (Geometry: corner origin, cell
+size, cell count, azimuth/dip/rake; cells x fastest, then y, then z) and
+BlockModel::centroids (:431-445) for a regular model. The engine generates
+the centroids on the device, in the reference's arithmetic order.
+"""
+
+import math
+
+import numpy as np
+
+from . import _native as N
+from .errors import InvalidInput
+
+
+class Geometry:
+    def __init__(self, origin, size, count, rotation=(0.0, 0.0, 0.0)):
+        self.origin = tuple(float(v) for v in origin)
+        self.size = tuple(float(v) for v in size)
+        self.count = tuple(int(v) for v in count)
+        self.rotation = tuple(float(v) for v in rotation)
+        # block_model.rs:29-56
+        if len(self.origin) != 3 or len(self.size) != 3 or len(self.count) != 3 or len(self.rotation) != 3:
+            raise InvalidInput("origin, size, count and rotation need 3 values each")
+        if any(not (math.isfinite(s) and s > 0) for s in self.size):
+            raise InvalidInput("cell sizes must be positive")
+        if any(c <= 0 for c in self.count):
+            raise InvalidInput("cell counts must be positive")
+        if any(not math.isfinite(v) for v in self.origin + self.rotation):
+            raise InvalidInput("origin and rotation must be finite")
+
+    def cells(self):
+        return self.count[0] * self.count[1] * self.count[2]
+
+    def to_c(self):
+        g = N.GeometryC()
+        for a in range(3):
+            g.origin[a], g.size[a], g.count[a], g.rotation[a] = self.origin[a], self.size[a], self.count[a], \
+                self.rotation[a]
+        return g
+
+    def __repr__(self):
+        return f"Geometry(origin={self.origin}, size={self.size}, count={self.count}, rotation={self.rotation})"
+
+
+class BlockModel:
+    """A regular block model: its `geometry` and the centroids of its cells."""
+
+    def __init__(self, geometry):
+        if not isinstance(geometry, Geometry):
+            raise InvalidInput("BlockModel needs a Geometry")
+        self.geometry = geometry
+
+    def __len__(self):
+        return self.geometry.cells()
+
+    def centroids(self, context=None):
+        """Cell centroids (n, 3) in cell order, computed by the engine on the device."""
+        from ._native import Context
+
+        ctx = context or Context()
+        n = self.geometry.cells()
+        out = np.empty((n, 3), dtype=np.float64)
+        g = self.geometry.to_c()
+        import ctypes
+
+        rc = ctx._lib.btk_centroids(ctx.handle, ctypes.byref(g), 0, n, out.ctypes.data)
+        ctx.check(rc, "centroids")
+        return out

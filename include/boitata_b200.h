@@ -1,0 +1,182 @@
+/* boitata_b200 — C ABI of the B200 kriging engine.
+ *
+ * Plain C, plain pointers and sizes; no CUDA or torch types in the
+ * signatures (streams travel as `void*` holding a cudaStream_t). Every
+ * entry point returns 0 on success or a negative BTK_E* code; the message of
+ * the last failure on a context is btk_last_error(ctx). Nothing here exits,
+ * throws or falls back to the CPU: without a usable CUDA device btk_create
+ * fails with BTK_ECUDA.
+ *
+ * The entry points replace the kriging path of gstvschlz/boitata, whose
+ * only interface today is the pyo3 estimator (no C ABI exists there):
+ *   - btk_fit         crates/py/src/estimation.rs:1244-1311 (`store`) and
+ *                     crates/estimation/src/search.rs:759-776 (SearchTree::new)
+ *   - btk_predict*    crates/py/src/estimation.rs:1600-1742 (`predict`) ->
+ *                     crates/estimation/src/batch.rs:15-38 (estimate_many) ->
+ *                     crates/estimation/src/krige.rs:83-95 (krige)
+ *   - btk_cross_validate  crates/py/src/estimation.rs:1811-1843 ->
+ *                     crates/estimation/src/batch.rs:165-190 (leave_one_out_at)
+ *   - btk_neighbors   crates/estimation/src/search.rs:944-982 (neighbors_in)
+ *   - btk_centroids   crates/core/src/block_model.rs:76-86, 431-445
+ * The parameter structs mirror crates/variogram/src/{composite,model,aniso}.rs
+ * and crates/estimation/src/search.rs:31-81.
+ */
+#ifndef BOITATA_B200_H
+#define BOITATA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes ---- */
+#define BTK_OK 0
+#define BTK_EINVAL (-1)       /* invalid parameter (reference: InvalidParameters) */
+#define BTK_EUNSUPPORTED (-2) /* a reference option this engine does not run */
+#define BTK_ECUDA (-3)        /* CUDA error; message in btk_last_error */
+#define BTK_ENOTFITTED (-4)   /* predict before fit */
+#define BTK_ENOMEM (-5)       /* device allocation failed */
+
+/* ---- per-target status (one int8 per target) ---- */
+#define BTK_ST_OK 0
+#define BTK_ST_SEARCH_FAILED 1 /* fewer than min_samples (EstimError::SearchFailed) */
+#define BTK_ST_SINGULAR 2      /* pivot <= 1e-12 * C(0) (kernel.rs:61) */
+#define BTK_ST_UNSUPPORTED 3   /* more than 64 samples */
+#define BTK_ST_FP64_FALLBACK 0x10 /* flag: the mixed form re-solved this system in FP64 */
+
+/* ---- variogram models (crates/variogram/src/model.rs:11-30) ---- */
+#define BTK_SPHERICAL 0
+#define BTK_EXPONENTIAL 1
+#define BTK_GAUSSIAN 2
+#define BTK_CUBIC 3
+#define BTK_PENTASPHERICAL 4
+#define BTK_CIRCULAR 5
+#define BTK_SINEHOLE 6
+#define BTK_MATERN 7 /* param = order */
+#define BTK_POWER 8  /* param = exponent; not stationary: BTK_EUNSUPPORTED */
+#define BTK_MAX_STRUCT 4
+
+/* ---- kriging kinds (crates/estimation/src/krige.rs:20-27) ---- */
+#define BTK_ORDINARY 0
+#define BTK_SIMPLE 1    /* kparam = mean */
+#define BTK_INDICATOR 2 /* kparam = threshold */
+
+/* ---- precision forms ---- */
+#define BTK_FP64 0  /* FP64 throughout */
+#define BTK_MIXED 1 /* FP32 factorisation, FP64 residual refinement, Lagrange and variance */
+
+/* Azimuth/dip/rake (degrees) and ranges of an anisotropy
+ * (crates/variogram/src/aniso.rs:18-26); on = 0 means none. */
+typedef struct {
+  int32_t on;
+  double azimuth, dip, rake, major, semi, minor;
+} btk_aniso;
+
+typedef struct { /* crates/variogram/src/model.rs:33-40 */
+  int32_t model;
+  double param; /* Matérn order or power exponent, else ignored */
+  double sill;
+  double range;
+} btk_structure;
+
+typedef struct { /* crates/variogram/src/composite.rs:13-18 */
+  double nugget;
+  int32_t nstruct;
+  btk_structure s[BTK_MAX_STRUCT];
+  btk_aniso aniso; /* shared by every structure */
+} btk_variogram;
+
+/* crates/estimation/src/search.rs:31-81; optional counts are -1 for None. */
+typedef struct {
+  int64_t min_samples, max_samples;
+  double radius;
+  int64_t max_per_hole;      /* -1: none (not run on the GPU: BTK_EUNSUPPORTED) */
+  int64_t octant;            /* 0/1 */
+  int64_t sectors;           /* plane sectors, 0: none (BTK_EUNSUPPORTED) */
+  int64_t max_per_sector;
+  int64_t max_per_octant;    /* -1: ceil(max_samples / sector count) */
+  int64_t min_sectors;       /* -1: none (BTK_EUNSUPPORTED when set) */
+  int64_t max_empty_sectors; /* -1: none (BTK_EUNSUPPORTED when set) */
+  int64_t min_holes;         /* -1: none (BTK_EUNSUPPORTED when set) */
+  btk_aniso aniso;           /* search ellipsoid; on = 0: the variogram's */
+} btk_search;
+
+/* Block-model parent grid (crates/core/src/block_model.rs:19-26): corner
+ * origin, cell size, cell count, azimuth/dip/rake; cells run x fastest. */
+typedef struct {
+  double origin[3];
+  double size[3];
+  int64_t count[3];
+  double rotation[3];
+} btk_geometry;
+
+/* Outputs of a prediction; any pointer but `value` may be NULL. */
+typedef struct {
+  double* value;
+  double* variance;
+  double* lagrange;
+  int32_t* n_used;
+  int8_t* status;
+} btk_outputs;
+
+typedef struct btk_ctx btk_ctx;
+
+const char* btk_version(void);
+
+/* A context on CUDA device `device` with its own stream and device buffers.
+ * One context per host thread. NULL on failure, with the reason in `err`. */
+btk_ctx* btk_create(int device, char* err, size_t errlen);
+void btk_destroy(btk_ctx* ctx);
+const char* btk_last_error(const btk_ctx* ctx);
+
+/* Stores the samples on the device and indexes them for `search`: the
+ * projections into the search frame (origin at the first sample) and the
+ * uniform grid over them. xyz is n x 3 row-major; err_var and holes may be
+ * NULL. The caller has already dropped exact duplicates (the fit rule of
+ * crates/py/src/args.rs:318-376). Replaces any earlier fit. */
+int btk_fit(btk_ctx* ctx, int64_t n, const double* xyz, const double* values, const double* err_var,
+            const int64_t* holes, const btk_search* search, const btk_variogram* vg);
+
+/* A new search (a later pass) over the fitted samples; re-indexes them when
+ * its ellipsoid differs. */
+int btk_set_search(btk_ctx* ctx, const btk_search* search);
+
+/* Kriging at m targets given as host arrays (xyz m x 3 row-major); outputs
+ * are host arrays of m entries. Host-device copies are part of the call. */
+int btk_predict(btk_ctx* ctx, int64_t m, const double* xyz, int32_t kind, double kparam, int32_t precision,
+                const btk_outputs* out);
+
+/* As btk_predict, with device pointers: d_xyz is 3 arrays (x, y, z) of m
+ * doubles laid out back to back; outputs are device arrays; the work is
+ * queued on `stream` (a cudaStream_t, NULL for the context's own). */
+int btk_predict_device(btk_ctx* ctx, int64_t m, const double* d_xyz, int32_t kind, double kparam,
+                       int32_t precision, const btk_outputs* d_out, void* stream);
+
+/* Kriging at the centroids of every cell of `g`, generated on the device;
+ * outputs are device arrays of count[0]*count[1]*count[2] entries in cell
+ * order, queued on `stream`. */
+int btk_predict_geometry_device(btk_ctx* ctx, const btk_geometry* g, int32_t kind, double kparam,
+                                int32_t precision, const btk_outputs* d_out, void* stream);
+
+/* Leave-one-out at every fitted sample (host outputs of n entries). */
+int btk_cross_validate(btk_ctx* ctx, int32_t kind, double kparam, int32_t precision, const btk_outputs* out);
+
+/* Neighbour lists of m host targets: `idx` (m x max_samples, -1 padded) in
+ * selection order, `count` per target, `ok` 1 where the search succeeds.
+ * With `loo` set the targets are the n fitted samples themselves (xyz and m
+ * ignored), each searched as if it were absent (search.rs:951-982). */
+int btk_neighbors(btk_ctx* ctx, int64_t m, const double* xyz, int32_t loo, int64_t* idx, int32_t* count,
+                  int8_t* ok);
+
+/* Centroids of cells [first, first + m) of `g` into host xyz (m x 3). */
+int btk_centroids(btk_ctx* ctx, const btk_geometry* g, int64_t first, int64_t m, double* xyz);
+
+/* Kernel launches issued by this context since it was created. */
+int64_t btk_launch_count(const btk_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BOITATA_B200_H */

@@ -1,0 +1,116 @@
+"""CPU-side checks: the C ABI library loads and exports every declared entry
+point, and the host layer validates parameters as the reference does."""
+
+import ctypes
+import os
+import re
+import warnings
+
+import numpy as np
+import pytest
+
+import boitata_b200 as bt
+from boitata_b200 import _native
+from boitata_b200.estimation import distinct, points
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if fn.endswith(".h"):
+            text = open(os.path.join(ROOT, "include", fn)).read()
+            names |= set(re.findall(r"\b(btk_[a-z_]+)\s*\(", text))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_entry_point():
+    from boitata_b200 import build
+
+    if not os.path.exists(_native.LIB_PATH):
+        build.build()
+    lib = ctypes.CDLL(_native.LIB_PATH)
+    names = declared()
+    assert "btk_predict_geometry_device" in names and len(names) >= 12
+    for name in names:
+        assert hasattr(lib, name), name
+    assert set(_native.SIGNATURES) <= set(names)
+    assert lib.btk_version  # loads without a GPU
+
+
+def test_engine_refuses_to_run_without_a_cuda_device():
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            pytest.skip("a CUDA device is present")
+    except ImportError:
+        pass
+    with pytest.raises(_native.EngineError, match="CUDA"):
+        bt.OrdinaryKriging(bt.Variogram([("spherical", 1.0, 10.0)]), bt.Search(radius=5)).fit(
+            [[0.0, 0.0], [1.0, 1.0]], [1.0, 2.0])
+
+
+def test_search_constructor_rules():
+    """crates/py/src/estimation.rs:414-510 and search.rs:214-264."""
+    with pytest.raises(bt.InvalidInput, match="radius or ranges, not both"):
+        bt.Search(radius=10, ranges=(10, 10, 10))
+    with pytest.raises(bt.InvalidInput, match="give radius or ranges"):
+        bt.Search()
+    with pytest.raises(bt.InvalidInput, match="ratios with radius"):
+        bt.Search(ranges=(10, 5, 2), ratios=(0.5, 0.5))
+    with pytest.raises(bt.InvalidInput, match="max_per_sector needs octant"):
+        bt.Search(radius=10, max_per_sector=2)
+    with pytest.raises(bt.InvalidInput, match="min_samples <= max_samples"):
+        bt.Search(radius=10, min_samples=20, max_samples=16)
+    with pytest.raises(bt.InvalidInput, match="min_sectors and max_empty_sectors need"):
+        bt.Search(radius=10, min_sectors=2)
+    s = bt.Search(ranges=(300, 300, 100), max_samples=16)
+    assert s.radius == 300 and s.anisotropy == (0.0, 0.0, 0.0, 1.0, 1.0, 1.0 / 3.0)
+    o = bt.Search(radius=250, octant=True, max_per_sector=4, max_samples=32)
+    assert o.max_per_octant == 4 and o.anisotropy is None
+    c = o.to_c()
+    assert c.octant == 1 and c.max_per_octant == 4 and c.max_per_hole == -1
+
+
+def test_variogram_constructor_rules():
+    """crates/py/src/variogram.rs:164-177, 328-361 and model.rs:47-59."""
+    with pytest.raises(bt.InvalidInput, match="nugget"):
+        bt.Variogram([("spherical", 1.0, 10.0)], nugget=-1)
+    with pytest.raises(bt.InvalidInput, match="unknown model"):
+        bt.Variogram([("sphere", 1.0, 10.0)])
+    with pytest.raises(bt.InvalidInput, match="range finite and > 0"):
+        bt.Structure("spherical", 1.0, 0.0)
+    vg = bt.Variogram([("Spherical", 0.5, 80.0), bt.Structure("matern", 0.45, 250.0)], nugget=0.05)
+    assert vg.anisotropy is None and vg.total_sill() == pytest.approx(1.0)
+    assert vg.structures[1].order == 1.5
+    assert bt.Variogram([("hole", 1, 10)]).structures[0].model == "sinehole"
+    assert bt.Variogram([("spherical", 1, 10)], rotation=(30, 10, 0), ratios=(0.75, 0.25)).anisotropy == (
+        30.0, 10.0, 0.0, 1.0, 0.75, 0.25)
+
+
+def test_simple_kriging_rejects_a_variogram_without_a_sill():
+    """python/tests/test_estimation.py:38-44."""
+    power = bt.Variogram([("power", 1.0, 1.5)])
+    with pytest.raises(bt.InvalidInput, match="simple kriging needs a variogram with a sill"):
+        bt.SimpleKriging(power, bt.Search(radius=1000), mean=1.0)
+
+
+def test_fit_drops_samples_sharing_a_location_with_a_warning():
+    """crates/py/src/args.rs:318-376: the first of each group is kept; -0 equals 0."""
+    locs = points([[0.0, 0.0], [1.0, 1.0], [-0.0, 0.0], [2.0, 2.0], [1.0, 1.0]])
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter("always")
+        keep = distinct(locs, ["a", "b", "c", "d", "e"])
+    assert keep.tolist() == [0, 1, 3]
+    assert "2 locations hold several samples" in str(w[0].message) and "holes a, c" in str(w[0].message)
+    assert distinct(points([[0.0, 0.0], [1.0, 0.0]])).tolist() == [0, 1]
+
+
+def test_coordinates_and_values_must_be_finite():
+    with pytest.raises(bt.InvalidInput, match="finite"):
+        points([[0.0, np.nan]])
+    with pytest.raises(bt.InvalidInput, match="shape"):
+        points([[0.0, 1.0, 2.0, 3.0]])
+    assert points([[1.0, 2.0]]).tolist() == [[1.0, 2.0, 0.0]]
