@@ -73,6 +73,9 @@ SIGNATURES = {
     "btk_neighbors": (ctypes.c_int, [P, ctypes.c_int64, P, ctypes.c_int32, P, P, P]),
     "btk_centroids": (ctypes.c_int, [P, ctypes.POINTER(GeometryC), ctypes.c_int64, ctypes.c_int64, P]),
     "btk_launch_count": (ctypes.c_int64, [P]),
+    "btk_set_timing": (ctypes.c_int, [P, ctypes.c_int32]),
+    "btk_phase_ms": (ctypes.c_int, [P, P]),
+    "btk_peak_flops": (ctypes.c_double, [P, ctypes.c_int32]),
 }
 
 _lib = None

@@ -124,7 +124,13 @@ struct btk_ctx {
   DevBuf<int8_t> sst, o_status;
   DevBuf<double> o_value, o_var, o_lag;
 
+  bool timing = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+
   Launch launch(cudaStream_t s) { return Launch{s ? s : stream, sm_count, &launches}; }
+  void mark(int k, cudaStream_t s) {
+    if (timing) cudaEventRecord(ev[k], s);
+  }
 };
 
 namespace {
@@ -324,7 +330,9 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
   int rc = ensure_scratch(ctx, m);
   if (rc) return rc;
   Launch L = ctx->launch(s);
+  ctx->mark(0, L.stream);
   CK(launch_search(L, ctx->spd, ctx->gd, tx, ty, tz, perm, nwork, loo, ctx->nbr.p, ctx->cnt.p, ctx->sst.p));
+  ctx->mark(1, L.stream);
   SolveDev a{};
   a.vg = ctx->vgd;
   a.kind = kind;
@@ -337,23 +345,26 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
   a.m = m;
   a.value = o->value, a.variance = o->variance, a.lagrange = o->lagrange, a.n_used = o->n_used, a.status = o->status;
   const bool two = ctx->search.max_samples > 32;
+  const int nb = two ? 2 : 1;
   if (two) CK(launch_bucket(L, m, ctx->cnt.p, ctx->sst.p, ctx->lists.p, ctx->lens.p));
-  for (int b = 0; b < (two ? 2 : 1); ++b) {
+  if (precision == BTK_MIXED) CK(cudaMemsetAsync(ctx->redo_len.p, 0, 2 * sizeof(int64_t), L.stream));
+  for (int b = 0; b < nb; ++b) {
     SolveDev ab = a;
     if (two) ab.list = ctx->lists.p + b * m, ab.list_len = ctx->lens.p + b;
     const int rows = b == 0 ? 32 : 64;
-    if (precision == BTK_FP64) {
+    if (precision == BTK_FP64)
       CK(launch_solve(L, ab, rows));
-    } else {
-      int64_t* redo = ctx->redo.p + b * m;
-      int64_t* redo_len = ctx->redo_len.p + b;
-      CK(cudaMemsetAsync(redo_len, 0, sizeof(int64_t), L.stream));
-      CK(launch_solve_mixed(L, ab, rows, redo, redo_len));
-      SolveDev ar = a;
-      ar.list = redo, ar.list_len = redo_len;
-      CK(launch_solve_redo(L, ar, rows));
-    }
+    else
+      CK(launch_solve_mixed(L, ab, rows, ctx->redo.p + b * m, ctx->redo_len.p + b));
   }
+  ctx->mark(2, L.stream);
+  if (precision == BTK_MIXED)
+    for (int b = 0; b < nb; ++b) {  // systems the FP32 factorisation left to FP64
+      SolveDev ar = a;
+      ar.list = ctx->redo.p + b * m, ar.list_len = ctx->redo_len.p + b;
+      CK(launch_solve_redo(L, ar, b == 0 ? 32 : 64));
+    }
+  ctx->mark(3, L.stream);
   return BTK_OK;
 }
 
@@ -458,7 +469,32 @@ void btk_destroy(btk_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream), cudaStreamDestroy(ctx->stream);
+  for (cudaEvent_t e : ctx->ev)
+    if (e) cudaEventDestroy(e);
   delete ctx;
+}
+
+int btk_set_timing(btk_ctx* ctx, int32_t on) {
+  if (!ctx) return BTK_EINVAL;
+  CK(cudaSetDevice(ctx->device));
+  for (cudaEvent_t& e : ctx->ev)
+    if (!e) CK(cudaEventCreate(&e));
+  ctx->timing = on != 0;
+  return BTK_OK;
+}
+
+int btk_phase_ms(btk_ctx* ctx, float* out3) {
+  if (!ctx || !out3) return BTK_EINVAL;
+  if (!ctx->timing) return fail(ctx, BTK_EINVAL, "timing is off; call btk_set_timing first");
+  CK(cudaEventSynchronize(ctx->ev[3]));
+  for (int k = 0; k < 3; ++k) CK(cudaEventElapsedTime(&out3[k], ctx->ev[k], ctx->ev[k + 1]));
+  return BTK_OK;
+}
+
+double btk_peak_flops(btk_ctx* ctx, int32_t fp64) {
+  if (!ctx) return -1.0;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return -1.0;
+  return measure_fma_flops(ctx->stream, ctx->sm_count, fp64, &ctx->launches);
 }
 
 const char* btk_last_error(const btk_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }

@@ -99,4 +99,7 @@ cudaError_t launch_solve_mixed(const Launch& L, const SolveDev& a, int rows, int
 // FP64 re-solve of the redo list (a.list / a.list_len point at it).
 cudaError_t launch_solve_redo(const Launch& L, const SolveDev& a, int rows);
 
+// FLOP/s of a CUDA-core FMA loop (fp64 != 0: double, else float).
+double measure_fma_flops(cudaStream_t s, int sm_count, int fp64, int64_t* counter);
+
 }  // namespace btk

@@ -176,6 +176,16 @@ int btk_centroids(btk_ctx* ctx, const btk_geometry* g, int64_t first, int64_t m,
 /* Kernel launches issued by this context since it was created. */
 int64_t btk_launch_count(const btk_ctx* ctx);
 
+/* Diagnostics with no counterpart in the reference. btk_set_timing records
+ * CUDA events around the phases of every prediction on this context;
+ * btk_phase_ms waits for the last one and gives its search, solve and FP64
+ * re-solve times in milliseconds. btk_peak_flops runs a CUDA-core FMA loop
+ * and returns the FLOP/s reached (fp64 != 0: double, else float), the
+ * denominator of the solve kernels' roofline. */
+int btk_set_timing(btk_ctx* ctx, int32_t on);
+int btk_phase_ms(btk_ctx* ctx, float* out3);
+double btk_peak_flops(btk_ctx* ctx, int32_t fp64);
+
 #ifdef __cplusplus
 }
 #endif
