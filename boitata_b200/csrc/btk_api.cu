@@ -428,6 +428,21 @@ int upload_targets(btk_ctx* ctx, int64_t m, const double* xyz) {
 
 }  // namespace
 
+namespace btk {
+
+int prepare_variogram(const btk_variogram* vg, VgDev* out, std::string* why) {
+  btk_ctx tmp;  // host-side only: its device buffers stay empty
+  int rc = check_vg(&tmp, vg);
+  if (rc != BTK_OK) {
+    *why = tmp.err;
+    return rc;
+  }
+  make_vgdev(*vg, *out);
+  return BTK_OK;
+}
+
+}  // namespace btk
+
 extern "C" {
 
 const char* btk_version(void) { return "boitata_b200 0.1.0 (sm_100a)"; }

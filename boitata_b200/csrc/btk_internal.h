@@ -2,6 +2,8 @@
 // blocks the kernels take by value and the launchers the C ABI calls.
 #pragma once
 #include <cstdint>
+#include <string>
+
 #include <cuda_runtime.h>
 
 #include "boitata_b200.h"
@@ -98,6 +100,15 @@ cudaError_t launch_solve(const Launch& L, const SolveDev& a, int rows);
 cudaError_t launch_solve_mixed(const Launch& L, const SolveDev& a, int rows, int64_t* redo, int64_t* redo_len);
 // FP64 re-solve of the redo list (a.list / a.list_len point at it).
 cudaError_t launch_solve_redo(const Launch& L, const SolveDev& a, int rows);
+
+// As launch_solve_mixed / launch_solve_redo for n <= 32, testing each
+// system's own sample pairs for coincidence instead of reading a.twin.
+cudaError_t launch_solve_mixed_pairs(const Launch& L, const SolveDev& a, int64_t* redo, int64_t* redo_len);
+cudaError_t launch_solve_redo_pairs(const Launch& L, const SolveDev& a);
+
+// Checks a variogram as btk_fit does and fills its device form; on failure
+// returns a BTK_E* code with the reason in *why.
+int prepare_variogram(const btk_variogram* vg, VgDev* out, std::string* why);
 
 // FLOP/s of a CUDA-core FMA loop (fp64 != 0: double, else float).
 double measure_fma_flops(cudaStream_t s, int sm_count, int fp64, int64_t* counter);

@@ -184,7 +184,8 @@ __device__ __forceinline__ void write_fail(const SolveDev& a, int64_t ti, int8_t
 // target ti, applies the coincident guard, projects into the variogram
 // frame, assembles T (strictly lower, packed) and returns this row's data.
 // Returns false (outputs written) when there is nothing to solve.
-template <int NW>
+// kPairs: no fit-time twin flags; the system's own sample pairs are tested.
+template <int NW, bool kPairs = false>
 __device__ __forceinline__ bool assemble(const SolveDev& a, SolveSmem<NW>& S, int gid, int wig, int row, int64_t ti,
                                          int& n, int& nn, bool& have, double& c, double& err, double& zf) {
   constexpr int R = 32 * NW;
@@ -205,10 +206,21 @@ __device__ __forceinline__ bool assemble(const SolveDev& a, SolveSmem<NW>& S, in
     w[0] = a.sx[j], w[1] = a.sy[j], w[2] = a.sz[j];
     z = a.sv[j];
     if (a.se) err = a.se[j];
-    tw = a.twin[j];
+    if (!kPairs) tw = a.twin[j];
   }
   zf = kind_f(a.kind, a.kparam, z);
   nn = n;
+  if (kPairs) {  // coincident.rs:27-31 on this system's samples
+    if (have) S.P[row][0] = w[0], S.P[row][1] = w[1], S.P[row][2] = w[2];
+    gsync<NW>(gid);
+    if (have)
+      for (int q = 0; q < row; ++q)
+        if (d2_exact(S.P[q][0], S.P[q][1], S.P[q][2], w[0], w[1], w[2]) <= kEps * kEps) {
+          tw = 1;
+          break;
+        }
+    gsync<NW>(gid);
+  }
   if (group_any<NW>(S, gid, wig, tw != 0)) {
     if (have) S.P[row][0] = w[0], S.P[row][1] = w[1], S.P[row][2] = w[2], S.me[row] = err, S.mz[row] = zf;
     gsync<NW>(gid);
@@ -265,7 +277,7 @@ __device__ __forceinline__ void epilogue(const SolveDev& a, int64_t ti, const do
   if (a.status) a.status[ti] = int8_t(BTK_ST_OK | flag);
 }
 
-template <int NW>
+template <int NW, bool kPairs = false>
 __global__ void __launch_bounds__(128) k_solve64(SolveDev a, int8_t flag) {
   constexpr int R = 32 * NW;
   constexpr int GROUPS = 128 / R;
@@ -280,7 +292,7 @@ __global__ void __launch_bounds__(128) k_solve64(SolveDev a, int8_t flag) {
     int n, nn;
     bool have;
     double c, err, zf;
-    if (!assemble<NW>(a, S, gid, wig, row, ti, n, nn, have, c, err, zf)) continue;
+    if (!assemble<NW, kPairs>(a, S, gid, wig, row, ti, n, nn, have, c, err, zf)) continue;
 
     double A[R];
     const int tri = row * (row - 1) / 2;
@@ -324,7 +336,7 @@ __global__ void __launch_bounds__(128) k_solve64(SolveDev a, int8_t flag) {
   }
 }
 
-template <int NW>
+template <int NW, bool kPairs = false>
 __global__ void __launch_bounds__(128) k_solve_mixed(SolveDev a, int64_t* redo, int64_t* redo_len) {
   constexpr int R = 32 * NW;
   constexpr int GROUPS = 128 / R;
@@ -341,7 +353,7 @@ __global__ void __launch_bounds__(128) k_solve_mixed(SolveDev a, int64_t* redo, 
     int n, nn;
     bool have;
     double c, err, zf;
-    if (!assemble<NW>(a, S, gid, wig, row, ti, n, nn, have, c, err, zf)) continue;
+    if (!assemble<NW, kPairs>(a, S, gid, wig, row, ti, n, nn, have, c, err, zf)) continue;
 
     // FP32 LDL^T with the forward substitution of (c, 1, f) fused in.
     float A[R];
@@ -440,10 +452,10 @@ int blocks_for(const Launch& L, K kern, size_t smem) {
   return L.sm_count * per_sm;
 }
 
-template <int NW>
+template <int NW, bool kPairs = false>
 cudaError_t run_fp64(const Launch& L, const SolveDev& a, int8_t flag) {
   const size_t smem = sizeof(SolveSmem<NW>) * (128 / (32 * NW));
-  auto kern = k_solve64<NW>;
+  auto kern = k_solve64<NW, kPairs>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   kern<<<blocks_for(L, kern, smem), 128, smem, L.stream>>>(a, flag);
@@ -451,10 +463,10 @@ cudaError_t run_fp64(const Launch& L, const SolveDev& a, int8_t flag) {
   return cudaGetLastError();
 }
 
-template <int NW>
+template <int NW, bool kPairs = false>
 cudaError_t run_mixed(const Launch& L, const SolveDev& a, int64_t* redo, int64_t* redo_len) {
   const size_t smem = sizeof(MixedSmem<NW>) * (128 / (32 * NW));
-  auto kern = k_solve_mixed<NW>;
+  auto kern = k_solve_mixed<NW, kPairs>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   kern<<<blocks_for(L, kern, smem), 128, smem, L.stream>>>(a, redo, redo_len);
@@ -487,6 +499,16 @@ cudaError_t launch_solve_mixed(const Launch& L, const SolveDev& a, int rows, int
 
 cudaError_t launch_solve_redo(const Launch& L, const SolveDev& a, int rows) {
   return rows > 32 ? run_fp64<2>(L, a, BTK_ST_FP64_FALLBACK) : run_fp64<1>(L, a, BTK_ST_FP64_FALLBACK);
+}
+
+// The same two kernels for systems of at most 32 samples without fit-time
+// twin flags (a.twin unused): each system tests its own sample pairs.
+cudaError_t launch_solve_mixed_pairs(const Launch& L, const SolveDev& a, int64_t* redo, int64_t* redo_len) {
+  return run_mixed<1, true>(L, a, redo, redo_len);
+}
+
+cudaError_t launch_solve_redo_pairs(const Launch& L, const SolveDev& a) {
+  return run_fp64<1, true>(L, a, BTK_ST_FP64_FALLBACK);
 }
 
 }  // namespace btk

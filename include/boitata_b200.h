@@ -186,6 +186,37 @@ int btk_set_timing(btk_ctx* ctx, int32_t on);
 int btk_phase_ms(btk_ctx* ctx, float* out3);
 double btk_peak_flops(btk_ctx* ctx, int32_t fp64);
 
+/* Kriging without any allocation. This entry point has no counterpart in the
+ * reference. It is for callers that cannot call cudaMalloc: a host that owns
+ * every device allocation (its own arena or pool allocator, a fixed device
+ * memory budget) or a plugin running inside another program's CUDA context.
+ * The caller passes device buffers for every input and output:
+ *   - samples d_x, d_y, d_z, d_values and d_err (NULL: no measurement error);
+ *   - m targets d_tx, d_ty, d_tz;
+ *   - each target's neighbour list d_nbr (m x max_samples sample indices, as
+ *     btk_neighbors gives them), its length d_count and its search status
+ *     d_status (BTK_ST_OK, or BTK_ST_SEARCH_FAILED);
+ *   - outputs d_out, as for btk_predict_device.
+ * It solves the systems in the mixed form (BTK_MIXED, FP64 re-solve where
+ * needed) on `stream`, with the results of btk_predict_device; coincident
+ * samples are detected within each system.
+ * Its only scratch is a static device array of BTK_NOALLOC_MAX_SYSTEMS + 1
+ * int64 (2 MiB), held by every GPU that loads the library until the process
+ * exits. Limits: at most BTK_NOALLOC_MAX_SYSTEMS systems per call (more
+ * return BTK_EINVAL: split the call) and at most 32 samples per system. The
+ * first call on a device looks the array's address up (cudaGetSymbolAddress),
+ * so make it before capturing a stream. Every call shares the array, so calls
+ * that overlap on the GPU race: serialise them on one stream. `device` is
+ * made current for the call and the caller's device restored afterwards;
+ * `err` (may be NULL) receives the reason of a failure. */
+#define BTK_NOALLOC_MAX_SYSTEMS 262144
+int btk_solve_noalloc(int device, const btk_variogram* vg, int32_t kind, double kparam, const double* d_x,
+                      const double* d_y, const double* d_z, const double* d_values, const double* d_err,
+                      int64_t m, const double* d_tx, const double* d_ty, const double* d_tz,
+                      const uint32_t* d_nbr, int32_t max_samples, const int32_t* d_count,
+                      const int8_t* d_status, const btk_outputs* d_out, void* stream, char* err,
+                      size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif
