@@ -225,6 +225,19 @@ void make_searchdev(btk_ctx* ctx) {
   d.cap = int(cap);
   put9(metric ? block_frame(metric->azimuth, metric->dip, metric->rake) : eye(), d.axes);
   put9(metric ? aniso_matrix(*metric) : eye(), d.frame);
+  // With a metric M = diag(1, 1/semi, 1/minor) R the octant frame is rows
+  // (-R1, R0, R2), so its x, y, z are -semi dp1, dp0, minor dp2; without one
+  // both frames are the identity.
+  const int ax_x = metric ? 1 : 0, sg_x = metric ? -1 : 1, ax_y = metric ? 0 : 1;
+  d.nbits = d.nsec == 8 ? 3 : (d.nsec == 4 ? 2 : 0);
+  if (d.nsec == 8) {  // index bx << 2 | by << 1 | bz
+    d.bit_axis[2] = ax_x, d.bit_sign[2] = sg_x, d.bit_mask[2] = 0xF0;
+    d.bit_axis[1] = ax_y, d.bit_sign[1] = 1, d.bit_mask[1] = 0xCC;
+    d.bit_axis[0] = 2, d.bit_sign[0] = 1, d.bit_mask[0] = 0xAA;
+  } else if (d.nsec == 4) {  // index bx << 1 | by
+    d.bit_axis[1] = ax_x, d.bit_sign[1] = sg_x, d.bit_mask[1] = 0xC;
+    d.bit_axis[0] = ax_y, d.bit_sign[0] = 1, d.bit_mask[0] = 0xA;
+  }
 }
 
 double frobenius(const double* m) {

@@ -35,6 +35,12 @@ struct SearchDev {
   double axes[9];   // block_frame of the search ellipsoid (octant signs)
   double frame[9];  // projection into the search space
   double origin[3];  // first sample (search.rs:704-745)
+  // Sector bit k of a sample is (approximately) bit_sign[k] * dp[bit_axis[k]] >= 0
+  // for its offset dp from the target in the search frame: sectors are
+  // orthants of the grid axes, which lets the search prune cells by sector.
+  int nbits;
+  int bit_axis[3], bit_sign[3];
+  unsigned bit_mask[3];  // sectors whose index has bit k set
 };
 
 // Uniform grid over the projected samples, which are stored sorted by cell.

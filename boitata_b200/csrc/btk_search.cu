@@ -12,16 +12,22 @@
 // `max_samples`. That is what this kernel keeps.
 //
 // B200 mapping: one warp serves a tile of 32 targets, one per lane (block-
-// model tiles are 4 x 4 x 2 cells). The warp walks grid cells outward from
-// the tile's bounding box shell by shell; each shell's candidate ranges are
-// contiguous in the cell-sorted sample arrays, staged 32 at a time through
-// shared memory (coalesced loads, broadcast reads), and every lane tests
-// every candidate against its own target with exact-order FP64. Each lane
-// keeps one max-heap per sector in shared memory ([slot][lane] layout, free
-// of bank conflicts). A lane is done once the distance from its target to
-// the unvisited cells exceeds its current threshold (radius^2, or the
-// largest sector root once every sector is full); the tile ends when all
-// lanes are done or the grid is exhausted.
+// model tiles are 4 x 4 x 2 cells). The warp grows a box of grid cells from
+// the tile's own cells; each new slab of the box is a set of cell rows, each
+// row a contiguous range of the cell-sorted sample arrays, staged 32 samples
+// at a time through shared memory (coalesced loads, broadcast reads). Every
+// lane tests every staged candidate against its own target with exact-order
+// FP64 and keeps one max-heap per sector in shared memory ([slot][lane]
+// layout, free of bank conflicts).
+//
+// Sectors are orthants of the grid axes in the search frame (SearchDev
+// bit_axis / bit_sign), so a row is scanned only if, for some lane, it can
+// hold a sample of a sector that is still open (fewer than `cap` kept) within
+// the radius, or of a full sector closer than that sector's largest kept
+// distance. The box grows only across faces beyond which some lane still
+// needs cells by the same test, and the tile ends when no face is needed.
+// A target whose empty octant points out of the data therefore stops as soon
+// as the cells in that orthant run out, not at the search radius.
 #include <climits>
 
 #include "btk_device.cuh"
@@ -45,35 +51,58 @@ __device__ __forceinline__ bool key_less(double da, uint32_t ia, double db, uint
   return da < db || (da == db && ia < ib);
 }
 
-// Squared lower bound on the distance from q to any point of the cells
-// [x0..x1] x [y0..y1] x [z0..z1], less the grid's rounding slack.
-__device__ __forceinline__ double box_lb2(const GridDev& g, const double q[3], int x0, int x1, int y0, int y1,
-                                          int z0, int z1) {
-  int a[3] = {x0, y0, z0}, b[3] = {x1, y1, z1};
+// Squared lower bound on the distance from q to the box [lo, hi], less the
+// grid's rounding slack.
+__device__ __forceinline__ double lb2(const GridDev& g, const double q[3], const double lo[3], const double hi[3]) {
   double s = 0.0;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    double lo = g.lo[d] + a[d] * g.h, hi = g.lo[d] + (b[d] + 1) * g.h;
-    double gap = fmax(fmax(lo - q[d], q[d] - hi), 0.0);
+    double gap = fmax(fmax(lo[d] - q[d], q[d] - hi[d]), 0.0);
     gap = fmax(gap - g.slack, 0.0);
     s += gap * gap;
   }
   return s * (1.0 - 1e-12);
 }
 
-// Squared lower bound on the distance from q to any cell outside the box
-// [c0..c1] (clipped to the grid): the nearest face with cells beyond it.
-__device__ __forceinline__ double outside_lb2(const GridDev& g, const double q[3], const int c0[3], const int c1[3]) {
-  double lb = INFINITY;
+// Sectors a sample in the box [lo, hi] may fall in, seen from q.
+__device__ __forceinline__ unsigned box_sectors(const SearchDev& sp, const GridDev& g, const double q[3],
+                                                const double lo[3], const double hi[3], unsigned all) {
+  unsigned mask = all;
+  const double d0l = lo[0] - q[0], d1l = lo[1] - q[1], d2l = lo[2] - q[2];
+  const double d0h = hi[0] - q[0], d1h = hi[1] - q[1], d2h = hi[2] - q[2];
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    if (c0[d] > 0) lb = fmin(lb, fmax(q[d] - (g.lo[d] + c0[d] * g.h), 0.0));
-    if (c1[d] < g.dims[d] - 1) lb = fmin(lb, fmax((g.lo[d] + (c1[d] + 1) * g.h) - q[d], 0.0));
+  for (int k = 0; k < 3; ++k) {
+    if (k >= sp.nbits) break;
+    const int a = sp.bit_axis[k];  // selected, not indexed: keeps lo/hi in registers
+    const double dlo = a == 0 ? d0l : (a == 1 ? d1l : d2l), dhi = a == 0 ? d0h : (a == 1 ? d1h : d2h);
+    const bool up = sp.bit_sign[k] > 0 ? dhi >= -g.slack : dlo <= g.slack;  // bit 1 possible
+    const bool dn = sp.bit_sign[k] > 0 ? dlo <= g.slack : dhi >= -g.slack;  // bit 0 possible
+    mask &= (up ? sp.bit_mask[k] : 0u) | (dn ? ~sp.bit_mask[k] : 0u);
   }
-  if (lb == INFINITY) return INFINITY;
-  lb = fmax(lb - g.slack, 0.0);
-  return lb * lb * (1.0 - 1e-12);
+  return mask & all;
 }
+
+__device__ __forceinline__ void cell_box(const GridDev& g, int x0, int x1, int y0, int y1, int z0, int z1,
+                                         double lo[3], double hi[3]) {
+  lo[0] = g.lo[0] + x0 * g.h, hi[0] = g.lo[0] + (x1 + 1) * g.h;
+  lo[1] = g.lo[1] + y0 * g.h, hi[1] = g.lo[1] + (y1 + 1) * g.h;
+  lo[2] = g.lo[2] + z0 * g.h, hi[2] = g.lo[2] + (z1 + 1) * g.h;
+}
+
+// Per-lane state of the sector lists used to decide what is still needed.
+struct Need {
+  double radius2;
+  unsigned open;   // sectors with fewer than `cap` kept
+  double root[8];  // largest kept (d2) of each full sector
+  __device__ __forceinline__ bool wants(unsigned mask, double l2) const {
+    if (mask & open) return l2 <= radius2;
+    double m = -1.0;
+#pragma unroll
+    for (int s = 0; s < 8; ++s)
+      if ((mask >> s) & 1u) m = fmax(m, root[s]);
+    return l2 <= m;
+  }
+};
 
 template <int SLOTS, bool OCT>
 __device__ __forceinline__ double max_root(const WarpSmem<SLOTS, OCT>& S, int lane, int nsec, int cap) {
@@ -82,10 +111,16 @@ __device__ __forceinline__ double max_root(const WarpSmem<SLOTS, OCT>& S, int la
   return m;
 }
 
+__device__ __forceinline__ void set_root(Need& nd, int sec, double v) {
+#pragma unroll
+  for (int s = 0; s < 8; ++s)
+    if (s == sec) nd.root[s] = v;
+}
+
 // Offers candidate (d2, idx) of sector `sec` to this lane's lists.
 template <int SLOTS, bool OCT>
 __device__ __forceinline__ void consider(WarpSmem<SLOTS, OCT>& S, int lane, int nsec, int cap, int sec, double d2,
-                                         uint32_t idx, double& thr, int& nfull) {
+                                         uint32_t idx, double& thr, Need& nd) {
   const int base = sec * cap;
   int c = S.cnt[sec][lane];
   if (c < cap) {  // heap not full: sift up
@@ -102,7 +137,11 @@ __device__ __forceinline__ void consider(WarpSmem<SLOTS, OCT>& S, int lane, int 
     S.hd[base + pos][lane] = d2;
     S.hi[base + pos][lane] = idx;
     S.cnt[sec][lane] = c + 1;
-    if (c + 1 == cap && ++nfull == nsec) thr = max_root(S, lane, nsec, cap);
+    if (c + 1 == cap) {
+      nd.open &= ~(1u << sec);
+      set_root(nd, sec, S.hd[base][lane]);
+      if (nd.open == 0) thr = max_root(S, lane, nsec, cap);
+    }
     return;
   }
   if (!key_less(d2, idx, S.hd[base][lane], S.hi[base][lane])) return;
@@ -124,7 +163,8 @@ __device__ __forceinline__ void consider(WarpSmem<SLOTS, OCT>& S, int lane, int 
   }
   S.hd[base + pos][lane] = d2;
   S.hi[base + pos][lane] = idx;
-  if (nfull == nsec) thr = max_root(S, lane, nsec, cap);
+  set_root(nd, sec, S.hd[base][lane]);
+  if (nd.open == 0) thr = max_root(S, lane, nsec, cap);
 }
 
 template <int SLOTS, bool OCT>
@@ -159,8 +199,11 @@ __global__ void k_search(SearchDev sp, GridDev g, const double* __restrict__ tx,
   const int wib = threadIdx.x >> 5;
   WarpSmem<SLOTS, OCT>& S = reinterpret_cast<WarpSmem<SLOTS, OCT>*>(smem_raw)[wib];
   const int nsec = OCT ? sp.nsec : 1;
+  const unsigned all = (1u << nsec) - 1u;
   const int cap = sp.cap;
   const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
+  const double glo[3] = {g.lo[0], g.lo[1], g.lo[2]};
+  const double ghi[3] = {g.lo[0] + g.dims[0] * g.h, g.lo[1] + g.dims[1] * g.h, g.lo[2] + g.dims[2] * g.h};
 
   for (int64_t tile = int64_t(blockIdx.x) * (blockDim.x >> 5) + wib; tile * 32 < m; tile += warps) {
     const int64_t k = tile * 32 + lane;
@@ -179,7 +222,7 @@ __global__ void k_search(SearchDev sp, GridDev g, const double* __restrict__ tx,
         cq[a] = cqh[a] = int(u);
       }
     }
-    int b0[3], b1[3];
+    int b0[3], b1[3];  // current box of cells (inclusive)
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       int lo = cq[a], hi = cqh[a];
@@ -193,35 +236,31 @@ __global__ void k_search(SearchDev sp, GridDev g, const double* __restrict__ tx,
 
     for (int s = 0; s < nsec; ++s) S.cnt[s][lane] = 0;
     double thr = active ? sp.radius2 : -1.0;
-    int nfull = 0;
-    bool done = !active;
-    const uint32_t left = (loo && active) ? uint32_t(ti) : 0xffffffffu;
-
-    for (int r = 0;; ++r) {
-      int c0[3], c1[3], p0[3], p1[3];
+    Need nd;
+    nd.radius2 = active ? sp.radius2 : -1.0;
+    nd.open = active ? all : 0u;
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        c0[a] = max(b0[a] - r, 0), c1[a] = min(b1[a] + r, g.dims[a] - 1);
-        p0[a] = max(b0[a] - r + 1, 0), p1[a] = min(b1[a] + r - 1, g.dims[a] - 1);
-      }
-      if (r > 0 && c0[0] == p0[0] && c1[0] == p1[0] && c0[1] == p0[1] && c1[1] == p1[1] && c0[2] == p0[2] &&
-          c1[2] == p1[2])
-        break;  // the grid is exhausted
-      const int ny = c1[1] - c0[1] + 1;
-      const int64_t nrows = int64_t(ny) * (c1[2] - c0[2] + 1);
+    for (int s = 0; s < 8; ++s) nd.root[s] = -1.0;
+    const uint32_t left = (loo && active) ? uint32_t(ti) : 0xffffffffu;
+    int p0[3] = {1, 1, 1}, p1[3] = {0, 0, 0};  // previous box: empty at first
+
+    while (true) {
+      // Rows of the new slab: (y, z) over the box; x segments outside the previous box.
+      const int ny = b1[1] - b0[1] + 1;
+      const int64_t nrows = int64_t(ny) * (b1[2] - b0[2] + 1);
       for (int64_t rb = 0; rb < nrows; rb += 32) {
         const int64_t row = rb + lane;
         uint32_t a1 = 0, e1 = 0, a2 = 0, e2 = 0;
         int y = 0, z = 0, xa1 = 0, xb1 = -1, xa2 = 0, xb2 = -1;
         if (row < nrows) {
-          y = c0[1] + int(row % ny), z = c0[2] + int(row / ny);
-          const bool inner = r > 0 && y >= p0[1] && y <= p1[1] && z >= p0[2] && z <= p1[2];
+          y = b0[1] + int(row % ny), z = b0[2] + int(row / ny);
+          const bool inner = y >= p0[1] && y <= p1[1] && z >= p0[2] && z <= p1[2];
           const int64_t base = int64_t(g.dims[0]) * (y + int64_t(g.dims[1]) * z);
           if (!inner) {
-            xa1 = c0[0], xb1 = c1[0];
+            xa1 = b0[0], xb1 = b1[0];
           } else {
-            if (p0[0] > c0[0]) xa1 = c0[0], xb1 = p0[0] - 1;
-            if (p1[0] < c1[0]) xa2 = p1[0] + 1, xb2 = c1[0];
+            if (p0[0] > b0[0]) xa1 = b0[0], xb1 = p0[0] - 1;
+            if (p1[0] < b1[0]) xa2 = p1[0] + 1, xb2 = b1[0];
           }
           if (xb1 >= xa1) a1 = g.start[base + xa1], e1 = g.start[base + xb1 + 1];
           if (xb2 >= xa2) a2 = g.start[base + xa2], e2 = g.start[base + xb2 + 1];
@@ -236,7 +275,9 @@ __global__ void k_search(SearchDev sp, GridDev g, const double* __restrict__ tx,
             const uint32_t a = __shfl_sync(kFull, seg ? a2 : a1, j), e = __shfl_sync(kFull, seg ? e2 : e1, j);
             if (a >= e) continue;
             const int xa = __shfl_sync(kFull, seg ? xa2 : xa1, j), xb = __shfl_sync(kFull, seg ? xb2 : xb1, j);
-            const bool need = !done && box_lb2(g, q, xa, xb, yj, yj, zj, zj) <= thr;
+            double lo[3], hi[3];
+            cell_box(g, xa, xb, yj, yj, zj, zj, lo, hi);
+            const bool need = active && nd.wants(box_sectors(sp, g, q, lo, hi, all), lb2(g, q, lo, hi));
             if (!__any_sync(kFull, need)) continue;
             for (uint32_t base = a; base < e; base += 32) {
               const int nc = int(min(32u, e - base));
@@ -258,7 +299,7 @@ __global__ void k_search(SearchDev sp, GridDev g, const double* __restrict__ tx,
                       const double w[3] = {S.cw[0][c], S.cw[1][c], S.cw[2][c]};
                       sec = sector_of(sp.axes, sp.planar, w, t);
                     }
-                    consider(S, lane, nsec, cap, sec, d2, idx, thr, nfull);
+                    consider(S, lane, nsec, cap, sec, d2, idx, thr, nd);
                   }
                 }
               }
@@ -267,8 +308,30 @@ __global__ void k_search(SearchDev sp, GridDev g, const double* __restrict__ tx,
           }
         }
       }
-      done = done || outside_lb2(g, q, c0, c1) > thr;
-      if (__all_sync(kFull, done)) break;
+      // Grow the box across each face some lane still needs cells beyond.
+#pragma unroll
+      for (int a = 0; a < 3; ++a) p0[a] = b0[a], p1[a] = b1[a];
+      bool grew = false;
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        const int a = f >> 1;
+        const bool high = f & 1;
+        if (high ? b1[a] >= g.dims[a] - 1 : b0[a] <= 0) continue;
+        double lo[3] = {glo[0], glo[1], glo[2]}, hi[3] = {ghi[0], ghi[1], ghi[2]};
+        if (high)
+          lo[a] = g.lo[a] + (b1[a] + 1) * g.h;
+        else
+          hi[a] = g.lo[a] + b0[a] * g.h;
+        const bool need = active && nd.wants(box_sectors(sp, g, q, lo, hi, all), lb2(g, q, lo, hi));
+        if (__any_sync(kFull, need)) {
+          if (high)
+            b1[a] += 1;
+          else
+            b0[a] -= 1;
+          grew = true;
+        }
+      }
+      if (!grew) break;
     }
 
     // Gather every kept entry, sort by (d2, index), keep max_samples.
