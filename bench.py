@@ -46,6 +46,7 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=400_000, help="blocks in the CPU baseline sample")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-grad", action="store_true")
     p.add_argument("--grid", default=None, help="block counts NXxNYxNZ in place of 200x200x80 (profiling cases)")
     p.add_argument("--profile", action="store_true",
                    help="profiling case: warm-up and two steps of each form, no timing, no JSON line")
@@ -154,6 +155,42 @@ def rel_err(a, b):
     ok = np.isfinite(a) & np.isfinite(b)
     e = np.abs(a[ok] - b[ok]) / (1 + np.maximum(np.abs(a[ok]), np.abs(b[ok])))
     return e
+
+
+def loo_gradient(args, dev):
+    """c4: leave-one-out loss of 20,000 samples (32 neighbours, frozen) and its 10-parameter gradient;
+    kernel times from CUDA events on the launch stream, forward alone and forward with the adjoint."""
+    import torch
+
+    from boitata_b200 import OrdinaryKriging, workloads
+    from boitata_b200.gradient import LeaveOneOut, theta_of
+
+    w = workloads.c4(device=dev)
+    torch.cuda.empty_cache()
+    est = OrdinaryKriging(w.variogram, w.search).fit(w.coords, w.values)
+    loo = LeaveOneOut(est)
+    theta = theta_of(w.variogram)
+    ctx = est._ctx
+    ctx._lib.btk_set_timing(ctx.handle, 1)
+    times = {}
+    for grad in (False, True):
+        ms = []
+        for i in range(args.warmup + max(args.steps, 3)):
+            loss, g, nv = loo.evaluate(theta, grad=grad)
+            p3 = (ctypes.c_float * 3)()
+            ctx.check(ctx._lib.btk_phase_ms(ctx.handle, p3), "phase timing")
+            if i >= args.warmup:
+                ms.append(p3[0])
+        times[grad] = float(np.median(ms))
+    ctx._lib.btk_set_timing(ctx.handle, 0)
+    return {"loo_grad_ms": times[True],
+            "loo_grad": {"samples": int(len(w.coords)), "parameters": int(len(theta)), "loss": loss,
+                         "forward_ms": times[False], "forward_and_adjoint_ms": times[True],
+                         "adjoint_over_forward": (times[True] - times[False]) / times[False],
+                         "grad_norm": float(np.linalg.norm(g)),
+                         "what": "c4: mean squared leave-one-out error of ordinary kriging, 32 nearest samples "
+                                 "frozen at theta0, gradient w.r.t. nugget, 2 sills, 2 ranges, 2 ratios, "
+                                 "3 angles (FP64 adjoint, one kernel with the forward)"}}
 
 
 def run_reference(args, ws, rank):
@@ -319,7 +356,6 @@ def main():
                      "peak_source": "measured in this run: CUDA-core FP64 FMA loop (btk_peak_flops)",
                      "fp32_peak": peak32 / 1e12,
                      "algorithmic_flops_per_step": flops},
-        "loo_grad_ms": None,
         "gpu_launches": int(launches[N.MIXED]),
         "clocks": clocks,
     }
@@ -350,6 +386,9 @@ def main():
                        "d2h_bytes_per_step": m * 16,
                        "path": "btk_predict (C ABI, host buffers): H2D of pinned targets, search, solve, D2H of "
                                "value and variance; wall clock around the synchronous call"}
+
+    if not args.no_grad:
+        line.update(loo_gradient(args, dev))
 
     if rank == 0 and ws == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(w, args.cpu_sample)

@@ -127,6 +127,13 @@ struct btk_ctx {
   bool timing = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
+  // leave-one-out neighbourhoods frozen for the gradient
+  bool frozen = false;
+  DevBuf<uint32_t> loo_nbr;
+  DevBuf<int32_t> loo_cnt;
+  DevBuf<int8_t> loo_sst;
+  DevBuf<double> g_part, g_sums, g_val;
+
   Launch launch(cudaStream_t s) { return Launch{s ? s : stream, sm_count, &launches}; }
   void mark(int k, cudaStream_t s) {
     if (timing) cudaEventRecord(ev[k], s);
@@ -441,6 +448,36 @@ int upload_targets(btk_ctx* ctx, int64_t m, const double* xyz) {
 
 }  // namespace
 
+namespace {
+
+// dM/dphi for M = diag(1, 1/semi, 1/minor) r3(rake) r2(dip) r1(az), angles in
+// degrees (crates/core/src/rotation.rs:8-16, aniso.rs:88-94).
+void aniso_derivatives(const btk_aniso& a, double dM[5][9]) {
+  const double k = 3.14159265358979323846 / 180.0;
+  const double sa = std::sin(a.azimuth * k), ca = std::cos(a.azimuth * k);
+  const double sd = std::sin(a.dip * k), cd = std::cos(a.dip * k);
+  const double sr = std::sin(a.rake * k), cr = std::cos(a.rake * k);
+  M3 r1 = rows(sa, ca, 0.0, -ca, sa, 0.0, 0.0, 0.0, 1.0);
+  M3 r2 = rows(cd, 0.0, -sd, 0.0, 1.0, 0.0, sd, 0.0, cd);
+  M3 r3 = rows(1.0, 0.0, 0.0, 0.0, cr, sr, 0.0, -sr, cr);
+  M3 d1 = rows(ca * k, -sa * k, 0.0, sa * k, ca * k, 0.0, 0.0, 0.0, 0.0);
+  M3 d2 = rows(-sd * k, 0.0, -cd * k, 0.0, 0.0, 0.0, cd * k, 0.0, -sd * k);
+  M3 d3 = rows(0.0, 0.0, 0.0, 0.0, -sr * k, cr * k, 0.0, -cr * k, -sr * k);
+  M3 D{};
+  D.m[0][0] = 1.0, D.m[1][1] = 1.0 / a.semi, D.m[2][2] = 1.0 / a.minor;
+  M3 R = mul(mul(r3, r2), r1);
+  M3 ds{}, dm{};
+  ds.m[1][1] = -1.0 / (a.semi * a.semi);
+  dm.m[2][2] = -1.0 / (a.minor * a.minor);
+  put9(mul(ds, R), dM[0]);
+  put9(mul(dm, R), dM[1]);
+  put9(mul(D, mul(mul(r3, r2), d1)), dM[2]);
+  put9(mul(D, mul(mul(r3, d2), r1)), dM[3]);
+  put9(mul(D, mul(mul(d3, r2), r1)), dM[4]);
+}
+
+}  // namespace
+
 namespace btk {
 
 int prepare_variogram(const btk_variogram* vg, VgDev* out, std::string* why) {
@@ -549,6 +586,7 @@ int btk_fit(btk_ctx* ctx, int64_t n, const double* xyz, const double* values, co
   }
   CK(cudaSetDevice(ctx->device));
   ctx->n = n;
+  ctx->frozen = false;
   ctx->search = *search;
   ctx->vg = *vg;
   ctx->has_err = err_var != nullptr;
@@ -576,6 +614,7 @@ int btk_set_search(btk_ctx* ctx, const btk_search* search) {
   if ((rc = check_search(ctx, search))) return rc;
   CK(cudaSetDevice(ctx->device));
   ctx->search = *search;
+  ctx->frozen = false;
   if ((rc = index_samples(ctx))) return rc;
   CK(cudaStreamSynchronize(ctx->stream));
   return BTK_OK;
@@ -677,6 +716,71 @@ int btk_neighbors(btk_ctx* ctx, int64_t m, const double* xyz, int32_t loo, int64
   CK(cudaStreamSynchronize(L.stream));
   for (size_t i = 0; i < nb.size(); ++i) idx[i] = nb[i] == 0xffffffffu ? -1 : int64_t(nb[i]);
   for (int64_t i = 0; i < m; ++i) ok[i] = st[i] == BTK_ST_OK ? 1 : 0;
+  return BTK_OK;
+}
+
+int btk_loo_freeze(btk_ctx* ctx) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if (ctx->search.max_samples > 32)
+    return fail(ctx, BTK_EUNSUPPORTED, "the leave-one-out gradient takes at most 32 samples per system");
+  CK(cudaSetDevice(ctx->device));
+  const int64_t n = ctx->n;
+  CK(ctx->loo_nbr.grow(size_t(n) * size_t(ctx->search.max_samples)));
+  CK(ctx->loo_cnt.grow(size_t(n)));
+  CK(ctx->loo_sst.grow(size_t(n)));
+  Launch L = ctx->launch(nullptr);
+  CK(launch_search(L, ctx->spd, ctx->gd, ctx->x.p, ctx->y.p, ctx->z.p, ctx->loo_perm.p, n, 1, ctx->loo_nbr.p,
+                   ctx->loo_cnt.p, ctx->loo_sst.p));
+  CK(cudaStreamSynchronize(L.stream));
+  ctx->frozen = true;
+  return BTK_OK;
+}
+
+int btk_loo_gradient(btk_ctx* ctx, const btk_variogram* vg, int32_t want_grad, double* loss, double* grad,
+                     int64_t* n_valid, double* values) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if (!ctx->frozen) return fail(ctx, BTK_EINVAL, "call btk_loo_freeze first");
+  if ((rc = check_vg(ctx, vg))) return rc;
+  if (!loss) return fail(ctx, BTK_EINVAL, "loss is required");
+  CK(cudaSetDevice(ctx->device));
+  btk_variogram v = *vg;
+  if (!v.aniso.on) v.aniso = btk_aniso{1, 0.0, 0.0, 0.0, 1.0, 1.0, 1.0};  // isotropic, as a point of theta
+  GradDev a{};
+  make_vgdev(v, a.vg);
+  aniso_derivatives(v.aniso, a.dM);
+  const int ntheta = 1 + 2 * v.nstruct + 5;
+  const int64_t n = ctx->n;
+  a.sx = ctx->x.p, a.sy = ctx->y.p, a.sz = ctx->z.p, a.sv = ctx->v.p, a.se = ctx->has_err ? ctx->e.p : nullptr;
+  a.twin = ctx->twin.p;
+  a.nbr = ctx->loo_nbr.p, a.count = ctx->loo_cnt.p, a.sstatus = ctx->loo_sst.p;
+  a.max_samples = int(ctx->search.max_samples);
+  a.n = n;
+  a.want_grad = want_grad ? 1 : 0;
+  a.stride = 2 + ntheta;
+  CK(ctx->g_part.grow(size_t(n) * size_t(a.stride)));
+  CK(ctx->g_sums.grow(size_t(a.stride)));
+  a.part = ctx->g_part.p;
+  if (values) {
+    CK(ctx->g_val.grow(size_t(n)));
+    a.value = ctx->g_val.p;
+  }
+  Launch L = ctx->launch(nullptr);
+  ctx->mark(0, L.stream);
+  CK(launch_loo_grad(L, a, ctx->g_sums.p));
+  ctx->mark(1, L.stream);
+  ctx->mark(2, L.stream);
+  ctx->mark(3, L.stream);
+  std::vector<double> sums(size_t(a.stride));
+  CK(cudaMemcpyAsync(sums.data(), ctx->g_sums.p, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, L.stream));
+  if (values) CK(cudaMemcpyAsync(values, a.value, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, L.stream));
+  CK(cudaStreamSynchronize(L.stream));
+  const double cnt = sums[1];
+  *loss = cnt > 0 ? sums[0] / cnt : NAN;
+  if (n_valid) *n_valid = int64_t(cnt);
+  if (grad && want_grad)
+    for (int k = 0; k < ntheta; ++k) grad[k] = cnt > 0 ? sums[2 + k] / cnt : NAN;
   return BTK_OK;
 }
 

@@ -76,6 +76,23 @@ struct SolveDev {
   int8_t* status;
 };
 
+// Leave-one-out loss and gradient over frozen neighbourhoods (btk_adjoint.cu).
+struct GradDev {
+  VgDev vg;         // the variogram at theta; vg.frame = M(theta), always set
+  double dM[5][9];  // dM/d(semi, minor, azimuth, dip, rake), degrees for angles
+  const double *sx, *sy, *sz, *sv, *se;
+  const uint8_t* twin;
+  const uint32_t* nbr;
+  const int32_t* count;
+  const int8_t* sstatus;
+  int max_samples;
+  int64_t n;
+  int want_grad;
+  int stride;     // 2 + number of parameters
+  double* part;   // [n][stride]: loss term, valid flag, gradient terms
+  double* value;  // leave-one-out estimates, or null
+};
+
 // ---- launchers (each returns the launch's error, if any) ----
 struct Launch {
   cudaStream_t stream;
@@ -111,6 +128,9 @@ cudaError_t launch_solve_redo(const Launch& L, const SolveDev& a, int rows);
 // system's own sample pairs for coincidence instead of reading a.twin.
 cudaError_t launch_solve_mixed_pairs(const Launch& L, const SolveDev& a, int64_t* redo, int64_t* redo_len);
 cudaError_t launch_solve_redo_pairs(const Launch& L, const SolveDev& a);
+
+// Leave-one-out loss and gradient; sums[stride] receives the column sums.
+cudaError_t launch_loo_grad(const Launch& L, const GradDev& a, double* sums);
 
 // Checks a variogram as btk_fit does and fills its device form; on failure
 // returns a BTK_E* code with the reason in *why.

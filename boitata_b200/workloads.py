@@ -21,6 +21,8 @@ another implementation can regenerate the same inputs.
   c3  c1's box with a sample density rising 10x along x (2,000 samples);
       Search(radius=150, min_samples=4, max_samples=64); simple kriging with
       mean 1.0 on every 10th target.
+  c4  20,000 samples in c1's box, Gaussian-field values; leave-one-out
+      loss and gradient (see c4 below).
 """
 
 from dataclasses import dataclass
@@ -124,3 +126,39 @@ def c3(seed=3):
 
 
 CONFIGS = {"c1": c1, "c2": c2, "c3": c3}
+
+
+def gaussian_field(xyz, normals, rng=150.0, device=None):
+    """Values of a zero-mean Gaussian field with covariance exp(-3 h / rng) (sill 1) at xyz: L @ normals
+    for the Cholesky factor L of the covariance matrix (batch.rs:626-648 makes its test fields this way).
+    With `device` (a torch device) the FP64 matrix and its factor are formed there."""
+    if device is None:
+        d = xyz[:, None, :] - xyz[None, :, :]
+        cov = np.exp(-3.0 * np.sqrt((d * d).sum(-1)) / rng)
+        return np.linalg.cholesky(cov) @ normals
+    import torch
+
+    x = torch.as_tensor(xyz, dtype=torch.float64, device=device)
+    cov = torch.cdist(x, x)
+    cov.mul_(-3.0 / rng).exp_()
+    low = torch.linalg.cholesky(cov)
+    del cov
+    out = low @ torch.as_tensor(normals, dtype=torch.float64, device=device)
+    return out.cpu().numpy()
+
+
+def c4(n=20000, seed=4, device=None):
+    """Leave-one-out gradient workload: n samples in c1's box with Gaussian-field values (exponential
+    covariance, sill 1, range 150 m); kriging variogram nugget 0.05 + spherical 0.5 (100 m) + exponential
+    0.45 (250 m), rotation (30, 10, 0), ratios (0.75, 0.5): 10 parameters; each held-out sample kriged from
+    its 32 nearest samples (Search(radius=inf, max_samples=32)), neighbourhoods frozen at these values."""
+    s = Stream(seed)
+    xyz = s.uniform(3 * n).reshape(n, 3) * np.array([1000.0, 1000.0, 200.0])
+    values = gaussian_field(xyz, s.normal(n), device=device)
+    vg = Variogram([Structure("spherical", 0.5, 100.0), Structure("exponential", 0.45, 250.0)], nugget=0.05,
+                   rotation=(30.0, 10.0, 0.0), ratios=(0.75, 0.5))
+    search = Search(radius=float("inf"), max_samples=32, min_samples=1)
+    return Workload("c4", xyz, values, vg, search, None)
+
+
+CONFIGS["c4"] = c4

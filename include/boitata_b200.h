@@ -173,6 +173,25 @@ int btk_neighbors(btk_ctx* ctx, int64_t m, const double* xyz, int32_t loo, int64
 /* Centroids of cells [first, first + m) of `g` into host xyz (m x 3). */
 int btk_centroids(btk_ctx* ctx, const btk_geometry* g, int64_t first, int64_t m, double* xyz);
 
+/* Leave-one-out loss and its gradient with respect to the variogram. This
+ * has no counterpart in the reference, which computes leave-one-out
+ * estimates (batch.rs:165-190) but no gradient of them.
+ * btk_loo_freeze runs the leave-one-out search of the fitted samples once
+ * and keeps each sample's neighbour list (at most 32), so every later loss
+ * and gradient uses those neighbourhoods, whatever variogram it is given.
+ * btk_loo_gradient evaluates, for the variogram `vg` (same structure count
+ * and models as needed, any parameters), the mean squared leave-one-out
+ * error of ordinary kriging over the samples whose system is solvable and
+ * holds no coincident samples (*n_valid of them), and, when want_grad is
+ * set, its gradient in the order: nugget, sill of each structure, major
+ * range of each structure, semi/major ratio, minor/major ratio, azimuth,
+ * dip, rake (degrees); 1 + 2 nstruct + 5 values. A variogram without
+ * anisotropy is taken as ratios 1, 1 and angles 0. `values` (n, or NULL)
+ * receives the leave-one-out estimates. */
+int btk_loo_freeze(btk_ctx* ctx);
+int btk_loo_gradient(btk_ctx* ctx, const btk_variogram* vg, int32_t want_grad, double* loss, double* grad,
+                     int64_t* n_valid, double* values);
+
 /* Kernel launches issued by this context since it was created. */
 int64_t btk_launch_count(const btk_ctx* ctx);
 

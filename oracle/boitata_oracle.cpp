@@ -1146,6 +1146,32 @@ int32_t orc_estimate_many(int64_t m, const double* targets, int32_t loo, int64_t
   return 0;
 }
 
+// krige (krige.rs:83-95) of m targets from given neighbour lists (m x k,
+// -1 padded): frozen neighbourhoods for the leave-one-out gradient checks.
+// With skip_coincident, a system holding two samples within 1e-6 m gets
+// status 5 and no estimate.
+int32_t orc_krige_lists(int64_t m, const double* targets, int64_t n, const double* xyz, const double* v,
+                        const double* err, const int64_t* nbr, int64_t k, const orc_variogram* vgp, int32_t kind,
+                        double kparam, int32_t skip_coincident, orc_result* res) {
+  std::vector<Sample> s = conv_samples(n, xyz, v, err, nullptr);
+  Variogram vg = conv_vg(vgp);
+  for (int64_t t = 0; t < m; ++t) {
+    std::vector<Sample> sel;
+    for (int64_t j = 0; j < k; ++j)
+      if (nbr[t * k + j] >= 0) sel.push_back(s[size_t(nbr[t * k + j])]);
+    Estimate e;
+    if (sel.empty()) { put(e, SEARCH_FAILED, &res[t]); continue; }
+    bool twins = false;
+    for (size_t i = 0; i < sel.size() && !twins; ++i)
+      for (size_t j = 0; j < i; ++j)
+        if (close(sel[i].loc, sel[j].loc)) { twins = true; break; }
+    if (skip_coincident && twins) { put(e, 5, &res[t]); continue; }
+    int st = krige(kind, kparam, &targets[3 * t], sel, vg, e);
+    put(e, st, &res[t]);
+  }
+  return 0;
+}
+
 // crates/core/src/block_model.rs:62-86: centroid of cell `index`, x fastest.
 void orc_centroids(const double* origin, const double* size, const int64_t* count, const double* rotation,
                    int64_t first, int64_t m, double* out) {

@@ -93,6 +93,9 @@ def lib():
                                                    ctypes.POINTER(Srch), ctypes.POINTER(Vario), ctypes.c_int32,
                                                    ctypes.c_double, ctypes.c_int32, P, P]),
             "orc_centroids": (None, [P, P, P, P, ctypes.c_int64, ctypes.c_int64, P]),
+            "orc_krige_lists": (ctypes.c_int32, [ctypes.c_int64, P, ctypes.c_int64, P, P, P, P, ctypes.c_int64,
+                                                 ctypes.POINTER(Vario), ctypes.c_int32, ctypes.c_double,
+                                                 ctypes.c_int32, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -242,8 +245,8 @@ class Tree:
         return bool(ok), out[: n.value].tolist()
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            lib().orc_tree_free(self._h)
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.orc_tree_free(self._h)
             self._h = None
 
 
@@ -287,6 +290,28 @@ def estimate_many(targets, xyz, values, s, vg, *, kind="ordinary", kparam=0.0, e
     if neighbors:
         out["neighbors"] = nbr
     return out
+
+
+def _records(res, m):
+    arr = np.ctypeslib.as_array(ctypes.cast(res, ctypes.POINTER(ctypes.c_byte)), shape=(ctypes.sizeof(Result) * m,))
+    rec = np.frombuffer(arr.tobytes(), dtype=np.dtype([("value", "f8"), ("variance", "f8"), ("lagrange", "f8"),
+                                                        ("support", "f8"), ("n_used", "i8"), ("status", "i4"),
+                                                        ("pad", "i4")]), count=m)
+    return {k: rec[k].copy() for k in ("value", "variance", "lagrange", "n_used", "status")}
+
+
+def krige_lists(targets, xyz, values, nbr, vg, *, kind="ordinary", kparam=0.0, err=None, skip_coincident=True):
+    """krige of each target from its given neighbour list (m x k, -1 padded)."""
+    xyz, t = _xyz(xyz), _xyz(targets)
+    nbr = np.ascontiguousarray(nbr, dtype=np.int64)
+    m, k = nbr.shape
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    e = None if err is None else np.ascontiguousarray(err, dtype=np.float64)
+    res = (Result * max(m, 1))()
+    cv = variogram(vg)
+    lib().orc_krige_lists(m, t.ctypes.data, len(xyz), xyz.ctypes.data, v.ctypes.data, _ptr(e), nbr.ctypes.data, k,
+                          ctypes.byref(cv), KINDS[kind], kparam, 1 if skip_coincident else 0, ctypes.cast(res, P))
+    return _records(res, m)
 
 
 def centroids(origin, size, count, rotation, first=0, m=None):

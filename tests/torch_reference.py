@@ -1,0 +1,62 @@
+"""FP64 dense reference of the leave-one-out loss (test infrastructure).
+
+Each held-out sample's bordered ordinary-kriging system [C 1; 1' 0] is
+built from the variogram parameters theta in torch and solved densely;
+torch autograd then gives the gradient the engine's adjoint kernel must
+match. The covariance follows crates/variogram/src/{model,composite}.rs and
+the frame crates/core/src/rotation.rs:8-16 with aniso.rs:88-94.
+"""
+
+import math
+
+import torch
+
+
+def shape(model, t):
+    if model == "spherical":
+        return torch.where(t >= 1, torch.ones_like(t), 1.5 * t - 0.5 * t ** 3)
+    if model == "exponential":
+        return 1 - torch.exp(-3 * t)
+    if model == "gaussian":
+        return 1 - torch.exp(-3 * t * t)
+    raise NotImplementedError(model)
+
+
+def frame(semi, minor, az, dip, rake):
+    k = math.pi / 180
+    sa, ca = torch.sin(az * k), torch.cos(az * k)
+    sd, cd = torch.sin(dip * k), torch.cos(dip * k)
+    sr, cr = torch.sin(rake * k), torch.cos(rake * k)
+    z, o = torch.zeros_like(sa), torch.ones_like(sa)
+    r1 = torch.stack([torch.stack([sa, ca, z]), torch.stack([-ca, sa, z]), torch.stack([z, z, o])])
+    r2 = torch.stack([torch.stack([cd, z, -sd]), torch.stack([z, o, z]), torch.stack([sd, z, cd])])
+    r3 = torch.stack([torch.stack([o, z, z]), torch.stack([z, cr, sr]), torch.stack([z, -sr, cr])])
+    d = torch.diag(torch.stack([o, 1 / semi, 1 / minor]))
+    return d @ (r3 @ r2 @ r1)
+
+
+def loo_loss(theta, models, coords, values, nbr):
+    """Mean squared leave-one-out error; nbr (n x k) frozen neighbour indices (all systems full)."""
+    ns = len(models)
+    nugget, sills, ranges = theta[0], theta[1:1 + ns], theta[1 + ns:1 + 2 * ns]
+    M = frame(*theta[1 + 2 * ns:])
+    X = coords[nbr]                       # n, k, 3
+    P = (X - coords[:, None, :]) @ M.T    # n, k, 3
+    n, k, _ = P.shape
+    eye = torch.eye(k, dtype=P.dtype)
+    D = P[:, :, None, :] - P[:, None, :, :]
+    H = torch.sqrt((D * D).sum(-1) + eye)  # the diagonal is replaced below
+    h0 = torch.sqrt((P * P).sum(-1))
+
+    def cov(h):
+        return sum(sills[s] * (1 - shape(models[s], h / ranges[s])) for s in range(ns))
+
+    C = cov(H) * (1 - eye) + eye * (nugget + sills.sum())
+    K = torch.ones((n, k + 1, k + 1), dtype=P.dtype)
+    K[:, :k, :k] = C
+    K[:, k, k] = 0
+    b = torch.ones((n, k + 1), dtype=P.dtype)
+    b[:, :k] = cov(h0)
+    x = torch.linalg.solve(K, b)
+    est = (x[:, :k] * values[nbr]).sum(-1)
+    return ((est - values) ** 2).mean()
