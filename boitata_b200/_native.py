@@ -68,6 +68,10 @@ SIGNATURES = {
                                           ctypes.POINTER(OutputsC), P]),
     "btk_predict_geometry_device": (ctypes.c_int, [P, ctypes.POINTER(GeometryC), ctypes.c_int32, ctypes.c_double,
                                                    ctypes.c_int32, ctypes.POINTER(OutputsC), P]),
+    "btk_predict_kinds": (ctypes.c_int, [P, ctypes.c_int64, P, P, ctypes.c_double, ctypes.c_int32,
+                                         ctypes.POINTER(OutputsC)]),
+    "btk_predict_kinds_device": (ctypes.c_int, [P, ctypes.c_int64, P, P, ctypes.c_double, ctypes.c_int32,
+                                                ctypes.POINTER(OutputsC), P]),
     "btk_cross_validate": (ctypes.c_int, [P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
                                           ctypes.POINTER(OutputsC)]),
     "btk_neighbors": (ctypes.c_int, [P, ctypes.c_int64, P, ctypes.c_int32, P, P, P]),

@@ -121,7 +121,7 @@ struct btk_ctx {
   DevBuf<int64_t> perm, lists, lens, redo, redo_len;
   DevBuf<uint32_t> nbr;
   DevBuf<int32_t> cnt, o_nused;
-  DevBuf<int8_t> sst, o_status;
+  DevBuf<int8_t> sst, o_status, kinds;
   DevBuf<double> o_value, o_var, o_lag;
 
   bool timing = false;
@@ -342,7 +342,7 @@ int ensure_scratch(btk_ctx* ctx, int64_t m) {
 // Search then solve for m targets whose coordinates are device SoA arrays.
 int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const double* ty, const double* tz,
              const int64_t* perm, int64_t nwork, int loo, int32_t kind, double kparam, int32_t precision,
-             const btk_outputs* o) {
+             const btk_outputs* o, const int8_t* kinds = nullptr) {
   if (kind < BTK_ORDINARY || kind > BTK_INDICATOR) return fail(ctx, BTK_EINVAL, "unknown kriging kind");
   if (precision != BTK_FP64 && precision != BTK_MIXED) return fail(ctx, BTK_EINVAL, "unknown precision");
   if (kind == BTK_SIMPLE && !std::isfinite(kparam)) return fail(ctx, BTK_EINVAL, "simple kriging needs a finite mean");
@@ -357,6 +357,7 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
   a.vg = ctx->vgd;
   a.kind = kind;
   a.kparam = kparam;
+  a.kinds = kinds;
   a.max_samples = int(ctx->search.max_samples);
   a.sx = ctx->x.p, a.sy = ctx->y.p, a.sz = ctx->z.p, a.sv = ctx->v.p, a.se = ctx->has_err ? ctx->e.p : nullptr;
   a.twin = ctx->twin.p;
@@ -644,6 +645,39 @@ int btk_predict(btk_ctx* ctx, int64_t m, const double* xyz, int32_t kind, double
   if ((rc = host_outputs(ctx, m, out, &d))) return rc;
   const double* t = ctx->txyz.p;
   if ((rc = run_path(ctx, nullptr, m, t, t + m, t + 2 * m, nullptr, m, 0, kind, kparam, precision, &d))) return rc;
+  return copy_out(ctx, m, &d, out);
+}
+
+int btk_predict_kinds_device(btk_ctx* ctx, int64_t m, const double* d_xyz, const int8_t* d_kinds, double kparam,
+                             int32_t precision, const btk_outputs* d_out, void* stream) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if (m < 0 || (m > 0 && (!d_xyz || !d_kinds))) return fail(ctx, BTK_EINVAL, "targets and kinds are required");
+  if (m == 0) return BTK_OK;
+  CK(cudaSetDevice(ctx->device));
+  return run_path(ctx, static_cast<cudaStream_t>(stream), m, d_xyz, d_xyz + m, d_xyz + 2 * m, nullptr, m, 0,
+                  BTK_ORDINARY, kparam, precision, d_out, d_kinds);
+}
+
+int btk_predict_kinds(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds, double kparam,
+                      int32_t precision, const btk_outputs* out) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if (!out || !out->value) return fail(ctx, BTK_EINVAL, "outputs need a value array");
+  if (m < 0 || (m > 0 && (!xyz || !kinds))) return fail(ctx, BTK_EINVAL, "targets and kinds are required");
+  for (int64_t i = 0; i < m; ++i)
+    if (kinds[i] < BTK_ORDINARY || kinds[i] > BTK_INDICATOR) return fail(ctx, BTK_EINVAL, "unknown kriging kind");
+  if (m == 0) return BTK_OK;
+  CK(cudaSetDevice(ctx->device));
+  if ((rc = upload_targets(ctx, m, xyz))) return rc;
+  CK(ctx->kinds.grow(size_t(m)));
+  CK(cudaMemcpyAsync(ctx->kinds.p, kinds, size_t(m), cudaMemcpyHostToDevice, ctx->stream));
+  btk_outputs d{};
+  if ((rc = host_outputs(ctx, m, out, &d))) return rc;
+  const double* t = ctx->txyz.p;
+  if ((rc = run_path(ctx, nullptr, m, t, t + m, t + 2 * m, nullptr, m, 0, BTK_ORDINARY, kparam, precision, &d,
+                     ctx->kinds.p)))
+    return rc;
   return copy_out(ctx, m, &d, out);
 }
 

@@ -61,6 +61,7 @@ struct SolveDev {
   VgDev vg;
   int kind;
   double kparam;
+  const int8_t* kinds;  // per-target kind (ordinary / simple / indicator), or null for `kind`
   int max_samples;
   const double *sx, *sy, *sz, *sv, *se;  // samples, original order; se may be null
   const uint8_t* twin;                    // 1 where another sample lies within 1e-6 m

@@ -103,6 +103,21 @@ __device__ __forceinline__ void group_sum5(SolveSmem<NW>& S, int gid, int wig, d
   gsync<NW>(gid);
 }
 
+// Maximum of one value over the group, on every lane.
+template <int NW>
+__device__ __forceinline__ double group_max(SolveSmem<NW>& S, int gid, int wig, double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o));
+  if (NW == 1) return v;
+  if ((threadIdx.x & 31) == 0) S.red[wig][7] = v;
+  gsync<NW>(gid);
+  double m = S.red[0][7];
+#pragma unroll
+  for (int w = 1; w < NW; ++w) m = fmax(m, S.red[w][7]);
+  gsync<NW>(gid);
+  return m;
+}
+
 __device__ __forceinline__ double kind_f(int kind, double kparam, double z) {
   return kind == BTK_SIMPLE ? z - kparam : (kind == BTK_INDICATOR ? (z <= kparam ? 1.0 : 0.0) : z);
 }
@@ -187,8 +202,10 @@ __device__ __forceinline__ void write_fail(const SolveDev& a, int64_t ti, int8_t
 // kPairs: no fit-time twin flags; the system's own sample pairs are tested.
 template <int NW, bool kPairs = false>
 __device__ __forceinline__ bool assemble(const SolveDev& a, SolveSmem<NW>& S, int gid, int wig, int row, int64_t ti,
-                                         int& n, int& nn, bool& have, double& c, double& err, double& zf) {
+                                         int& n, int& nn, bool& have, double& c, double& err, double& zf,
+                                         int& kind) {
   constexpr int R = 32 * NW;
+  kind = a.kinds ? int(a.kinds[ti]) : a.kind;
   n = a.count[ti];
   const int8_t st = a.sstatus[ti];
   if (st != BTK_ST_OK || n <= 0 || n > R) {
@@ -208,7 +225,7 @@ __device__ __forceinline__ bool assemble(const SolveDev& a, SolveSmem<NW>& S, in
     if (a.se) err = a.se[j];
     if (!kPairs) tw = a.twin[j];
   }
-  zf = kind_f(a.kind, a.kparam, z);
+  zf = kind_f(kind, a.kparam, z);
   nn = n;
   if (kPairs) {  // coincident.rs:27-31 on this system's samples
     if (have) S.P[row][0] = w[0], S.P[row][1] = w[1], S.P[row][2] = w[2];
@@ -257,17 +274,18 @@ __device__ __forceinline__ bool assemble(const SolveDev& a, SolveSmem<NW>& S, in
 // Estimate, variance and Lagrange multiplier from the five forms
 // s[0] = 1'C^-1 c, s[1] = 1'C^-1 1, s[2] = f'C^-1 c, s[3] = f'C^-1 1,
 // s[4] = c'C^-1 c (kernel.rs:86-122).
-__device__ __forceinline__ void epilogue(const SolveDev& a, int64_t ti, const double s[5], int n_used, int8_t flag) {
+__device__ __forceinline__ void epilogue(const SolveDev& a, int kind, int64_t ti, const double s[5], int n_used,
+                                         int8_t flag) {
   const double c0 = a.vg.c0;
   double mu, value, swc;
-  if (a.kind == BTK_SIMPLE) {
+  if (kind == BTK_SIMPLE) {
     mu = 0.0;
     value = a.kparam + s[2];
     swc = s[4];
   } else {
     mu = (s[0] - 1.0) / s[1];
     value = s[2] - mu * s[3];
-    if (a.kind == BTK_INDICATOR) value = value < 0.0 ? 0.0 : (value > 1.0 ? 1.0 : value);
+    if (kind == BTK_INDICATOR) value = value < 0.0 ? 0.0 : (value > 1.0 ? 1.0 : value);
     swc = s[4] - mu * s[0];
   }
   a.value[ti] = value;
@@ -289,10 +307,10 @@ __global__ void __launch_bounds__(128) k_solve64(SolveDev a, int8_t flag) {
   for (int64_t item = int64_t(blockIdx.x) * GROUPS + gid; item < nitems; item += int64_t(gridDim.x) * GROUPS) {
     const int64_t ti = a.list ? a.list[item] : item;
     gsync<NW>(gid);
-    int n, nn;
+    int n, nn, kind;
     bool have;
     double c, err, zf;
-    if (!assemble<NW, kPairs>(a, S, gid, wig, row, ti, n, nn, have, c, err, zf)) continue;
+    if (!assemble<NW, kPairs>(a, S, gid, wig, row, ti, n, nn, have, c, err, zf, kind)) continue;
 
     double A[R];
     const int tri = row * (row - 1) / 2;
@@ -332,7 +350,7 @@ __global__ void __launch_bounds__(128) k_solve64(SolveDev a, int8_t flag) {
     const double wt = have ? 1.0 / dme : 0.0;
     double s[5] = {y1 * y0 * wt, y1 * y1 * wt, y2 * y0 * wt, y2 * y1 * wt, y0 * y0 * wt};
     group_sum5<NW>(S, gid, wig, s);
-    if (row == 0) epilogue(a, ti, s, n, flag);
+    if (row == 0) epilogue(a, kind, ti, s, n, flag);
   }
 }
 
@@ -350,10 +368,10 @@ __global__ void __launch_bounds__(128) k_solve_mixed(SolveDev a, int64_t* redo, 
   for (int64_t item = int64_t(blockIdx.x) * GROUPS + gid; item < nitems; item += int64_t(gridDim.x) * GROUPS) {
     const int64_t ti = a.list ? a.list[item] : item;
     gsync<NW>(gid);
-    int n, nn;
+    int n, nn, kind;
     bool have;
     double c, err, zf;
-    if (!assemble<NW, kPairs>(a, S, gid, wig, row, ti, n, nn, have, c, err, zf)) continue;
+    if (!assemble<NW, kPairs>(a, S, gid, wig, row, ti, n, nn, have, c, err, zf, kind)) continue;
 
     // FP32 LDL^T with the forward substitution of (c, 1, f) fused in.
     float A[R];
@@ -424,15 +442,23 @@ __global__ void __launch_bounds__(128) k_solve_mixed(SolveDev a, int64_t* redo, 
       }
       r0 = c - a0, r1 = 1.0 - a1, r2 = zf - a2;
     }
+    // Refinement residual test: the corrected forms below err by about
+    // rho^2 C0 / D_min (rho the FP32 solve's relative residual, D_min its
+    // smallest pivot); above 1e-8 the system is re-solved in FP64.
+    const double cmax = group_max<NW>(S, gid, wig, have ? fabs(c) : 0.0);
+    const double zmax = group_max<NW>(S, gid, wig, have ? fabs(zf) : 0.0);
+    const double rho = group_max<NW>(S, gid, wig, have ? fmax(fmax(fabs(r0) / fmax(cmax, 1e-300), fabs(r1)),
+                                                              fabs(r2) / fmax(zmax, 1e-300)) : 0.0);
+    const double dmin = -group_max<NW>(S, gid, wig, have ? -double(dme) : -1e300);
     // Corrected forms u'x_v + x_u'r_v (error second order in the residuals).
     double s[5] = {x0 + x1 * r0, x1 + x1 * r1, zf * x0 + x2 * r0, zf * x1 + x2 * r1, c * x0 + x0 * r0};
     if (!have) s[0] = s[1] = s[2] = s[3] = s[4] = 0.0;
     group_sum5<NW>(S, gid, wig, s);
-    if (!(s[1] > 0.0) || !(fabs(s[0]) < 1e30)) {
+    if (!(rho * rho * c0 / dmin <= 1e-8) || !(s[1] > 0.0) || !(fabs(s[0]) < 1e30)) {
       if (row == 0) redo[atomicAdd(reinterpret_cast<unsigned long long*>(redo_len), 1ull)] = ti;
       continue;
     }
-    if (row == 0) epilogue(a, ti, s, n, 0);
+    if (row == 0) epilogue(a, kind, ti, s, n, 0);
   }
 }
 

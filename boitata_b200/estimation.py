@@ -256,6 +256,29 @@ class _Base:
             return res["value"], res["variance"]
         return res["value"]
 
+    def predict_kinds(self, targets, kinds, *, mean=0.0, precision=None):
+        """Every output at `targets` with a kriging kind per target ("ordinary" / "simple" / "indicator", or
+        0 / 1 / 2) in one launch, sharing `mean` (simple) or threshold (indicator); first pass only."""
+        self._fitted()
+        precision = precision or self.precision
+        codes = {"ordinary": N.ORDINARY, "simple": N.SIMPLE, "indicator": N.INDICATOR}
+        k = np.array([codes.get(x, x) if isinstance(x, str) else x for x in kinds], dtype=np.int8)
+        xyz = points(targets)
+        m = len(xyz)
+        if len(k) != m:
+            raise InvalidInput(f"kinds: expected {m} values, got {len(k)}")
+        out = {key: np.full(m, np.nan) for key in ("value", "variance", "lagrange")}
+        out["n_used"] = np.zeros(m, dtype=np.int32)
+        out["status"] = np.zeros(m, dtype=np.int8)
+        self._use_pass(0)
+        o = N.OutputsC(out["value"].ctypes.data, out["variance"].ctypes.data, out["lagrange"].ctypes.data,
+                       out["n_used"].ctypes.data, out["status"].ctypes.data)
+        ctx = self._ctx
+        rc = ctx._lib.btk_predict_kinds(ctx.handle, m, xyz.ctypes.data, k.ctypes.data, float(mean),
+                                        PRECISIONS[precision], ctypes.byref(o))
+        ctx.check(rc, "predict")
+        return out
+
     def cross_validate(self, *, folds=None, precision=None):
         """Re-estimates every sample from the others, through the same passes (estimation.py:337-355)."""
         self._fitted()

@@ -162,3 +162,30 @@ def c4(n=20000, seed=4, device=None):
 
 
 CONFIGS["c4"] = c4
+
+
+def c5(holes=1600, seed=5):
+    """Large and ill-conditioned: holes (1600 -> 200,000 composites) in 40 clusters in a 1000 x 1000 x 250 m
+    box, 125 composites at 2 m each, plus a copy of 10 % of the samples 0.01 m away (beyond the 1e-6 m
+    coincident guard); lognormal values; Gaussian variogram (nugget 1e-4, sill 1, range 200 m), near-singular
+    systems; 400 x 400 x 64 blocks (10.24M); octant search, 8 per octant, 64 at most, radius 300 m."""
+    s = Stream(seed)
+    centres = s.uniform(2 * 40).reshape(40, 2) * 1000.0
+    u = s.uniform(3 * holes).reshape(holes, 3)
+    c = centres[(u[:, 0] * 40).astype(int) % 40]
+    cx = np.clip(c[:, 0] + (u[:, 1] - 0.5) * 100.0, 0.0, 1000.0)
+    cy = np.clip(c[:, 1] + (u[:, 2] - 0.5) * 100.0, 0.0, 1000.0)
+    z = 249.0 - 2.0 * np.arange(125)
+    xyz = np.column_stack([np.repeat(cx, 125), np.repeat(cy, 125), np.tile(z, holes)])
+    n = len(xyz)
+    pick = np.nonzero(s.uniform(n) < 0.1)[0]
+    twins = xyz[pick] + np.array([0.01, 0.0, 0.0])
+    xyz = np.vstack([xyz, twins])
+    values = np.exp(s.normal(len(xyz)))
+    vg = Variogram([Structure("gaussian", 1.0, 200.0)], nugget=1e-4)
+    search = Search(radius=300.0, octant=True, max_per_sector=8, max_samples=64)
+    geo = Geometry((0.0, 0.0, 0.0), (2.5, 2.5, 250.0 / 64), (400, 400, 64))
+    return Workload("c5", xyz, values, vg, search, geo)
+
+
+CONFIGS["c5"] = c5

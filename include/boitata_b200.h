@@ -160,6 +160,16 @@ int btk_predict_device(btk_ctx* ctx, int64_t m, const double* d_xyz, int32_t kin
 int btk_predict_geometry_device(btk_ctx* ctx, const btk_geometry* g, int32_t kind, double kparam,
                                 int32_t precision, const btk_outputs* d_out, void* stream);
 
+/* As btk_predict / btk_predict_device with a kriging kind per target
+ * (BTK_ORDINARY, BTK_SIMPLE or BTK_INDICATOR, one int8 each; host or device
+ * array like the coordinates) sharing `kparam` (the simple-kriging mean or
+ * the indicator threshold), so ordinary and simple kriging run in one launch.
+ * No counterpart in the reference, whose estimator has one kind. */
+int btk_predict_kinds(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds, double kparam,
+                      int32_t precision, const btk_outputs* out);
+int btk_predict_kinds_device(btk_ctx* ctx, int64_t m, const double* d_xyz, const int8_t* d_kinds, double kparam,
+                             int32_t precision, const btk_outputs* d_out, void* stream);
+
 /* Leave-one-out at every fitted sample (host outputs of n entries). */
 int btk_cross_validate(btk_ctx* ctx, int32_t kind, double kparam, int32_t precision, const btk_outputs* out);
 

@@ -253,3 +253,45 @@ def test_passes_fill_what_earlier_passes_left(oracle):
     assert later.any() and np.all(both["pass"][later] == 2)
     second = OrdinaryKriging(model, wide).fit(coords, values).predict(grid)
     np.testing.assert_array_equal(both["value"][later], second[later])
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 1e-6)])
+def test_ordinary_and_simple_kriging_in_one_launch(oracle, precision, tol):
+    # c3: uneven neighbour counts (4-64) with simple kriging (mean 1.0) on every 10th target.
+    w = W.c3()
+    targets = centroids(oracle, w, 3)
+    kinds = np.where(np.arange(len(targets)) % 10 == 0, "simple", "ordinary")
+    est = OrdinaryKriging(w.variogram, w.search, precision=precision).fit(w.coords, w.values)
+    got = est.predict_kinds(targets, kinds, mean=1.0)
+    for kind in ("ordinary", "simple"):
+        sel = kinds == kind
+        ref = oracle.estimate_many(targets[sel], w.coords, w.values, w.search, w.variogram, kind=kind, kparam=1.0,
+                                   neighbors=False)
+        assert_same_estimates({k: v[sel] for k, v in got.items()}, ref, tol)
+
+
+def test_ill_conditioned_systems(oracle):
+    # c5 in small: clustered holes, 10 % of samples copied 0.01 m away, Gaussian model with a 1e-4 nugget,
+    # 64 neighbours. Condition numbers reach ~5e5, so two FP64 evaluation orders differ by up to ~1e-15
+    # times the condition number: each system is held to max(1e-10, 2e-15 cond). The mixed form must hand
+    # every such system to its FP64 re-solve.
+    w = W.c5(holes=160)
+    rng = np.random.default_rng(0)
+    cent = centroids(oracle, w)
+    targets = cent[rng.choice(len(cent), 2000, replace=False)]
+    ref = oracle.estimate_many(targets, w.coords, w.values, w.search, w.variogram)
+    fp64 = OrdinaryKriging(w.variogram, w.search).fit(w.coords, w.values)
+    assert_same_neighbors(fp64, oracle, w.coords, w.search, w.variogram, targets[:300])
+    got = fp64.predict_full(targets)
+    fin = np.isfinite(ref["value"])
+    assert np.array_equal(fin, np.isfinite(got["value"])) and np.array_equal(got["status"], ref["status"])
+    for t in np.nonzero(fin & ~close(got["value"], ref["value"], 1e-10))[0]:
+        nb = [i for i in ref["neighbors"][t] if i >= 0]
+        d = np.sqrt(((w.coords[nb][:, None] - w.coords[nb][None]) ** 2).sum(-1))
+        cov = np.where(d > 0, np.exp(-3 * (d / 200.0) ** 2), 1.0 + 1e-4)
+        assert close(got["value"][t], ref["value"][t], max(1e-10, 2e-15 * np.linalg.cond(cov))), t
+    assert np.all(close(got["variance"][fin], ref["variance"][fin], 1e-10))
+    mixed = OrdinaryKriging(w.variogram, w.search, precision="mixed").fit(w.coords, w.values).predict_full(targets)
+    assert np.all((mixed["status"][fin] & 0x10) != 0)
+    for k in ("value", "variance", "lagrange"):
+        np.testing.assert_array_equal(mixed[k], got[k])
