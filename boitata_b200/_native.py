@@ -49,6 +49,11 @@ class GeometryC(ctypes.Structure):
                 ("rotation", ctypes.c_double * 3)]
 
 
+class TuningC(ctypes.Structure):
+    _fields_ = [("samples_per_cell", ctypes.c_double), ("tile", ctypes.c_int32 * 3), ("search_warps", ctypes.c_int32),
+                ("solve_blocks_per_sm", ctypes.c_int32)]
+
+
 class OutputsC(ctypes.Structure):
     _fields_ = [("value", ctypes.c_void_p), ("variance", ctypes.c_void_p), ("lagrange", ctypes.c_void_p),
                 ("n_used", ctypes.c_void_p), ("status", ctypes.c_void_p)]
@@ -77,6 +82,11 @@ SIGNATURES = {
     "btk_neighbors": (ctypes.c_int, [P, ctypes.c_int64, P, ctypes.c_int32, P, P, P]),
     "btk_centroids": (ctypes.c_int, [P, ctypes.POINTER(GeometryC), ctypes.c_int64, ctypes.c_int64, P]),
     "btk_launch_count": (ctypes.c_int64, [P]),
+    "btk_get_tuning": (ctypes.c_int, [P, ctypes.POINTER(TuningC)]),
+    "btk_set_tuning": (ctypes.c_int, [P, ctypes.POINTER(TuningC)]),
+    "btk_graph_capture_geometry": (ctypes.c_int, [P, ctypes.POINTER(GeometryC), ctypes.c_int32, ctypes.c_double,
+                                                  ctypes.c_int32, ctypes.POINTER(OutputsC)]),
+    "btk_graph_launch": (ctypes.c_int, [P, P]),
     "btk_set_timing": (ctypes.c_int, [P, ctypes.c_int32]),
     "btk_phase_ms": (ctypes.c_int, [P, P]),
     "btk_peak_flops": (ctypes.c_double, [P, ctypes.c_int32]),

@@ -1,0 +1,138 @@
+"""Autotuner for the engine's launch configuration.
+
+The tunables (btk_tuning in include/boitata_b200.h):
+- samples per grid cell (the cell size of the search grid);
+- the block-model tile one search warp serves (32 cells);
+- warps per search CTA (shared-memory granularity);
+- resident solve CTAs per SM.
+
+They are picked by timing the real workload. The time is the sum of the search and solve kernels, taken
+with CUDA events on the launch stream. Two stages run: cell size x tile first, then the CTA shapes at the
+best of those. The choice is cached per workload signature in a JSON file (BTK_TUNING_CACHE, or
+~/.cache/boitata_b200/tuning.json) and applied to the context.
+"""
+
+import ctypes
+import json
+import os
+
+import numpy as np
+
+from . import _native as N
+
+TILES = [(4, 4, 2), (8, 4, 1), (2, 4, 4), (4, 8, 1), (8, 2, 2), (4, 2, 4), (2, 2, 8)]
+SAMPLES_PER_CELL = [1.0, 2.0, 4.0]
+SEARCH_WARPS = [0, 2, 8]
+SOLVE_BLOCKS = [0, 2, 3]
+
+
+def cache_path():
+    return os.environ.get("BTK_TUNING_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "boitata_b200",
+                                                           "tuning.json"))
+
+
+def get_tuning(ctx):
+    t = N.TuningC()
+    ctx.check(ctx._lib.btk_get_tuning(ctx.handle, ctypes.byref(t)), "tuning")
+    return {"samples_per_cell": t.samples_per_cell, "tile": tuple(t.tile), "search_warps": t.search_warps,
+            "solve_blocks_per_sm": t.solve_blocks_per_sm}
+
+
+def set_tuning(ctx, cfg):
+    t = N.TuningC()
+    t.samples_per_cell = float(cfg["samples_per_cell"])
+    for a in range(3):
+        t.tile[a] = int(cfg["tile"][a])
+    t.search_warps = int(cfg["search_warps"])
+    t.solve_blocks_per_sm = int(cfg["solve_blocks_per_sm"])
+    ctx.check(ctx._lib.btk_set_tuning(ctx.handle, ctypes.byref(t)), "tuning")
+
+
+def signature(estimator, geometry, precision):
+    s = estimator.searches[0]
+    return json.dumps({"n": int(len(estimator._samples[0])), "max": s.max_samples, "octant": s.octant,
+                       "radius": s.radius, "anisotropy": s.anisotropy or estimator.variogram.anisotropy,
+                       "models": [x.model for x in estimator.variogram.structures], "count": geometry.count,
+                       "precision": precision}, sort_keys=True, default=str)
+
+
+def time_geometry(estimator, geometry, precision, steps=2):
+    """Median search + solve kernel time (ms) of one prediction over `geometry`."""
+    import torch
+
+    ctx = estimator._ctx
+    m = geometry.cells()
+    dev = torch.device("cuda", estimator._device)
+    outs = [torch.empty(m, dtype=torch.float64, device=dev) for _ in range(3)]
+    outs += [torch.empty(m, dtype=torch.int32, device=dev), torch.empty(m, dtype=torch.int8, device=dev)]
+    oc = N.OutputsC(*(t.data_ptr() for t in outs))
+    g = geometry.to_c()
+    prec = {"fp64": N.FP64, "mixed": N.MIXED}[precision]
+    ctx.check(ctx._lib.btk_set_timing(ctx.handle, 1), "timing")
+    times = []
+    try:
+        for i in range(steps + 1):
+            ctx.check(ctx._lib.btk_predict_geometry_device(ctx.handle, ctypes.byref(g), estimator._kind,
+                                                           estimator._kparam, prec, ctypes.byref(oc), None),
+                      "predict")
+            p = (ctypes.c_float * 3)()
+            ctx.check(ctx._lib.btk_phase_ms(ctx.handle, p), "timing")
+            if i > 0:
+                times.append(sum(p))
+    finally:
+        ctx._lib.btk_set_timing(ctx.handle, 0)
+    return float(np.median(times))
+
+
+def autotune_geometry(estimator, geometry, *, precision="mixed", steps=2, use_cache=True):
+    """Picks and applies the fastest tuning for kriging `geometry` with `estimator` (fitted, first pass).
+    Returns {"best": config, "ms": time, "table": [(config, ms), ...], "cached": bool}."""
+    estimator._fitted()
+    estimator._use_pass(0)
+    ctx = estimator._ctx
+    key = signature(estimator, geometry, precision)
+    path = cache_path()
+    cache = {}
+    if use_cache and os.path.exists(path):
+        try:
+            with open(path) as f:
+                cache = json.load(f)
+        except (OSError, ValueError):
+            cache = {}
+    if use_cache and key in cache:
+        cfg = cache[key]["best"]
+        cfg["tile"] = tuple(cfg["tile"])
+        set_tuning(ctx, cfg)
+        return {"best": cfg, "ms": cache[key]["ms"], "table": [], "cached": True}
+    base = get_tuning(ctx)
+    table = []
+    best, best_ms = dict(base), float("inf")
+    for ppc in SAMPLES_PER_CELL:
+        for tile in TILES:
+            cfg = dict(base, samples_per_cell=ppc, tile=tile)
+            set_tuning(ctx, cfg)
+            ms = time_geometry(estimator, geometry, precision, steps)
+            table.append((dict(cfg), ms))
+            if ms < best_ms:
+                best, best_ms = dict(cfg), ms
+    stage1 = dict(best)
+    for sw in SEARCH_WARPS:
+        for sb in SOLVE_BLOCKS:
+            cfg = dict(stage1, search_warps=sw, solve_blocks_per_sm=sb)
+            if cfg == stage1:
+                continue
+            set_tuning(ctx, cfg)
+            ms = time_geometry(estimator, geometry, precision, steps)
+            table.append((dict(cfg), ms))
+            if ms < best_ms:
+                best, best_ms = dict(cfg), ms
+    set_tuning(ctx, best)
+    if use_cache:
+        cache[key] = {"best": {**best, "tile": list(best["tile"])}, "ms": best_ms}
+        try:
+            os.makedirs(os.path.dirname(path), exist_ok=True)
+            with open(path, "w") as f:
+                json.dump(cache, f, indent=1)
+        except OSError:
+            pass
+    return {"best": best, "ms": best_ms, "table": table, "cached": False}

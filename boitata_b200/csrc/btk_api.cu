@@ -91,6 +91,15 @@ void put9(const M3& m, double* out) {
   for (int i = 0; i < 9; ++i) out[i] = m.m[i / 3][i % 3];
 }
 
+// block_frame(rotation)^T of a geometry (crates/core/src/block_model.rs:84).
+btk::Frame9 transposed_frame(const btk_geometry& g) {
+  M3 f = block_frame(g.rotation[0], g.rotation[1], g.rotation[2]);
+  btk::Frame9 out;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) out.m[3 * i + j] = f.m[j][i];
+  return out;
+}
+
 }  // namespace
 
 struct btk_ctx {
@@ -117,7 +126,7 @@ struct btk_ctx {
   DevBuf<int64_t> loo_perm;
 
   // per-call scratch, grown on demand
-  DevBuf<double> txyz, aos, ft9;
+  DevBuf<double> txyz, aos;
   DevBuf<int64_t> perm, lists, lens, redo, redo_len;
   DevBuf<uint32_t> nbr;
   DevBuf<int32_t> cnt, o_nused;
@@ -134,7 +143,12 @@ struct btk_ctx {
   DevBuf<int8_t> loo_sst;
   DevBuf<double> g_part, g_sums, g_val;
 
-  Launch launch(cudaStream_t s) { return Launch{s ? s : stream, sm_count, &launches}; }
+  Tuning tuning;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  int64_t graph_kernels = 0;
+
+  Launch launch(cudaStream_t s) { return Launch{s ? s : stream, sm_count, &launches, tuning}; }
   void mark(int k, cudaStream_t s) {
     if (timing) cudaEventRecord(ev[k], s);
   }
@@ -537,7 +551,90 @@ void btk_destroy(btk_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream), cudaStreamDestroy(ctx->stream);
   for (cudaEvent_t e : ctx->ev)
     if (e) cudaEventDestroy(e);
+  if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+  if (ctx->graph) cudaGraphDestroy(ctx->graph);
   delete ctx;
+}
+
+int btk_get_tuning(const btk_ctx* ctx, btk_tuning* out) {
+  if (!ctx || !out) return BTK_EINVAL;
+  out->samples_per_cell = ctx->ppc;
+  for (int a = 0; a < 3; ++a) out->tile[a] = ctx->tuning.tile[a];
+  out->search_warps = ctx->tuning.search_warps;
+  out->solve_blocks_per_sm = ctx->tuning.solve_blocks_per_sm;
+  return BTK_OK;
+}
+
+int btk_set_tuning(btk_ctx* ctx, const btk_tuning* t) {
+  if (!ctx || !t) return BTK_EINVAL;
+  const int prod = t->tile[0] * t->tile[1] * t->tile[2];
+  if (t->tile[0] < 1 || t->tile[1] < 1 || t->tile[2] < 1 || prod != 32)
+    return fail(ctx, BTK_EINVAL, "the tile must hold 32 cells");
+  if (!(t->search_warps == 0 || t->search_warps == 1 || t->search_warps == 2 || t->search_warps == 4 ||
+        t->search_warps == 8))
+    return fail(ctx, BTK_EINVAL, "search_warps must be 0, 1, 2, 4 or 8");
+  if (t->solve_blocks_per_sm < 0) return fail(ctx, BTK_EINVAL, "solve_blocks_per_sm must be >= 0");
+  if (!(t->samples_per_cell > 0.0 && t->samples_per_cell <= 1e6))
+    return fail(ctx, BTK_EINVAL, "samples_per_cell must be > 0");
+  for (int a = 0; a < 3; ++a) ctx->tuning.tile[a] = t->tile[a];
+  ctx->tuning.search_warps = t->search_warps;
+  ctx->tuning.solve_blocks_per_sm = t->solve_blocks_per_sm;
+  if (t->samples_per_cell != ctx->ppc) {
+    ctx->ppc = t->samples_per_cell;
+    if (ctx->fitted) {
+      CK(cudaSetDevice(ctx->device));
+      ctx->frozen = false;
+      int rc = index_samples(ctx);
+      if (rc) return rc;
+      CK(cudaStreamSynchronize(ctx->stream));
+    }
+  }
+  return BTK_OK;
+}
+
+int btk_graph_capture_geometry(btk_ctx* ctx, const btk_geometry* g, int32_t kind, double kparam,
+                               int32_t precision, const btk_outputs* d_out) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  // One plain call sizes every buffer and sets every kernel attribute first.
+  if ((rc = btk_predict_geometry_device(ctx, g, kind, kparam, precision, d_out, ctx->stream))) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->graph_exec) {
+    CK(cudaGraphExecDestroy(ctx->graph_exec));
+    ctx->graph_exec = nullptr;
+  }
+  if (ctx->graph) {
+    CK(cudaGraphDestroy(ctx->graph));
+    ctx->graph = nullptr;
+  }
+  const bool timing = ctx->timing;
+  ctx->timing = false;
+  const int64_t before = ctx->launches;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+  rc = btk_predict_geometry_device(ctx, g, kind, kparam, precision, d_out, ctx->stream);
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+  ctx->timing = timing;
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  CK(e);
+  ctx->graph = graph;
+  ctx->graph_kernels = ctx->launches - before;
+  ctx->launches = before;
+  CK(cudaGraphInstantiate(&ctx->graph_exec, graph, 0));
+  return BTK_OK;
+}
+
+int btk_graph_launch(btk_ctx* ctx, void* stream) {
+  if (!ctx) return BTK_EINVAL;
+  if (!ctx->graph_exec) return fail(ctx, BTK_EINVAL, "no captured graph; call btk_graph_capture_geometry first");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaGraphLaunch(ctx->graph_exec, stream ? static_cast<cudaStream_t>(stream) : ctx->stream));
+  ctx->launches += ctx->graph_kernels;
+  return BTK_OK;
 }
 
 int btk_set_timing(btk_ctx* ctx, int32_t on) {
@@ -693,19 +790,15 @@ int btk_predict_geometry_device(btk_ctx* ctx, const btk_geometry* g, int32_t kin
   }
   CK(cudaSetDevice(ctx->device));
   const int64_t m = g->count[0] * g->count[1] * g->count[2];
-  const int64_t tiles = ((g->count[0] + 3) / 4) * ((g->count[1] + 3) / 4) * ((g->count[2] + 1) / 2);
+  const int* tw = ctx->tuning.tile;
+  const int64_t tiles = ((g->count[0] + tw[0] - 1) / tw[0]) * ((g->count[1] + tw[1] - 1) / tw[1]) *
+                        ((g->count[2] + tw[2] - 1) / tw[2]);
   const int64_t nwork = tiles * 32;
   CK(ctx->txyz.grow(3 * size_t(m)));
   CK(ctx->perm.grow(size_t(nwork)));
-  CK(ctx->ft9.grow(9));
-  M3 f = block_frame(g->rotation[0], g->rotation[1], g->rotation[2]);
-  double ft[9];
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) ft[3 * i + j] = f.m[j][i];
   Launch L = ctx->launch(static_cast<cudaStream_t>(stream));
-  CK(cudaMemcpyAsync(ctx->ft9.p, ft, sizeof ft, cudaMemcpyHostToDevice, L.stream));
   double* t = ctx->txyz.p;
-  CK(launch_centroids(L, *g, ctx->ft9.p, 0, nwork, t, t + m, t + 2 * m, ctx->perm.p));
+  CK(launch_centroids(L, *g, transposed_frame(*g), 0, nwork, t, t + m, t + 2 * m, ctx->perm.p));
   return run_path(ctx, L.stream, m, t, t + m, t + 2 * m, ctx->perm.p, nwork, 0, kind, kparam, precision, d_out);
 }
 
@@ -822,16 +915,10 @@ int btk_centroids(btk_ctx* ctx, const btk_geometry* g, int64_t first, int64_t m,
   if (!ctx || !g || m < 0) return fail(ctx, BTK_EINVAL, "geometry and a non-negative count are required");
   if (m == 0) return BTK_OK;
   CK(cudaSetDevice(ctx->device));
-  M3 f = block_frame(g->rotation[0], g->rotation[1], g->rotation[2]);
-  double ft[9];
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) ft[3 * i + j] = f.m[j][i];
-  CK(ctx->ft9.grow(9));
   CK(ctx->txyz.grow(3 * size_t(m)));
   Launch L = ctx->launch(nullptr);
-  CK(cudaMemcpyAsync(ctx->ft9.p, ft, sizeof ft, cudaMemcpyHostToDevice, L.stream));
   double* t = ctx->txyz.p;
-  CK(launch_centroids(L, *g, ctx->ft9.p, first, m, t, t + m, t + 2 * m, nullptr));
+  CK(launch_centroids(L, *g, transposed_frame(*g), first, m, t, t + m, t + 2 * m, nullptr));
   std::vector<double> a(3 * size_t(m));
   CK(cudaMemcpyAsync(a.data(), t, a.size() * sizeof(double), cudaMemcpyDeviceToHost, L.stream));
   CK(cudaStreamSynchronize(L.stream));

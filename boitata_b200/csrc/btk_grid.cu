@@ -143,21 +143,21 @@ __global__ void k_twins(int64_t n, GridDev g, int reach, const double* x, const 
 
 // Centroids of block-model cells (crates/core/src/block_model.rs:76-86):
 // origin + block_frame^T * ((ijk + 0.5) * size), exact order. With
-// `perm_tiles` the work items are 4 x 4 x 2 tiles of cells (32 per tile, one
-// per search lane) and perm_tiles[k] is the cell of work item k, or -1.
-__global__ void k_centroids(btk_geometry geo, const double* __restrict__ ft, int64_t first, int64_t m, double* tx,
-                            double* ty, double* tz, int64_t* perm_tiles) {
+// `perm_tiles` the work items are tiles of tw[0] x tw[1] x tw[2] = 32 cells
+// (one per search lane) and perm_tiles[k] is the cell of work item k, or -1.
+__global__ void k_centroids(btk_geometry geo, Frame9 ft, int tx0, int ty0, int tz0, int64_t first, int64_t m,
+                            double* tx, double* ty, double* tz, int64_t* perm_tiles) {
   double F[9];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) F[k] = ft[k];
+  for (int k = 0; k < 9; ++k) F[k] = ft.m[k];
   const int64_t nx = geo.count[0], ny = geo.count[1], nz = geo.count[2];
-  const int64_t tx_n = (nx + 3) / 4, ty_n = (ny + 3) / 4;
+  const int64_t tx_n = (nx + tx0 - 1) / tx0, ty_n = (ny + ty0 - 1) / ty0;
   for (int64_t k = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; k < m; k += int64_t(gridDim.x) * blockDim.x) {
     int64_t i, j, l, cell;
     if (perm_tiles) {
       int64_t tile = k >> 5, lane = k & 31;
       int64_t a = tile % tx_n, b = tile / tx_n % ty_n, c = tile / (tx_n * ty_n);
-      i = 4 * a + (lane & 3), j = 4 * b + ((lane >> 2) & 3), l = 2 * c + (lane >> 4);
+      i = tx0 * a + lane % tx0, j = ty0 * b + lane / tx0 % ty0, l = tz0 * c + lane / (tx0 * ty0);
       if (i >= nx || j >= ny || l >= nz) {
         perm_tiles[k] = -1;
         continue;
@@ -228,9 +228,11 @@ cudaError_t launch_twins(const Launch& L, int64_t n, GridDev g, int reach, const
   return cudaGetLastError();
 }
 
-cudaError_t launch_centroids(const Launch& L, btk_geometry g, const double* frame_t, int64_t first, int64_t m,
+cudaError_t launch_centroids(const Launch& L, btk_geometry g, Frame9 frame_t, int64_t first, int64_t m,
                              double* tx, double* ty, double* tz, int64_t* perm_tiles) {
-  k_centroids<<<grid_blocks(L, m, 256), 256, 0, L.stream>>>(g, frame_t, first, m, tx, ty, tz, perm_tiles);
+  const int* t = L.tuning.tile;
+  k_centroids<<<grid_blocks(L, m, 256), 256, 0, L.stream>>>(g, frame_t, t[0], t[1], t[2], first, m, tx, ty, tz,
+                                                            perm_tiles);
   ++*L.counter;
   return cudaGetLastError();
 }

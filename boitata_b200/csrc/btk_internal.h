@@ -95,10 +95,22 @@ struct GradDev {
 };
 
 // ---- launchers (each returns the launch's error, if any) ----
+// Tunables the autotuner picks (btk_tuning).
+struct Tuning {
+  int tile[3] = {4, 4, 2};       // block-model tile of one search warp (product 32)
+  int search_warps = 0;          // warps per search CTA; 0: 4 (2 with 64 list slots)
+  int solve_blocks_per_sm = 0;   // resident solve CTAs per SM; 0: as many as fit
+};
+
 struct Launch {
   cudaStream_t stream;
   int sm_count;
   int64_t* counter;  // launches issued, for btk_launch_count
+  Tuning tuning;
+};
+
+struct Frame9 {
+  double m[9];
 };
 
 cudaError_t launch_project(const Launch& L, int64_t n, const double* x, const double* y, const double* z,
@@ -111,7 +123,7 @@ cudaError_t launch_grid_build(const Launch& L, int64_t n, const double* x, const
                               double* swx, double* swy, double* swz, uint32_t* sidx);
 cudaError_t launch_twins(const Launch& L, int64_t n, GridDev g, int reach, const double* x, const double* y,
                          const double* z, uint8_t* twin);
-cudaError_t launch_centroids(const Launch& L, btk_geometry g, const double* frame_t, int64_t first, int64_t m,
+cudaError_t launch_centroids(const Launch& L, btk_geometry g, Frame9 frame_t, int64_t first, int64_t m,
                              double* tx, double* ty, double* tz, int64_t* perm_tiles);
 cudaError_t launch_search(const Launch& L, const SearchDev& sp, const GridDev& g, const double* tx,
                           const double* ty, const double* tz, const int64_t* perm, int64_t m, int loo,

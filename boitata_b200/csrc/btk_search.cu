@@ -375,7 +375,7 @@ template <int SLOTS, bool OCT>
 cudaError_t run(const Launch& L, const SearchDev& sp, const GridDev& g, const double* tx, const double* ty,
                 const double* tz, const int64_t* perm, int64_t m, int loo, uint32_t* nbr, int32_t* count,
                 int8_t* status) {
-  constexpr int kWarps = SLOTS > 32 ? 2 : 4;
+  const int kWarps = L.tuning.search_warps > 0 ? L.tuning.search_warps : (SLOTS > 32 ? 2 : 4);
   const size_t smem = sizeof(WarpSmem<SLOTS, OCT>) * kWarps;
   auto kern = k_search<SLOTS, OCT>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));

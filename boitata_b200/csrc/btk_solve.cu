@@ -475,6 +475,7 @@ template <class K>
 int blocks_for(const Launch& L, K kern, size_t smem) {
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+  if (L.tuning.solve_blocks_per_sm > 0 && L.tuning.solve_blocks_per_sm < per_sm) per_sm = L.tuning.solve_blocks_per_sm;
   return L.sm_count * per_sm;
 }
 

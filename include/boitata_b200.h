@@ -121,6 +121,16 @@ typedef struct {
   int8_t* status;
 } btk_outputs;
 
+/* Launch tunables (no counterpart in the reference): grid cell size in
+ * samples per cell, the block-model tile one search warp serves (product
+ * 32), warps per search CTA and resident solve CTAs per SM (0: defaults). */
+typedef struct {
+  double samples_per_cell;
+  int32_t tile[3];
+  int32_t search_warps;
+  int32_t solve_blocks_per_sm;
+} btk_tuning;
+
 typedef struct btk_ctx btk_ctx;
 
 const char* btk_version(void);
@@ -204,6 +214,19 @@ int btk_loo_gradient(btk_ctx* ctx, const btk_variogram* vg, int32_t want_grad, d
 
 /* Kernel launches issued by this context since it was created. */
 int64_t btk_launch_count(const btk_ctx* ctx);
+
+/* Tunables of this context; setting samples_per_cell re-indexes the fitted
+ * samples. boitata_b200/autotune.py picks them by timing candidates. */
+int btk_get_tuning(const btk_ctx* ctx, btk_tuning* out);
+int btk_set_tuning(btk_ctx* ctx, const btk_tuning* tuning);
+
+/* Captures btk_predict_geometry_device(g, ...) (centroids, search,
+ * bucketing, solves, FP64 re-solves) into one CUDA graph held by the context;
+ * btk_graph_launch replays it on `stream` (NULL: the context's stream),
+ * writing the same d_out. No counterpart in the reference. */
+int btk_graph_capture_geometry(btk_ctx* ctx, const btk_geometry* g, int32_t kind, double kparam,
+                               int32_t precision, const btk_outputs* d_out);
+int btk_graph_launch(btk_ctx* ctx, void* stream);
 
 /* Diagnostics with no counterpart in the reference. btk_set_timing records
  * CUDA events around the phases of every prediction on this context;
