@@ -4,11 +4,12 @@ The tunables (btk_tuning in include/boitata_b200.h):
 - samples per grid cell (the cell size of the search grid);
 - the block-model tile one search warp serves (32 cells);
 - warps per search CTA (shared-memory granularity);
-- resident solve CTAs per SM.
+- resident solve CTAs per SM;
+- the table size of the tile-shared solve (0: per-system assembly).
 
 They are picked by timing the real workload. The time is the sum of the search and solve kernels, taken
-with CUDA events on the launch stream. Two stages run: cell size x tile first, then the CTA shapes at the
-best of those. The choice is cached per workload signature in a JSON file (BTK_TUNING_CACHE, or
+with CUDA events on the launch stream. Three stages run, each at the best of the one before: cell size x
+tile, then search CTA warps, then table size x solve CTAs per SM. The choice is cached per workload signature in a JSON file (BTK_TUNING_CACHE, or
 ~/.cache/boitata_b200/tuning.json) and applied to the context.
 """
 
@@ -24,6 +25,7 @@ TILES = [(4, 4, 2), (8, 4, 1), (2, 4, 4), (4, 8, 1), (8, 2, 2), (4, 2, 4), (2, 2
 SAMPLES_PER_CELL = [1.0, 2.0, 4.0]
 SEARCH_WARPS = [0, 2, 8]
 SOLVE_BLOCKS = [0, 2, 3]
+TILE_UNION = [0, 64, 72, 96]
 
 
 def cache_path():
@@ -35,7 +37,7 @@ def get_tuning(ctx):
     t = N.TuningC()
     ctx.check(ctx._lib.btk_get_tuning(ctx.handle, ctypes.byref(t)), "tuning")
     return {"samples_per_cell": t.samples_per_cell, "tile": tuple(t.tile), "search_warps": t.search_warps,
-            "solve_blocks_per_sm": t.solve_blocks_per_sm}
+            "solve_blocks_per_sm": t.solve_blocks_per_sm, "tile_union": t.tile_union}
 
 
 def set_tuning(ctx, cfg):
@@ -45,6 +47,7 @@ def set_tuning(ctx, cfg):
         t.tile[a] = int(cfg["tile"][a])
     t.search_warps = int(cfg["search_warps"])
     t.solve_blocks_per_sm = int(cfg["solve_blocks_per_sm"])
+    t.tile_union = int(cfg.get("tile_union", 72))
     ctx.check(ctx._lib.btk_set_tuning(ctx.handle, ctypes.byref(t)), "tuning")
 
 
@@ -117,9 +120,19 @@ def autotune_geometry(estimator, geometry, *, precision="mixed", steps=2, use_ca
                 best, best_ms = dict(cfg), ms
     stage1 = dict(best)
     for sw in SEARCH_WARPS:
+        cfg = dict(stage1, search_warps=sw)
+        if cfg == stage1:
+            continue
+        set_tuning(ctx, cfg)
+        ms = time_geometry(estimator, geometry, precision, steps)
+        table.append((dict(cfg), ms))
+        if ms < best_ms:
+            best, best_ms = dict(cfg), ms
+    stage2 = dict(best)
+    for tu in TILE_UNION:
         for sb in SOLVE_BLOCKS:
-            cfg = dict(stage1, search_warps=sw, solve_blocks_per_sm=sb)
-            if cfg == stage1:
+            cfg = dict(stage2, tile_union=tu, solve_blocks_per_sm=sb)
+            if cfg == stage2:
                 continue
             set_tuning(ctx, cfg)
             ms = time_geometry(estimator, geometry, precision, steps)

@@ -380,12 +380,27 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
   a.m = m;
   a.value = o->value, a.variance = o->variance, a.lagrange = o->lagrange, a.n_used = o->n_used, a.status = o->status;
   const bool two = ctx->search.max_samples > 32;
+  const bool tiled = ctx->tuning.tile_union > 0;
   const int nb = two ? 2 : 1;
-  if (two) CK(launch_bucket(L, m, ctx->cnt.p, ctx->sst.p, ctx->lists.p, ctx->lens.p));
   if (precision == BTK_MIXED) CK(cudaMemsetAsync(ctx->redo_len.p, 0, 2 * sizeof(int64_t), L.stream));
+  if (tiled) {
+    // Tile-shared solve of the n <= 32 systems; the rest go to the lists.
+    CK(cudaMemsetAsync(ctx->lens.p, 0, 2 * sizeof(int64_t), L.stream));
+    TileDev td{};
+    td.s = a;
+    td.perm = perm;
+    td.nwork = nwork;
+    td.umax = ctx->tuning.tile_union;
+    td.small = ctx->lists.p, td.small_len = ctx->lens.p;
+    td.large = ctx->lists.p + m, td.large_len = ctx->lens.p + 1;
+    td.redo = ctx->redo.p, td.redo_len = ctx->redo_len.p;
+    CK(launch_tile(L, td, precision == BTK_MIXED));
+  } else if (two) {
+    CK(launch_bucket(L, m, ctx->cnt.p, ctx->sst.p, ctx->lists.p, ctx->lens.p));
+  }
   for (int b = 0; b < nb; ++b) {
     SolveDev ab = a;
-    if (two) ab.list = ctx->lists.p + b * m, ab.list_len = ctx->lens.p + b;
+    if (two || tiled) ab.list = ctx->lists.p + b * m, ab.list_len = ctx->lens.p + b;
     const int rows = b == 0 ? 32 : 64;
     if (precision == BTK_FP64)
       CK(launch_solve(L, ab, rows));
@@ -562,6 +577,7 @@ int btk_get_tuning(const btk_ctx* ctx, btk_tuning* out) {
   for (int a = 0; a < 3; ++a) out->tile[a] = ctx->tuning.tile[a];
   out->search_warps = ctx->tuning.search_warps;
   out->solve_blocks_per_sm = ctx->tuning.solve_blocks_per_sm;
+  out->tile_union = ctx->tuning.tile_union;
   return BTK_OK;
 }
 
@@ -574,11 +590,14 @@ int btk_set_tuning(btk_ctx* ctx, const btk_tuning* t) {
         t->search_warps == 8))
     return fail(ctx, BTK_EINVAL, "search_warps must be 0, 1, 2, 4 or 8");
   if (t->solve_blocks_per_sm < 0) return fail(ctx, BTK_EINVAL, "solve_blocks_per_sm must be >= 0");
+  if (t->tile_union != 0 && (t->tile_union < 32 || t->tile_union > 255))
+    return fail(ctx, BTK_EINVAL, "tile_union must be 0 or in 32..255");
   if (!(t->samples_per_cell > 0.0 && t->samples_per_cell <= 1e6))
     return fail(ctx, BTK_EINVAL, "samples_per_cell must be > 0");
   for (int a = 0; a < 3; ++a) ctx->tuning.tile[a] = t->tile[a];
   ctx->tuning.search_warps = t->search_warps;
   ctx->tuning.solve_blocks_per_sm = t->solve_blocks_per_sm;
+  ctx->tuning.tile_union = t->tile_union;
   if (t->samples_per_cell != ctx->ppc) {
     ctx->ppc = t->samples_per_cell;
     if (ctx->fitted) {

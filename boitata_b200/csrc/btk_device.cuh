@@ -157,4 +157,77 @@ __device__ __forceinline__ float shape32(int model, float param, float t) {
   return 0.f;
 }
 
+// ---- shared by the solve kernels (btk_solve.cu, btk_tile.cu) ----
+// Lag |M (b - a)| between world points a and b, M the variogram frame
+// (identity without anisotropy): the difference is taken in world
+// coordinates, then rotated, with a fixed operation order, so the value
+// depends on the pair alone (and is symmetric bit for bit) whichever kernel
+// or tile evaluates it (kernel.rs:34-42 projects the same differences).
+__device__ __forceinline__ double lag_world(const VgDev& vg, double ax, double ay, double az, double bx, double by,
+                                            double bz) {
+  double d0 = bx - ax, d1 = by - ay, d2 = bz - az;
+  if (vg.has_frame) {
+    const double* M = vg.frame;
+    const double r0 = fma(M[2], d2, fma(M[1], d1, M[0] * d0));
+    const double r1 = fma(M[5], d2, fma(M[4], d1, M[3] * d0));
+    const double r2 = fma(M[8], d2, fma(M[7], d1, M[6] * d0));
+    d0 = r0, d1 = r1, d2 = r2;
+  }
+  return sqrt(fma(d2, d2, fma(d1, d1, d0 * d0)));
+}
+
+__device__ __forceinline__ double kind_f(int kind, double kparam, double z) {
+  return kind == BTK_SIMPLE ? z - kparam : (kind == BTK_INDICATOR ? (z <= kparam ? 1.0 : 0.0) : z);
+}
+
+__device__ __forceinline__ double lag64(const VgDev& vg, const double* a, const double* b) {
+  double d[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+  if (vg.has_frame) {
+    double r[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) r[k] = vg.frame[3 * k] * d[0] + vg.frame[3 * k + 1] * d[1] + vg.frame[3 * k + 2] * d[2];
+    d[0] = r[0], d[1] = r[1], d[2] = r[2];
+  }
+  return sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+}
+
+__device__ __forceinline__ void tri_index(int e, int& i, int& j) {
+  int r = int((1.0f + sqrtf(8.0f * float(e) + 1.0f)) * 0.5f);
+  while (r * (r - 1) / 2 > e) --r;
+  while ((r + 1) * r / 2 <= e) ++r;
+  i = r, j = e - r * (r - 1) / 2;
+}
+
+__device__ __forceinline__ void write_fail(const SolveDev& a, int64_t ti, int8_t st, int n_used) {
+  a.value[ti] = NAN;
+  if (a.variance) a.variance[ti] = NAN;
+  if (a.lagrange) a.lagrange[ti] = NAN;
+  if (a.n_used) a.n_used[ti] = n_used;
+  if (a.status) a.status[ti] = st;
+}
+
+// Estimate, variance and Lagrange multiplier from the five forms
+// s[0] = 1'C^-1 c, s[1] = 1'C^-1 1, s[2] = f'C^-1 c, s[3] = f'C^-1 1,
+// s[4] = c'C^-1 c (kernel.rs:86-122).
+__device__ __forceinline__ void epilogue(const SolveDev& a, int kind, int64_t ti, const double s[5], int n_used,
+                                         int8_t flag) {
+  const double c0 = a.vg.c0;
+  double mu, value, swc;
+  if (kind == BTK_SIMPLE) {
+    mu = 0.0;
+    value = a.kparam + s[2];
+    swc = s[4];
+  } else {
+    mu = (s[0] - 1.0) / s[1];
+    value = s[2] - mu * s[3];
+    if (kind == BTK_INDICATOR) value = value < 0.0 ? 0.0 : (value > 1.0 ? 1.0 : value);
+    swc = s[4] - mu * s[0];
+  }
+  a.value[ti] = value;
+  if (a.variance) a.variance[ti] = fmax(c0 - swc - mu, 0.0);
+  if (a.lagrange) a.lagrange[ti] = mu;
+  if (a.n_used) a.n_used[ti] = n_used;
+  if (a.status) a.status[ti] = int8_t(BTK_ST_OK | flag);
+}
+
 }  // namespace btk

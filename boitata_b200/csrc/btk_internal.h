@@ -77,6 +77,20 @@ struct SolveDev {
   int8_t* status;
 };
 
+// Tile-shared solve (btk_tile.cu): the systems of kTileTargets consecutive
+// work slots share one covariance table over the union of their samples.
+constexpr int kTileTargets = 16;
+struct TileDev {
+  SolveDev s;           // system inputs and outputs (s.list unused)
+  const int64_t* perm;  // work slot -> target index, -1 for padding; null: identity
+  int64_t nwork;
+  int umax;             // most distinct samples a tile's table holds
+  int stride;           // row stride of the table, in doubles
+  int64_t *small, *small_len;  // n <= 32 systems left to the per-system kernels
+  int64_t *large, *large_len;  // n > 32
+  int64_t *redo, *redo_len;    // mixed form: systems left to the FP64 re-solve
+};
+
 // Leave-one-out loss and gradient over frozen neighbourhoods (btk_adjoint.cu).
 struct GradDev {
   VgDev vg;         // the variogram at theta; vg.frame = M(theta), always set
@@ -100,6 +114,7 @@ struct Tuning {
   int tile[3] = {4, 4, 2};       // block-model tile of one search warp (product 32)
   int search_warps = 0;          // warps per search CTA; 0: 4 (2 with 64 list slots)
   int solve_blocks_per_sm = 0;   // resident solve CTAs per SM; 0: as many as fit
+  int tile_union = 72;           // tile-shared solve: most distinct samples per tile; 0: per-system solve
 };
 
 struct Launch {
@@ -141,6 +156,11 @@ cudaError_t launch_solve_redo(const Launch& L, const SolveDev& a, int rows);
 // system's own sample pairs for coincidence instead of reading a.twin.
 cudaError_t launch_solve_mixed_pairs(const Launch& L, const SolveDev& a, int64_t* redo, int64_t* redo_len);
 cudaError_t launch_solve_redo_pairs(const Launch& L, const SolveDev& a);
+
+// Tile-shared solve of every work slot's system with n <= 32 (mixed: FP32
+// factor with FP64 refinement, else FP64); the others go to a.small / a.large
+// (and, mixed, a.redo) for the per-system kernels. Counts must start at 0.
+cudaError_t launch_tile(const Launch& L, const TileDev& a, bool mixed);
 
 // Leave-one-out loss and gradient; sums[stride] receives the column sums.
 cudaError_t launch_loo_grad(const Launch& L, const GradDev& a, double* sums);

@@ -118,21 +118,6 @@ __device__ __forceinline__ double group_max(SolveSmem<NW>& S, int gid, int wig, 
   return m;
 }
 
-__device__ __forceinline__ double kind_f(int kind, double kparam, double z) {
-  return kind == BTK_SIMPLE ? z - kparam : (kind == BTK_INDICATOR ? (z <= kparam ? 1.0 : 0.0) : z);
-}
-
-__device__ __forceinline__ double lag64(const VgDev& vg, const double* a, const double* b) {
-  double d[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
-  if (vg.has_frame) {
-    double r[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) r[k] = vg.frame[3 * k] * d[0] + vg.frame[3 * k + 1] * d[1] + vg.frame[3 * k + 2] * d[2];
-    d[0] = r[0], d[1] = r[1], d[2] = r[2];
-  }
-  return sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-}
-
 // Coincident guard on one lane (coincident.rs:27-82): samples within 1e-6 m
 // of a cluster's first member join it; each cluster becomes one datum at the
 // first member with the mean of f(z) (the value the spread weights give,
@@ -178,21 +163,6 @@ __device__ void merge_clusters(SolveSmem<NW>& S, int n, const VgDev& vg, int* nn
     S.me[c] = err, S.mz[c] = zb;
   }
   *nn_out = nc;
-}
-
-__device__ __forceinline__ void tri_index(int e, int& i, int& j) {
-  int r = int((1.0f + sqrtf(8.0f * float(e) + 1.0f)) * 0.5f);
-  while (r * (r - 1) / 2 > e) --r;
-  while ((r + 1) * r / 2 <= e) ++r;
-  i = r, j = e - r * (r - 1) / 2;
-}
-
-__device__ __forceinline__ void write_fail(const SolveDev& a, int64_t ti, int8_t st, int n_used) {
-  a.value[ti] = NAN;
-  if (a.variance) a.variance[ti] = NAN;
-  if (a.lagrange) a.lagrange[ti] = NAN;
-  if (a.n_used) a.n_used[ti] = n_used;
-  if (a.status) a.status[ti] = st;
 }
 
 // Everything up to the packed covariance triangle: loads the system of
@@ -248,51 +218,18 @@ __device__ __forceinline__ bool assemble(const SolveDev& a, SolveSmem<NW>& S, in
     if (have) w[0] = S.P[row][0], w[1] = S.P[row][1], w[2] = S.P[row][2], err = S.me[row], zf = S.mz[row];
     gsync<NW>(gid);
   }
-  // Samples relative to the target, in the variogram's frame (kernel.rs:34-42).
-  double p[3] = {w[0] - t[0], w[1] - t[1], w[2] - t[2]};
-  if (a.vg.has_frame) {
-    const double* M = a.vg.frame;
-    double r[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) r[k] = M[3 * k] * p[0] + M[3 * k + 1] * p[1] + M[3 * k + 2] * p[2];
-    p[0] = r[0], p[1] = r[1], p[2] = r[2];
-  }
-  if (have) S.P[row][0] = p[0], S.P[row][1] = p[1], S.P[row][2] = p[2];
+  // World coordinates; every lag is taken by lag_world (kernel.rs:34-42).
+  if (have) S.P[row][0] = w[0], S.P[row][1] = w[1], S.P[row][2] = w[2];
   gsync<NW>(gid);
   const int E = nn * (nn - 1) / 2;
   for (int e = row; e < E; e += R) {
     int i, j;
     tri_index(e, i, j);
-    const double dx = S.P[i][0] - S.P[j][0], dy = S.P[i][1] - S.P[j][1], dz = S.P[i][2] - S.P[j][2];
-    S.T[e] = cov64(a.vg, sqrt(dx * dx + dy * dy + dz * dz));
+    S.T[e] = cov64(a.vg, lag_world(a.vg, S.P[j][0], S.P[j][1], S.P[j][2], S.P[i][0], S.P[i][1], S.P[i][2]));
   }
-  c = have ? cov64(a.vg, sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2])) : 0.0;
+  c = have ? cov64(a.vg, lag_world(a.vg, t[0], t[1], t[2], w[0], w[1], w[2])) : 0.0;
   gsync<NW>(gid);
   return true;
-}
-
-// Estimate, variance and Lagrange multiplier from the five forms
-// s[0] = 1'C^-1 c, s[1] = 1'C^-1 1, s[2] = f'C^-1 c, s[3] = f'C^-1 1,
-// s[4] = c'C^-1 c (kernel.rs:86-122).
-__device__ __forceinline__ void epilogue(const SolveDev& a, int kind, int64_t ti, const double s[5], int n_used,
-                                         int8_t flag) {
-  const double c0 = a.vg.c0;
-  double mu, value, swc;
-  if (kind == BTK_SIMPLE) {
-    mu = 0.0;
-    value = a.kparam + s[2];
-    swc = s[4];
-  } else {
-    mu = (s[0] - 1.0) / s[1];
-    value = s[2] - mu * s[3];
-    if (kind == BTK_INDICATOR) value = value < 0.0 ? 0.0 : (value > 1.0 ? 1.0 : value);
-    swc = s[4] - mu * s[0];
-  }
-  a.value[ti] = value;
-  if (a.variance) a.variance[ti] = fmax(c0 - swc - mu, 0.0);
-  if (a.lagrange) a.lagrange[ti] = mu;
-  if (a.n_used) a.n_used[ti] = n_used;
-  if (a.status) a.status[ti] = int8_t(BTK_ST_OK | flag);
 }
 
 template <int NW, bool kPairs = false>

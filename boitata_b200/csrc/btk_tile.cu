@@ -1,0 +1,498 @@
+// Tile-shared kriging solve: the systems of kTileTargets consecutive work
+// slots (half of a 32-target search tile, so a compact patch of blocks)
+// share one covariance table over the union of their samples.
+//
+// Reference: crates/estimation/src/kernel.rs:24-123 (per-system assembly,
+// factorisation, estimate and variance); the quantities are the same as in
+// btk_solve.cu, only the assembly is shared. Neighbouring blocks of a block
+// model draw on nearly the same samples (a 4 x 4 block patch of the 3.2M-block
+// drill-hole model needs about 52 distinct samples for its 16 x 32 system
+// rows), so evaluating C(s_u, s_v) once per tile instead of once per system
+// cuts the covariance evaluations per target from n(n-1)/2 = 496 to about 85.
+// A system then gathers its rows from the table by union index.
+//
+// Per tile (one CTA of 128 threads):
+//   1. the union of the tile's neighbour lists through a shared-memory hash
+//      (open addressing, 1024 slots for at most 16 x 32 keys);
+//   2. the union's world coordinates and the table C[u][v] (FP64, full
+//      square, diagonal C0 + the sample's error variance), every lag from
+//      lag_world, so an entry is bit for bit the one the per-system kernels
+//      assemble and results do not depend on the tiling;
+//   3. the systems: FP64 form one per warp, lane = row, the right-looking
+//      LDL^T of btk_solve.cu; mixed form two per warp (a half-warp each, lane l
+//      holding rows l and l + 16 in FP32 registers), LDL^T with packed FP32
+//      FMA (fma.rn.f32x2), a register-only backward sweep for x = C^-1 v, FP64
+//      residuals r = v - C x from the FP64 table and the corrected forms
+//      u'x_v + x_u'r_v, as in btk_solve.cu's mixed kernel.
+// Each row keeps the full symmetric row (not only its lower part). After the
+// elimination, lane i's slots q > i then hold D_i L[q][i], the i-th column of
+// L, which is what the backward sweep needs, so no transpose goes through
+// shared memory.
+//
+// Systems the tile does not take: a failed search (outputs written here),
+// n > 32 (appended to `large`), a sample flagged coincident at fit time or a
+// tile whose union exceeds the table (appended to `small`), and, in the mixed
+// form, systems whose FP32 pivots or residuals fail the refinement tests
+// (appended to `redo`). The per-system kernels of btk_solve.cu take those.
+// The table entries do not depend on the order in which samples enter the
+// union or on the tile (each is a function of its sample pair alone), so the
+// FP64 form gives bit for bit the per-system kernel's results.
+#include "btk_device.cuh"
+
+namespace btk {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kT = kTileTargets;
+constexpr int kHash = 1024;
+constexpr uint32_t kEmpty = 0xffffffffu;
+constexpr int kThreads = 128;
+
+struct TileHead {
+  int64_t ti[kT];
+  int n[kT];
+  int kind[kT];
+  int twin[kT];
+  int go[kT];
+  int nu;
+  int any;
+  uint8_t map[kT][32];
+  uint16_t slot[kT][32];
+};
+
+struct WarpFp64 {
+  double col[2][32];
+  double rhs[2][4];
+};
+
+struct WarpMixed {
+  float colf[2][2][32];  // [half][buffer][row]
+  float rhsf[2][2][4];
+  double xs[2][32][4];   // [half][row]: x_c, x_1, x_f
+};
+
+__host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+struct Layout {
+  size_t head, ukey, p, z, e, table, warp, total;
+};
+
+__host__ __device__ inline Layout layout(int umax, int stride, bool mixed) {
+  Layout l;
+  l.head = 0;
+  l.ukey = align16(sizeof(TileHead));
+  l.p = align16(l.ukey + sizeof(uint32_t) * umax);
+  l.z = l.p + sizeof(double) * 3 * umax;
+  l.e = l.z + sizeof(double) * umax;
+  l.table = align16(l.e + sizeof(double) * umax);
+  size_t tb = sizeof(double) * size_t(umax) * stride;
+  const size_t hash = sizeof(uint32_t) * kHash + sizeof(uint8_t) * kHash;
+  if (tb < hash) tb = hash;
+  l.warp = align16(l.table + tb);
+  l.total = l.warp + (kThreads / 32) * (mixed ? sizeof(WarpMixed) : sizeof(WarpFp64));
+  return l;
+}
+
+__device__ __forceinline__ float rcp_approx(float d) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+  return r;
+}
+
+__device__ __forceinline__ float slot_of(const float2* A, int q) { return (q & 1) ? A[q >> 1].y : A[q >> 1].x; }
+
+// The tile's targets, union and covariance table; false when nothing is left
+// for the solve phase. Ends with the block synchronised.
+__device__ bool build_tile(const TileDev& a, int64_t tile, unsigned char* smem, const Layout& lay) {
+  const SolveDev& s = a.s;
+  TileHead& H = *reinterpret_cast<TileHead*>(smem + lay.head);
+  uint32_t* ukey = reinterpret_cast<uint32_t*>(smem + lay.ukey);
+  double* P = reinterpret_cast<double*>(smem + lay.p);
+  double* Z = reinterpret_cast<double*>(smem + lay.z);
+  double* E = reinterpret_cast<double*>(smem + lay.e);
+  double* UU = reinterpret_cast<double*>(smem + lay.table);
+  uint32_t* keys = reinterpret_cast<uint32_t*>(smem + lay.table);  // phase 1 only
+  uint8_t* uidx = reinterpret_cast<uint8_t*>(keys + kHash);
+  const int tid = threadIdx.x;
+  const int umax = a.umax, S = a.stride;
+
+  if (tid < kT) {
+    const int64_t w = tile * kT + tid;
+    int64_t ti = w < a.nwork ? (a.perm ? a.perm[w] : w) : -1;
+    int n = 0, kd = s.kind;
+    if (ti >= 0) {
+      n = s.count[ti];
+      const int8_t st = s.sstatus[ti];
+      if (s.kinds) kd = s.kinds[ti];
+      if (st != BTK_ST_OK) {
+        write_fail(s, ti, st, 0);
+        ti = -1;
+      } else if (n <= 0) {
+        write_fail(s, ti, BTK_ST_SEARCH_FAILED, 0);
+        ti = -1;
+      } else if (n > 32) {
+        a.large[atomicAdd(reinterpret_cast<unsigned long long*>(a.large_len), 1ull)] = ti;
+        ti = -1;
+      }
+    }
+    H.ti[tid] = ti;
+    H.n[tid] = ti >= 0 ? n : 0;
+    H.kind[tid] = kd;
+    H.twin[tid] = 0;
+  }
+  if (tid == 0) H.nu = 0;
+  for (int i = tid; i < kHash; i += kThreads) keys[i] = kEmpty;
+  __syncthreads();
+
+  // 1. Union of the neighbour lists.
+  for (int e = tid; e < kT * 32; e += kThreads) {
+    const int t = e >> 5, r = e & 31;
+    const int64_t ti = H.ti[t];
+    if (ti < 0 || r >= H.n[t]) continue;
+    const uint32_t key = s.nbr[ti * s.max_samples + r];
+    if (s.twin && s.twin[key]) H.twin[t] = 1;
+    uint32_t h = (key * 2654435761u) >> 22;  // multiplicative hash, 10 bits
+    for (int probe = 0; probe < kHash; ++probe) {  // at most kT * 32 < kHash keys: a free slot exists
+      const uint32_t old = atomicCAS(&keys[h], kEmpty, key);
+      if (old == kEmpty || old == key) break;
+      h = (h + 1) & (kHash - 1);
+    }
+    H.slot[t][r] = uint16_t(h);
+  }
+  __syncthreads();
+  for (int i = tid; i < kHash; i += kThreads) {
+    const uint32_t k = keys[i];
+    if (k == kEmpty) continue;
+    const int u = atomicAdd(&H.nu, 1);
+    uidx[i] = uint8_t(u < 255 ? u : 255);
+    if (u < umax) ukey[u] = k;
+  }
+  __syncthreads();
+  const int nu = H.nu;
+  if (nu > umax) {  // the table would not hold this tile: per-system kernels
+    if (tid < kT && H.ti[tid] >= 0) a.small[atomicAdd(reinterpret_cast<unsigned long long*>(a.small_len), 1ull)] = H.ti[tid];
+    __syncthreads();
+    return false;
+  }
+  for (int e = tid; e < kT * 32; e += kThreads) {
+    const int t = e >> 5, r = e & 31;
+    H.map[t][r] = (H.ti[t] >= 0 && r < H.n[t]) ? uidx[H.slot[t][r]] : uint8_t(0);
+  }
+  if (tid < kT) {
+    const int64_t ti = H.ti[tid];
+    const bool go = ti >= 0 && !H.twin[tid];
+    if (ti >= 0 && !go) a.small[atomicAdd(reinterpret_cast<unsigned long long*>(a.small_len), 1ull)] = ti;
+    H.go[tid] = go;
+  }
+  if (tid == 0) {
+    int any = 0;
+    for (int t = 0; t < kT; ++t) any |= H.ti[t] >= 0 && !H.twin[t];
+    H.any = any;
+  }
+  __syncthreads();
+  if (!H.any) return false;  // uniform: every thread read the same H.any
+
+  // 2. Union coordinates (world) and the covariance table.
+  for (int u = tid; u < nu; u += kThreads) {
+    const uint32_t k = ukey[u];
+    P[u] = s.sx[k], P[umax + u] = s.sy[k], P[2 * umax + u] = s.sz[k];
+    Z[u] = s.sv[k];
+    E[u] = s.se ? s.se[k] : 0.0;
+  }
+  __syncthreads();  // the hash is dead from here: its space becomes the table
+  const int npairs = nu * (nu - 1) / 2;
+  for (int e = tid; e < npairs; e += kThreads) {
+    int i, j;
+    tri_index(e, i, j);
+    const double c = cov64(s.vg, lag_world(s.vg, P[j], P[umax + j], P[2 * umax + j], P[i], P[umax + i], P[2 * umax + i]));
+    UU[i * S + j] = c;
+    UU[j * S + i] = c;
+  }
+  for (int u = tid; u < nu; u += kThreads) UU[u * S + u] = s.vg.c0 + E[u];
+  __syncthreads();
+  return true;
+}
+
+// C(target, union sample u).
+__device__ __forceinline__ double cov_to(const VgDev& vg, const double* P, int umax, int u, const double t[3]) {
+  return cov64(vg, lag_world(vg, t[0], t[1], t[2], P[u], P[umax + u], P[2 * umax + u]));
+}
+
+// FP64 form: system t of the tile on one warp.
+__device__ void solve_fp64(const TileDev& a, const TileHead& H, const double* P, const double* Z, const double* UU,
+                           int umax, int S, WarpFp64& W, int t) {
+  const SolveDev& s = a.s;
+  const int lane = threadIdx.x & 31;
+  const int64_t ti = H.ti[t];
+  const int n = H.n[t], kind = H.kind[t];
+  const double c0 = s.vg.c0;
+  const bool have = lane < n;
+  const int ma = H.map[t][lane];
+  const double pt[3] = {s.tx[ti], s.ty[ti], s.tz[ti]};
+  const double c = have ? cov_to(s.vg, P, umax, ma, pt) : 0.0;
+  const double zf = have ? kind_f(kind, s.kparam, Z[ma]) : 0.0;
+  const double* Ur = UU + ma * S;
+  double A[32];
+#pragma unroll
+  for (int q = 0; q < 32; ++q) A[q] = (have && q < n) ? Ur[H.map[t][q]] : (q == lane ? 1.0 : 0.0);
+  double y0 = have ? c : 0.0, y1 = have ? 1.0 : 0.0, y2 = have ? zf : 0.0;
+  double dme = 1.0;
+  bool sing = false;
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    if (k >= n) break;
+    const int b = k & 1;
+    W.col[b][lane] = A[k];
+    if (lane == k) W.rhs[b][0] = y0, W.rhs[b][1] = y1, W.rhs[b][2] = y2;
+    __syncwarp();
+    const double d = W.col[b][k];
+    if (!(d > kPivot * c0)) {  // NaN or at most 1e-12 C0 (kernel.rs:61)
+      sing = true;
+      break;
+    }
+    if (lane == k) dme = d;
+    const double f = lane > k ? A[k] * (1.0 / d) : 0.0;
+#pragma unroll
+    for (int q = k + 1; q < 32; ++q) A[q] = fma(-f, W.col[b][q], A[q]);
+    y0 = fma(-f, W.rhs[b][0], y0);
+    y1 = fma(-f, W.rhs[b][1], y1);
+    y2 = fma(-f, W.rhs[b][2], y2);
+  }
+  __syncwarp();
+  if (sing) {
+    if (lane == 0) write_fail(s, ti, BTK_ST_SINGULAR, 0);
+    return;
+  }
+  const double wt = have ? 1.0 / dme : 0.0;
+  double v[5] = {y1 * y0 * wt, y1 * y1 * wt, y2 * y0 * wt, y2 * y1 * wt, y0 * y0 * wt};
+#pragma unroll
+  for (int q = 0; q < 5; ++q)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(kFull, v[q], o);
+  if (lane == 0) epilogue(s, kind, ti, v, n, 0);
+}
+
+__device__ __forceinline__ double half_max(double v) {
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+
+// Mixed form: systems 2p (lanes 0-15) and 2p + 1 (lanes 16-31) of the tile.
+__device__ void solve_mixed(const TileDev& a, const TileHead& H, const double* P, const double* Z, const double* UU,
+                            int umax, int S, WarpMixed& W, int p) {
+  const SolveDev& s = a.s;
+  const int lane = threadIdx.x & 31, half = lane >> 4, l = lane & 15;
+  const int t = 2 * p + half;
+  const bool go = H.go[t] != 0;
+  const int64_t ti = go ? H.ti[t] : -1;
+  const int n = go ? H.n[t] : 0;
+  const int kind = H.kind[t];
+  const double c0 = s.vg.c0;
+  const int r1 = l, r2 = l + 16;
+  const bool have1 = r1 < n, have2 = r2 < n;
+  const int m1 = H.map[t][r1], m2 = H.map[t][r2];
+  double c1 = 0.0, c2 = 0.0, zf1 = 0.0, zf2 = 0.0;
+  if (go) {
+    const double pt[3] = {s.tx[ti], s.ty[ti], s.tz[ti]};
+    if (have1) c1 = cov_to(s.vg, P, umax, m1, pt), zf1 = kind_f(kind, s.kparam, Z[m1]);
+    if (have2) c2 = cov_to(s.vg, P, umax, m2, pt), zf2 = kind_f(kind, s.kparam, Z[m2]);
+  }
+  const int nmax = max(n, __shfl_xor_sync(kFull, n, 16));
+  const double* U1 = UU + m1 * S;
+  const double* U2 = UU + m2 * S;
+  float2 A1[16], A2[16];
+#pragma unroll
+  for (int q2 = 0; q2 < 16; ++q2) {
+    const int qa = 2 * q2, qb = qa + 1;
+    const int ma = H.map[t][qa], mb = H.map[t][qb];
+    A1[q2].x = (have1 && qa < n) ? float(U1[ma]) : (qa == r1 ? 1.f : 0.f);
+    A1[q2].y = (have1 && qb < n) ? float(U1[mb]) : (qb == r1 ? 1.f : 0.f);
+    A2[q2].x = (have2 && qa < n) ? float(U2[ma]) : (qa == r2 ? 1.f : 0.f);
+    A2[q2].y = (have2 && qb < n) ? float(U2[mb]) : (qb == r2 ? 1.f : 0.f);
+  }
+  float y1[3] = {float(c1), have1 ? 1.f : 0.f, float(zf1)};
+  float y2[3] = {float(c2), have2 ? 1.f : 0.f, float(zf2)};
+  float d1 = 1.f, d2 = 1.f;
+  bool weak = false;
+  const float thr = 1e-5f * float(c0);
+  // LDL^T with the forward substitution of (c, 1, f) fused in.
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    if (k >= nmax) break;
+    const int b = k & 1;
+    float* col = W.colf[half][b];
+    col[r1] = slot_of(A1, k);
+    col[r2] = slot_of(A2, k);
+    if (k < 16) {
+      if (l == k) W.rhsf[half][b][0] = y1[0], W.rhsf[half][b][1] = y1[1], W.rhsf[half][b][2] = y1[2];
+    } else {
+      if (l == k - 16) W.rhsf[half][b][0] = y2[0], W.rhsf[half][b][1] = y2[1], W.rhsf[half][b][2] = y2[2];
+    }
+    __syncwarp();
+    const float d = col[k];
+    weak |= !(d > thr);
+    const float rd = rcp_approx(d);
+    const float f1 = r1 > k ? slot_of(A1, k) * rd : 0.f;
+    const float f2 = r2 > k ? slot_of(A2, k) * rd : 0.f;
+    if (k < 16) {
+      if (r1 == k) d1 = d;
+    } else {
+      if (r2 == k) d2 = d;
+    }
+    const float2 nf1 = make_float2(-f1, -f1), nf2 = make_float2(-f2, -f2);
+    // Pairs from the one holding slot k + 1 (slot k itself, when it is in
+    // the first pair, only changes entries that are not read again), then
+    // groups of four slots from a 16-byte aligned shared-memory line.
+    const int q2s = (k + 1) >> 1;
+    if (q2s & 1) {
+      const float2 cv = *reinterpret_cast<const float2*>(&col[2 * q2s]);
+      A1[q2s] = __ffma2_rn(nf1, cv, A1[q2s]);
+      A2[q2s] = __ffma2_rn(nf2, cv, A2[q2s]);
+    }
+#pragma unroll
+    for (int g = (q2s + 1) >> 1; g < 8; ++g) {
+      const float4 c4 = *reinterpret_cast<const float4*>(&col[4 * g]);
+      const float2 lo = make_float2(c4.x, c4.y), hi = make_float2(c4.z, c4.w);
+      A1[2 * g] = __ffma2_rn(nf1, lo, A1[2 * g]);
+      A2[2 * g] = __ffma2_rn(nf2, lo, A2[2 * g]);
+      A1[2 * g + 1] = __ffma2_rn(nf1, hi, A1[2 * g + 1]);
+      A2[2 * g + 1] = __ffma2_rn(nf2, hi, A2[2 * g + 1]);
+    }
+    const float4 rk = *reinterpret_cast<const float4*>(W.rhsf[half][b]);
+    y1[0] = fmaf(-f1, rk.x, y1[0]), y1[1] = fmaf(-f1, rk.y, y1[1]), y1[2] = fmaf(-f1, rk.z, y1[2]);
+    y2[0] = fmaf(-f2, rk.x, y2[0]), y2[1] = fmaf(-f2, rk.y, y2[1]), y2[2] = fmaf(-f2, rk.z, y2[2]);
+  }
+  // Backward sweep L^T x = D^-1 y, one row per step; lane i's slots q > i
+  // hold D_i L[q][i]: x_k = (y_k - sum_{q>k} slot_k[q] x_q) / D_k.
+  const float rd1 = rcp_approx(d1), rd2 = rcp_approx(d2);
+  float acc1[3] = {0.f, 0.f, 0.f}, acc2[3] = {0.f, 0.f, 0.f};
+  float x1[3] = {0.f, 0.f, 0.f}, x2[3] = {0.f, 0.f, 0.f};
+  const int src_base = half << 4;
+#pragma unroll
+  for (int k = 31; k >= 0; --k) {
+    if (k >= nmax) continue;
+    float z[3];
+    if (k < 16) {
+#pragma unroll
+      for (int v = 0; v < 3; ++v) z[v] = (y1[v] - acc1[v]) * rd1;
+    } else {
+#pragma unroll
+      for (int v = 0; v < 3; ++v) z[v] = (y2[v] - acc2[v]) * rd2;
+    }
+#pragma unroll
+    for (int v = 0; v < 3; ++v) z[v] = __shfl_sync(kFull, z[v], src_base + (k & 15));
+    if (k < 16) {
+      if (l == k) x1[0] = z[0], x1[1] = z[1], x1[2] = z[2];
+    } else {
+      if (l == k - 16) x2[0] = z[0], x2[1] = z[1], x2[2] = z[2];
+    }
+    const float s1 = slot_of(A1, k), s2 = slot_of(A2, k);
+#pragma unroll
+    for (int v = 0; v < 3; ++v) acc1[v] = fmaf(s1, z[v], acc1[v]), acc2[v] = fmaf(s2, z[v], acc2[v]);
+  }
+  // FP64 residuals r_v = v - C x_v from the FP64 table.
+  double xa[3], xb[3];
+#pragma unroll
+  for (int v = 0; v < 3; ++v) xa[v] = have1 ? double(x1[v]) : 0.0, xb[v] = have2 ? double(x2[v]) : 0.0;
+  W.xs[half][r1][0] = xa[0], W.xs[half][r1][1] = xa[1], W.xs[half][r1][2] = xa[2];
+  W.xs[half][r2][0] = xb[0], W.xs[half][r2][1] = xb[1], W.xs[half][r2][2] = xb[2];
+  __syncwarp();
+  double a1[3] = {0.0, 0.0, 0.0}, a2[3] = {0.0, 0.0, 0.0};
+  for (int j = 0; j < nmax; ++j) {
+    const int mj = H.map[t][j];  // 0 beyond this half's n, where x_j = 0
+    const double2 x01 = *reinterpret_cast<const double2*>(&W.xs[half][j][0]);
+    const double x2j = W.xs[half][j][2];
+    const double cj1 = U1[mj], cj2 = U2[mj];
+    a1[0] = fma(cj1, x01.x, a1[0]), a1[1] = fma(cj1, x01.y, a1[1]), a1[2] = fma(cj1, x2j, a1[2]);
+    a2[0] = fma(cj2, x01.x, a2[0]), a2[1] = fma(cj2, x01.y, a2[1]), a2[2] = fma(cj2, x2j, a2[2]);
+  }
+  double ra[3] = {0.0, 0.0, 0.0}, rb[3] = {0.0, 0.0, 0.0};
+  if (have1) ra[0] = c1 - a1[0], ra[1] = 1.0 - a1[1], ra[2] = zf1 - a1[2];
+  if (have2) rb[0] = c2 - a2[0], rb[1] = 1.0 - a2[1], rb[2] = zf2 - a2[2];
+  // Refinement tests, as in the per-system mixed kernel: the corrected forms
+  // err by about rho^2 C0 / D_min.
+  const double cmax = half_max(fmax(have1 ? fabs(c1) : 0.0, have2 ? fabs(c2) : 0.0));
+  const double zmax = half_max(fmax(have1 ? fabs(zf1) : 0.0, have2 ? fabs(zf2) : 0.0));
+  const double ic = 1.0 / fmax(cmax, 1e-300), iz = 1.0 / fmax(zmax, 1e-300);
+  const double rho1 = fmax(fmax(fabs(ra[0]) * ic, fabs(ra[1])), fabs(ra[2]) * iz);
+  const double rho2 = fmax(fmax(fabs(rb[0]) * ic, fabs(rb[1])), fabs(rb[2]) * iz);
+  const double rho = half_max(fmax(rho1, rho2));
+  const double dmin = -half_max(fmax(have1 ? -double(d1) : -1e300, have2 ? -double(d2) : -1e300));
+  double v[5] = {xa[0] + xa[1] * ra[0] + xb[0] + xb[1] * rb[0],
+                 xa[1] + xa[1] * ra[1] + xb[1] + xb[1] * rb[1],
+                 zf1 * xa[0] + xa[2] * ra[0] + zf2 * xb[0] + xb[2] * rb[0],
+                 zf1 * xa[1] + xa[2] * ra[1] + zf2 * xb[1] + xb[2] * rb[1],
+                 c1 * xa[0] + xa[0] * ra[0] + c2 * xb[0] + xb[0] * rb[0]};
+#pragma unroll
+  for (int q = 0; q < 5; ++q)
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) v[q] += __shfl_xor_sync(kFull, v[q], o);
+  const unsigned wb = __ballot_sync(kFull, weak);
+  const bool weak_half = ((wb >> (half << 4)) & 0xffffu) != 0;
+  if (go && l == 0) {
+    if (weak_half || !(rho * rho * c0 / dmin <= 1e-8) || !(v[1] > 0.0) || !(fabs(v[0]) < 1e30))
+      a.redo[atomicAdd(reinterpret_cast<unsigned long long*>(a.redo_len), 1ull)] = ti;
+    else
+      epilogue(s, kind, ti, v, n, 0);
+  }
+  __syncwarp();
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(kThreads) k_tile(TileDev a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const Layout lay = layout(a.umax, a.stride, MIXED);
+  const TileHead& H = *reinterpret_cast<const TileHead*>(smem + lay.head);
+  const double* P = reinterpret_cast<const double*>(smem + lay.p);
+  const double* Z = reinterpret_cast<const double*>(smem + lay.z);
+  const double* UU = reinterpret_cast<const double*>(smem + lay.table);
+  const int warp = threadIdx.x >> 5;
+  const int64_t ntiles = (a.nwork + kT - 1) / kT;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    __syncthreads();  // the previous tile's systems are done with the table
+    if (!build_tile(a, tile, smem, lay)) continue;
+    if (MIXED) {
+      WarpMixed& W = reinterpret_cast<WarpMixed*>(smem + lay.warp)[warp];
+      for (int p = warp; p < kT / 2; p += kThreads / 32)
+        if (H.go[2 * p] || H.go[2 * p + 1]) solve_mixed(a, H, P, Z, UU, a.umax, a.stride, W, p);
+    } else {
+      WarpFp64& W = reinterpret_cast<WarpFp64*>(smem + lay.warp)[warp];
+      for (int t = warp; t < kT; t += kThreads / 32)
+        if (H.go[t]) solve_fp64(a, H, P, Z, UU, a.umax, a.stride, W, t);
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_tile(const Launch& L, const TileDev& a0, bool mixed) {
+  TileDev a = a0;
+  if (a.umax < 2 || a.umax > 255) return cudaErrorInvalidValue;
+  a.stride = a.umax | 1;  // odd row stride
+  const size_t smem = layout(a.umax, a.stride, mixed).total;
+  cudaError_t e;
+  int per_sm = 0;
+  if (mixed) {
+    e = cudaFuncSetAttribute(k_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<true>, kThreads, smem);
+  } else {
+    e = cudaFuncSetAttribute(k_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<false>, kThreads, smem);
+  }
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  if (L.tuning.solve_blocks_per_sm > 0 && L.tuning.solve_blocks_per_sm < per_sm) per_sm = L.tuning.solve_blocks_per_sm;
+  const int64_t ntiles = (a.nwork + kT - 1) / kT;
+  int64_t blocks = int64_t(L.sm_count) * per_sm;
+  if (blocks > ntiles) blocks = ntiles;
+  if (blocks < 1) blocks = 1;
+  if (mixed)
+    k_tile<true><<<int(blocks), kThreads, smem, L.stream>>>(a);
+  else
+    k_tile<false><<<int(blocks), kThreads, smem, L.stream>>>(a);
+  ++*L.counter;
+  return cudaGetLastError();
+}
+
+}  // namespace btk

@@ -123,12 +123,15 @@ typedef struct {
 
 /* Launch tunables (no counterpart in the reference): grid cell size in
  * samples per cell, the block-model tile one search warp serves (product
- * 32), warps per search CTA and resident solve CTAs per SM (0: defaults). */
+ * 32), warps per search CTA, resident solve CTAs per SM (0: defaults), and
+ * the most distinct samples the tile-shared solve tabulates for 16
+ * consecutive targets (32..255; 0: every system assembles its own matrix). */
 typedef struct {
   double samples_per_cell;
   int32_t tile[3];
   int32_t search_warps;
   int32_t solve_blocks_per_sm;
+  int32_t tile_union;
 } btk_tuning;
 
 typedef struct btk_ctx btk_ctx;

@@ -39,11 +39,34 @@ def test_results_do_not_depend_on_the_tuning():
     outs, oc = device_outputs(geo.cells())
     base = predict(est, geo, N.FP64, outs, oc)
     cfg = get_tuning(est._ctx)
-    for ppc, tile, sw, sb in [(1.0, (8, 4, 1), 2, 2), (4.0, (2, 2, 8), 8, 3), (2.0, (4, 4, 2), 0, 0)]:
-        set_tuning(est._ctx, dict(cfg, samples_per_cell=ppc, tile=tile, search_warps=sw, solve_blocks_per_sm=sb))
+    assert cfg["tile_union"] > 0  # the tile-shared solve is the default
+    for ppc, tile, sw, sb, tu in [(1.0, (8, 4, 1), 2, 2, 0), (4.0, (2, 2, 8), 8, 3, 64), (2.0, (4, 4, 2), 0, 0, 96),
+                                  (2.0, (4, 4, 2), 0, 0, 32)]:
+        set_tuning(est._ctx, dict(cfg, samples_per_cell=ppc, tile=tile, search_warps=sw, solve_blocks_per_sm=sb,
+                                  tile_union=tu))
         got = predict(est, geo, N.FP64, outs, oc)
         for a, b in zip(got, base):
             np.testing.assert_array_equal(a, b)
+
+
+def test_tile_and_per_system_mixed_forms_agree():
+    """The mixed form through the tile-shared kernel and through the per-system kernel: both refine to the
+    FP64 solution, so they agree far inside the mixed form's 1e-6 tolerance."""
+    w = W.c2()
+    geo = Geometry((100.0, 100.0, 50.0), (2.5, 2.5, 3.125), (40, 40, 40))
+    est = OrdinaryKriging(w.variogram, w.search).fit(w.coords, w.values)
+    outs, oc = device_outputs(geo.cells())
+    cfg = get_tuning(est._ctx)
+    tiled = predict(est, geo, N.MIXED, outs, oc)
+    exact = predict(est, geo, N.FP64, outs, oc)
+    set_tuning(est._ctx, dict(cfg, tile_union=0))
+    per_system = predict(est, geo, N.MIXED, outs, oc)
+    for k in (0, 1):
+        scale = 1.0 + np.maximum(np.abs(exact[k]), np.abs(tiled[k]))
+        assert np.nanmax(np.abs(tiled[k] - exact[k]) / scale) < 1e-9
+        assert np.nanmax(np.abs(tiled[k] - per_system[k]) / scale) < 1e-9
+    np.testing.assert_array_equal(tiled[3], per_system[3])
+    np.testing.assert_array_equal(tiled[4] & 0x0F, per_system[4] & 0x0F)
 
 
 def test_graph_replay_matches_the_call_and_autotune_keeps_results():
@@ -70,7 +93,7 @@ def test_graph_replay_matches_the_call_and_autotune_keeps_results():
         for a, b in zip([t.cpu().numpy() for t in outs], want):
             np.testing.assert_array_equal(a, b)
     tuned = autotune_geometry(est, geo, precision="mixed", steps=1, use_cache=False)
-    assert tuned["ms"] > 0 and len(tuned["table"]) >= 21
+    assert tuned["ms"] > 0 and len(tuned["table"]) >= 21 + 2 + 11
     got = predict(est, geo, N.MIXED, outs, oc)
     for a, b in zip(got, predict(est, geo, N.MIXED, outs, oc)):
         np.testing.assert_array_equal(a, b)
