@@ -61,7 +61,7 @@ struct TileHead {
 };
 
 struct WarpFp64 {
-  double col[2][32];
+  double col[2][36];  // [buffer]: column below the pivot (0..30), pivot (32), sink (33)
   double rhs[2][4];
 };
 
@@ -160,12 +160,19 @@ __device__ bool build_tile(const TileDev& a, int64_t tile, unsigned char* smem, 
     H.slot[t][r] = uint16_t(h);
   }
   __syncthreads();
-  for (int i = tid; i < kHash; i += kThreads) {
+  for (int i = tid; i < kHash; i += kThreads) {  // one atomic per warp and round
     const uint32_t k = keys[i];
-    if (k == kEmpty) continue;
-    const int u = atomicAdd(&H.nu, 1);
-    uidx[i] = uint8_t(u < 255 ? u : 255);
-    if (u < umax) ukey[u] = k;
+    const bool occ = k != kEmpty;
+    const unsigned bal = __ballot_sync(kFull, occ);
+    const int lane = tid & 31;
+    int base = 0;
+    if (lane == 0 && bal) base = atomicAdd(&H.nu, __popc(bal));
+    base = __shfl_sync(kFull, base, 0);
+    if (occ) {
+      const int u = base + __popc(bal & ((1u << lane) - 1u));
+      uidx[i] = uint8_t(u < 255 ? u : 255);
+      if (u < umax) ukey[u] = k;
+    }
   }
   __syncthreads();
   const int nu = H.nu;
@@ -218,6 +225,41 @@ __device__ __forceinline__ double cov_to(const VgDev& vg, const double* P, int u
   return cov64(vg, lag_world(vg, t[0], t[1], t[2], P[u], P[umax + u], P[2 * umax + u]));
 }
 
+// Pivots k0 .. k1-1 of the FP64 right-looking LDL^T with the forward
+// substitution of y fused in. The row is kept shifted so that slot 0 holds
+// the current pivot column: a step writes it to the warp's line, then
+// A[q] <- A[q+1] - f col[q] over the W slots that still hold live columns
+// (the shift makes the loop body the same for every k, so it is a runtime
+// loop and the code stays small). Same operations, in the same order, as
+// the unrolled per-system kernel.
+template <int W>
+__device__ __forceinline__ void eliminate(double (&A)[32], int k0, int k1, int lane, WarpFp64& Ws, double (&y)[3],
+                                          double& dme, bool& sing, double thr) {
+  for (int k = k0; k < k1; ++k) {
+    const int b = k & 1;
+    Ws.col[b][lane > k ? lane - k - 1 : (lane == k ? 32 : 33)] = A[0];
+    if (lane == k) Ws.rhs[b][0] = y[0], Ws.rhs[b][1] = y[1], Ws.rhs[b][2] = y[2];
+    __syncwarp();
+    const double d = Ws.col[b][32];
+    if (!(d > thr)) {  // NaN or at most 1e-12 C0 (kernel.rs:61)
+      sing = true;
+      return;
+    }
+    if (lane == k) dme = d;
+    const double f = lane > k ? A[0] * (1.0 / d) : 0.0;
+#pragma unroll
+    for (int q = 0; q < W; q += 2) {
+      const double2 cv = *reinterpret_cast<const double2*>(&Ws.col[b][q]);
+      A[q] = fma(-f, cv.x, A[q + 1]);
+      A[q + 1] = q + 2 < 32 ? fma(-f, cv.y, A[q + 2]) : 0.0;
+    }
+    const double2 r01 = *reinterpret_cast<const double2*>(&Ws.rhs[b][0]);
+    y[0] = fma(-f, r01.x, y[0]);
+    y[1] = fma(-f, r01.y, y[1]);
+    y[2] = fma(-f, Ws.rhs[b][2], y[2]);
+  }
+}
+
 // FP64 form: system t of the tile on one warp.
 __device__ void solve_fp64(const TileDev& a, const TileHead& H, const double* P, const double* Z, const double* UU,
                            int umax, int S, WarpFp64& W, int t) {
@@ -235,34 +277,23 @@ __device__ void solve_fp64(const TileDev& a, const TileHead& H, const double* P,
   double A[32];
 #pragma unroll
   for (int q = 0; q < 32; ++q) A[q] = (have && q < n) ? Ur[H.map[t][q]] : (q == lane ? 1.0 : 0.0);
-  double y0 = have ? c : 0.0, y1 = have ? 1.0 : 0.0, y2 = have ? zf : 0.0;
+  double y[3] = {have ? c : 0.0, have ? 1.0 : 0.0, have ? zf : 0.0};
   double dme = 1.0;
   bool sing = false;
-#pragma unroll
-  for (int k = 0; k < 32; ++k) {
-    if (k >= n) break;
-    const int b = k & 1;
-    W.col[b][lane] = A[k];
-    if (lane == k) W.rhs[b][0] = y0, W.rhs[b][1] = y1, W.rhs[b][2] = y2;
-    __syncwarp();
-    const double d = W.col[b][k];
-    if (!(d > kPivot * c0)) {  // NaN or at most 1e-12 C0 (kernel.rs:61)
-      sing = true;
-      break;
-    }
-    if (lane == k) dme = d;
-    const double f = lane > k ? A[k] * (1.0 / d) : 0.0;
-#pragma unroll
-    for (int q = k + 1; q < 32; ++q) A[q] = fma(-f, W.col[b][q], A[q]);
-    y0 = fma(-f, W.rhs[b][0], y0);
-    y1 = fma(-f, W.rhs[b][1], y1);
-    y2 = fma(-f, W.rhs[b][2], y2);
-  }
+  const double thr = kPivot * c0;
+  // Four stages of eight pivots over windows of 32, 24, 16 and 8 slots (the
+  // columns a step can still change), each a runtime loop.
+  const int n1 = min(n, 8), n2 = min(n, 16), n3 = min(n, 24);
+  eliminate<32>(A, 0, n1, lane, W, y, dme, sing, thr);
+  if (!sing) eliminate<24>(A, n1, n2, lane, W, y, dme, sing, thr);
+  if (!sing) eliminate<16>(A, n2, n3, lane, W, y, dme, sing, thr);
+  if (!sing) eliminate<8>(A, n3, n, lane, W, y, dme, sing, thr);
   __syncwarp();
   if (sing) {
     if (lane == 0) write_fail(s, ti, BTK_ST_SINGULAR, 0);
     return;
   }
+  const double y0 = y[0], y1 = y[1], y2 = y[2];
   const double wt = have ? 1.0 / dme : 0.0;
   double v[5] = {y1 * y0 * wt, y1 * y1 * wt, y2 * y0 * wt, y2 * y1 * wt, y0 * y0 * wt};
 #pragma unroll
@@ -440,7 +471,7 @@ __device__ void solve_mixed(const TileDev& a, const TileHead& H, const double* P
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(kThreads) k_tile(TileDev a) {
+__global__ void __launch_bounds__(kThreads, MIXED ? 3 : 4) k_tile(TileDev a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Layout lay = layout(a.umax, a.stride, MIXED);
   const TileHead& H = *reinterpret_cast<const TileHead*>(smem + lay.head);
