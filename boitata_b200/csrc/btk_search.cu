@@ -117,13 +117,15 @@ __device__ __forceinline__ void set_root(Need& nd, int sec, double v) {
     if (s == sec) nd.root[s] = v;
 }
 
-// Offers candidate (d2, idx) of sector `sec` to this lane's lists.
+// Inserts (d2, idx) into sector list `base` holding c entries (a max-heap
+// on (d2, index) in this lane's column): sift up while the list is filling,
+// else replace the root and sift down. Returns the new root's d2. Kept out
+// of line: it runs for a small share of the candidates, and the candidate
+// loop around it runs faster when its code stays small.
 template <int SLOTS, bool OCT>
-__device__ __forceinline__ void consider(WarpSmem<SLOTS, OCT>& S, int lane, int nsec, int cap, int sec, double d2,
-                                         uint32_t idx, double& thr, Need& nd) {
-  const int base = sec * cap;
-  int c = S.cnt[sec][lane];
-  if (c < cap) {  // heap not full: sift up
+__device__ __noinline__ double heap_insert(WarpSmem<SLOTS, OCT>& S, int lane, int base, int cap, int c, double d2,
+                                           uint32_t idx) {
+  if (c < cap) {
     int pos = c;
     while (pos > 0) {
       int par = (pos - 1) >> 1;
@@ -136,16 +138,9 @@ __device__ __forceinline__ void consider(WarpSmem<SLOTS, OCT>& S, int lane, int 
     }
     S.hd[base + pos][lane] = d2;
     S.hi[base + pos][lane] = idx;
-    S.cnt[sec][lane] = c + 1;
-    if (c + 1 == cap) {
-      nd.open &= ~(1u << sec);
-      set_root(nd, sec, S.hd[base][lane]);
-      if (nd.open == 0) thr = max_root(S, lane, nsec, cap);
-    }
-    return;
+    return S.hd[base][lane];
   }
-  if (!key_less(d2, idx, S.hd[base][lane], S.hi[base][lane])) return;
-  int pos = 0;  // replace the root (the largest kept) and sift down
+  int pos = 0;
   while (true) {
     int ch = 2 * pos + 1;
     if (ch >= cap) break;
@@ -163,8 +158,23 @@ __device__ __forceinline__ void consider(WarpSmem<SLOTS, OCT>& S, int lane, int 
   }
   S.hd[base + pos][lane] = d2;
   S.hi[base + pos][lane] = idx;
-  set_root(nd, sec, S.hd[base][lane]);
-  if (nd.open == 0) thr = max_root(S, lane, nsec, cap);
+  return S.hd[base][lane];
+}
+
+// Offers candidate (d2, idx) of sector `sec` to this lane's lists.
+template <int SLOTS, bool OCT>
+__device__ __forceinline__ void consider(WarpSmem<SLOTS, OCT>& S, int lane, int nsec, int cap, int sec, double d2,
+                                         uint32_t idx, double& thr, Need& nd) {
+  const int base = sec * cap;
+  const int c = S.cnt[sec][lane];
+  if (c >= cap && !key_less(d2, idx, S.hd[base][lane], S.hi[base][lane])) return;
+  const double root = heap_insert(S, lane, base, cap, c, d2, idx);
+  if (c < cap) S.cnt[sec][lane] = c + 1;
+  if (c + 1 >= cap) {  // full (now or before): the root bounds what the sector still takes
+    nd.open &= ~(1u << sec);
+    set_root(nd, sec, root);
+    if (nd.open == 0) thr = max_root(S, lane, nsec, cap);
+  }
 }
 
 template <int SLOTS, bool OCT>

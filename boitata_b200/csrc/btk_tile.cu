@@ -65,11 +65,28 @@ struct WarpFp64 {
   double rhs[2][4];
 };
 
+// Mixed form: two systems per warp, a float2 (system a, system b) per slot.
+// Column k of the elimination (D_k L[j][k] for j > k, both systems) goes to
+// lt[kLtPad + col_off(k) + j - k - 1]; a column starts on an even index and
+// its length is rounded up to even, so it can be read in 16-byte lines. The
+// pads keep the reads past a column's end, and the backward sweep's reads
+// for rows that no longer need them, inside the warp's own area.
+constexpr int kLtPad = 32;
+constexpr int kLtLen = 512;  // sum over k of (31 - k) rounded up to even
 struct WarpMixed {
-  float colf[2][2][32];  // [half][buffer][row]
-  float rhsf[2][2][4];
-  double xs[2][32][4];   // [half][row]: x_c, x_1, x_f
+  union {
+    float2 lt[kLtPad + kLtLen + kLtPad];
+    double xs[32][6];  // after the backward sweep: x of row j (a: c, 1, f; b: c, 1, f)
+  };
+  float2 piv[2];
+  float2 rhs[2][4];
 };
+
+// Start of column k in the packed triangle (see WarpMixed).
+__device__ __forceinline__ int col_off(int k) {
+  const int m = k >> 1;
+  return 64 * m - 2 * m * m + ((k & 1) ? 32 - 2 * m : 0);
+}
 
 __host__ __device__ constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
@@ -98,8 +115,6 @@ __device__ __forceinline__ float rcp_approx(float d) {
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
   return r;
 }
-
-__device__ __forceinline__ float slot_of(const float2* A, int q) { return (q & 1) ? A[q >> 1].y : A[q >> 1].x; }
 
 // The tile's targets, union and covariance table; false when nothing is left
 // for the solve phase. Ends with the block synchronised.
@@ -303,169 +318,169 @@ __device__ void solve_fp64(const TileDev& a, const TileHead& H, const double* P,
   if (lane == 0) epilogue(s, kind, ti, v, n, 0);
 }
 
-__device__ __forceinline__ double half_max(double v) {
+__device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
-  for (int o = 8; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o));
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
   return v;
 }
 
-// Mixed form: systems 2p (lanes 0-15) and 2p + 1 (lanes 16-31) of the tile.
+__device__ __forceinline__ float warp_maxf(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+
+__device__ __forceinline__ float2 rcp2(float2 d) { return make_float2(rcp_approx(d.x), rcp_approx(d.y)); }
+
+// Pivots k0 .. k1-1 of the FP32 LDL^T of two systems at once (float2 lanes:
+// system a in .x, b in .y), forward substitution of y fused in; the row is
+// kept shifted (slot 0 = the current pivot column) and a step updates the W
+// slots that can still hold live columns, as in the FP64 eliminate().
+template <int W>
+__device__ __forceinline__ void eliminate2(float2 (&A)[32], int k0, int k1, int lane, WarpMixed& Ws,
+                                           float2 (&y)[3], float2& dme, bool& weak_a, bool& weak_b, float thr) {
+  for (int k = k0; k < k1; ++k) {
+    const int b = k & 1;
+    float2* col = Ws.lt + kLtPad + col_off(k);
+    if (lane > k) col[lane - k - 1] = A[0];
+    if (lane == k) {
+      Ws.piv[b] = A[0];
+      Ws.rhs[b][0] = y[0], Ws.rhs[b][1] = y[1], Ws.rhs[b][2] = y[2];
+    }
+    __syncwarp();
+    const float2 d = Ws.piv[b];
+    weak_a |= !(d.x > thr);
+    weak_b |= !(d.y > thr);
+    if (lane == k) dme = d;
+    const float2 rd = rcp2(d);
+    const float2 f = lane > k ? make_float2(A[0].x * rd.x, A[0].y * rd.y) : make_float2(0.f, 0.f);
+    const float2 nf = make_float2(-f.x, -f.y);
+#pragma unroll
+    for (int q = 0; q < W; q += 2) {
+      const float4 c4 = *reinterpret_cast<const float4*>(&col[q]);
+      A[q] = __ffma2_rn(nf, make_float2(c4.x, c4.y), A[q + 1]);
+      A[q + 1] = q + 2 < 32 ? __ffma2_rn(nf, make_float2(c4.z, c4.w), A[q + 2]) : make_float2(0.f, 0.f);
+    }
+    const float4 r01 = *reinterpret_cast<const float4*>(&Ws.rhs[b][0]);
+    const float2 r2 = Ws.rhs[b][2];
+    y[0] = __ffma2_rn(nf, make_float2(r01.x, r01.y), y[0]);
+    y[1] = __ffma2_rn(nf, make_float2(r01.z, r01.w), y[1]);
+    y[2] = __ffma2_rn(nf, r2, y[2]);
+  }
+}
+
+// Mixed form: systems 2p (a) and 2p + 1 (b) of the tile on one warp, lane = row.
 __device__ void solve_mixed(const TileDev& a, const TileHead& H, const double* P, const double* Z, const double* UU,
                             int umax, int S, WarpMixed& W, int p) {
   const SolveDev& s = a.s;
-  const int lane = threadIdx.x & 31, half = lane >> 4, l = lane & 15;
-  const int t = 2 * p + half;
-  const bool go = H.go[t] != 0;
-  const int64_t ti = go ? H.ti[t] : -1;
-  const int n = go ? H.n[t] : 0;
-  const int kind = H.kind[t];
+  const int lane = threadIdx.x & 31;
+  const int ta = 2 * p, tb = 2 * p + 1;
+  const bool go_a = H.go[ta] != 0, go_b = H.go[tb] != 0;
+  const int na = go_a ? H.n[ta] : 0, nb = go_b ? H.n[tb] : 0;
+  const int nmax = max(na, nb);
   const double c0 = s.vg.c0;
-  const int r1 = l, r2 = l + 16;
-  const bool have1 = r1 < n, have2 = r2 < n;
-  const int m1 = H.map[t][r1], m2 = H.map[t][r2];
-  double c1 = 0.0, c2 = 0.0, zf1 = 0.0, zf2 = 0.0;
-  if (go) {
+  const bool ha = lane < na, hb = lane < nb;
+  const int ma = H.map[ta][lane], mb = H.map[tb][lane];
+  double ca = 0.0, cb = 0.0, za = 0.0, zb = 0.0;
+  if (ha) {
+    const int64_t ti = H.ti[ta];
     const double pt[3] = {s.tx[ti], s.ty[ti], s.tz[ti]};
-    if (have1) c1 = cov_to(s.vg, P, umax, m1, pt), zf1 = kind_f(kind, s.kparam, Z[m1]);
-    if (have2) c2 = cov_to(s.vg, P, umax, m2, pt), zf2 = kind_f(kind, s.kparam, Z[m2]);
+    ca = cov_to(s.vg, P, umax, ma, pt);
+    za = kind_f(H.kind[ta], s.kparam, Z[ma]);
   }
-  const int nmax = max(n, __shfl_xor_sync(kFull, n, 16));
-  const double* U1 = UU + m1 * S;
-  const double* U2 = UU + m2 * S;
-  float2 A1[16], A2[16];
+  if (hb) {
+    const int64_t ti = H.ti[tb];
+    const double pt[3] = {s.tx[ti], s.ty[ti], s.tz[ti]};
+    cb = cov_to(s.vg, P, umax, mb, pt);
+    zb = kind_f(H.kind[tb], s.kparam, Z[mb]);
+  }
+  const double* Ua = UU + ma * S;
+  const double* Ub = UU + mb * S;
+  float2 A[32];
 #pragma unroll
-  for (int q2 = 0; q2 < 16; ++q2) {
-    const int qa = 2 * q2, qb = qa + 1;
-    const int ma = H.map[t][qa], mb = H.map[t][qb];
-    A1[q2].x = (have1 && qa < n) ? float(U1[ma]) : (qa == r1 ? 1.f : 0.f);
-    A1[q2].y = (have1 && qb < n) ? float(U1[mb]) : (qb == r1 ? 1.f : 0.f);
-    A2[q2].x = (have2 && qa < n) ? float(U2[ma]) : (qa == r2 ? 1.f : 0.f);
-    A2[q2].y = (have2 && qb < n) ? float(U2[mb]) : (qb == r2 ? 1.f : 0.f);
+  for (int q = 0; q < 32; ++q) {
+    A[q].x = (ha && q < na) ? float(Ua[H.map[ta][q]]) : (q == lane ? 1.f : 0.f);
+    A[q].y = (hb && q < nb) ? float(Ub[H.map[tb][q]]) : (q == lane ? 1.f : 0.f);
   }
-  float y1[3] = {float(c1), have1 ? 1.f : 0.f, float(zf1)};
-  float y2[3] = {float(c2), have2 ? 1.f : 0.f, float(zf2)};
-  float d1 = 1.f, d2 = 1.f;
-  bool weak = false;
+  float2 y[3] = {make_float2(float(ca), float(cb)), make_float2(ha ? 1.f : 0.f, hb ? 1.f : 0.f),
+                 make_float2(float(za), float(zb))};
+  float2 dme = make_float2(1.f, 1.f);
+  bool weak_a = false, weak_b = false;
   const float thr = 1e-5f * float(c0);
-  // LDL^T with the forward substitution of (c, 1, f) fused in.
-#pragma unroll
-  for (int k = 0; k < 32; ++k) {
-    if (k >= nmax) break;
-    const int b = k & 1;
-    float* col = W.colf[half][b];
-    col[r1] = slot_of(A1, k);
-    col[r2] = slot_of(A2, k);
-    if (k < 16) {
-      if (l == k) W.rhsf[half][b][0] = y1[0], W.rhsf[half][b][1] = y1[1], W.rhsf[half][b][2] = y1[2];
-    } else {
-      if (l == k - 16) W.rhsf[half][b][0] = y2[0], W.rhsf[half][b][1] = y2[1], W.rhsf[half][b][2] = y2[2];
-    }
-    __syncwarp();
-    const float d = col[k];
-    weak |= !(d > thr);
-    const float rd = rcp_approx(d);
-    const float f1 = r1 > k ? slot_of(A1, k) * rd : 0.f;
-    const float f2 = r2 > k ? slot_of(A2, k) * rd : 0.f;
-    if (k < 16) {
-      if (r1 == k) d1 = d;
-    } else {
-      if (r2 == k) d2 = d;
-    }
-    const float2 nf1 = make_float2(-f1, -f1), nf2 = make_float2(-f2, -f2);
-    // Pairs from the one holding slot k + 1 (slot k itself, when it is in
-    // the first pair, only changes entries that are not read again), then
-    // groups of four slots from a 16-byte aligned shared-memory line.
-    const int q2s = (k + 1) >> 1;
-    if (q2s & 1) {
-      const float2 cv = *reinterpret_cast<const float2*>(&col[2 * q2s]);
-      A1[q2s] = __ffma2_rn(nf1, cv, A1[q2s]);
-      A2[q2s] = __ffma2_rn(nf2, cv, A2[q2s]);
-    }
-#pragma unroll
-    for (int g = (q2s + 1) >> 1; g < 8; ++g) {
-      const float4 c4 = *reinterpret_cast<const float4*>(&col[4 * g]);
-      const float2 lo = make_float2(c4.x, c4.y), hi = make_float2(c4.z, c4.w);
-      A1[2 * g] = __ffma2_rn(nf1, lo, A1[2 * g]);
-      A2[2 * g] = __ffma2_rn(nf2, lo, A2[2 * g]);
-      A1[2 * g + 1] = __ffma2_rn(nf1, hi, A1[2 * g + 1]);
-      A2[2 * g + 1] = __ffma2_rn(nf2, hi, A2[2 * g + 1]);
-    }
-    const float4 rk = *reinterpret_cast<const float4*>(W.rhsf[half][b]);
-    y1[0] = fmaf(-f1, rk.x, y1[0]), y1[1] = fmaf(-f1, rk.y, y1[1]), y1[2] = fmaf(-f1, rk.z, y1[2]);
-    y2[0] = fmaf(-f2, rk.x, y2[0]), y2[1] = fmaf(-f2, rk.y, y2[1]), y2[2] = fmaf(-f2, rk.z, y2[2]);
-  }
-  // Backward sweep L^T x = D^-1 y, one row per step; lane i's slots q > i
-  // hold D_i L[q][i]: x_k = (y_k - sum_{q>k} slot_k[q] x_q) / D_k.
-  const float rd1 = rcp_approx(d1), rd2 = rcp_approx(d2);
-  float acc1[3] = {0.f, 0.f, 0.f}, acc2[3] = {0.f, 0.f, 0.f};
-  float x1[3] = {0.f, 0.f, 0.f}, x2[3] = {0.f, 0.f, 0.f};
-  const int src_base = half << 4;
-#pragma unroll
-  for (int k = 31; k >= 0; --k) {
-    if (k >= nmax) continue;
-    float z[3];
-    if (k < 16) {
-#pragma unroll
-      for (int v = 0; v < 3; ++v) z[v] = (y1[v] - acc1[v]) * rd1;
-    } else {
-#pragma unroll
-      for (int v = 0; v < 3; ++v) z[v] = (y2[v] - acc2[v]) * rd2;
-    }
-#pragma unroll
-    for (int v = 0; v < 3; ++v) z[v] = __shfl_sync(kFull, z[v], src_base + (k & 15));
-    if (k < 16) {
-      if (l == k) x1[0] = z[0], x1[1] = z[1], x1[2] = z[2];
-    } else {
-      if (l == k - 16) x2[0] = z[0], x2[1] = z[1], x2[2] = z[2];
-    }
-    const float s1 = slot_of(A1, k), s2 = slot_of(A2, k);
-#pragma unroll
-    for (int v = 0; v < 3; ++v) acc1[v] = fmaf(s1, z[v], acc1[v]), acc2[v] = fmaf(s2, z[v], acc2[v]);
-  }
-  // FP64 residuals r_v = v - C x_v from the FP64 table.
-  double xa[3], xb[3];
-#pragma unroll
-  for (int v = 0; v < 3; ++v) xa[v] = have1 ? double(x1[v]) : 0.0, xb[v] = have2 ? double(x2[v]) : 0.0;
-  W.xs[half][r1][0] = xa[0], W.xs[half][r1][1] = xa[1], W.xs[half][r1][2] = xa[2];
-  W.xs[half][r2][0] = xb[0], W.xs[half][r2][1] = xb[1], W.xs[half][r2][2] = xb[2];
+  const int n1 = min(nmax, 8), n2 = min(nmax, 16), n3 = min(nmax, 24);
+  eliminate2<32>(A, 0, n1, lane, W, y, dme, weak_a, weak_b, thr);
+  eliminate2<24>(A, n1, n2, lane, W, y, dme, weak_a, weak_b, thr);
+  eliminate2<16>(A, n2, n3, lane, W, y, dme, weak_a, weak_b, thr);
+  eliminate2<8>(A, n3, nmax, lane, W, y, dme, weak_a, weak_b, thr);
   __syncwarp();
-  double a1[3] = {0.0, 0.0, 0.0}, a2[3] = {0.0, 0.0, 0.0};
-  for (int j = 0; j < nmax; ++j) {
-    const int mj = H.map[t][j];  // 0 beyond this half's n, where x_j = 0
-    const double2 x01 = *reinterpret_cast<const double2*>(&W.xs[half][j][0]);
-    const double x2j = W.xs[half][j][2];
-    const double cj1 = U1[mj], cj2 = U2[mj];
-    a1[0] = fma(cj1, x01.x, a1[0]), a1[1] = fma(cj1, x01.y, a1[1]), a1[2] = fma(cj1, x2j, a1[2]);
-    a2[0] = fma(cj2, x01.x, a2[0]), a2[1] = fma(cj2, x01.y, a2[1]), a2[2] = fma(cj2, x2j, a2[2]);
+  // Backward sweep L^T x = D^-1 y, column-oriented: once x_k is known every
+  // row i < k takes D_i L[k][i] x_k (column i of the triangle) into acc_i,
+  // and x_i = (y_i - acc_i) / D_i.
+  const float2 rdme = rcp2(dme);
+  float2 acc[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+  float2 x[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+  const float2* my_col = W.lt + kLtPad + col_off(lane) - lane - 1;  // + k: D_i L[k][i]
+  for (int k = nmax - 1; k >= 0; --k) {
+    float2 z[3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      const float2 w = make_float2((y[v].x - acc[v].x) * rdme.x, (y[v].y - acc[v].y) * rdme.y);
+      z[v].x = __shfl_sync(kFull, w.x, k);
+      z[v].y = __shfl_sync(kFull, w.y, k);
+    }
+    if (lane == k) x[0] = z[0], x[1] = z[1], x[2] = z[2];
+    const float2 l = my_col[k];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) acc[v] = __ffma2_rn(l, z[v], acc[v]);
   }
+  __syncwarp();  // the triangle is dead: its space holds x for the residuals
+  const double xa[3] = {ha ? double(x[0].x) : 0.0, ha ? double(x[1].x) : 0.0, ha ? double(x[2].x) : 0.0};
+  const double xb[3] = {hb ? double(x[0].y) : 0.0, hb ? double(x[1].y) : 0.0, hb ? double(x[2].y) : 0.0};
+  W.xs[lane][0] = xa[0], W.xs[lane][1] = xa[1], W.xs[lane][2] = xa[2];
+  W.xs[lane][3] = xb[0], W.xs[lane][4] = xb[1], W.xs[lane][5] = xb[2];
+  __syncwarp();
+  // FP64 residuals r_v = v - C x_v from the FP64 table (rows past n have x = 0).
+  double aa[3] = {0.0, 0.0, 0.0}, ab[3] = {0.0, 0.0, 0.0};
+  for (int j = 0; j < nmax; ++j) {
+    const double2 x01 = *reinterpret_cast<const double2*>(&W.xs[j][0]);
+    const double2 x23 = *reinterpret_cast<const double2*>(&W.xs[j][2]);
+    const double2 x45 = *reinterpret_cast<const double2*>(&W.xs[j][4]);
+    const double cja = Ua[H.map[ta][j]], cjb = Ub[H.map[tb][j]];
+    aa[0] = fma(cja, x01.x, aa[0]), aa[1] = fma(cja, x01.y, aa[1]), aa[2] = fma(cja, x23.x, aa[2]);
+    ab[0] = fma(cjb, x23.y, ab[0]), ab[1] = fma(cjb, x45.x, ab[1]), ab[2] = fma(cjb, x45.y, ab[2]);
+  }
+  __syncwarp();
   double ra[3] = {0.0, 0.0, 0.0}, rb[3] = {0.0, 0.0, 0.0};
-  if (have1) ra[0] = c1 - a1[0], ra[1] = 1.0 - a1[1], ra[2] = zf1 - a1[2];
-  if (have2) rb[0] = c2 - a2[0], rb[1] = 1.0 - a2[1], rb[2] = zf2 - a2[2];
+  if (ha) ra[0] = ca - aa[0], ra[1] = 1.0 - aa[1], ra[2] = za - aa[2];
+  if (hb) rb[0] = cb - ab[0], rb[1] = 1.0 - ab[1], rb[2] = zb - ab[2];
   // Refinement tests, as in the per-system mixed kernel: the corrected forms
-  // err by about rho^2 C0 / D_min.
-  const double cmax = half_max(fmax(have1 ? fabs(c1) : 0.0, have2 ? fabs(c2) : 0.0));
-  const double zmax = half_max(fmax(have1 ? fabs(zf1) : 0.0, have2 ? fabs(zf2) : 0.0));
-  const double ic = 1.0 / fmax(cmax, 1e-300), iz = 1.0 / fmax(zmax, 1e-300);
-  const double rho1 = fmax(fmax(fabs(ra[0]) * ic, fabs(ra[1])), fabs(ra[2]) * iz);
-  const double rho2 = fmax(fmax(fabs(rb[0]) * ic, fabs(rb[1])), fabs(rb[2]) * iz);
-  const double rho = half_max(fmax(rho1, rho2));
-  const double dmin = -half_max(fmax(have1 ? -double(d1) : -1e300, have2 ? -double(d2) : -1e300));
-  double v[5] = {xa[0] + xa[1] * ra[0] + xb[0] + xb[1] * rb[0],
-                 xa[1] + xa[1] * ra[1] + xb[1] + xb[1] * rb[1],
-                 zf1 * xa[0] + xa[2] * ra[0] + zf2 * xb[0] + xb[2] * rb[0],
-                 zf1 * xa[1] + xa[2] * ra[1] + zf2 * xb[1] + xb[2] * rb[1],
-                 c1 * xa[0] + xa[0] * ra[0] + c2 * xb[0] + xb[0] * rb[0]};
+  // err by about rho^2 C0 / D_min (rho the relative residual).
+  const float cmax_a = warp_maxf(ha ? float(fabs(ca)) : 0.f), cmax_b = warp_maxf(hb ? float(fabs(cb)) : 0.f);
+  const float zmax_a = warp_maxf(ha ? float(fabs(za)) : 0.f), zmax_b = warp_maxf(hb ? float(fabs(zb)) : 0.f);
+  const double ica = 1.0 / fmax(double(cmax_a), 1e-300), iza = 1.0 / fmax(double(zmax_a), 1e-300);
+  const double icb = 1.0 / fmax(double(cmax_b), 1e-300), izb = 1.0 / fmax(double(zmax_b), 1e-300);
+  const float rho_a = warp_maxf(float(fmax(fmax(fabs(ra[0]) * ica, fabs(ra[1])), fabs(ra[2]) * iza)));
+  const float rho_b = warp_maxf(float(fmax(fmax(fabs(rb[0]) * icb, fabs(rb[1])), fabs(rb[2]) * izb)));
+  const float dmin_a = -warp_maxf(ha ? -dme.x : -3.0e38f), dmin_b = -warp_maxf(hb ? -dme.y : -3.0e38f);
+  double va[5] = {xa[0] + xa[1] * ra[0], xa[1] + xa[1] * ra[1], za * xa[0] + xa[2] * ra[0], za * xa[1] + xa[2] * ra[1],
+                  ca * xa[0] + xa[0] * ra[0]};
+  double vb[5] = {xb[0] + xb[1] * rb[0], xb[1] + xb[1] * rb[1], zb * xb[0] + xb[2] * rb[0], zb * xb[1] + xb[2] * rb[1],
+                  cb * xb[0] + xb[0] * rb[0]};
 #pragma unroll
-  for (int q = 0; q < 5; ++q)
-#pragma unroll
-    for (int o = 8; o > 0; o >>= 1) v[q] += __shfl_xor_sync(kFull, v[q], o);
-  const unsigned wb = __ballot_sync(kFull, weak);
-  const bool weak_half = ((wb >> (half << 4)) & 0xffffu) != 0;
-  if (go && l == 0) {
-    if (weak_half || !(rho * rho * c0 / dmin <= 1e-8) || !(v[1] > 0.0) || !(fabs(v[0]) < 1e30))
-      a.redo[atomicAdd(reinterpret_cast<unsigned long long*>(a.redo_len), 1ull)] = ti;
-    else
-      epilogue(s, kind, ti, v, n, 0);
+  for (int q = 0; q < 5; ++q) va[q] = warp_sum(va[q]), vb[q] = warp_sum(vb[q]);
+  if (lane < 2) {
+    const bool is_a = lane == 0;
+    const bool go = is_a ? go_a : go_b;
+    if (go) {
+      const int64_t ti = H.ti[is_a ? ta : tb];
+      const double* v = is_a ? va : vb;
+      const double rho = is_a ? rho_a : rho_b, dmin = is_a ? dmin_a : dmin_b;
+      const bool weak = is_a ? weak_a : weak_b;
+      if (weak || !(rho * rho * c0 / dmin <= 1e-8) || !(v[1] > 0.0) || !(fabs(v[0]) < 1e30))
+        a.redo[atomicAdd(reinterpret_cast<unsigned long long*>(a.redo_len), 1ull)] = ti;
+      else
+        epilogue(s, H.kind[is_a ? ta : tb], ti, v, is_a ? na : nb, 0);
+    }
   }
   __syncwarp();
 }
