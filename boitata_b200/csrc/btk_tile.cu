@@ -78,8 +78,7 @@ struct WarpMixed {
     float2 lt[kLtPad + kLtLen + kLtPad];
     double xs[32][6];  // after the backward sweep: x of row j (a: c, 1, f; b: c, 1, f)
   };
-  float2 piv[2];
-  float2 rhs[2][4];
+  float2 prhs[2][4];  // [buffer]: pivot, y_c, y_1, y_f of the pivot row
 };
 
 // Start of column k in the packed triangle (see WarpMixed).
@@ -338,34 +337,32 @@ __device__ __forceinline__ float2 rcp2(float2 d) { return make_float2(rcp_approx
 // slots that can still hold live columns, as in the FP64 eliminate().
 template <int W>
 __device__ __forceinline__ void eliminate2(float2 (&A)[32], int k0, int k1, int lane, WarpMixed& Ws,
-                                           float2 (&y)[3], float2& dme, bool& weak_a, bool& weak_b, float thr) {
+                                           float2 (&y)[3], float2& dme, float2& dmin) {
+  float2* col = Ws.lt + kLtPad + col_off(k0);
   for (int k = k0; k < k1; ++k) {
     const int b = k & 1;
-    float2* col = Ws.lt + kLtPad + col_off(k);
     if (lane > k) col[lane - k - 1] = A[0];
-    if (lane == k) {
-      Ws.piv[b] = A[0];
-      Ws.rhs[b][0] = y[0], Ws.rhs[b][1] = y[1], Ws.rhs[b][2] = y[2];
+    if (lane == k) {  // pivot and right-hand side, two 16-byte stores
+      reinterpret_cast<float4*>(Ws.prhs[b])[0] = make_float4(A[0].x, A[0].y, y[0].x, y[0].y);
+      reinterpret_cast<float4*>(Ws.prhs[b])[1] = make_float4(y[1].x, y[1].y, y[2].x, y[2].y);
     }
     __syncwarp();
-    const float2 d = Ws.piv[b];
-    weak_a |= !(d.x > thr);
-    weak_b |= !(d.y > thr);
-    if (lane == k) dme = d;
-    const float2 rd = rcp2(d);
-    const float2 f = lane > k ? make_float2(A[0].x * rd.x, A[0].y * rd.y) : make_float2(0.f, 0.f);
-    const float2 nf = make_float2(-f.x, -f.y);
+    const float4 p0 = reinterpret_cast<const float4*>(Ws.prhs[b])[0];
+    const float4 p1 = reinterpret_cast<const float4*>(Ws.prhs[b])[1];
+    dmin.x = fminf(dmin.x, p0.x), dmin.y = fminf(dmin.y, p0.y);
+    if (lane == k) dme = make_float2(p0.x, p0.y);
+    const float2 nrd = make_float2(rcp_approx(-p0.x), rcp_approx(-p0.y));
+    const float2 nf = lane > k ? __fmul2_rn(A[0], nrd) : make_float2(0.f, 0.f);  // -L[lane][k]
 #pragma unroll
     for (int q = 0; q < W; q += 2) {
       const float4 c4 = *reinterpret_cast<const float4*>(&col[q]);
       A[q] = __ffma2_rn(nf, make_float2(c4.x, c4.y), A[q + 1]);
       A[q + 1] = q + 2 < 32 ? __ffma2_rn(nf, make_float2(c4.z, c4.w), A[q + 2]) : make_float2(0.f, 0.f);
     }
-    const float4 r01 = *reinterpret_cast<const float4*>(&Ws.rhs[b][0]);
-    const float2 r2 = Ws.rhs[b][2];
-    y[0] = __ffma2_rn(nf, make_float2(r01.x, r01.y), y[0]);
-    y[1] = __ffma2_rn(nf, make_float2(r01.z, r01.w), y[1]);
-    y[2] = __ffma2_rn(nf, r2, y[2]);
+    y[0] = __ffma2_rn(nf, make_float2(p0.z, p0.w), y[0]);
+    y[1] = __ffma2_rn(nf, make_float2(p1.x, p1.y), y[1]);
+    y[2] = __ffma2_rn(nf, make_float2(p1.z, p1.w), y[2]);
+    col += (32 - k) & ~1;  // the next column: this one's length rounded up to even
   }
 }
 
@@ -404,14 +401,15 @@ __device__ void solve_mixed(const TileDev& a, const TileHead& H, const double* P
   }
   float2 y[3] = {make_float2(float(ca), float(cb)), make_float2(ha ? 1.f : 0.f, hb ? 1.f : 0.f),
                  make_float2(float(za), float(zb))};
-  float2 dme = make_float2(1.f, 1.f);
-  bool weak_a = false, weak_b = false;
-  const float thr = 1e-5f * float(c0);
+  float2 dme = make_float2(1.f, 1.f), pmin = make_float2(3.0e38f, 3.0e38f);
   const int n1 = min(nmax, 8), n2 = min(nmax, 16), n3 = min(nmax, 24);
-  eliminate2<32>(A, 0, n1, lane, W, y, dme, weak_a, weak_b, thr);
-  eliminate2<24>(A, n1, n2, lane, W, y, dme, weak_a, weak_b, thr);
-  eliminate2<16>(A, n2, n3, lane, W, y, dme, weak_a, weak_b, thr);
-  eliminate2<8>(A, n3, nmax, lane, W, y, dme, weak_a, weak_b, thr);
+  eliminate2<32>(A, 0, n1, lane, W, y, dme, pmin);
+  eliminate2<24>(A, n1, n2, lane, W, y, dme, pmin);
+  eliminate2<16>(A, n2, n3, lane, W, y, dme, pmin);
+  eliminate2<8>(A, n3, nmax, lane, W, y, dme, pmin);
+  // NaN or at most 1e-5 C0 among the FP32 pivots: the FP64 form takes it.
+  const float thr = 1e-5f * float(c0);
+  const bool weak_a = !(pmin.x > thr), weak_b = !(pmin.y > thr);
   __syncwarp();
   // Backward sweep L^T x = D^-1 y, column-oriented: once x_k is known every
   // row i < k takes D_i L[k][i] x_k (column i of the triangle) into acc_i,
