@@ -280,7 +280,7 @@ __global__ void k_search(SearchDev sp, GridDev g, const double* __restrict__ tx,
           const int j = __ffs(pending) - 1;
           pending &= pending - 1;
           const int yj = __shfl_sync(kFull, y, j), zj = __shfl_sync(kFull, z, j);
-#pragma unroll
+#pragma unroll 1  // one copy of the candidate loop: the kernel is instruction-fetch bound
           for (int seg = 0; seg < 2; ++seg) {
             const uint32_t a = __shfl_sync(kFull, seg ? a2 : a1, j), e = __shfl_sync(kFull, seg ? e2 : e1, j);
             if (a >= e) continue;
@@ -299,6 +299,7 @@ __global__ void k_search(SearchDev sp, GridDev g, const double* __restrict__ tx,
               }
               __syncwarp();
               if (need) {
+#pragma unroll 1
                 for (int c = 0; c < nc; ++c) {
                   const double d2 = d2_exact(S.cp[0][c], S.cp[1][c], S.cp[2][c], q[0], q[1], q[2]);
                   if (d2 <= thr) {
