@@ -143,6 +143,12 @@ struct btk_ctx {
   DevBuf<int8_t> loo_sst;
   DevBuf<double> g_part, g_sums, g_val;
 
+  // spatial order of caller-supplied targets (btk_order.cu)
+  DevBuf<uint64_t> ord_keys;
+  DevBuf<int64_t> ord_vals;
+  DevBuf<uint8_t> ord_temp;
+  DevBuf<double> ord_part, ord_b6;
+
   Tuning tuning;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -353,6 +359,9 @@ int ensure_scratch(btk_ctx* ctx, int64_t m) {
   return BTK_OK;
 }
 
+// Fewest caller-supplied targets that are put in spatial order first.
+constexpr int64_t kOrderMin = 2048;
+
 // Search then solve for m targets whose coordinates are device SoA arrays.
 int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const double* ty, const double* tz,
              const int64_t* perm, int64_t nwork, int loo, int32_t kind, double kparam, int32_t precision,
@@ -364,6 +373,18 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
   int rc = ensure_scratch(ctx, m);
   if (rc) return rc;
   Launch L = ctx->launch(s);
+  if (!perm && m >= kOrderMin) {  // caller's order: sort into Morton order so warps and tiles are compact
+    const size_t tb = morton_temp_bytes(m);
+    if (tb == 0) return fail(ctx, BTK_ECUDA, "radix sort sizing failed");
+    CK(ctx->ord_keys.grow(2 * size_t(m)));
+    CK(ctx->ord_vals.grow(2 * size_t(m)));
+    CK(ctx->ord_temp.grow(tb));
+    CK(ctx->ord_part.grow(6 * 1024));
+    CK(ctx->ord_b6.grow(6));
+    CK(launch_morton_order(L, m, tx, ty, tz, ctx->ord_part.p, ctx->ord_b6.p, ctx->ord_keys.p, ctx->ord_vals.p,
+                           ctx->ord_temp.p, tb, &perm));
+    nwork = m;
+  }
   ctx->mark(0, L.stream);
   CK(launch_search(L, ctx->spd, ctx->gd, tx, ty, tz, perm, nwork, loo, ctx->nbr.p, ctx->cnt.p, ctx->sst.p));
   ctx->mark(1, L.stream);

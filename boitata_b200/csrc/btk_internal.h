@@ -162,6 +162,14 @@ cudaError_t launch_solve_redo_pairs(const Launch& L, const SolveDev& a);
 // (and, mixed, a.redo) for the per-system kernels. Counts must start at 0.
 cudaError_t launch_tile(const Launch& L, const TileDev& a, bool mixed);
 
+// Work-slot permutation of m caller-supplied targets in Morton order of
+// their positions (btk_order.cu). keys and vals hold 2m entries each; temp
+// holds morton_temp_bytes(m). *perm points into vals on return.
+size_t morton_temp_bytes(int64_t m);
+cudaError_t launch_morton_order(const Launch& L, int64_t m, const double* x, const double* y, const double* z,
+                                double* partial, double* b6, uint64_t* keys, int64_t* vals, void* temp,
+                                size_t temp_bytes, const int64_t** perm);
+
 // Leave-one-out loss and gradient; sums[stride] receives the column sums.
 cudaError_t launch_loo_grad(const Launch& L, const GradDev& a, double* sums);
 

@@ -97,3 +97,19 @@ def test_graph_replay_matches_the_call_and_autotune_keeps_results():
     got = predict(est, geo, N.MIXED, outs, oc)
     for a, b in zip(got, predict(est, geo, N.MIXED, outs, oc)):
         np.testing.assert_array_equal(a, b)
+
+
+def test_caller_order_does_not_change_results():
+    """btk_predict sorts caller-supplied targets into Morton order; the FP64 form gives the same bits for any
+    input order, and a result lands at its own target's index."""
+    w = W.c2()
+    rng = np.random.default_rng(7)
+    t = np.column_stack([rng.uniform(50, 450, 20000), rng.uniform(50, 450, 20000), rng.uniform(10, 240, 20000)])
+    est = OrdinaryKriging(w.variogram, w.search).fit(w.coords, w.values)
+    a = est.predict_full(t)
+    perm = rng.permutation(len(t))
+    b = est.predict_full(t[perm])
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(len(perm))
+    for k in a:
+        np.testing.assert_array_equal(np.asarray(b[k])[inv], np.asarray(a[k]))
