@@ -37,7 +37,7 @@ def get_tuning(ctx):
     t = N.TuningC()
     ctx.check(ctx._lib.btk_get_tuning(ctx.handle, ctypes.byref(t)), "tuning")
     return {"samples_per_cell": t.samples_per_cell, "tile": tuple(t.tile), "search_warps": t.search_warps,
-            "solve_blocks_per_sm": t.solve_blocks_per_sm, "tile_union": t.tile_union}
+            "solve_blocks_per_sm": t.solve_blocks_per_sm, "tile_union": t.tile_union, "host_chunk": t.host_chunk}
 
 
 def set_tuning(ctx, cfg):
@@ -48,6 +48,7 @@ def set_tuning(ctx, cfg):
     t.search_warps = int(cfg["search_warps"])
     t.solve_blocks_per_sm = int(cfg["solve_blocks_per_sm"])
     t.tile_union = int(cfg.get("tile_union", 72))
+    t.host_chunk = int(cfg.get("host_chunk", 0))
     ctx.check(ctx._lib.btk_set_tuning(ctx.handle, ctypes.byref(t)), "tuning")
 
 

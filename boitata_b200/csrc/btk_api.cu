@@ -143,6 +143,10 @@ struct btk_ctx {
   DevBuf<int8_t> loo_sst;
   DevBuf<double> g_part, g_sums, g_val;
 
+  // pipelined host calls: copies in and out on their own streams
+  cudaStream_t up = nullptr, down = nullptr;
+  cudaEvent_t cev[16] = {};
+
   // spatial order of caller-supplied targets (btk_order.cu)
   DevBuf<uint64_t> ord_keys;
   DevBuf<int64_t> ord_vals;
@@ -381,7 +385,14 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
     CK(ctx->ord_temp.grow(tb));
     CK(ctx->ord_part.grow(6 * 1024));
     CK(ctx->ord_b6.grow(6));
-    CK(launch_morton_order(L, m, tx, ty, tz, ctx->ord_part.p, ctx->ord_b6.p, ctx->ord_keys.p, ctx->ord_vals.p,
+    // World axes weighted by the search metric's stretch along each (column
+    // norms of the search frame): key cells stay aligned with a block lattice
+    // but are as long, in search distance, along every axis.
+    double wgt[3];
+    for (int d = 0; d < 3; ++d)
+      wgt[d] = std::sqrt(ctx->spd.frame[d] * ctx->spd.frame[d] + ctx->spd.frame[3 + d] * ctx->spd.frame[3 + d] +
+                         ctx->spd.frame[6 + d] * ctx->spd.frame[6 + d]);
+    CK(launch_morton_order(L, m, tx, ty, tz, wgt, ctx->ord_part.p, ctx->ord_b6.p, ctx->ord_keys.p, ctx->ord_vals.p,
                            ctx->ord_temp.p, tb, &perm));
     nwork = m;
   }
@@ -587,6 +598,10 @@ void btk_destroy(btk_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream), cudaStreamDestroy(ctx->stream);
   for (cudaEvent_t e : ctx->ev)
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : ctx->cev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->up) cudaStreamSynchronize(ctx->up), cudaStreamDestroy(ctx->up);
+  if (ctx->down) cudaStreamSynchronize(ctx->down), cudaStreamDestroy(ctx->down);
   if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
   if (ctx->graph) cudaGraphDestroy(ctx->graph);
   delete ctx;
@@ -599,6 +614,7 @@ int btk_get_tuning(const btk_ctx* ctx, btk_tuning* out) {
   out->search_warps = ctx->tuning.search_warps;
   out->solve_blocks_per_sm = ctx->tuning.solve_blocks_per_sm;
   out->tile_union = ctx->tuning.tile_union;
+  out->host_chunk = ctx->tuning.host_chunk;
   return BTK_OK;
 }
 
@@ -613,12 +629,14 @@ int btk_set_tuning(btk_ctx* ctx, const btk_tuning* t) {
   if (t->solve_blocks_per_sm < 0) return fail(ctx, BTK_EINVAL, "solve_blocks_per_sm must be >= 0");
   if (t->tile_union != 0 && (t->tile_union < 32 || t->tile_union > 255))
     return fail(ctx, BTK_EINVAL, "tile_union must be 0 or in 32..255");
+  if (t->host_chunk < 0) return fail(ctx, BTK_EINVAL, "host_chunk must be >= 0");
   if (!(t->samples_per_cell > 0.0 && t->samples_per_cell <= 1e6))
     return fail(ctx, BTK_EINVAL, "samples_per_cell must be > 0");
   for (int a = 0; a < 3; ++a) ctx->tuning.tile[a] = t->tile[a];
   ctx->tuning.search_warps = t->search_warps;
   ctx->tuning.solve_blocks_per_sm = t->solve_blocks_per_sm;
   ctx->tuning.tile_union = t->tile_union;
+  ctx->tuning.host_chunk = t->host_chunk;
   if (t->samples_per_cell != ctx->ppc) {
     ctx->ppc = t->samples_per_cell;
     if (ctx->fitted) {
@@ -769,6 +787,71 @@ int btk_predict_device(btk_ctx* ctx, int64_t m, const double* d_xyz, int32_t kin
                   kparam, precision, d_out);
 }
 
+namespace {
+
+// Host targets in, host outputs out, in chunks of tuning.host_chunk targets
+// (at most 8 chunks; 0: one): the copy of chunk c + 1 in and of chunk c - 1
+// out overlap chunk c's search and solve. Each chunk is a run_path of its own over the
+// context's scratch, which the compute stream serialises; chunks write
+// disjoint slices of the staged inputs and outputs.
+int predict_host(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds, int32_t kind, double kparam,
+                 int32_t precision, const btk_outputs* out) {
+  int64_t chunk = ctx->tuning.host_chunk > 0 ? int64_t(ctx->tuning.host_chunk) : m;
+  if ((m + chunk - 1) / chunk > 8) chunk = (m + 7) / 8;
+  const int64_t nc = (m + chunk - 1) / chunk;
+  const size_t mm = size_t(m);
+  CK(ctx->aos.grow(3 * mm));
+  CK(ctx->txyz.grow(3 * mm));
+  if (kinds) CK(ctx->kinds.grow(mm));
+  btk_outputs d{};
+  int rc = host_outputs(ctx, m, out, &d);
+  if (rc) return rc;
+  if (!ctx->up) CK(cudaStreamCreateWithFlags(&ctx->up, cudaStreamNonBlocking));
+  if (!ctx->down) CK(cudaStreamCreateWithFlags(&ctx->down, cudaStreamNonBlocking));
+  for (cudaEvent_t& e : ctx->cev)
+    if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaEvent_t* in_done = ctx->cev;
+  cudaEvent_t* out_ready = ctx->cev + 8;
+  for (int64_t c = 0; c < nc; ++c) {
+    const int64_t off = c * chunk, mc = std::min(chunk, m - off);
+    CK(cudaMemcpyAsync(ctx->aos.p + 3 * off, xyz + 3 * off, 3 * size_t(mc) * sizeof(double), cudaMemcpyHostToDevice,
+                       ctx->up));
+    if (kinds) CK(cudaMemcpyAsync(ctx->kinds.p + off, kinds + off, size_t(mc), cudaMemcpyHostToDevice, ctx->up));
+    CK(cudaEventRecord(in_done[c], ctx->up));
+  }
+  double* t = ctx->txyz.p;
+  for (int64_t c = 0; c < nc; ++c) {
+    const int64_t off = c * chunk, mc = std::min(chunk, m - off);
+    CK(cudaStreamWaitEvent(ctx->stream, in_done[c], 0));
+    int64_t b = (mc + 255) / 256;
+    if (b > int64_t(ctx->sm_count) * 8) b = int64_t(ctx->sm_count) * 8;
+    k_split_xyz<<<int(b), 256, 0, ctx->stream>>>(mc, ctx->aos.p + 3 * off, t + off, t + m + off, t + 2 * m + off);
+    ++ctx->launches;
+    CK(cudaGetLastError());
+    btk_outputs dc{d.value + off, d.variance + off, d.lagrange + off, d.n_used + off, d.status + off};
+    if ((rc = run_path(ctx, ctx->stream, mc, t + off, t + m + off, t + 2 * m + off, nullptr, mc, 0, kind, kparam,
+                       precision, &dc, kinds ? ctx->kinds.p + off : nullptr)))
+      return rc;
+    CK(cudaEventRecord(out_ready[c], ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->down, out_ready[c], 0));
+    const size_t n = size_t(mc);
+    CK(cudaMemcpyAsync(out->value + off, dc.value, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->down));
+    if (out->variance)
+      CK(cudaMemcpyAsync(out->variance + off, dc.variance, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->down));
+    if (out->lagrange)
+      CK(cudaMemcpyAsync(out->lagrange + off, dc.lagrange, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->down));
+    if (out->n_used)
+      CK(cudaMemcpyAsync(out->n_used + off, dc.n_used, n * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->down));
+    if (out->status)
+      CK(cudaMemcpyAsync(out->status + off, dc.status, n * sizeof(int8_t), cudaMemcpyDeviceToHost, ctx->down));
+  }
+  CK(cudaStreamSynchronize(ctx->down));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return BTK_OK;
+}
+
+}  // namespace
+
 int btk_predict(btk_ctx* ctx, int64_t m, const double* xyz, int32_t kind, double kparam, int32_t precision,
                 const btk_outputs* out) {
   int rc = need_fit(ctx);
@@ -777,12 +860,7 @@ int btk_predict(btk_ctx* ctx, int64_t m, const double* xyz, int32_t kind, double
   if (m < 0 || (m > 0 && !xyz)) return fail(ctx, BTK_EINVAL, "targets are required");
   if (m == 0) return BTK_OK;
   CK(cudaSetDevice(ctx->device));
-  if ((rc = upload_targets(ctx, m, xyz))) return rc;
-  btk_outputs d{};
-  if ((rc = host_outputs(ctx, m, out, &d))) return rc;
-  const double* t = ctx->txyz.p;
-  if ((rc = run_path(ctx, nullptr, m, t, t + m, t + 2 * m, nullptr, m, 0, kind, kparam, precision, &d))) return rc;
-  return copy_out(ctx, m, &d, out);
+  return predict_host(ctx, m, xyz, nullptr, kind, kparam, precision, out);
 }
 
 int btk_predict_kinds_device(btk_ctx* ctx, int64_t m, const double* d_xyz, const int8_t* d_kinds, double kparam,
@@ -806,16 +884,7 @@ int btk_predict_kinds(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* 
     if (kinds[i] < BTK_ORDINARY || kinds[i] > BTK_INDICATOR) return fail(ctx, BTK_EINVAL, "unknown kriging kind");
   if (m == 0) return BTK_OK;
   CK(cudaSetDevice(ctx->device));
-  if ((rc = upload_targets(ctx, m, xyz))) return rc;
-  CK(ctx->kinds.grow(size_t(m)));
-  CK(cudaMemcpyAsync(ctx->kinds.p, kinds, size_t(m), cudaMemcpyHostToDevice, ctx->stream));
-  btk_outputs d{};
-  if ((rc = host_outputs(ctx, m, out, &d))) return rc;
-  const double* t = ctx->txyz.p;
-  if ((rc = run_path(ctx, nullptr, m, t, t + m, t + 2 * m, nullptr, m, 0, BTK_ORDINARY, kparam, precision, &d,
-                     ctx->kinds.p)))
-    return rc;
-  return copy_out(ctx, m, &d, out);
+  return predict_host(ctx, m, xyz, kinds, BTK_ORDINARY, kparam, precision, out);
 }
 
 int btk_predict_geometry_device(btk_ctx* ctx, const btk_geometry* g, int32_t kind, double kparam, int32_t precision,

@@ -115,6 +115,7 @@ struct Tuning {
   int search_warps = 0;          // warps per search CTA; 0: 4 (2 with 64 list slots)
   int solve_blocks_per_sm = 0;   // resident solve CTAs per SM; 0: as many as fit
   int tile_union = 72;           // tile-shared solve: most distinct samples per tile; 0: per-system solve
+  int host_chunk = 0;            // host-buffer calls: targets per pipelined chunk; 0: one chunk
 };
 
 struct Launch {
@@ -163,12 +164,13 @@ cudaError_t launch_solve_redo_pairs(const Launch& L, const SolveDev& a);
 cudaError_t launch_tile(const Launch& L, const TileDev& a, bool mixed);
 
 // Work-slot permutation of m caller-supplied targets in Morton order of
-// their positions (btk_order.cu). keys and vals hold 2m entries each; temp
-// holds morton_temp_bytes(m). *perm points into vals on return.
+// their positions, axis d weighted by w[d] (btk_order.cu). keys and vals
+// hold 2m entries each; temp holds morton_temp_bytes(m). *perm points into
+// vals on return.
 size_t morton_temp_bytes(int64_t m);
 cudaError_t launch_morton_order(const Launch& L, int64_t m, const double* x, const double* y, const double* z,
-                                double* partial, double* b6, uint64_t* keys, int64_t* vals, void* temp,
-                                size_t temp_bytes, const int64_t** perm);
+                                const double w[3], double* partial, double* b6, uint64_t* keys, int64_t* vals,
+                                void* temp, size_t temp_bytes, const int64_t** perm);
 
 // Leave-one-out loss and gradient; sums[stride] receives the column sums.
 cudaError_t launch_loo_grad(const Launch& L, const GradDev& a, double* sums);

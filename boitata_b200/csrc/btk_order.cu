@@ -2,9 +2,9 @@
 // the caller's order on CPU threads (crates/estimation/src/batch.rs:15-38);
 // here a search warp serves 32 consecutive work slots and a solve tile 16, so
 // targets that arrive in row-major order (a block model flattened x fastest)
-// would put 80 m strips into one warp. A Morton key over the targets'
-// bounding box (21 bits per axis, one scale for all three axes so that key
-// cells are cubes) is sorted on the device with CUB's radix sort, and the
+// would put 80 m strips into one warp. A Morton key (21 bits per axis) over
+// the targets' bounding box, each axis weighted by the caller's w[d] with one
+// scale for all three, is sorted on the device with CUB's radix sort, and the
 // sorted indices are the work-slot permutation. Results are written by target
 // index, so the order is invisible to the caller.
 #include <cub/device/device_radix_sort.cuh>
@@ -26,15 +26,16 @@ __device__ __forceinline__ uint64_t spread3(uint32_t v) {
 }
 
 __global__ void k_morton(int64_t m, const double* __restrict__ x, const double* __restrict__ y,
-                         const double* __restrict__ z, const double* __restrict__ b6, uint64_t* __restrict__ key,
-                         int64_t* __restrict__ idx) {
-  const double ext = fmax(fmax(b6[3] - b6[0], b6[4] - b6[1]), b6[5] - b6[2]);
+                         const double* __restrict__ z, Frame9 w, const double* __restrict__ b6,
+                         uint64_t* __restrict__ key, int64_t* __restrict__ idx) {
+  const double ext = fmax(fmax((b6[3] - b6[0]) * w.m[0], (b6[4] - b6[1]) * w.m[1]), (b6[5] - b6[2]) * w.m[2]);
   const double s = ext > 0.0 ? 2097151.0 / ext : 0.0;
+  const double sx = s * w.m[0], sy = s * w.m[1], sz = s * w.m[2];
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < m; i += int64_t(gridDim.x) * blockDim.x) {
     // fmax maps NaN to the low edge; clamping keeps every key in 63 bits
-    const uint32_t qx = uint32_t(fmin(fmax((x[i] - b6[0]) * s, 0.0), 2097151.0));
-    const uint32_t qy = uint32_t(fmin(fmax((y[i] - b6[1]) * s, 0.0), 2097151.0));
-    const uint32_t qz = uint32_t(fmin(fmax((z[i] - b6[2]) * s, 0.0), 2097151.0));
+    const uint32_t qx = uint32_t(fmin(fmax((x[i] - b6[0]) * sx, 0.0), 2097151.0));
+    const uint32_t qy = uint32_t(fmin(fmax((y[i] - b6[1]) * sy, 0.0), 2097151.0));
+    const uint32_t qz = uint32_t(fmin(fmax((z[i] - b6[2]) * sz, 0.0), 2097151.0));
     key[i] = spread3(qx) | (spread3(qy) << 1) | (spread3(qz) << 2);
     idx[i] = i;
   }
@@ -51,14 +52,16 @@ size_t morton_temp_bytes(int64_t m) {
 }
 
 cudaError_t launch_morton_order(const Launch& L, int64_t m, const double* x, const double* y, const double* z,
-                                double* partial, double* b6, uint64_t* keys, int64_t* vals, void* temp,
-                                size_t temp_bytes, const int64_t** perm) {
+                                const double w[3], double* partial, double* b6, uint64_t* keys, int64_t* vals,
+                                void* temp, size_t temp_bytes, const int64_t** perm) {
+  Frame9 wk{};
+  for (int d = 0; d < 3; ++d) wk.m[d] = w[d] > 0.0 ? w[d] : 1.0;
   cudaError_t e = launch_bounds(L, m, x, y, z, partial, b6);
   if (e != cudaSuccess) return e;
   int64_t b = (m + 255) / 256;
   if (b > int64_t(L.sm_count) * 8) b = int64_t(L.sm_count) * 8;
   if (b < 1) b = 1;
-  k_morton<<<int(b), 256, 0, L.stream>>>(m, x, y, z, b6, keys, vals);
+  k_morton<<<int(b), 256, 0, L.stream>>>(m, x, y, z, wk, b6, keys, vals);
   ++*L.counter;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   cub::DoubleBuffer<uint64_t> k(keys, keys + m);

@@ -125,13 +125,16 @@ typedef struct {
  * samples per cell, the block-model tile one search warp serves (product
  * 32), warps per search CTA, resident solve CTAs per SM (0: defaults), and
  * the most distinct samples the tile-shared solve tabulates for 16
- * consecutive targets (32..255; 0: every system assembles its own matrix). */
+ * consecutive targets (32..255; 0: every system assembles its own matrix),
+ * and for calls with host buffers the targets per chunk of the copy/compute
+ * pipeline (0: the whole call at once; at most 8 chunks). */
 typedef struct {
   double samples_per_cell;
   int32_t tile[3];
   int32_t search_warps;
   int32_t solve_blocks_per_sm;
   int32_t tile_union;
+  int32_t host_chunk;
 } btk_tuning;
 
 typedef struct btk_ctx btk_ctx;
