@@ -33,6 +33,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# DRAM bytes per system of k_tile<mixed>: (132,788,224 read + 13,551,104 written) / 800,000 systems in the
+# ncu capture of profiles/k_tile_c2_800k_blocks.md.
+TILE_DRAM_BYTES_PER_SYSTEM = (132788224 + 13551104) / 800000
+
 METRIC = "OK blocks/s @3.2M blocks n≤32: mixed vs FP64 GPU at ≤1e-6 rel; LOO-grad ms"
 UNIT = "blocks/s"
 
@@ -369,9 +373,14 @@ def main():
         "phases_ms": {"mixed": {"search": phases[N.MIXED][0], "solve": phases[N.MIXED][1],
                                 "fp64_resolve": phases[N.MIXED][2]},
                       "fp64": {"search": phases[N.FP64][0], "solve": phases[N.FP64][1]}},
-        "roofline": {"bound": "fp64", "kernel": "k_solve_mixed<1> (assembly FP64, factor FP32)",
+        "roofline": {"bound": "fp64", "kernel": "k_tile<mixed> (tile-shared FP64 covariance table, FP32 factor, "
+                                               "FP64 refinement) and the per-system kernels for its leftovers",
                      "achieved": flops / (solve_ms * 1e-3) / 1e12, "peak": peak64 / 1e12, "unit": "TFLOP/s",
-                     "frac": (flops / (solve_ms * 1e-3)) / peak64, "traffic": None,
+                     "frac": (flops / (solve_ms * 1e-3)) / peak64,
+                     "traffic": TILE_DRAM_BYTES_PER_SYSTEM * m,
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of k_tile<mixed> from one ncu "
+                                       "capture at 800,000 blocks (profiles/k_tile_c2_800k_blocks.md), scaled by "
+                                       "the systems per launch (the per-target streams grow in proportion)",
                      "peak_source": "measured in this run: CUDA-core FP64 FMA loop (btk_peak_flops)",
                      "fp32_peak": peak32 / 1e12,
                      "algorithmic_flops_per_step": flops},
