@@ -1,9 +1,9 @@
 // ORACLE — test infrastructure only.
 //
 // A CPU restatement, in plain C++17, of boitatá's ordinary / simple /
-// indicator kriging path (gstvschlz/boitata, workspace 0.7.1). It is the
-// checker for the CUDA engine in boitata_b200/ and the timed CPU baseline
-// ("port") of bench.py. Nothing in the product links, loads or calls it.
+// indicator kriging path (gstvschlz/boitata, workspace 0.7.1). The tests
+// compare the CUDA engine in boitata_b200/ with it, and bench.py times it as
+// the CPU baseline ("port"). Nothing in the product links, loads or calls it.
 //
 // Every function cites the reference file:line it follows. Floating-point
 // evaluation order follows the reference wherever the result must be

@@ -3,7 +3,8 @@
 ctypes access to the C++ restatement of the reference kriging path
 (oracle/boitata_oracle.cpp, built into oracle/_build/liboracle.so by
 oracle/Makefile). Only tests/, __graft_entry__.smoke() and bench.py's CPU
-baseline use it, as the checker; the product never does.
+baseline use it, as the reference results are compared with; the product
+never does.
 
 Parameter objects are read by attribute (nugget, structures, anisotropy for
 a variogram; radius, counts, octant, anisotropy for a search), so the
