@@ -162,12 +162,14 @@ def rel_err(a, b):
     return e
 
 
-def loo_gradient(args, dev):
+def loo_gradient(args, dev, ws=1, rank=0):
     """c4: leave-one-out loss of 20,000 samples (32 neighbours, frozen) and its 10-parameter gradient;
-    kernel times from CUDA events on the launch stream, forward alone and forward with the adjoint."""
+    kernel times from CUDA events on the launch stream, forward alone and forward with the adjoint. With
+    several ranks the samples are split over them (boitata_b200.shard) and the partial sums are
+    all-reduced; the time is the slowest rank's kernel time."""
     import torch
 
-    from boitata_b200 import OrdinaryKriging, workloads
+    from boitata_b200 import OrdinaryKriging, shard, workloads
     from boitata_b200.gradient import LeaveOneOut, theta_of
 
     w = workloads.c4(device=dev)
@@ -175,27 +177,37 @@ def loo_gradient(args, dev):
     est = OrdinaryKriging(w.variogram, w.search).fit(w.coords, w.values)
     loo = LeaveOneOut(est)
     theta = theta_of(w.variogram)
+    first, count = shard.split(loo.n, ws)[rank]
     ctx = est._ctx
     ctx._lib.btk_set_timing(ctx.handle, 1)
     times = {}
     for grad in (False, True):
         ms = []
         for i in range(args.warmup + max(args.steps, 3)):
-            loss, g, nv = loo.evaluate(theta, grad=grad)
+            sums = shard.loo_sums(loo, theta, first, count, grad)
             p3 = (ctypes.c_float * 3)()
             ctx.check(ctx._lib.btk_phase_ms(ctx.handle, p3), "phase timing")
             if i >= args.warmup:
                 ms.append(p3[0])
-        times[grad] = float(np.median(ms))
+        t = np.array([float(np.median(ms))])
+        if ws > 1:
+            import torch.distributed as dist
+
+            tt = torch.tensor(t, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = tt.cpu().numpy()
+        times[grad] = float(t[0])
+    loss, g, _ = shard.finish(shard.all_reduce_sum(sums))
     ctx._lib.btk_set_timing(ctx.handle, 0)
     return {"loo_grad_ms": times[True],
             "loo_grad": {"samples": int(len(w.coords)), "parameters": int(len(theta)), "loss": loss,
                          "forward_ms": times[False], "forward_and_adjoint_ms": times[True],
                          "adjoint_over_forward": (times[True] - times[False]) / times[False],
-                         "grad_norm": float(np.linalg.norm(g)),
+                         "grad_norm": float(np.linalg.norm(g)), "ranks": ws,
                          "what": "c4: mean squared leave-one-out error of ordinary kriging, 32 nearest samples "
                                  "frozen at theta0, gradient w.r.t. nugget, 2 sills, 2 ranges, 2 ratios, "
-                                 "3 angles (FP64 adjoint, one kernel with the forward)"}}
+                                 "3 angles (FP64 adjoint, one kernel with the forward); samples split over the "
+                                 "ranks, partial sums all-reduced"}}
 
 
 def run_reference(args, ws, rank):
@@ -416,7 +428,7 @@ def main():
                                "value and variance; wall clock around the synchronous call"}
 
     if not args.no_grad:
-        line.update(loo_gradient(args, dev))
+        line.update(loo_gradient(args, dev, ws, rank))
 
     if rank == 0 and ws == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(w, args.cpu_sample)

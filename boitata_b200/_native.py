@@ -93,6 +93,8 @@ SIGNATURES = {
     "btk_peak_flops": (ctypes.c_double, [P, ctypes.c_int32]),
     "btk_loo_freeze": (ctypes.c_int, [P]),
     "btk_loo_gradient": (ctypes.c_int, [P, ctypes.POINTER(VariogramC), ctypes.c_int32, P, P, P, P]),
+    "btk_loo_gradient_range": (ctypes.c_int, [P, ctypes.POINTER(VariogramC), ctypes.c_int64, ctypes.c_int64,
+                                              ctypes.c_int32, P]),
     "btk_solve_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(VariogramC), ctypes.c_int32, ctypes.c_double,
                                          P, P, P, P, P, ctypes.c_int64, P, P, P, P, ctypes.c_int32, P, P,
                                          ctypes.POINTER(OutputsC), P, ctypes.c_char_p, ctypes.c_size_t]),

@@ -92,14 +92,15 @@ __global__ void __launch_bounds__(128) k_loo_grad(GradDev a) {
   for (int64_t i = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); i < a.n; i += warps) {
     __syncwarp();
     double* out = a.part + i * a.stride;
-    const int n = a.count[i];
-    bool skip = a.sstatus[i] != BTK_ST_OK || n <= 0 || n > R;
+    const int64_t si = a.first + i;  // the left-out sample
+    const int n = a.count[si];
+    bool skip = a.sstatus[si] != BTK_ST_OK || n <= 0 || n > R;
     const bool have = !skip && lane < n;
-    const double t[3] = {a.sx[i], a.sy[i], a.sz[i]};
+    const double t[3] = {a.sx[si], a.sy[si], a.sz[si]};
     double w0 = 0, w1 = 0, w2 = 0, z = 0, err = 0;
     int tw = 0;
     if (have) {
-      const uint32_t j = a.nbr[i * a.max_samples + lane];
+      const uint32_t j = a.nbr[si * a.max_samples + lane];
       w0 = a.sx[j], w1 = a.sy[j], w2 = a.sz[j], z = a.sv[j];
       if (a.se) err = a.se[j];
       tw = a.twin[j];
@@ -110,7 +111,7 @@ __global__ void __launch_bounds__(128) k_loo_grad(GradDev a) {
     if (skip) {
       if (lane == 0) {
         for (int k = 0; k < a.stride; ++k) out[k] = 0.0;
-        if (a.value) a.value[i] = NAN;
+        if (a.value) a.value[si] = NAN;
       }
       continue;
     }
@@ -171,7 +172,7 @@ __global__ void __launch_bounds__(128) k_loo_grad(GradDev a) {
     if (sing) {
       if (lane == 0) {
         for (int k = 0; k < a.stride; ++k) out[k] = 0.0;
-        if (a.value) a.value[i] = NAN;
+        if (a.value) a.value[si] = NAN;
       }
       continue;
     }
@@ -198,12 +199,12 @@ __global__ void __launch_bounds__(128) k_loo_grad(GradDev a) {
     const double est = warp_sum(have ? wl * z : 0.0);
     const double nu = se / sb;
     const double lam = u2 - nu * u1;  // adjoint weights
-    const double resid = est - a.sv[i];
+    const double resid = est - a.sv[si];
     const double adj = have ? 2.0 * resid * lam : 0.0;
     if (lane == 0) {
       out[0] = resid * resid;
       out[1] = 1.0;
-      if (a.value) a.value[i] = est;
+      if (a.value) a.value[si] = est;
     }
     if (!a.want_grad) continue;
     S.w[lane] = have ? wl : 0.0, S.adj[lane] = adj;

@@ -973,13 +973,20 @@ int btk_loo_freeze(btk_ctx* ctx) {
   return BTK_OK;
 }
 
-int btk_loo_gradient(btk_ctx* ctx, const btk_variogram* vg, int32_t want_grad, double* loss, double* grad,
-                     int64_t* n_valid, double* values) {
+namespace {
+
+// Sums over the frozen leave-one-out systems first .. first + count - 1:
+// sums[0] = squared-error sum, sums[1] = systems in the loss, sums[2 + k] =
+// gradient sum of parameter k. values (full length n, or null) gets the
+// range's leave-one-out estimates.
+int loo_sums(btk_ctx* ctx, const btk_variogram* vg, int64_t first, int64_t count, int32_t want_grad,
+             std::vector<double>& sums, double* values) {
   int rc = need_fit(ctx);
   if (rc) return rc;
   if (!ctx->frozen) return fail(ctx, BTK_EINVAL, "call btk_loo_freeze first");
   if ((rc = check_vg(ctx, vg))) return rc;
-  if (!loss) return fail(ctx, BTK_EINVAL, "loss is required");
+  if (first < 0 || count < 0 || first + count > ctx->n)
+    return fail(ctx, BTK_EINVAL, "the range must lie within the fitted samples");
   CK(cudaSetDevice(ctx->device));
   btk_variogram v = *vg;
   if (!v.aniso.on) v.aniso = btk_aniso{1, 0.0, 0.0, 0.0, 1.0, 1.0, 1.0};  // isotropic, as a point of theta
@@ -987,19 +994,21 @@ int btk_loo_gradient(btk_ctx* ctx, const btk_variogram* vg, int32_t want_grad, d
   make_vgdev(v, a.vg);
   aniso_derivatives(v.aniso, a.dM);
   const int ntheta = 1 + 2 * v.nstruct + 5;
-  const int64_t n = ctx->n;
   a.sx = ctx->x.p, a.sy = ctx->y.p, a.sz = ctx->z.p, a.sv = ctx->v.p, a.se = ctx->has_err ? ctx->e.p : nullptr;
   a.twin = ctx->twin.p;
   a.nbr = ctx->loo_nbr.p, a.count = ctx->loo_cnt.p, a.sstatus = ctx->loo_sst.p;
   a.max_samples = int(ctx->search.max_samples);
-  a.n = n;
+  a.first = first;
+  a.n = count;
   a.want_grad = want_grad ? 1 : 0;
   a.stride = 2 + ntheta;
-  CK(ctx->g_part.grow(size_t(n) * size_t(a.stride)));
+  sums.assign(size_t(a.stride), 0.0);
+  if (count == 0) return BTK_OK;
+  CK(ctx->g_part.grow(size_t(count) * size_t(a.stride)));
   CK(ctx->g_sums.grow(size_t(a.stride)));
   a.part = ctx->g_part.p;
   if (values) {
-    CK(ctx->g_val.grow(size_t(n)));
+    CK(ctx->g_val.grow(size_t(ctx->n)));
     a.value = ctx->g_val.p;
   }
   Launch L = ctx->launch(nullptr);
@@ -1008,15 +1017,38 @@ int btk_loo_gradient(btk_ctx* ctx, const btk_variogram* vg, int32_t want_grad, d
   ctx->mark(1, L.stream);
   ctx->mark(2, L.stream);
   ctx->mark(3, L.stream);
-  std::vector<double> sums(size_t(a.stride));
   CK(cudaMemcpyAsync(sums.data(), ctx->g_sums.p, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, L.stream));
-  if (values) CK(cudaMemcpyAsync(values, a.value, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, L.stream));
+  if (values)
+    CK(cudaMemcpyAsync(values + first, a.value + first, size_t(count) * sizeof(double), cudaMemcpyDeviceToHost,
+                       L.stream));
   CK(cudaStreamSynchronize(L.stream));
+  return BTK_OK;
+}
+
+}  // namespace
+
+int btk_loo_gradient(btk_ctx* ctx, const btk_variogram* vg, int32_t want_grad, double* loss, double* grad,
+                     int64_t* n_valid, double* values) {
+  if (!loss) return fail(ctx, BTK_EINVAL, "loss is required");
+  std::vector<double> sums;
+  const int rc = loo_sums(ctx, vg, 0, ctx ? ctx->n : 0, want_grad, sums, values);
+  if (rc) return rc;
+  const int ntheta = int(sums.size()) - 2;
   const double cnt = sums[1];
   *loss = cnt > 0 ? sums[0] / cnt : NAN;
   if (n_valid) *n_valid = int64_t(cnt);
   if (grad && want_grad)
     for (int k = 0; k < ntheta; ++k) grad[k] = cnt > 0 ? sums[2 + k] / cnt : NAN;
+  return BTK_OK;
+}
+
+int btk_loo_gradient_range(btk_ctx* ctx, const btk_variogram* vg, int64_t first, int64_t count, int32_t want_grad,
+                           double* sums) {
+  if (!sums) return fail(ctx, BTK_EINVAL, "sums is required");
+  std::vector<double> s;
+  const int rc = loo_sums(ctx, vg, first, count, want_grad, s, nullptr);
+  if (rc) return rc;
+  for (size_t k = 0; k < s.size(); ++k) sums[k] = (k < 2 || want_grad) ? s[k] : 0.0;
   return BTK_OK;
 }
 

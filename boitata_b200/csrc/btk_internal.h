@@ -101,6 +101,7 @@ struct GradDev {
   const int32_t* count;
   const int8_t* sstatus;
   int max_samples;
+  int64_t first;  // systems first .. first + n - 1 (the left-out samples)
   int64_t n;
   int want_grad;
   int stride;     // 2 + number of parameters

@@ -55,16 +55,20 @@ class BlockModel:
     def __len__(self):
         return self.geometry.cells()
 
-    def centroids(self, context=None):
-        """Cell centroids (n, 3) in cell order, computed by the engine on the device."""
+    def centroids(self, context=None, first=0, count=None):
+        """Centroids (count, 3) of cells first .. first + count - 1 (all by default), cell order, computed by
+        the engine on the device (block_model.rs:431-445: row index i + nx (j + ny k))."""
+        import ctypes
+
         from ._native import Context
 
         ctx = context or Context()
         n = self.geometry.cells()
-        out = np.empty((n, 3), dtype=np.float64)
+        count = n - first if count is None else count
+        if first < 0 or count < 0 or first + count > n:
+            raise InvalidInput("the cell range must lie within the block model")
+        out = np.empty((count, 3), dtype=np.float64)
         g = self.geometry.to_c()
-        import ctypes
-
-        rc = ctx._lib.btk_centroids(ctx.handle, ctypes.byref(g), 0, n, out.ctypes.data)
+        rc = ctx._lib.btk_centroids(ctx.handle, ctypes.byref(g), first, count, out.ctypes.data)
         ctx.check(rc, "centroids")
         return out

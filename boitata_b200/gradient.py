@@ -51,9 +51,13 @@ def _variogram_c(vg):
 
 class LeaveOneOut:
     """Leave-one-out loss and gradient of a fitted ordinary-kriging estimator,
-    neighbourhoods frozen at the time of construction."""
+    neighbourhoods frozen at the time of construction. With sharded=True
+    (one process per GPU under torch.distributed, the estimator fitted on
+    every rank) each rank takes a contiguous share of the left-out samples and
+    one all-reduce over `group` combines the partial sums (boitata_b200.shard),
+    so every rank gets the whole loss and gradient."""
 
-    def __init__(self, estimator):
+    def __init__(self, estimator, *, sharded=False, group=None):
         estimator._fitted()
         if estimator._kind != N.ORDINARY:
             raise InvalidInput("the leave-one-out gradient is for ordinary kriging")
@@ -63,6 +67,7 @@ class LeaveOneOut:
         ctx = estimator._ctx
         ctx.check(ctx._lib.btk_loo_freeze(ctx.handle), "freeze")
         self.n = len(estimator._samples[0])
+        self.sharded, self.group = sharded, group
 
     @property
     def theta0(self):
@@ -70,6 +75,12 @@ class LeaveOneOut:
 
     def evaluate(self, theta, grad=True, values=False):
         """(loss, gradient or None, number of samples in the loss[, estimates])."""
+        if self.sharded:
+            if values:
+                raise InvalidInput("leave-one-out estimates are per rank; evaluate(values=True) needs sharded=False")
+            from .shard import loo_loss_sharded
+
+            return loo_loss_sharded(self, theta, group=self.group, grad=grad)
         vg = variogram_of(self.template, theta)
         c = _variogram_c(vg)
         ns = len(vg.structures)

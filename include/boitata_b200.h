@@ -218,6 +218,15 @@ int btk_loo_freeze(btk_ctx* ctx);
 int btk_loo_gradient(btk_ctx* ctx, const btk_variogram* vg, int32_t want_grad, double* loss, double* grad,
                      int64_t* n_valid, double* values);
 
+/* The same over the left-out samples first .. first + count - 1 only, as
+ * sums for a reduction across ranks: sums[0] = sum of squared errors,
+ * sums[1] = systems in the loss, sums[2 + k] = gradient sum of parameter k
+ * (zero without want_grad); 2 + 1 + 2 nstruct + 5 values. The loss over a
+ * partition of the samples is sum(sums[0]) / sum(sums[1]), and the gradient
+ * sum(sums[2 + k]) / sum(sums[1]). */
+int btk_loo_gradient_range(btk_ctx* ctx, const btk_variogram* vg, int64_t first, int64_t count, int32_t want_grad,
+                           double* sums);
+
 /* Kernel launches issued by this context since it was created. */
 int64_t btk_launch_count(const btk_ctx* ctx);
 

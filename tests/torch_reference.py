@@ -35,13 +35,17 @@ def frame(semi, minor, az, dip, rake):
     return d @ (r3 @ r2 @ r1)
 
 
-def loo_loss(theta, models, coords, values, nbr):
-    """Mean squared leave-one-out error; nbr (n x k) frozen neighbour indices (all systems full)."""
+def loo_loss(theta, models, coords, values, nbr, rows=None):
+    """Mean squared leave-one-out error; nbr (n x k) frozen neighbour indices (all systems full). With
+    `rows` (indices of left-out samples) the mean over those samples only."""
     ns = len(models)
     nugget, sills, ranges = theta[0], theta[1:1 + ns], theta[1 + ns:1 + 2 * ns]
     M = frame(*theta[1 + 2 * ns:])
-    X = coords[nbr]                       # n, k, 3
-    P = (X - coords[:, None, :]) @ M.T    # n, k, 3
+    if rows is None:
+        rows = torch.arange(len(coords))
+    nbr = nbr[rows]
+    X = coords[nbr]                             # n, k, 3
+    P = (X - coords[rows][:, None, :]) @ M.T    # n, k, 3
     n, k, _ = P.shape
     eye = torch.eye(k, dtype=P.dtype)
     D = P[:, :, None, :] - P[:, None, :, :]
@@ -59,4 +63,4 @@ def loo_loss(theta, models, coords, values, nbr):
     b[:, :k] = cov(h0)
     x = torch.linalg.solve(K, b)
     est = (x[:, :k] * values[nbr]).sum(-1)
-    return ((est - values) ** 2).mean()
+    return ((est - values[rows]) ** 2).mean()
