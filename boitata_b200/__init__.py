@@ -1,19 +1,21 @@
 """boitata_b200 — B200-native ordinary / simple / indicator kriging of block models.
 
 A drop-in for the kriging path of gstvschlz/boitata (`OrdinaryKriging`,
-`SimpleKriging`, `IndicatorKriging`, `Variogram`, `Structure`, `Search`):
+`SimpleKriging`, `IndicatorKriging`, `BlockKriging`, `Variogram`,
+`Structure`, `Search`):
 neighbour search, covariance assembly, bordered solve and estimate /
 variance run as hand-written sm_100a CUDA kernels behind the C ABI of
 include/boitata_b200.h.
 """
 
 from .errors import InvalidInput, Unsupported
-from .estimation import CrossValidation, IndicatorKriging, OrdinaryKriging, SimpleKriging
+from .estimation import BlockKriging, CrossValidation, IndicatorKriging, OrdinaryKriging, SimpleKriging
 from .geometry import BlockModel, Geometry
 from .search import Search
 from .variogram import Structure, Variogram
 
 __all__ = [
+    "BlockKriging",
     "BlockModel",
     "CrossValidation",
     "Geometry",

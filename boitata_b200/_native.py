@@ -83,6 +83,8 @@ SIGNATURES = {
     "btk_neighbors": (ctypes.c_int, [P, ctypes.c_int64, P, ctypes.c_int32, P, P, P]),
     "btk_centroids": (ctypes.c_int, [P, ctypes.POINTER(GeometryC), ctypes.c_int64, ctypes.c_int64, P]),
     "btk_launch_count": (ctypes.c_int64, [P]),
+    "btk_set_support": (ctypes.c_int, [P, P, P, P]),
+    "btk_support_variance": (ctypes.c_int, [P, P]),
     "btk_get_tuning": (ctypes.c_int, [P, ctypes.POINTER(TuningC)]),
     "btk_set_tuning": (ctypes.c_int, [P, ctypes.POINTER(TuningC)]),
     "btk_graph_capture_geometry": (ctypes.c_int, [P, ctypes.POINTER(GeometryC), ctypes.c_int32, ctypes.c_double,

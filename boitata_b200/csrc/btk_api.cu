@@ -100,6 +100,30 @@ btk::Frame9 transposed_frame(const btk_geometry& g) {
   return out;
 }
 
+// Discretization offsets of a block (crates/estimation/src/block.rs:40-72:
+// Discretization::points centred at the origin, i outer and k inner, then
+// block_frame(rotation)^T * p in nalgebra's column order).
+std::vector<double> block_offsets(const double size[3], const int32_t nd[3], const double rot[3]) {
+  const M3 f = block_frame(rot[0], rot[1], rot[2]);
+  const double dx = size[0] / double(nd[0]), dy = size[1] / double(nd[1]), dz = size[2] / double(nd[2]);
+  const double x0 = 0.0 - size[0] / 2.0 + dx / 2.0, y0 = 0.0 - size[1] / 2.0 + dy / 2.0,
+               z0 = 0.0 - size[2] / 2.0 + dz / 2.0;
+  std::vector<double> out;
+  out.reserve(3 * size_t(nd[0]) * nd[1] * nd[2]);
+  for (int i = 0; i < nd[0]; ++i)
+    for (int j = 0; j < nd[1]; ++j)
+      for (int k = 0; k < nd[2]; ++k) {
+        const double p[3] = {x0 + double(i) * dx, y0 + double(j) * dy, z0 + double(k) * dz};
+        for (int r = 0; r < 3; ++r) {  // (f^T p)_r = sum_c f[c][r] p_c, column by column
+          double y = f.m[0][r] * p[0];
+          y = f.m[1][r] * p[1] + y;
+          y = f.m[2][r] * p[2] + y;
+          out.push_back(y);
+        }
+      }
+  return out;
+}
+
 }  // namespace
 
 struct btk_ctx {
@@ -152,6 +176,10 @@ struct btk_ctx {
   DevBuf<int64_t> ord_vals;
   DevBuf<uint8_t> ord_temp;
   DevBuf<double> ord_part, ord_b6;
+
+  // block support (btk_set_support): discretization offsets, C(B,B)
+  DevBuf<double> sup, sup_cbb;
+  int sup_n = 0;
 
   Tuning tuning;
   cudaGraph_t graph = nullptr;
@@ -411,6 +439,10 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
   a.nbr = ctx->nbr.p, a.count = ctx->cnt.p, a.sstatus = ctx->sst.p;
   a.m = m;
   a.value = o->value, a.variance = o->variance, a.lagrange = o->lagrange, a.n_used = o->n_used, a.status = o->status;
+  if (ctx->sup_n > 0 && !loo) {  // block support; cross-validation stays at point support
+    CK(launch_support_cbb(L, ctx->vgd, ctx->sup.p, ctx->sup_n, ctx->sup_cbb.p));
+    a.sup = ctx->sup.p, a.sup_n = ctx->sup_n, a.sup_cbb = ctx->sup_cbb.p;
+  }
   const bool two = ctx->search.max_samples > 32;
   const bool tiled = ctx->tuning.tile_union > 0;
   const int nb = two ? 2 : 1;
@@ -605,6 +637,49 @@ void btk_destroy(btk_ctx* ctx) {
   if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
   if (ctx->graph) cudaGraphDestroy(ctx->graph);
   delete ctx;
+}
+
+int btk_set_support(btk_ctx* ctx, const double* size, const int32_t* disc, const double* rotation) {
+  if (!ctx) return BTK_EINVAL;
+  if (!size) {
+    ctx->sup_n = 0;
+    return BTK_OK;
+  }
+  if (!disc) return fail(ctx, BTK_EINVAL, "a block size needs a discretization");
+  for (int d = 0; d < 3; ++d) {
+    if (disc[d] < 1)
+      return fail(ctx, BTK_EINVAL, "discretization must be at least 1 per axis, got (" + std::to_string(disc[0]) +
+                                       ", " + std::to_string(disc[1]) + ", " + std::to_string(disc[2]) + ")");
+    if (!(std::isfinite(size[d]) && size[d] > 0.0)) return fail(ctx, BTK_EINVAL, "size must be finite and > 0");
+    if (rotation && !std::isfinite(rotation[d])) return fail(ctx, BTK_EINVAL, "rotation must be finite");
+  }
+  const int64_t nd = int64_t(disc[0]) * disc[1] * disc[2];
+  if (nd > BTK_MAX_SUPPORT_POINTS) return fail(ctx, BTK_EINVAL, "block discretization has more than 4096 points");
+  const double zero[3] = {0.0, 0.0, 0.0};
+  const std::vector<double> off = block_offsets(size, disc, rotation ? rotation : zero);
+  CK(cudaSetDevice(ctx->device));
+  CK(ctx->sup.grow(off.size()));
+  CK(ctx->sup_cbb.grow(1));
+  CK(cudaMemcpyAsync(ctx->sup.p, off.data(), off.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->sup_n = int(nd);
+  return BTK_OK;
+}
+
+int btk_support_variance(btk_ctx* ctx, double* out) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if (!out) return fail(ctx, BTK_EINVAL, "out is required");
+  if (ctx->sup_n == 0) {
+    *out = ctx->vgd.c0;
+    return BTK_OK;
+  }
+  CK(cudaSetDevice(ctx->device));
+  Launch L = ctx->launch(nullptr);
+  CK(launch_support_cbb(L, ctx->vgd, ctx->sup.p, ctx->sup_n, ctx->sup_cbb.p));
+  CK(cudaMemcpyAsync(out, ctx->sup_cbb.p, sizeof(double), cudaMemcpyDeviceToHost, L.stream));
+  CK(cudaStreamSynchronize(L.stream));
+  return BTK_OK;
 }
 
 int btk_get_tuning(const btk_ctx* ctx, btk_tuning* out) {

@@ -209,9 +209,26 @@ __device__ __forceinline__ void write_fail(const SolveDev& a, int64_t ti, int8_t
 // Estimate, variance and Lagrange multiplier from the five forms
 // s[0] = 1'C^-1 c, s[1] = 1'C^-1 1, s[2] = f'C^-1 c, s[3] = f'C^-1 1,
 // s[4] = c'C^-1 c (kernel.rs:86-122).
+// Covariance of sample (sx, sy, sz) with the target (tx, ty, tz): point
+// support, or, with block support, the mean over the block's discretization
+// points of the point covariance with the nugget left out at zero lag (one
+// point: point support) (crates/estimation/src/block.rs:101-116 with
+// crates/variogram/src/composite.rs:108-115).
+__device__ __forceinline__ double support_cov(const SolveDev& a, double tx, double ty, double tz, double sx,
+                                              double sy, double sz) {
+  if (a.sup_n <= 0) return cov64(a.vg, lag_world(a.vg, tx, ty, tz, sx, sy, sz));
+  double sum = 0.0;
+  for (int k = 0; k < a.sup_n; ++k) {
+    const double h = lag_world(a.vg, tx + a.sup[3 * k], ty + a.sup[3 * k + 1], tz + a.sup[3 * k + 2], sx, sy, sz);
+    sum += a.sup_n == 1 || h > 0.0 ? cov64(a.vg, h) : a.vg.c0 - a.vg.nugget;
+  }
+  return sum / double(a.sup_n);
+}
+
 __device__ __forceinline__ void epilogue(const SolveDev& a, int kind, int64_t ti, const double s[5], int n_used,
                                          int8_t flag) {
-  const double c0 = a.vg.c0;
+  // C(0) for point support; C(B,B) for a block (block.rs:186-187)
+  const double c0 = a.sup_n > 0 ? *a.sup_cbb : a.vg.c0;
   double mu, value, swc;
   if (kind == BTK_SIMPLE) {
     mu = 0.0;

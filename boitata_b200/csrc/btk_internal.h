@@ -75,6 +75,12 @@ struct SolveDev {
   double *value, *variance, *lagrange;
   int32_t* n_used;
   int8_t* status;
+  // Block support (block kriging): sup_n discretization offsets (x, y, z
+  // triples, world frame) around each target, and the block's mean
+  // covariance C(B,B) on the device; sup_n == 0 for point support.
+  const double* sup;
+  int sup_n;
+  const double* sup_cbb;
 };
 
 // Tile-shared solve (btk_tile.cu): the systems of kTileTargets consecutive
@@ -172,6 +178,11 @@ size_t morton_temp_bytes(int64_t m);
 cudaError_t launch_morton_order(const Launch& L, int64_t m, const double* x, const double* y, const double* z,
                                 const double w[3], double* partial, double* b6, uint64_t* keys, int64_t* vals,
                                 void* temp, size_t temp_bytes, const int64_t** perm);
+
+// C(B,B) of a block discretized by nd offsets (x, y, z triples) into *cbb:
+// the mean over pairs of point covariances with the nugget left out at zero
+// lag; the total sill for one point (btk_support.cu).
+cudaError_t launch_support_cbb(const Launch& L, const VgDev& vg, const double* off, int nd, double* cbb);
 
 // Leave-one-out loss and gradient; sums[stride] receives the column sums.
 cudaError_t launch_loo_grad(const Launch& L, const GradDev& a, double* sums);

@@ -227,7 +227,7 @@ __device__ __forceinline__ bool assemble(const SolveDev& a, SolveSmem<NW>& S, in
     tri_index(e, i, j);
     S.T[e] = cov64(a.vg, lag_world(a.vg, S.P[j][0], S.P[j][1], S.P[j][2], S.P[i][0], S.P[i][1], S.P[i][2]));
   }
-  c = have ? cov64(a.vg, lag_world(a.vg, t[0], t[1], t[2], w[0], w[1], w[2])) : 0.0;
+  c = have ? support_cov(a, t[0], t[1], t[2], w[0], w[1], w[2]) : 0.0;
   gsync<NW>(gid);
   return true;
 }

@@ -235,8 +235,8 @@ __device__ bool build_tile(const TileDev& a, int64_t tile, unsigned char* smem, 
 }
 
 // C(target, union sample u).
-__device__ __forceinline__ double cov_to(const VgDev& vg, const double* P, int umax, int u, const double t[3]) {
-  return cov64(vg, lag_world(vg, t[0], t[1], t[2], P[u], P[umax + u], P[2 * umax + u]));
+__device__ __forceinline__ double cov_to(const SolveDev& s, const double* P, int umax, int u, const double t[3]) {
+  return support_cov(s, t[0], t[1], t[2], P[u], P[umax + u], P[2 * umax + u]);
 }
 
 // Pivots k0 .. k1-1 of the FP64 right-looking LDL^T with the forward
@@ -285,7 +285,7 @@ __device__ void solve_fp64(const TileDev& a, const TileHead& H, const double* P,
   const bool have = lane < n;
   const int ma = H.map[t][lane];
   const double pt[3] = {s.tx[ti], s.ty[ti], s.tz[ti]};
-  const double c = have ? cov_to(s.vg, P, umax, ma, pt) : 0.0;
+  const double c = have ? cov_to(s, P, umax, ma, pt) : 0.0;
   const double zf = have ? kind_f(kind, s.kparam, Z[ma]) : 0.0;
   const double* Ur = UU + ma * S;
   double A[32];
@@ -382,13 +382,13 @@ __device__ void solve_mixed(const TileDev& a, const TileHead& H, const double* P
   if (ha) {
     const int64_t ti = H.ti[ta];
     const double pt[3] = {s.tx[ti], s.ty[ti], s.tz[ti]};
-    ca = cov_to(s.vg, P, umax, ma, pt);
+    ca = cov_to(s, P, umax, ma, pt);
     za = kind_f(H.kind[ta], s.kparam, Z[ma]);
   }
   if (hb) {
     const int64_t ti = H.ti[tb];
     const double pt[3] = {s.tx[ti], s.ty[ti], s.tz[ti]};
-    cb = cov_to(s.vg, P, umax, mb, pt);
+    cb = cov_to(s, P, umax, mb, pt);
     zb = kind_f(H.kind[tb], s.kparam, Z[mb]);
   }
   const double* Ua = UU + ma * S;

@@ -10,6 +10,7 @@ the CUDA engine through its C ABI; `precision` selects the FP64 form
 (default, the reference's arithmetic) or the mixed FP32/FP64 form.
 """
 
+import contextlib
 import ctypes
 import math
 import warnings
@@ -223,6 +224,14 @@ class _Base:
                 xyz[:, 2] = z
         else:
             xyz = points(targets)
+        with self._support(targets):
+            return self._passes(xyz, precision)
+
+    def _support(self, targets):
+        """Context manager setting the engine's target support for one prediction (point support here)."""
+        return contextlib.nullcontext()
+
+    def _passes(self, xyz, precision):
         m = len(xyz)
         res = None
         remaining = np.arange(m)
@@ -352,3 +361,58 @@ class IndicatorKriging(_Base):
     def __init__(self, variogram, search, threshold, *, precision="fp64", device=0):
         super().__init__(variogram, search, kparam=float(threshold), precision=precision, device=device)
         self.threshold = float(threshold)
+
+
+class BlockKriging(_Base):
+    """Ordinary kriging of block averages; targets are block centres of `size`
+    (python/boitata/estimation.py:475-485, crates/estimation/src/block.rs).
+
+    `size` runs along the axes of a rotated BlockModel given as targets, and
+    along the world axes for coordinates. Each size must be finite and > 0,
+    and `discretization` at least 1 per axis, or InvalidInput is raised; a
+    ``(1, 1, 1)`` discretization is point support, nugget included.
+    Cross-validation runs at point support, as in the reference.
+    """
+
+    _kind = N.ORDINARY
+
+    def __init__(self, variogram, search, size, *, discretization=(4, 4, 1), precision="fp64", device=0):
+        size = [float(v) for v in size]
+        if len(size) == 2:
+            size.append(1.0)
+        if len(size) != 3:
+            raise InvalidInput(f"size needs 2 or 3 values, got {len(size)}")
+        disc = tuple(int(v) for v in discretization)
+        if len(disc) != 3 or any(v < 1 for v in disc):
+            raise InvalidInput(f"discretization must be at least 1 per axis, got {disc}")
+        if not all(math.isfinite(v) and v > 0.0 for v in size):
+            raise InvalidInput(f"size must be finite and > 0, got {tuple(size)}")
+        if disc[0] * disc[1] * disc[2] > 4096:
+            raise Unsupported("block discretizations of more than 4096 points are not run by this engine")
+        super().__init__(variogram, search, precision=precision, device=device)
+        self.size = tuple(size)
+        self.discretization = disc
+
+    @contextlib.contextmanager
+    def _support(self, targets):
+        rot = targets.geometry.rotation if isinstance(targets, BlockModel) else (0.0, 0.0, 0.0)
+        ctx = self._ctx
+        size = (ctypes.c_double * 3)(*self.size)
+        disc = (ctypes.c_int32 * 3)(*self.discretization)
+        r = (ctypes.c_double * 3)(*rot)
+        ctx.check(ctx._lib.btk_set_support(ctx.handle, size, disc, r), "block support")
+        try:
+            yield
+        finally:
+            ctx._lib.btk_set_support(ctx.handle, None, None, None)
+
+    def support_variance(self, targets=None):
+        """C(B,B), the mean covariance within a block (the reference's support_variance), for blocks turned
+        as `targets` (a BlockModel or Geometry) or along the world axes."""
+        self._fitted()
+        if isinstance(targets, Geometry):
+            targets = BlockModel(targets)
+        out = ctypes.c_double(0.0)
+        with self._support(targets):
+            self._ctx.check(self._ctx._lib.btk_support_variance(self._ctx.handle, ctypes.byref(out)), "support")
+        return out.value

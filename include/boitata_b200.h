@@ -230,6 +230,22 @@ int btk_loo_gradient_range(btk_ctx* ctx, const btk_variogram* vg, int64_t first,
 /* Kernel launches issued by this context since it was created. */
 int64_t btk_launch_count(const btk_ctx* ctx);
 
+/* Block support for this context's later predictions (block kriging,
+ * replacing BlockKriging / Method::Block: crates/py/src/estimation.rs:
+ * 1414-1439 and 775-784, crates/estimation/src/block.rs:40-198). Each
+ * target is then a block centre: the block of `size` (along the axes turned
+ * by `rotation`, azimuth/dip/rake in degrees, NULL for none) is discretized
+ * into disc[0] x disc[1] x disc[2] points, each sample's covariance with
+ * the target is its mean covariance with those points (nugget left out at
+ * zero lag), and the variance is C(B,B) - sum w C(x, B) - mu. One point is
+ * point kriging. size NULL returns to point support. Cross-validation stays
+ * at point support. At most BTK_MAX_SUPPORT_POINTS points. */
+#define BTK_MAX_SUPPORT_POINTS 4096
+int btk_set_support(btk_ctx* ctx, const double* size, const int32_t* disc, const double* rotation);
+/* C(B,B) of the current support for the fitted variogram (C(0) for point
+ * support): the reference's support_variance. */
+int btk_support_variance(btk_ctx* ctx, double* out);
+
 /* Tunables of this context; setting samples_per_cell re-indexes the fitted
  * samples. boitata_b200/autotune.py picks them by timing candidates. */
 int btk_get_tuning(const btk_ctx* ctx, btk_tuning* out);

@@ -288,6 +288,22 @@ struct Variogram {
   double cov(double h) const { return h <= 0.0 ? total_sill() : total_sill() - gamma(h); }  // :79-85
   double lag(const double p[3], const double q[3]) const { return aniso_lag(aniso, p, q); }  // :88-93
   double cov_points(const double p[3], const double q[3]) const { return cov(lag(p, q)); }  // :101-103
+  // composite.rs:108-115: the nugget left out at zero lag (block support)
+  double block_cov_points(const double p[3], const double q[3]) const {
+    double h = lag(p, q);
+    return h <= 0.0 ? total_sill() - nugget : cov(h);
+  }
+  // composite.rs:120-129
+  double block_mean_cov(const std::vector<std::array<double, 3>>& pts) const {
+    if (pts.size() == 1) return total_sill();
+    double total = -0.0;
+    for (auto& a : pts) {
+      double row = -0.0;
+      for (auto& b : pts) row = row + block_cov_points(a.data(), b.data());
+      total = total + row;
+    }
+    return total / double(pts.size() * pts.size());
+  }
 };
 
 // ------------------------------------------------------------------ kriging
@@ -556,6 +572,133 @@ int krige(int kind, double kparam, const double t[3], const std::vector<Sample>&
   int st = kernel_krige(kind, kparam, t, smp, vg, out);
   if (st != NONE) return st;
   return krige_lu(kind, kparam, t, smp, vg, out);
+}
+
+// ---------------------------------------------------------- block kriging
+// crates/estimation/src/block.rs:40-57 (Discretization::points): i outer,
+// k inner.
+std::vector<std::array<double, 3>> disc_points(const double c[3], const double size[3], const int64_t nd[3]) {
+  std::vector<std::array<double, 3>> pts;
+  double dx = size[0] / double(nd[0]), dy = size[1] / double(nd[1]), dz = size[2] / double(nd[2]);
+  double x0 = c[0] - size[0] / 2.0 + dx / 2.0, y0 = c[1] - size[1] / 2.0 + dy / 2.0, z0 = c[2] - size[2] / 2.0 + dz / 2.0;
+  for (int64_t i = 0; i < nd[0]; ++i)
+    for (int64_t j = 0; j < nd[1]; ++j)
+      for (int64_t k = 0; k < nd[2]; ++k)
+        pts.push_back({x0 + double(i) * dx, y0 + double(j) * dy, z0 + double(k) * dz});
+  return pts;
+}
+
+// block.rs:61-72 (Discretization::offsets): block_frame(rotation)^T times the
+// points of a block centred at the origin (nalgebra Matrix3 * Vector3).
+std::vector<std::array<double, 3>> disc_offsets(const double size[3], const int64_t nd[3], const double rot[3]) {
+  M3 f = block_frame(rot[0], rot[1], rot[2]);
+  M3 ft;
+  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) ft.m[i][j] = f.m[j][i];
+  const double zero[3] = {0.0, 0.0, 0.0};
+  auto pts = disc_points(zero, size, nd);
+  for (auto& p : pts) {
+    double y[3];
+    mulv(ft, p.data(), y);
+    p = {y[0], y[1], y[2]};
+  }
+  return pts;
+}
+
+// block.rs:101-116 (block_covariances): the mean covariance of each sample
+// with the discretization, point support for a single point.
+void block_rhs(const std::vector<std::array<double, 3>>& pts, const std::vector<Sample>& smp, const Variogram& vg,
+               std::vector<double>& rhs, double& cbb) {
+  double np = double(pts.size());
+  rhs.assign(smp.size(), 0.0);
+  for (size_t i = 0; i < smp.size(); ++i) {
+    double sum = -0.0;
+    for (auto& p : pts)
+      sum = sum + (pts.size() == 1 ? vg.cov_points(smp[i].loc, p.data()) : vg.block_cov_points(smp[i].loc, p.data()));
+    rhs[i] = sum / np;
+  }
+  cbb = vg.block_mean_cov(pts);
+}
+
+// block.rs:120-198 (block_krige_points, Kind::Ordinary as Method::Block calls
+// it, crates/py/src/estimation.rs:775-784), with the coincident guard of
+// coincident.rs:27-111 as in krige().
+int block_krige_points(const std::vector<std::array<double, 3>>& pts, const std::vector<Sample>& smp,
+                       const Variogram& vg, Estimate& out) {
+  size_t n = smp.size();
+  if (n == 0) return INSUFFICIENT;
+  if (pts.empty()) return INVALID;
+  for (auto& p : pts)
+    if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) return INVALID;
+  bool any = false;
+  for (size_t i = 0; i < n && !any; ++i)
+    for (size_t j = 0; j < i; ++j)
+      if (close(smp[i].loc, smp[j].loc)) { any = true; break; }
+  if (any) {
+    std::vector<size_t> of;
+    std::vector<std::vector<size_t>> members;
+    for (size_t i = 0; i < n; ++i) {
+      size_t c = members.size();
+      for (size_t m = 0; m < members.size(); ++m)
+        if (close(smp[members[m][0]].loc, smp[i].loc)) { c = m; break; }
+      if (c == members.size()) members.push_back({i});
+      else members[c].push_back(i);
+      of.push_back(c);
+    }
+    double c0 = vg.total_sill();
+    std::vector<Sample> merged;
+    for (auto& m : members) {
+      Sample first = smp[m[0]];
+      if (m.size() > 1) {
+        double k = double(m.size());
+        double var = 0.0;
+        for (size_t i : m) {
+          var += smp[i].err;
+          for (size_t j : m) var += vg.cov_points(smp[i].loc, smp[j].loc);
+        }
+        double vs = -0.0;
+        for (size_t i : m) vs = vs + smp[i].value;
+        first.value = vs / k;
+        first.err = var / (k * k) - c0;
+      }
+      merged.push_back(first);
+    }
+    Estimate e;
+    int st = block_krige_points(pts, merged, vg, e);
+    if (st != OK) return st;
+    std::vector<double> w(n);
+    for (size_t i = 0; i < n; ++i) w[i] = e.weights[of[i]] / double(members[of[i]].size());
+    e.weights = w;
+    e.value = kind_value(ORDINARY, 0.0, w, smp);
+    e.n_used = n;
+    out = e;
+    return OK;
+  }
+  std::vector<double> rhs;
+  double cbb;
+  block_rhs(pts, smp, vg, rhs, cbb);
+  size_t dim = n + 1;
+  std::vector<double> A(dim * dim, 0.0), b(dim, 0.0);
+  for (size_t i = 0; i < n; ++i) {
+    for (size_t j = 0; j < n; ++j) A[i * dim + j] = vg.cov_points(smp[i].loc, smp[j].loc);
+    A[i * dim + i] += smp[i].err;
+    A[i * dim + n] = 1.0, A[n * dim + i] = 1.0;
+    b[i] = rhs[i];
+  }
+  b[n] = 1.0;
+  std::vector<double> x = b;
+  if (!lu_solve(A, dim, x)) return SINGULAR;
+  out.weights.assign(x.begin(), x.begin() + n);
+  double value = -0.0;
+  for (size_t i = 0; i < n; ++i) value = value + out.weights[i] * smp[i].value;
+  double swc = -0.0;
+  for (size_t i = 0; i < n; ++i) swc = swc + out.weights[i] * b[i];
+  double mu = x[n];
+  out.value = value;
+  out.variance = std::fmax(cbb - swc - mu, 0.0);
+  out.n_used = n;
+  out.lagrange = mu;
+  out.support = cbb;
+  return OK;
 }
 
 // ---------------------------------------------------------------- search
@@ -1169,6 +1312,67 @@ int32_t orc_krige_lists(int64_t m, const double* targets, int64_t n, const doubl
     int st = krige(kind, kparam, &targets[3 * t], sel, vg, e);
     put(e, st, &res[t]);
   }
+  return 0;
+}
+
+// Discretization offsets (nd0 nd1 nd2 x 3) of a block of `size` turned by
+// `rotation` (block.rs:61-72).
+void orc_block_offsets(const double* size, const int64_t* nd, const double* rotation, double* out) {
+  auto o = disc_offsets(size, nd, rotation);
+  for (size_t k = 0; k < o.size(); ++k) out[3 * k] = o[k][0], out[3 * k + 1] = o[k][1], out[3 * k + 2] = o[k][2];
+}
+
+// block_krige_points of one block centred at t from the given samples (for
+// the block.rs tests): the points are t + offsets (np x 3).
+int32_t orc_block_krige(const double* t, int64_t np, const double* offsets, int64_t n, const double* xyz,
+                        const double* v, const double* err, const orc_variogram* vgp, orc_result* res,
+                        double* weights) {
+  Variogram vg = conv_vg(vgp);
+  std::vector<Sample> s = conv_samples(n, xyz, v, err, nullptr);
+  std::vector<std::array<double, 3>> pts(static_cast<size_t>(np));
+  for (int64_t k = 0; k < np; ++k) pts[k] = {t[0] + offsets[3 * k], t[1] + offsets[3 * k + 1], t[2] + offsets[3 * k + 2]};
+  Estimate e;
+  int st = block_krige_points(pts, s, vg, e);
+  put(e, st, res);
+  if (st == OK && weights) std::copy(e.weights.begin(), e.weights.end(), weights);
+  return st;
+}
+
+// Block kriging of m block centres (crates/py/src/estimation.rs:775-784 via
+// estimate_many, batch.rs:15-38): the search at the centre, then
+// block_krige_points over centre + offsets (np x 3).
+int32_t orc_estimate_block(int64_t m, const double* targets, int64_t n, const double* xyz, const double* v,
+                           const double* err, const int64_t* hole, const orc_search* sp, const orc_variogram* vgp,
+                           int64_t np, const double* offsets, int32_t nthreads, orc_result* res) {
+  std::vector<Sample> s = conv_samples(n, xyz, v, err, hole);
+  SearchP p = conv_search(sp);
+  if (!check(p)) return -1;
+  Variogram vg = conv_vg(vgp);
+  Tree tree(s, p, &vg);
+  auto work = [&](int64_t k0, int64_t k1) {
+    for (int64_t k = k0; k < k1; ++k) {
+      const double* t = &targets[3 * k];
+      std::vector<size_t> chosen;
+      bool ok = tree.neighbors(t, -1, chosen);
+      if (!ok) { Estimate e; put(e, SEARCH_FAILED, &res[k]); continue; }
+      std::vector<Sample> sel;
+      for (size_t i : chosen) sel.push_back(s[i]);
+      std::vector<std::array<double, 3>> pts(static_cast<size_t>(np));
+      for (int64_t q = 0; q < np; ++q)
+        pts[q] = {t[0] + offsets[3 * q], t[1] + offsets[3 * q + 1], t[2] + offsets[3 * q + 2]};
+      Estimate e;
+      int st = block_krige_points(pts, sel, vg, e);
+      put(e, st, &res[k]);
+    }
+  };
+  int nt = nthreads > 0 ? nthreads : orc_num_threads();
+  std::vector<std::thread> pool;
+  int64_t chunk = (m + nt - 1) / nt;
+  for (int w = 0; w < nt; ++w) {
+    int64_t k0 = int64_t(w) * chunk, k1 = std::min(m, k0 + chunk);
+    if (k0 < k1) pool.emplace_back(work, k0, k1);
+  }
+  for (auto& th : pool) th.join();
   return 0;
 }
 

@@ -97,6 +97,12 @@ def lib():
             "orc_krige_lists": (ctypes.c_int32, [ctypes.c_int64, P, ctypes.c_int64, P, P, P, P, ctypes.c_int64,
                                                  ctypes.POINTER(Vario), ctypes.c_int32, ctypes.c_double,
                                                  ctypes.c_int32, P]),
+            "orc_block_offsets": (None, [P, P, P, P]),
+            "orc_block_krige": (ctypes.c_int32, [P, ctypes.c_int64, P, ctypes.c_int64, P, P, P,
+                                                 ctypes.POINTER(Vario), ctypes.POINTER(Result), P]),
+            "orc_estimate_block": (ctypes.c_int32, [ctypes.c_int64, P, ctypes.c_int64, P, P, P, P,
+                                                    ctypes.POINTER(Srch), ctypes.POINTER(Vario), ctypes.c_int64, P,
+                                                    ctypes.c_int32, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -330,3 +336,49 @@ def centroids(origin, size, count, rotation, first=0, m=None):
 
 def num_threads():
     return lib().orc_num_threads()
+
+
+def block_offsets(size, disc, rotation=(0.0, 0.0, 0.0)):
+    """Discretization::offsets (block.rs:61-72): (nx ny nz, 3) points of a block of `size` centred at the
+    origin, turned by `rotation`."""
+    sz = np.ascontiguousarray(size, dtype=np.float64)
+    nd = np.ascontiguousarray(disc, dtype=np.int64)
+    r = np.ascontiguousarray(rotation, dtype=np.float64)
+    out = np.empty((int(np.prod(nd)), 3))
+    lib().orc_block_offsets(sz.ctypes.data, nd.ctypes.data, r.ctypes.data, out.ctypes.data)
+    return out
+
+
+def block_krige(target, offsets, xyz, values, vg, *, err=None):
+    """block_krige_points (block.rs:120-198, ordinary) of one block centred at `target`: (status,
+    {value, variance, lagrange, support, n_used}, weights)."""
+    xyz = _xyz(xyz)
+    n = len(xyz)
+    t = np.ascontiguousarray(target, dtype=np.float64)
+    off = np.ascontiguousarray(offsets, dtype=np.float64).reshape(-1, 3)
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    e = None if err is None else np.ascontiguousarray(err, dtype=np.float64)
+    r = Result()
+    w = np.zeros(max(n, 1))
+    st = lib().orc_block_krige(t.ctypes.data, len(off), off.ctypes.data, n, xyz.ctypes.data, v.ctypes.data,
+                               _ptr(e), ctypes.byref(variogram(vg)), ctypes.byref(r), w.ctypes.data)
+    out = dict(value=r.value, variance=r.variance, lagrange=r.lagrange, support=r.support, n_used=r.n_used)
+    return int(st), out, w[:n]
+
+
+def estimate_block(targets, xyz, values, s, vg, offsets, *, err=None, holes=None, threads=0):
+    """Block kriging of block centres `targets` (search at the centre, then block_krige_points over centre +
+    offsets), as crates/py/src/estimation.rs:775-784 runs Method::Block."""
+    xyz, t = _xyz(xyz), _xyz(targets)
+    off = np.ascontiguousarray(offsets, dtype=np.float64).reshape(-1, 3)
+    m = len(t)
+    res = (Result * max(m, 1))()
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    e = None if err is None else np.ascontiguousarray(err, dtype=np.float64)
+    h = None if holes is None else np.ascontiguousarray(holes, dtype=np.int64)
+    rc = lib().orc_estimate_block(m, t.ctypes.data, len(xyz), xyz.ctypes.data, v.ctypes.data, _ptr(e), _ptr(h),
+                                  ctypes.byref(search(s)), ctypes.byref(variogram(vg)), len(off), off.ctypes.data,
+                                  threads, ctypes.cast(res, P))
+    if rc != 0:
+        raise ValueError("oracle: invalid search parameters")
+    return _records(res, m)

@@ -114,3 +114,20 @@ def test_coordinates_and_values_must_be_finite():
     with pytest.raises(bt.InvalidInput, match="shape"):
         points([[0.0, 1.0, 2.0, 3.0]])
     assert points([[1.0, 2.0]]).tolist() == [[1.0, 2.0, 0.0]]
+
+
+def test_block_kriging_arguments_are_checked_as_the_reference_does():
+    """crates/py/src/estimation.rs:1414-1439: size finite and > 0, discretization at least 1 per axis."""
+    import pytest
+
+    from boitata_b200 import BlockKriging, InvalidInput, Search, Structure, Variogram
+
+    vg = Variogram([Structure("spherical", 1.0, 100.0)])
+    s = Search(radius=100.0, max_samples=8)
+    for size, disc in [((10.0, 0.0, 10.0), (4, 4, 1)), ((10.0, float("nan"), 1.0), (4, 4, 1)),
+                       ((10.0, 10.0, -1.0), (4, 4, 1)), ((10.0, 10.0, 10.0), (0, 4, 1)),
+                       ((10.0, 10.0, 10.0), (4, 4)), ((10.0,), (4, 4, 1))]:
+        with pytest.raises(InvalidInput):
+            BlockKriging(vg, s, size, discretization=disc)
+    b = BlockKriging(vg, s, (10.0, 20.0))
+    assert b.size == (10.0, 20.0, 1.0) and b.discretization == (4, 4, 1)

@@ -390,3 +390,83 @@ def test_results_do_not_depend_on_thread_count(oracle):
     b = oracle.estimate_many(targets, coords, values, s, vg, threads=8)
     for k in ("value", "variance"):
         assert np.array_equal(a[k].view(np.uint64), b[k].view(np.uint64))
+
+
+# ---- block kriging (crates/estimation/src/block.rs:200-371) ----
+
+def test_block_discretization_centres_on_the_block(oracle):
+    """block.rs:205-212."""
+    off = oracle.block_offsets((10.0, 10.0, 10.0), (3, 3, 3))
+    assert len(off) == 27
+    pts = off + np.array([100.0, 200.0, 300.0])
+    assert abs(pts[:, 0].mean() - 100.0) < 1e-9
+
+
+def test_block_variance_below_point_variance(oracle):
+    """block.rs:214-248."""
+    vg = sph()
+    xyz = np.array([[0.0, 0, 0], [60.0, 0, 0], [0.0, 60, 0]])
+    vals = [1.0, 2.0, 3.0]
+    c = (30.0, 30.0, 0.0)
+    st, block, w = oracle.block_krige(c, oracle.block_offsets((20.0, 20.0, 20.0), (3, 3, 3)), xyz, vals, vg)
+    _, point, _ = oracle.krige("ordinary", c, xyz, vals, vg)
+    assert st == 0 and block["variance"] <= point["variance"] + 1e-9
+    assert abs(w.sum() - 1.0) < 1e-9
+
+
+def test_block_nugget_averages_out(oracle):
+    """block.rs:267-296: C(B,B) = C - gamma_bar over a segment; a pure nugget leaves 0 and variance 1/2."""
+    c0, c, a, l = 0.4, 1.0, 100.0, 60.0
+    xyz = np.array([[-50.0, 0, 0], [70.0, 0, 0]])
+    off = oracle.block_offsets((l, 0.0, 0.0), (400, 1, 1))
+    _, e, _ = oracle.block_krige((0.0, 0.0, 0.0), off, xyz, [1.0, 2.0], sph(c, a, c0))
+    gamma_bar = c * (l / (2 * a) - l ** 3 / (20 * a ** 3))
+    assert abs(e["support"] - (c - gamma_bar)) < 1e-4
+    pure = Variogram([], nugget=1.0)
+    off = oracle.block_offsets((l, 1.0, 1.0), (400, 1, 1))
+    _, e, _ = oracle.block_krige((0.0, 0.0, 0.0), off, xyz, [1.0, 2.0], pure)
+    assert e["support"] == 0.0 and abs(e["variance"] - 0.5) < 1e-12
+
+
+def test_block_sample_on_a_node_sees_no_nugget(oracle):
+    """block.rs:298-310."""
+    off = oracle.block_offsets((30.0, 30.0, 30.0), (3, 3, 3))
+
+    def block(x):
+        return oracle.block_krige((0.0, 0.0, 0.0), off, np.array([[x, 0.0, 0.0], [40.0, 25.0, 0.0]]), [1.0, 3.0],
+                                  sph(nugget=0.5))
+
+    (_, on, won), (_, off_, woff) = block(0.0), block(1e-9)
+    assert abs(won[0] - woff[0]) < 1e-9 and abs(on["variance"] - off_["variance"]) < 1e-9
+
+
+def test_one_point_block_is_point_kriging(oracle):
+    """block.rs:312-340."""
+    vg = Variogram([Structure("spherical", 0.7, 100.0)], nugget=0.3)
+    one = oracle.block_offsets((10.0, 10.0, 10.0), (1, 1, 1))
+    c = (0.0, 0.0, 0.0)
+    xyz = np.array([[50.0, 0.0, 0.0]])
+    _, point, _ = oracle.krige("ordinary", c, xyz, [1.0], vg)
+    _, block, _ = oracle.block_krige(c, one, xyz, [1.0], vg)
+    gamma50 = 0.3 + 0.7 * (1.5 * 0.5 - 0.5 * 0.5 ** 3)
+    assert abs(point["variance"] - 2 * gamma50) < 1e-9 and abs(block["variance"] - point["variance"]) < 1e-9
+    assert block["support"] == 1.0
+    xyz = np.array([[0.0, 0.0, 0.0], [40.0, 25.0, 0.0]])
+    _, point, wp = oracle.krige("ordinary", c, xyz, [1.0, 3.0], vg)
+    _, block, wb = oracle.block_krige(c, one, xyz, [1.0, 3.0], vg)
+    assert abs(wb[0] - wp[0]) < 1e-9 and abs(block["variance"] - point["variance"]) < 1e-9
+
+
+def test_block_with_no_nugget_uses_point_covariances(oracle):
+    """With no nugget, block_cov_points equals cov_points (block.rs:355-370). Checked here on the results:
+    the oracle's block kriging equals a dense numpy solve of the same bordered system."""
+    off = oracle.block_offsets((30.0, 30.0, 30.0), (3, 3, 3))
+    xyz = np.array([[0.0, 0.0, 0.0], [40.0, 25.0, 0.0], [-20.0, 10.0, 5.0]])
+    _, e, w = oracle.block_krige((0.0, 0.0, 0.0), off, xyz, [1.0, 3.0, 2.0], sph())
+    pts = off
+    cov = lambda h: 1.0 - (1.5 * (h / 100) - 0.5 * (h / 100) ** 3 if h < 100 else 1.0)
+    rhs = np.array([np.mean([cov(np.linalg.norm(x - p)) for p in pts]) for x in xyz])
+    C = np.array([[cov(np.linalg.norm(a - b)) for b in xyz] for a in xyz])
+    K = np.block([[C, np.ones((3, 1))], [np.ones((1, 3)), np.zeros((1, 1))]])
+    sol = np.linalg.solve(K, np.r_[rhs, 1.0])
+    assert np.allclose(w, sol[:3], atol=1e-12) and abs(e["lagrange"] - sol[3]) < 1e-12
