@@ -177,6 +177,10 @@ struct btk_ctx {
   DevBuf<uint8_t> ord_temp;
   DevBuf<double> ord_part, ord_b6;
 
+  // hole codes of the fitted samples (btk_fit), for the search's hole rules
+  DevBuf<uint32_t> hole;
+  bool has_hole = false;
+
   // block support (btk_set_support): discretization offsets, C(B,B)
   DevBuf<double> sup, sup_cbb;
   int sup_n = 0;
@@ -240,10 +244,13 @@ int check_search(btk_ctx* ctx, const btk_search* s) {
   if (s->max_per_octant == 0) return fail(ctx, BTK_EINVAL, "max_per_sector must be >= 1");
   if (s->max_samples > kMaxN)
     return fail(ctx, BTK_EUNSUPPORTED, "more than 64 samples per system (the reference solves these by LU)");
-  if (s->max_per_hole >= 0) return fail(ctx, BTK_EUNSUPPORTED, "max_per_hole is not run on the GPU");
-  if (s->sectors > 0) return fail(ctx, BTK_EUNSUPPORTED, "plane sectors are not run on the GPU");
-  if (s->min_sectors >= 0 || s->max_empty_sectors >= 0 || s->min_holes >= 0)
-    return fail(ctx, BTK_EUNSUPPORTED, "min_sectors, max_empty_sectors and min_holes are not run on the GPU");
+  if (s->sectors > 0 && (s->sectors < 2 || s->sectors > 360 || s->max_per_sector < 1))
+    return fail(ctx, BTK_EINVAL, "sectors need 2 <= count <= 360 and max_per_sector >= 1");
+  const bool balances = s->octant || s->sectors > 0;
+  if ((s->min_sectors >= 0 || s->max_empty_sectors >= 0) && !balances)
+    return fail(ctx, BTK_EINVAL, "min_sectors and max_empty_sectors need octant or sectors");
+  if (s->min_holes == 0 || s->min_holes > s->max_samples)
+    return fail(ctx, BTK_EINVAL, "min_holes must be at least 1 and at most max_samples");
   const btk_aniso& a = s->aniso;
   if (a.on && (!(a.major > 0 && a.semi > 0 && a.minor > 0) || !fin(a.azimuth) || !fin(a.dip) ||
                !fin(a.rake)))
@@ -289,6 +296,17 @@ void make_searchdev(btk_ctx* ctx) {
   // both frames are the identity.
   const int ax_x = metric ? 1 : 0, sg_x = metric ? -1 : 1, ax_y = metric ? 0 : 1;
   d.nbits = d.nsec == 8 ? 3 : (d.nsec == 4 ? 2 : 0);
+  // Hole and sector rules (search.rs:476-577): the greedy selection kernel.
+  d.plane = s.sectors > 0 ? int(s.sectors) : 0;
+  d.balances = (s.octant || s.sectors > 0) ? 1 : 0;
+  d.rules = (s.max_per_hole >= 0 || s.sectors > 0 || s.min_sectors >= 0 || s.max_empty_sectors >= 0 ||
+             s.min_holes >= 0) ? 1 : 0;
+  d.max_per_hole = s.max_per_hole;
+  d.min_sectors = int(s.min_sectors), d.max_empty_sectors = int(s.max_empty_sectors), d.min_holes = int(s.min_holes);
+  d.rsec = d.plane ? d.plane : (s.octant ? d.nsec : 0);
+  d.rcap = d.plane ? int(s.max_per_sector) : (s.octant ? int(cap) : INT32_MAX);
+  d.hole = ctx->has_hole ? ctx->hole.p : nullptr;
+  d.sx = ctx->x.p, d.sy = ctx->y.p, d.sz = ctx->z.p;
   if (d.nsec == 8) {  // index bx << 2 | by << 1 | bz
     d.bit_axis[2] = ax_x, d.bit_sign[2] = sg_x, d.bit_mask[2] = 0xF0;
     d.bit_axis[1] = ax_y, d.bit_sign[1] = 1, d.bit_mask[1] = 0xCC;
@@ -800,7 +818,6 @@ int64_t btk_launch_count(const btk_ctx* ctx) { return ctx ? ctx->launches : 0; }
 int btk_fit(btk_ctx* ctx, int64_t n, const double* xyz, const double* values, const double* err_var,
             const int64_t* holes, const btk_search* search, const btk_variogram* vg) {
   if (!ctx) return BTK_EINVAL;
-  (void)holes;  // per-hole rules are refused by check_search
   ctx->fitted = false;
   if (n <= 0 || !xyz || !values) return fail(ctx, BTK_EINVAL, "fit needs at least one sample with coordinates and values");
   if (n >= int64_t(0xffffffffu)) return fail(ctx, BTK_EINVAL, "too many samples");
@@ -833,6 +850,17 @@ int btk_fit(btk_ctx* ctx, int64_t n, const double* xyz, const double* values, co
   CK(cudaMemcpyAsync(ctx->z.p, hz.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(ctx->v.p, values, n * sizeof(double), cudaMemcpyHostToDevice, s));
   if (err_var) CK(cudaMemcpyAsync(ctx->e.p, err_var, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  ctx->has_hole = holes != nullptr;
+  if (holes) {  // hole codes (crates/py/src/args.rs:276-292), equal codes = one hole
+    std::vector<uint32_t> hc(n);
+    for (int64_t i = 0; i < n; ++i) {
+      if (holes[i] < 0 || holes[i] >= int64_t(0xffffffffu)) return fail(ctx, BTK_EINVAL, "hole codes must be in 0 .. 2^32 - 2");
+      hc[i] = uint32_t(holes[i]);
+    }
+    CK(ctx->hole.grow(n));
+    CK(cudaMemcpyAsync(ctx->hole.p, hc.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+  }
   if ((rc = index_samples(ctx))) return rc;
   CK(cudaStreamSynchronize(s));
   ctx->fitted = true;

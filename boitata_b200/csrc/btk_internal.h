@@ -41,6 +41,18 @@ struct SearchDev {
   int nbits;
   int bit_axis[3], bit_sign[3];
   unsigned bit_mask[3];  // sectors whose index has bit k set
+  // Hole and sector rules (search.rs:476-577). When `rules` is set the
+  // search runs the reference's greedy selection over each target's nearest
+  // candidates (k_search_rules) instead of the per-sector lists.
+  int rules;
+  int64_t max_per_hole;                            // -1: none
+  int min_sectors, max_empty_sectors, min_holes;   // -1: none
+  int plane;     // plane sector count (2..360), 0: octants / quadrants or none
+  int balances;  // octants or plane sectors
+  int rsec;      // sector count when balancing
+  int rcap;      // samples per sector when balancing
+  const uint32_t* hole;        // hole code per sample, original order; null: each sample its own hole
+  const double *sx, *sy, *sz;  // sample world coordinates, original order
 };
 
 // Uniform grid over the projected samples, which are stored sorted by cell.

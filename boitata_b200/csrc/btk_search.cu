@@ -404,11 +404,371 @@ cudaError_t run(const Launch& L, const SearchDev& sp, const GridDev& g, const do
   return cudaGetLastError();
 }
 
+// ---- searches with hole and sector rules ----------------------------------
+// search.rs:476-577: per-hole caps, plane sectors, min_sectors,
+// max_empty_sectors and min_holes make a sample's acceptance depend on
+// earlier samples of other sectors, so the per-sector lists above no longer
+// give the selection. Here one warp serves one target: it grows a box of
+// cells from the target's cell, keeps every candidate within the threshold
+// (the radius, then the K-th nearest once more than 2K - 32 were seen: a
+// bitonic sort keeps the K nearest), sorts them by (d2, index), computes
+// their sectors in parallel, and lane 0 runs the reference's greedy selector
+// (Selector::offer / finish) over them. When the selection is not full and
+// candidates within the radius were cut, further rounds rescan for the
+// candidates beyond the last one offered that could still be accepted (open
+// sectors, holes below their cap; cells pruned by octant), until the
+// selection is full, no sector is open or the radius is exhausted: the
+// result is the reference's for any number of candidates.
+constexpr int kRulesK = BTK_RULES_CANDIDATES;
+constexpr int kHoleHash = 128;  // > 2 x 64 accepted holes
+constexpr uint32_t kNoHole = 0xffffffffu;
+
+struct RulesSmem {
+  double cd[2 * kRulesK];
+  uint32_t ci[2 * kRulesK];
+  uint16_t sec[2 * kRulesK];
+  uint32_t hkey[kHoleHash];
+  int hcnt[kHoleHash];
+  int per_sector[360];
+  uint32_t chosen[kMaxN];
+};
+
+// Ascending bitonic sort of (d2, index) keys 0 .. n-1 by one warp, padded to a
+// power of two with +inf keys.
+__device__ void warp_sort(double* d, uint32_t* ix, int n, int lane) {
+  int n2 = 1;
+  while (n2 < n) n2 <<= 1;
+  for (int j = n + lane; j < n2; j += 32) d[j] = INFINITY, ix[j] = 0xffffffffu;
+  __syncwarp();
+  for (int size = 2; size <= n2; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int t = lane; t < n2 / 2; t += 32) {
+        const int lo = 2 * t - (t & (stride - 1)), hi = lo + stride;
+        const bool up = (lo & size) == 0;
+        const bool sw = up ? key_less(d[hi], ix[hi], d[lo], ix[lo]) : key_less(d[lo], ix[lo], d[hi], ix[hi]);
+        if (sw) {
+          const double td = d[lo];
+          const uint32_t ti = ix[lo];
+          d[lo] = d[hi], ix[lo] = ix[hi];
+          d[hi] = td, ix[hi] = ti;
+        }
+      }
+      __syncwarp();
+    }
+}
+
+// Sectors::of (search.rs:427-441): plane sectors by angle in the major /
+// semi-major plane, else octants / quadrants.
+__device__ __forceinline__ int rules_sector(const SearchDev& sp, const double w[3], const double t[3]) {
+  if (!sp.plane) return sector_of(sp.axes, sp.planar, w, t);
+  const double v[3] = {xsub(w[0], t[0]), xsub(w[1], t[1]), xsub(w[2], t[2])};
+  double d[3];
+  mulv_exact(sp.axes, v, d);
+  constexpr double kTau = 6.283185307179586;
+  double turn = atan2(-d[0], d[1]);
+  turn = fmod(turn, kTau);
+  if (turn < 0.0) turn += kTau;
+  const int k = int(turn / kTau * double(sp.plane));
+  return k < sp.plane - 1 ? k : sp.plane - 1;
+}
+
+// Sectors::longest_empty (search.rs:445-467).
+__device__ int longest_empty(const SearchDev& sp, const int* counts) {
+  auto ring_run = [&](const int* ring, int len) {
+    bool all = true;
+    for (int i = 0; i < len; ++i) all = all && counts[ring[i]] == 0;
+    if (all) return len;
+    int run = 0, longest = 0;
+    for (int i = 0; i < 2 * len; ++i) {
+      run = counts[ring[i % len]] == 0 ? run + 1 : 0;
+      longest = max(longest, run);
+    }
+    return longest;
+  };
+  if (sp.plane) {
+    bool all = true;
+    for (int i = 0; i < sp.plane; ++i) all = all && counts[i] == 0;
+    if (all) return sp.plane;
+    int run = 0, longest = 0;
+    for (int i = 0; i < 2 * sp.plane; ++i) {
+      run = counts[i % sp.plane] == 0 ? run + 1 : 0;
+      longest = max(longest, run);
+    }
+    return longest;
+  }
+  if (sp.planar) {
+    const int ring[4] = {3, 1, 0, 2};
+    return ring_run(ring, 4);
+  }
+  const int up[4] = {7, 3, 1, 5}, down[4] = {6, 2, 0, 4};
+  return max(ring_run(up, 4), ring_run(down, 4));
+}
+
+// Hole slot of h in the warp's table of accepted holes (the free slot where
+// it would go when absent).
+__device__ __forceinline__ int hole_slot(const RulesSmem& S, uint32_t h) {
+  int k = int((h * 2654435761u) >> 25);  // 7 bits
+  for (int probe = 0; probe < kHoleHash; ++probe) {
+    if (S.hkey[k] == h || S.hkey[k] == kNoHole) break;
+    k = (k + 1) & (kHoleHash - 1);
+  }
+  return k;
+}
+
+// One pass over the cells around target q: every candidate with key above
+// (after_d, after_i), d2 within the threshold, and, once `filter` is set, in
+// an open sector (per_sector below the cap) from a hole below its cap, goes
+// into the warp's buffer; above 2K - 32 candidates the buffer keeps its K
+// nearest. Returns the count; *dropped tells whether candidates were cut.
+__device__ int rules_scan(const SearchDev& sp, const GridDev& g, RulesSmem& S, const double q[3], const double t[3],
+                          uint32_t left, double after_d, uint32_t after_i, bool filter, unsigned openmask,
+                          bool& dropped, int lane) {
+  const double glo[3] = {g.lo[0], g.lo[1], g.lo[2]};
+  const double ghi[3] = {g.lo[0] + g.dims[0] * g.h, g.lo[1] + g.dims[1] * g.h, g.lo[2] + g.dims[2] * g.h};
+  const unsigned all = sp.nsec > 1 ? (1u << sp.nsec) - 1u : 1u;
+  const bool prune = filter && sp.balances && !sp.plane;  // orthant pruning of rows and faces
+  int b0[3], b1[3], p0[3] = {1, 1, 1}, p1[3] = {0, 0, 0};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double u = fmin(fmax(floor((q[a] - g.lo[a]) / g.h), 0.0), double(g.dims[a] - 1));
+    b0[a] = b1[a] = int(u);
+  }
+  int n = 0;
+  double thr = sp.radius2;
+  dropped = false;
+  while (true) {
+    const int ny = b1[1] - b0[1] + 1;
+    const int64_t nrows = int64_t(ny) * (b1[2] - b0[2] + 1);
+    for (int64_t rb = 0; rb < nrows; rb += 32) {
+      const int64_t row = rb + lane;
+      uint32_t a1 = 0, e1 = 0, a2 = 0, e2 = 0;
+      if (row < nrows) {
+        const int y = b0[1] + int(row % ny), z = b0[2] + int(row / ny);
+        const bool inner = y >= p0[1] && y <= p1[1] && z >= p0[2] && z <= p1[2];
+        const int64_t base = int64_t(g.dims[0]) * (y + int64_t(g.dims[1]) * z);
+        int xa1 = 0, xb1 = -1, xa2 = 0, xb2 = -1;
+        if (!inner) {
+          xa1 = b0[0], xb1 = b1[0];
+        } else {
+          if (p0[0] > b0[0]) xa1 = b0[0], xb1 = p0[0] - 1;
+          if (p1[0] < b1[0]) xa2 = p1[0] + 1, xb2 = b1[0];
+        }
+        double lo[3], hi[3];
+        if (xb1 >= xa1) {
+          cell_box(g, xa1, xb1, y, y, z, z, lo, hi);
+          if (lb2(g, q, lo, hi) <= thr && (!prune || (box_sectors(sp, g, q, lo, hi, all) & openmask)))
+            a1 = g.start[base + xa1], e1 = g.start[base + xb1 + 1];
+        }
+        if (xb2 >= xa2) {
+          cell_box(g, xa2, xb2, y, y, z, z, lo, hi);
+          if (lb2(g, q, lo, hi) <= thr && (!prune || (box_sectors(sp, g, q, lo, hi, all) & openmask)))
+            a2 = g.start[base + xa2], e2 = g.start[base + xb2 + 1];
+        }
+      }
+      unsigned pending = __ballot_sync(kFull, e1 > a1 || e2 > a2);
+      while (pending) {
+        const int j = __ffs(pending) - 1;
+        pending &= pending - 1;
+#pragma unroll 1
+        for (int seg = 0; seg < 2; ++seg) {
+          const uint32_t a = __shfl_sync(kFull, seg ? a2 : a1, j), e = __shfl_sync(kFull, seg ? e2 : e1, j);
+          for (uint32_t base = a; base < e; base += 32) {
+            const uint32_t c = base + lane;
+            bool keep = false;
+            double d2 = 0.0;
+            uint32_t idx = 0;
+            if (c < e) {
+              d2 = d2_exact(g.px[c], g.py[c], g.pz[c], q[0], q[1], q[2]);
+              idx = g.idx[c];
+              keep = d2 <= thr && idx != left && key_less(after_d, after_i, d2, idx);
+              if (keep && filter) {
+                if (sp.balances) {
+                  const double wv[3] = {sp.sx[idx], sp.sy[idx], sp.sz[idx]};
+                  keep = S.per_sector[rules_sector(sp, wv, t)] < sp.rcap;
+                }
+                if (keep && sp.max_per_hole >= 0 && sp.hole) {
+                  const uint32_t h = sp.hole[idx];
+                  const int k = hole_slot(S, h);
+                  keep = !(S.hkey[k] == h && S.hcnt[k] >= sp.max_per_hole);
+                }
+              }
+            }
+            const unsigned bal = __ballot_sync(kFull, keep);
+            if (keep) {
+              const int pos = n + __popc(bal & ((1u << lane) - 1u));
+              S.cd[pos] = d2, S.ci[pos] = idx;
+            }
+            n += __popc(bal);
+            if (n > 2 * kRulesK - 32) {  // keep the K nearest
+              __syncwarp();
+              warp_sort(S.cd, S.ci, n, lane);
+              n = kRulesK;
+              thr = S.cd[kRulesK - 1];
+              dropped = true;
+            }
+            __syncwarp();
+          }
+        }
+      }
+    }
+    // Grow the box across each face beyond which cells may hold a candidate.
+#pragma unroll
+    for (int a = 0; a < 3; ++a) p0[a] = b0[a], p1[a] = b1[a];
+    bool grew = false;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      const int a = f >> 1;
+      const bool high = f & 1;
+      if (high ? b1[a] >= g.dims[a] - 1 : b0[a] <= 0) continue;
+      double lo[3] = {glo[0], glo[1], glo[2]}, hi[3] = {ghi[0], ghi[1], ghi[2]};
+      if (high)
+        lo[a] = g.lo[a] + (b1[a] + 1) * g.h;
+      else
+        hi[a] = g.lo[a] + b0[a] * g.h;
+      if (lb2(g, q, lo, hi) <= thr && (!prune || (box_sectors(sp, g, q, lo, hi, all) & openmask))) {
+        if (high)
+          b1[a] += 1;
+        else
+          b0[a] -= 1;
+        grew = true;
+      }
+    }
+    if (!grew) break;
+  }
+  __syncwarp();
+  if (n > 0) warp_sort(S.cd, S.ci, n, lane);
+  return n;
+}
+
+__global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, const double* __restrict__ tx,
+                                                      const double* __restrict__ ty, const double* __restrict__ tz,
+                                                      const int64_t* __restrict__ perm, int64_t m, int loo,
+                                                      uint32_t* __restrict__ nbr, int32_t* __restrict__ count,
+                                                      int8_t* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31;
+  RulesSmem& S = reinterpret_cast<RulesSmem*>(smem_raw)[threadIdx.x >> 5];
+  const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t w = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); w < m; w += warps) {
+    const int64_t ti = perm ? perm[w] : w;
+    if (ti < 0) continue;
+    const double t[3] = {tx[ti], ty[ti], tz[ti]};
+    double q[3];
+    {
+      const double d[3] = {xsub(t[0], sp.origin[0]), xsub(t[1], sp.origin[1]), xsub(t[2], sp.origin[2])};
+      mulv_exact(sp.frame, d, q);
+    }
+    const uint32_t left = loo ? uint32_t(ti) : 0xffffffffu;
+    for (int i = lane; i < kHoleHash; i += 32) S.hkey[i] = kNoHole, S.hcnt[i] = 0;
+    for (int i = lane; i < 360; i += 32) S.per_sector[i] = 0;
+    __syncwarp();
+    // Selector state (lane 0's copy is the one that counts)
+    int nchosen = 0, untagged = 0, nholes = 0;
+    double after_d = -1.0;
+    uint32_t after_i = 0u;
+    bool filter = false;
+    unsigned openmask = 0xffffffffu;
+    bool dropped = false;
+    // Each round offers the next candidates in (d2, index) order; a round
+    // after the first takes only candidates that could still be accepted.
+    for (int round = 0; round < 1 << 20; ++round) {
+      // After a cut, only the K nearest are an exact prefix of the (d2, index)
+      // order: entries kept since then can skip cut ones of equal d2.
+      const int nscan = rules_scan(sp, g, S, q, t, left, after_d, after_i, filter, openmask, dropped, lane);
+      const int n = dropped ? kRulesK : nscan;
+      if (sp.balances)
+        for (int i = lane; i < n; i += 32) {
+          const uint32_t idx = S.ci[i];
+          const double wv[3] = {sp.sx[idx], sp.sy[idx], sp.sz[idx]};
+          S.sec[i] = uint16_t(rules_sector(sp, wv, t));
+        }
+      __syncwarp();
+      if (lane == 0)  // Selector::offer (search.rs:535-559)
+        for (int i = 0; i < n && nchosen < sp.max_samples; ++i) {
+          const uint32_t idx = S.ci[i];
+          const uint32_t h = sp.hole ? sp.hole[idx] : kNoHole;
+          int slot = -1;
+          if (h != kNoHole) {
+            slot = hole_slot(S, h);
+            if (sp.max_per_hole >= 0 && S.hkey[slot] == h && S.hcnt[slot] >= sp.max_per_hole) continue;
+          }
+          if (sp.balances) {
+            const int o = S.sec[i];
+            if (S.per_sector[o] >= sp.rcap) continue;
+            S.per_sector[o] += 1;
+          }
+          if (h != kNoHole) {
+            if (S.hkey[slot] != h) S.hkey[slot] = h, ++nholes;
+            S.hcnt[slot] += 1;
+          } else {
+            ++untagged;
+          }
+          S.chosen[nchosen++] = idx;
+        }
+      nchosen = __shfl_sync(kFull, nchosen, 0);
+      __syncwarp();
+      if (nchosen >= sp.max_samples || !dropped || n == 0) break;
+      // Candidates beyond the last one offered may still be taken: those in
+      // sectors below their cap, from holes below theirs.
+      after_d = S.cd[n - 1], after_i = S.ci[n - 1];
+      filter = true;
+      openmask = 0u;
+      if (sp.balances) {
+        bool any_open = false;
+        for (int o = 0; o < sp.rsec; ++o) {
+          const bool open = S.per_sector[o] < sp.rcap;
+          any_open = any_open || open;
+          if (open && o < 32) openmask |= 1u << o;
+        }
+        if (!any_open) break;
+        if (sp.plane) openmask = 0xffffffffu;
+      } else {
+        openmask = 0xffffffffu;
+      }
+      __syncwarp();
+    }
+    if (lane == 0) {  // Selector::finish (search.rs:561-590)
+      int8_t st = BTK_ST_OK;
+      if (nchosen < sp.min_samples || (loo && nchosen == 0)) {
+        st = BTK_ST_SEARCH_FAILED;
+      } else if (sp.min_sectors >= 0) {
+        int held = 0;
+        for (int o = 0; o < sp.rsec; ++o) held += S.per_sector[o] > 0;
+        if (held < sp.min_sectors) st = BTK_ST_SEARCH_FAILED;
+      }
+      if (st == BTK_ST_OK && sp.max_empty_sectors >= 0 && longest_empty(sp, S.per_sector) > sp.max_empty_sectors)
+        st = BTK_ST_SEARCH_FAILED;
+      if (st == BTK_ST_OK && sp.min_holes >= 0 && nholes + untagged < sp.min_holes) st = BTK_ST_SEARCH_FAILED;
+      count[ti] = nchosen;
+      status[ti] = st;
+    }
+    __syncwarp();
+    for (int j = lane; j < sp.max_samples; j += 32) nbr[ti * sp.max_samples + j] = j < nchosen ? S.chosen[j] : 0xffffffffu;
+    __syncwarp();
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_search(const Launch& L, const SearchDev& sp, const GridDev& g, const double* tx,
                           const double* ty, const double* tz, const int64_t* perm, int64_t m, int loo,
                           uint32_t* nbr, int32_t* count, int8_t* status) {
+  if (sp.rules) {
+    constexpr int kWarps = 4;
+    const size_t smem = sizeof(RulesSmem) * kWarps;
+    cudaError_t e = cudaFuncSetAttribute(k_search_rules, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search_rules, kWarps * 32, smem);
+    if (e != cudaSuccess) return e;
+    int64_t blocks = int64_t(L.sm_count) * (per_sm > 0 ? per_sm : 1);
+    const int64_t need = (m + kWarps - 1) / kWarps;
+    if (blocks > need) blocks = need;
+    if (blocks < 1) blocks = 1;
+    k_search_rules<<<int(blocks), kWarps * 32, smem, L.stream>>>(sp, g, tx, ty, tz, perm, m, loo, nbr, count, status);
+    ++*L.counter;
+    return cudaGetLastError();
+  }
   const int slots = sp.nsec * sp.cap;
   const bool oct = sp.nsec > 1;
   if (slots > kMaxSlots) return cudaErrorInvalidValue;

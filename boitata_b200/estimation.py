@@ -50,6 +50,26 @@ def finite(values, what, n=None):
     return v
 
 
+def hole_codes(labels):
+    """Integer codes of hole labels (crates/py/src/args.rs:276-292): one per distinct label, in order of
+    first appearance, and a fresh one for each row without a label (None or NaN), which then counts as a
+    hole of its own."""
+    codes, out = {}, np.empty(len(labels), dtype=np.int64)
+    nxt = 0
+    for i, v in enumerate(labels):
+        missing = v is None or (isinstance(v, float) and math.isnan(v))
+        if missing:
+            out[i] = nxt
+            nxt += 1
+            continue
+        key = str(v)
+        if key not in codes:
+            codes[key] = nxt
+            nxt += 1
+        out[i] = codes[key]
+    return out
+
+
 def distinct(locs, holes=None):
     """Rows to keep so no two samples share a location: the first of each group,
     with a UserWarning naming the dropped groups (args.rs:318-376 over
@@ -151,6 +171,7 @@ class _Base:
         keep = distinct(locs, holes)
         locs, vals = np.ascontiguousarray(locs[keep]), np.ascontiguousarray(vals[keep])
         err = None if err is None else np.ascontiguousarray(err[keep])
+        self._holes = None if holes is None else np.ascontiguousarray(hole_codes(holes)[keep])
         self._samples = (locs, vals, err)
         if self._ctx is None:
             self._ctx = N.Context(self._device)
@@ -166,8 +187,10 @@ class _Base:
         if self._pass is None:
             locs, vals, err = self._samples
             vg = self.variogram.to_c()
+            holes = getattr(self, "_holes", None)
             rc = ctx._lib.btk_fit(ctx.handle, len(locs), locs.ctypes.data, vals.ctypes.data,
-                                  None if err is None else err.ctypes.data, None, ctypes.byref(s), ctypes.byref(vg))
+                                  None if err is None else err.ctypes.data,
+                                  None if holes is None else holes.ctypes.data, ctypes.byref(s), ctypes.byref(vg))
             ctx.check(rc, "fit")
         else:
             ctx.check(ctx._lib.btk_set_search(ctx.handle, ctypes.byref(s)), "search")

@@ -44,6 +44,7 @@ extern "C" {
 #define BTK_ST_SEARCH_FAILED 1 /* fewer than min_samples (EstimError::SearchFailed) */
 #define BTK_ST_SINGULAR 2      /* pivot <= 1e-12 * C(0) (kernel.rs:61) */
 #define BTK_ST_UNSUPPORTED 3   /* more than 64 samples */
+#define BTK_RULES_CANDIDATES 512 /* candidates a hole / sector rule search sorts per round */
 #define BTK_ST_FP64_FALLBACK 0x10 /* flag: the mixed form re-solved this system in FP64 */
 
 /* ---- variogram models (crates/variogram/src/model.rs:11-30) ---- */
@@ -92,14 +93,14 @@ typedef struct { /* crates/variogram/src/composite.rs:13-18 */
 typedef struct {
   int64_t min_samples, max_samples;
   double radius;
-  int64_t max_per_hole;      /* -1: none (not run on the GPU: BTK_EUNSUPPORTED) */
+  int64_t max_per_hole;      /* -1: none; holes from btk_fit */
   int64_t octant;            /* 0/1 */
-  int64_t sectors;           /* plane sectors, 0: none (BTK_EUNSUPPORTED) */
-  int64_t max_per_sector;
+  int64_t sectors;           /* plane sectors (2..360), 0: none */
+  int64_t max_per_sector;    /* plane sectors: samples per sector */
   int64_t max_per_octant;    /* -1: ceil(max_samples / sector count) */
-  int64_t min_sectors;       /* -1: none (BTK_EUNSUPPORTED when set) */
-  int64_t max_empty_sectors; /* -1: none (BTK_EUNSUPPORTED when set) */
-  int64_t min_holes;         /* -1: none (BTK_EUNSUPPORTED when set) */
+  int64_t min_sectors;       /* -1: none */
+  int64_t max_empty_sectors; /* -1: none */
+  int64_t min_holes;         /* -1: none; a sample without a hole counts as its own */
   btk_aniso aniso;           /* search ellipsoid; on = 0: the variogram's */
 } btk_search;
 

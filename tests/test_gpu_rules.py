@@ -1,0 +1,88 @@
+"""Searches with hole and sector rules (search.rs:476-577) on the GPU against the oracle's SearchTree:
+neighbour lists identical index for index and in order, equal success flags, and the estimates and
+leave-one-out estimates to 1e-10 (FP64 form)."""
+
+import numpy as np
+import pytest
+from test_gpu_parity import assert_same_estimates
+
+from boitata_b200 import OrdinaryKriging, Search
+from boitata_b200 import workloads as W
+from boitata_b200.estimation import hole_codes
+
+pytestmark = pytest.mark.gpu
+
+
+def drill_holes(holes=12):
+    """c2's drill holes, cut to `holes` x `holes` collars; hole label per composite."""
+    w = W.c2(holes=holes)
+    labels = [f"DH{i // 125:03d}" for i in range(len(w.coords))]
+    return w, labels
+
+
+def assert_same_neighbors(est, oracle, coords, search, vg, targets, codes):
+    idx, cnt, good = est.neighbors(targets)
+    tree = oracle.Tree(coords, search, vg, codes)
+    for t, target in enumerate(targets):
+        want_ok, want = tree.neighbors(target)
+        got = idx[t, : cnt[t]].tolist()
+        assert got == want, f"target {t} at {target}: {got} != {want}"
+        assert bool(good[t]) == want_ok, f"target {t}"
+
+
+def targets_in(w, k, seed, lo=(0, 0, 0), hi=(300, 300, 250)):
+    rng = np.random.default_rng(seed)
+    return rng.uniform(lo, hi, (k, 3))
+
+
+@pytest.mark.parametrize("search", [
+    Search(radius=250.0, octant=True, max_per_sector=4, max_samples=32, max_per_hole=3),
+    Search(radius=250.0, max_samples=24, max_per_hole=2),
+    Search(radius=120.0, octant=True, max_per_sector=2, max_samples=24, min_sectors=6, max_empty_sectors=1,
+           max_per_hole=2, min_holes=6),
+    Search(radius=200.0, sectors=6, max_per_sector=3, max_samples=16, max_per_hole=4),
+    Search(radius=90.0, sectors=12, max_per_sector=2, max_samples=20, min_sectors=9, max_empty_sectors=2,
+           min_holes=4),
+], ids=["octant+hole", "hole", "all-rules", "plane+hole", "plane-rules"])
+def test_rule_searches_match_the_oracle(oracle, search):
+    w, labels = drill_holes()
+    codes = hole_codes(labels)
+    t = targets_in(w, 400, 5)
+    est = OrdinaryKriging(w.variogram, search).fit(w.coords, w.values, holes=labels)
+    assert_same_neighbors(est, oracle, w.coords, search, w.variogram, t, codes)
+    got = est.predict_full(t)
+    ref = oracle.estimate_many(t, w.coords, w.values, search, w.variogram, holes=codes, neighbors=False)
+    assert_same_estimates(got, ref, 1e-10)
+
+
+def test_unlabelled_samples_count_as_their_own_holes(oracle):
+    w, _ = drill_holes(8)
+    s = Search(radius=150.0, octant=True, max_per_sector=3, max_samples=24, min_holes=20, max_per_hole=1)
+    t = targets_in(w, 200, 6, hi=(200, 200, 250))
+    est = OrdinaryKriging(w.variogram, s).fit(w.coords, w.values)
+    assert_same_neighbors(est, oracle, w.coords, s, w.variogram, t, None)
+
+
+def test_leave_one_out_with_hole_rules(oracle):
+    w, labels = drill_holes(6)
+    codes = hole_codes(labels)
+    s = Search(radius=150.0, octant=True, max_per_sector=3, max_samples=16, max_per_hole=2, min_holes=3)
+    est = OrdinaryKriging(w.variogram, s).fit(w.coords, w.values, holes=labels)
+    cv = est.cross_validate()
+    ref = oracle.estimate_many(None, w.coords, w.values, s, w.variogram, holes=codes, loo=True, neighbors=False)
+    fin = np.isfinite(ref["value"])
+    assert np.array_equal(fin, np.isfinite(np.asarray(cv.estimate)))
+    a, b = np.asarray(cv.estimate)[fin], ref["value"][fin]
+    assert np.all(np.abs(a - b) <= 1e-10 * (1 + np.maximum(np.abs(a), np.abs(b))))
+
+
+def test_quadrants_with_a_hole_cap_on_planar_data(oracle):
+    rng = np.random.default_rng(9)
+    xyz = np.column_stack([rng.uniform(0, 500, 3000), rng.uniform(0, 500, 3000), np.full(3000, 10.0)])
+    vals = rng.lognormal(size=3000)
+    labels = [f"L{i % 400}" for i in range(3000)]
+    w = W.c1()
+    s = Search(radius=200.0, octant=True, max_per_sector=3, max_samples=12, max_per_hole=1, max_empty_sectors=1)
+    est = OrdinaryKriging(w.variogram, s).fit(xyz, vals, holes=labels)
+    t = np.column_stack([rng.uniform(0, 500, 300), rng.uniform(0, 500, 300), np.full(300, 10.0)])
+    assert_same_neighbors(est, oracle, xyz, s, w.variogram, t, hole_codes(labels))
