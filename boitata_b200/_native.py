@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libboitata_b200.so")
 
 OK, EINVAL, EUNSUPPORTED, ECUDA, ENOTFITTED, ENOMEM = 0, -1, -2, -3, -4, -5
-ST_OK, ST_SEARCH_FAILED, ST_SINGULAR, ST_UNSUPPORTED, ST_FP64_FALLBACK = 0, 1, 2, 3, 0x10
+ST_OK, ST_SEARCH_FAILED, ST_SINGULAR, ST_UNSUPPORTED, ST_INVALID, ST_FP64_FALLBACK = 0, 1, 2, 3, 4, 0x10
 MODELS = {
     "spherical": 0, "exponential": 1, "gaussian": 2, "cubic": 3, "pentaspherical": 4,
     "circular": 5, "sinehole": 6, "matern": 7, "power": 8,

@@ -211,8 +211,8 @@ int fail(btk_ctx* c, int code, const std::string& msg) {
 
 bool fin(double v) { return std::isfinite(v); }
 
-// crates/variogram/src/{composite,model,aniso}.rs validate(); power has no
-// sill and goes to the reference's LU path, which this engine does not run.
+// crates/variogram/src/{composite,model,aniso}.rs validate(). A power
+// structure has no sill; its systems go to the dense LU (krige.rs:127-201).
 int check_vg(btk_ctx* ctx, const btk_variogram* vg) {
   if (!vg) return fail(ctx, BTK_EINVAL, "variogram is required");
   if (!(vg->nugget >= 0.0 && fin(vg->nugget))) return fail(ctx, BTK_EINVAL, "nugget must be finite and >= 0");
@@ -223,8 +223,6 @@ int check_vg(btk_ctx* ctx, const btk_variogram* vg) {
     if (!(s.sill >= 0.0 && fin(s.sill) && s.range > 0.0 && fin(s.range)))
       return fail(ctx, BTK_EINVAL, "structure sill must be finite and >= 0, range finite and > 0");
     if (s.model < BTK_SPHERICAL || s.model > BTK_POWER) return fail(ctx, BTK_EINVAL, "unknown variogram model");
-    if (s.model == BTK_POWER)
-      return fail(ctx, BTK_EUNSUPPORTED, "the power model has no sill (the reference solves it by LU)");
   }
   const btk_aniso& a = vg->aniso;
   if (a.on && (!(a.major > 0 && a.semi > 0 && a.minor > 0) || !fin(a.major) || !fin(a.semi) ||
@@ -242,8 +240,8 @@ int check_search(btk_ctx* ctx, const btk_search* s) {
   if (s->sectors > 0 && s->octant) return fail(ctx, BTK_EINVAL, "give octant or sectors, not both");
   if (s->max_per_octant >= 0 && !s->octant) return fail(ctx, BTK_EINVAL, "max_per_octant needs octant");
   if (s->max_per_octant == 0) return fail(ctx, BTK_EINVAL, "max_per_sector must be >= 1");
-  if (s->max_samples > kMaxN)
-    return fail(ctx, BTK_EUNSUPPORTED, "more than 64 samples per system (the reference solves these by LU)");
+  if (s->max_samples > kMaxLU)
+    return fail(ctx, BTK_EUNSUPPORTED, "more than 128 samples per system (the dense LU's shared-memory limit)");
   if (s->sectors > 0 && (s->sectors < 2 || s->sectors > 360 || s->max_per_sector < 1))
     return fail(ctx, BTK_EINVAL, "sectors need 2 <= count <= 360 and max_per_sector >= 1");
   const bool balances = s->octant || s->sectors > 0;
@@ -273,6 +271,9 @@ void make_vgdev(const btk_variogram& vg, VgDev& d) {
   }
   d.has_frame = vg.aniso.on ? 1 : 0;
   put9(vg.aniso.on ? aniso_matrix(vg.aniso) : eye(), d.frame);
+  d.stationary = 1;
+  for (int k = 0; k < vg.nstruct; ++k)
+    if (vg.s[k].model == BTK_POWER) d.stationary = 0;
 }
 
 // Search frame and sector set-up (search.rs:343-348, 395-425, 488-512).
@@ -299,8 +300,10 @@ void make_searchdev(btk_ctx* ctx) {
   // Hole and sector rules (search.rs:476-577): the greedy selection kernel.
   d.plane = s.sectors > 0 ? int(s.sectors) : 0;
   d.balances = (s.octant || s.sectors > 0) ? 1 : 0;
+  // More than 64 samples also take this kernel: its candidate buffer, not a
+  // per-lane heap, holds the list.
   d.rules = (s.max_per_hole >= 0 || s.sectors > 0 || s.min_sectors >= 0 || s.max_empty_sectors >= 0 ||
-             s.min_holes >= 0) ? 1 : 0;
+             s.min_holes >= 0 || s.max_samples > kMaxN) ? 1 : 0;
   d.max_per_hole = s.max_per_hole;
   d.min_sectors = int(s.min_sectors), d.max_empty_sectors = int(s.max_empty_sectors), d.min_holes = int(s.min_holes);
   d.rsec = d.plane ? d.plane : (s.octant ? d.nsec : 0);
@@ -402,8 +405,8 @@ int ensure_scratch(btk_ctx* ctx, int64_t m) {
   CK(ctx->nbr.grow(mm * size_t(ctx->search.max_samples)));
   CK(ctx->cnt.grow(mm));
   CK(ctx->sst.grow(mm));
-  CK(ctx->lists.grow(2 * mm));
-  CK(ctx->lens.grow(2));
+  CK(ctx->lists.grow(3 * mm));  // n <= 32, 32 < n <= 64, dense LU
+  CK(ctx->lens.grow(3));
   CK(ctx->redo.grow(2 * mm));
   CK(ctx->redo_len.grow(2));
   return BTK_OK;
@@ -461,6 +464,21 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
     CK(launch_support_cbb(L, ctx->vgd, ctx->sup.p, ctx->sup_n, ctx->sup_cbb.p));
     a.sup = ctx->sup.p, a.sup_n = ctx->sup_n, a.sup_cbb = ctx->sup_cbb.p;
   }
+  if (!ctx->vgd.stationary) {
+    // A power structure: every system through the dense LU, as the reference
+    // sends every non-stationary system to krige_lu (kernel.rs:31).
+    SolveDev al = a;
+    al.perm = perm, al.nwork = perm ? nwork : m;
+    ctx->mark(2, L.stream);
+    CK(launch_solve_lu(L, al, int(ctx->search.max_samples)));
+    ctx->mark(3, L.stream);
+    return BTK_OK;
+  }
+  const bool big = ctx->search.max_samples > kMaxN;
+  if (big) {
+    CK(cudaMemsetAsync(ctx->lens.p + 2, 0, sizeof(int64_t), L.stream));
+    a.lu = ctx->lists.p + 2 * m, a.lu_len = ctx->lens.p + 2;
+  }
   const bool two = ctx->search.max_samples > 32;
   const bool tiled = ctx->tuning.tile_union > 0;
   const int nb = two ? 2 : 1;
@@ -496,6 +514,11 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
       ar.list = ctx->redo.p + b * m, ar.list_len = ctx->redo_len.p + b;
       CK(launch_solve_redo(L, ar, b == 0 ? 32 : 64));
     }
+  if (big) {  // systems of more than 64 samples (FP64 in both precisions)
+    SolveDev al = a;
+    al.list = a.lu, al.list_len = a.lu_len;
+    CK(launch_solve_lu(L, al, int(ctx->search.max_samples)));
+  }
   ctx->mark(3, L.stream);
   return BTK_OK;
 }
@@ -1088,6 +1111,9 @@ int loo_sums(btk_ctx* ctx, const btk_variogram* vg, int64_t first, int64_t count
   if (rc) return rc;
   if (!ctx->frozen) return fail(ctx, BTK_EINVAL, "call btk_loo_freeze first");
   if ((rc = check_vg(ctx, vg))) return rc;
+  for (int k = 0; k < vg->nstruct; ++k)
+    if (vg->s[k].model == BTK_POWER)
+      return fail(ctx, BTK_EUNSUPPORTED, "the leave-one-out gradient takes stationary variograms (no power structure)");
   if (first < 0 || count < 0 || first + count > ctx->n)
     return fail(ctx, BTK_EINVAL, "the range must lie within the fitted samples");
   CK(cudaSetDevice(ctx->device));

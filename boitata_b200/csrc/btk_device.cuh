@@ -75,6 +75,7 @@ __device__ __forceinline__ double shape64(int model, double param, double t) {
       if (o == 1) return 1.0 - (1.0 + delta) * e;
       return 1.0 - (1.0 + delta + delta * delta / 3.0) * e;
     }
+    case BTK_POWER: return pow(t, param);  // unbounded (model.rs:124)
   }
   return 0.0;
 }

@@ -10,7 +10,8 @@
 
 namespace btk {
 
-constexpr int kMaxN = 64;       // most samples per system (kernel.rs:11)
+constexpr int kMaxN = 64;       // most samples per system of the warp kernels (kernel.rs:11)
+constexpr int kMaxLU = 128;     // most samples per system of the dense LU (krige.rs:127-201)
 constexpr int kMaxSlots = 64;   // most list entries per search lane
 constexpr double kPivot = 1e-12;  // kernel.rs:17
 constexpr double kEps = 1e-6;     // coincident.rs:11
@@ -23,6 +24,7 @@ struct VgDev {
   double param[BTK_MAX_STRUCT], sill[BTK_MAX_STRUCT], inv_range[BTK_MAX_STRUCT];
   int has_frame;
   double frame[9];  // diag(1/major, 1/semi, 1/minor) * rotation (aniso.rs:88-94)
+  int stationary;   // no power structure (composite.rs:64-66)
 };
 
 // Search parameters in the form the search kernel uses.
@@ -93,6 +95,12 @@ struct SolveDev {
   const double* sup;
   int sup_n;
   const double* sup_cbb;
+  // Dense LU path: systems of more than 64 samples go to `lu` (count at
+  // *lu_len); the LU kernel over every target walks `perm` (work slots, -1
+  // padding) when it is set, else targets 0 .. m-1.
+  int64_t *lu, *lu_len;
+  const int64_t* perm;
+  int64_t nwork;
 };
 
 // Tile-shared solve (btk_tile.cu): the systems of kTileTargets consecutive
@@ -195,6 +203,11 @@ cudaError_t launch_morton_order(const Launch& L, int64_t m, const double* x, con
 // the mean over pairs of point covariances with the nugget left out at zero
 // lag; the total sill for one point (btk_support.cu).
 cudaError_t launch_support_cbb(const Launch& L, const VgDev& vg, const double* off, int nd, double* cbb);
+
+// FP64 dense LU of the bordered system (btk_lu.cu) for the systems of
+// a.list (or every target, through a.perm / a.nwork when a.list is null),
+// at most kmax (<= kMaxLU) samples each.
+cudaError_t launch_solve_lu(const Launch& L, const SolveDev& a, int kmax);
 
 // Leave-one-out loss and gradient; sums[stride] receives the column sums.
 cudaError_t launch_loo_grad(const Launch& L, const GradDev& a, double* sums);

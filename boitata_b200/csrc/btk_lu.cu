@@ -1,0 +1,273 @@
+// Dense LU solve of the bordered kriging system, FP64, one CTA per system:
+// crates/estimation/src/krige.rs:127-201 (krige_lu), the reference's path
+// beyond kernel.rs (kernel.rs:11): systems of more than 64 samples, and
+// variograms that are not stationary (a power structure, composite.rs:64-66),
+// whose bordered matrix is not positive definite.
+//
+// The system and its LU live in shared memory. The factorisation follows
+// nalgebra 0.33's LU (lu.rs: partial pivoting on the first largest |a_ri| of
+// the column, a zero pivot column skipped, the column scaled by 1 / pivot,
+// the trailing block updated); solve applies the row swaps in order, then the
+// unit-lower and upper substitutions, and a zero U diagonal makes the system
+// singular, as LU::solve returning None does. The coincident guard
+// (coincident.rs:27-111) and block support apply as in the other solve paths.
+#include "btk_device.cuh"
+
+namespace btk {
+namespace {
+
+constexpr int kThreads = 128;
+
+struct LuHead {
+  int64_t ti;
+  int n, nn, dim, kind, twin, sing, nperm;
+  int best_i[kThreads];
+  double best_v[kThreads];
+  int cof[kMaxLU], cfirst[kMaxLU], csize[kMaxLU];
+};
+
+struct LuLayout {
+  size_t head, p, e, f, b, x, perm, a, total;
+  int stride;
+};
+
+__host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
+
+__host__ __device__ inline LuLayout lu_layout(int kmax) {
+  LuLayout l;
+  const int dmax = kmax + 1;
+  l.stride = dmax | 1;
+  l.head = 0;
+  l.p = align16(sizeof(LuHead));
+  l.e = l.p + sizeof(double) * 3 * kmax;
+  l.f = l.e + sizeof(double) * kmax;
+  l.b = l.f + sizeof(double) * kmax;
+  l.x = l.b + sizeof(double) * dmax;
+  l.perm = l.x + sizeof(double) * dmax;
+  l.a = align16(l.perm + sizeof(int) * 2 * dmax);
+  l.total = l.a + sizeof(double) * size_t(dmax) * l.stride;
+  return l;
+}
+
+__global__ void __launch_bounds__(kThreads) k_solve_lu(SolveDev a, int kmax) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const LuLayout lay = lu_layout(kmax);
+  LuHead& H = *reinterpret_cast<LuHead*>(smem + lay.head);
+  double* P = reinterpret_cast<double*>(smem + lay.p);  // [3][kmax], world
+  double* E = reinterpret_cast<double*>(smem + lay.e);
+  double* F = reinterpret_cast<double*>(smem + lay.f);  // f(z)
+  double* B = reinterpret_cast<double*>(smem + lay.b);
+  double* X = reinterpret_cast<double*>(smem + lay.x);
+  int* pa = reinterpret_cast<int*>(smem + lay.perm);
+  int* pb = pa + kmax + 1;
+  double* A = reinterpret_cast<double*>(smem + lay.a);
+  const int S = lay.stride;
+  const int tid = threadIdx.x;
+  const int64_t nitems = a.list ? *a.list_len : (a.perm ? a.nwork : a.m);
+  const VgDev& vg = a.vg;
+  for (int64_t item = blockIdx.x; item < nitems; item += gridDim.x) {
+    __syncthreads();
+    if (tid == 0) {
+      int64_t ti = a.list ? a.list[item] : (a.perm ? a.perm[item] : item);
+      H.ti = ti, H.n = 0, H.twin = 0, H.sing = 0, H.nperm = 0;
+      if (ti >= 0) {
+        const int n = a.count[ti];
+        const int8_t st = a.sstatus[ti];
+        H.kind = a.kinds ? int(a.kinds[ti]) : a.kind;
+        if (st != BTK_ST_OK) {
+          write_fail(a, ti, st, 0);
+          H.ti = -1;
+        } else if (n <= 0) {
+          write_fail(a, ti, BTK_ST_SEARCH_FAILED, 0);
+          H.ti = -1;
+        } else if (n > kmax) {
+          write_fail(a, ti, BTK_ST_UNSUPPORTED, 0);
+          H.ti = -1;
+        } else if (H.kind == BTK_SIMPLE && !vg.stationary) {  // check_simple (krige.rs:117-124)
+          write_fail(a, ti, BTK_ST_INVALID, 0);
+          H.ti = -1;
+        } else {
+          H.n = n;
+        }
+      }
+    }
+    __syncthreads();
+    const int64_t ti = H.ti;
+    if (ti < 0) continue;
+    const int n = H.n;
+    for (int r = tid; r < n; r += kThreads) {
+      const uint32_t j = a.nbr[ti * a.max_samples + r];
+      P[r] = a.sx[j], P[kmax + r] = a.sy[j], P[2 * kmax + r] = a.sz[j];
+      E[r] = a.se ? a.se[j] : 0.0;
+      F[r] = kind_f(H.kind, a.kparam, a.sv[j]);
+      if (a.twin && a.twin[j]) H.twin = 1;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int nn = n;
+      if (H.twin) {  // coincident guard, as merge_clusters in btk_solve.cu
+        const double eps2 = kEps * kEps;
+        int nc = 0;
+        for (int i = 0; i < n; ++i) {
+          int c = -1;
+          for (int q = 0; q < nc && c < 0; ++q) {
+            const int f = H.cfirst[q];
+            if (d2_exact(P[f], P[kmax + f], P[2 * kmax + f], P[i], P[kmax + i], P[2 * kmax + i]) <= eps2) c = q;
+          }
+          if (c < 0) c = nc, H.cfirst[nc] = i, H.csize[nc] = 0, ++nc;
+          H.cof[i] = c;
+          H.csize[c] += 1;
+        }
+        for (int c = 0; c < nc; ++c) {
+          const int f = H.cfirst[c];
+          double x0 = P[f], x1 = P[kmax + f], x2 = P[2 * kmax + f], err = E[f], zb = F[f];
+          if (H.csize[c] > 1) {
+            const double k = double(H.csize[c]);
+            double var = 0.0, zs = 0.0;
+            for (int i = f; i < n; ++i) {
+              if (H.cof[i] != c) continue;
+              var += E[i];
+              zs += F[i];
+              for (int j = f; j < n; ++j)
+                if (H.cof[j] == c)
+                  var += cov64(vg, lag_world(vg, P[i], P[kmax + i], P[2 * kmax + i], P[j], P[kmax + j],
+                                             P[2 * kmax + j]));
+            }
+            err = var / (k * k) - vg.c0;
+            zb = zs / k;
+          }
+          P[c] = x0, P[kmax + c] = x1, P[2 * kmax + c] = x2, E[c] = err, F[c] = zb;
+        }
+        nn = nc;
+      }
+      H.nn = nn;
+      H.dim = H.kind == BTK_SIMPLE ? nn : nn + 1;
+    }
+    __syncthreads();
+    const int nn = H.nn, dim = H.dim;
+    const double t0 = a.tx[ti], t1 = a.ty[ti], t2 = a.tz[ti];
+    // The bordered system (krige.rs:150-166) and its right-hand side.
+    for (int e = tid; e < dim * dim; e += kThreads) {
+      const int i = e / dim, j = e % dim;
+      double v;
+      if (i < nn && j < nn)
+        v = i == j ? vg.c0 + E[i]
+                   : cov64(vg, lag_world(vg, P[j], P[kmax + j], P[2 * kmax + j], P[i], P[kmax + i], P[2 * kmax + i]));
+      else
+        v = (i == nn && j == nn) ? 0.0 : 1.0;
+      A[i * S + j] = v;
+    }
+    for (int i = tid; i < dim; i += kThreads) {
+      const double v = i < nn ? support_cov(a, t0, t1, t2, P[i], P[kmax + i], P[2 * kmax + i]) : 1.0;
+      B[i] = v, X[i] = v;
+    }
+    __syncthreads();
+    // LU with partial pivoting (nalgebra lu.rs).
+    for (int k = 0; k < dim; ++k) {
+      double bv = -1.0;
+      int bi = k;
+      for (int r = k + tid; r < dim; r += kThreads) {
+        const double v = fabs(A[r * S + k]);
+        if (v > bv) bv = v, bi = r;
+      }
+      H.best_v[tid] = bv, H.best_i[tid] = bi;
+      __syncthreads();
+      for (int w = kThreads / 2; w > 0; w >>= 1) {
+        if (tid < w) {
+          const double v2 = H.best_v[tid + w];
+          const int i2 = H.best_i[tid + w];
+          if (v2 > H.best_v[tid] || (v2 == H.best_v[tid] && i2 < H.best_i[tid]))
+            H.best_v[tid] = v2, H.best_i[tid] = i2;
+        }
+        __syncthreads();
+      }
+      const int piv = H.best_i[0];
+      const double diag = A[piv * S + k];
+      __syncthreads();
+      if (diag == 0.0) continue;  // uniform: every thread read the same pivot
+      if (piv != k) {
+        for (int j = tid; j < dim; j += kThreads) {
+          const double tmp = A[k * S + j];
+          A[k * S + j] = A[piv * S + j];
+          A[piv * S + j] = tmp;
+        }
+        if (tid == 0) pa[H.nperm] = k, pb[H.nperm] = piv, ++H.nperm;
+      }
+      __syncthreads();
+      const double inv = 1.0 / diag;
+      for (int r = k + 1 + tid; r < dim; r += kThreads) A[r * S + k] *= inv;
+      __syncthreads();
+      const int rest = dim - k - 1;
+      for (int e = tid; e < rest * rest; e += kThreads) {
+        const int r = k + 1 + e / rest, c = k + 1 + e % rest;
+        A[r * S + c] = fma(-A[k * S + c], A[r * S + k], A[r * S + c]);
+      }
+      __syncthreads();
+    }
+    // LU::solve: row swaps, then L (unit lower) and U substitutions.
+    if (tid == 0)
+      for (int q = 0; q < H.nperm; ++q) {
+        const double tmp = X[pa[q]];
+        X[pa[q]] = X[pb[q]];
+        X[pb[q]] = tmp;
+      }
+    __syncthreads();
+    for (int i = 0; i < dim; ++i) {
+      const double coeff = X[i];
+      for (int r = i + 1 + tid; r < dim; r += kThreads) X[r] = fma(-coeff, A[r * S + i], X[r]);
+      __syncthreads();
+    }
+    for (int i = dim - 1; i >= 0; --i) {
+      const double diag = A[i * S + i];
+      if (diag == 0.0) {  // uniform
+        if (tid == 0) H.sing = 1;
+        break;
+      }
+      const double coeff = X[i] / diag;
+      __syncthreads();
+      if (tid == 0) X[i] = coeff;
+      for (int r = tid; r < i; r += kThreads) X[r] = fma(-coeff, A[r * S + i], X[r]);
+      __syncthreads();
+    }
+    __syncthreads();
+    if (tid == 0) {
+      if (H.sing) {
+        write_fail(a, ti, BTK_ST_SINGULAR, 0);
+      } else {  // krige.rs:177-200
+        double value = 0.0, swc = 0.0;
+        for (int i = 0; i < nn; ++i) value += X[i] * F[i], swc += X[i] * B[i];
+        const int kind = H.kind;
+        if (kind == BTK_SIMPLE) value = a.kparam + value;
+        if (kind == BTK_INDICATOR) value = value < 0.0 ? 0.0 : (value > 1.0 ? 1.0 : value);
+        const double mu = kind == BTK_SIMPLE ? 0.0 : X[nn];
+        const double cb = a.sup_n > 0 ? *a.sup_cbb : vg.c0;
+        a.value[ti] = value;
+        if (a.variance) a.variance[ti] = fmax(cb - swc - mu, 0.0);
+        if (a.lagrange) a.lagrange[ti] = mu;
+        if (a.n_used) a.n_used[ti] = n;
+        if (a.status) a.status[ti] = BTK_ST_OK;
+      }
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_solve_lu(const Launch& L, const SolveDev& a, int kmax) {
+  if (kmax < 1 || kmax > kMaxLU) return cudaErrorInvalidValue;
+  const size_t smem = lu_layout(kmax).total;
+  cudaError_t e = cudaFuncSetAttribute(k_solve_lu, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_lu, kThreads, smem);
+  if (e != cudaSuccess) return e;
+  int64_t blocks = int64_t(L.sm_count) * (per_sm > 0 ? per_sm : 1);
+  const int64_t items = a.perm ? a.nwork : a.m;
+  if (!a.list && blocks > items) blocks = items;
+  if (blocks < 1) blocks = 1;
+  k_solve_lu<<<int(blocks), kThreads, smem, L.stream>>>(a, kmax);
+  ++*L.counter;
+  return cudaGetLastError();
+}
+
+}  // namespace btk

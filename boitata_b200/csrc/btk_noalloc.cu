@@ -70,6 +70,8 @@ extern "C" int btk_solve_noalloc(int device, const btk_variogram* vg, int32_t ki
   std::string why;
   int rc = btk::prepare_variogram(vg, &vgd, &why);
   if (rc != BTK_OK) return say(err, errlen, rc, why);
+  if (!vgd.stationary)
+    return say(err, errlen, BTK_EUNSUPPORTED, "btk_solve_noalloc takes stationary variograms (no power structure)");
   if (m == 0) return BTK_OK;
 
   int before = 0;

@@ -430,7 +430,7 @@ struct RulesSmem {
   uint32_t hkey[kHoleHash];
   int hcnt[kHoleHash];
   int per_sector[360];
-  uint32_t chosen[kMaxN];
+  uint32_t chosen[kMaxLU];
 };
 
 // Ascending bitonic sort of (d2, index) keys 0 .. n-1 by one warp, padded to a

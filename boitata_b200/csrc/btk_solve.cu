@@ -178,6 +178,10 @@ __device__ __forceinline__ bool assemble(const SolveDev& a, SolveSmem<NW>& S, in
   kind = a.kinds ? int(a.kinds[ti]) : a.kind;
   n = a.count[ti];
   const int8_t st = a.sstatus[ti];
+  if (st == BTK_ST_OK && n > R && a.lu) {  // beyond this kernel: the dense LU takes it
+    if (row == 0) a.lu[atomicAdd(reinterpret_cast<unsigned long long*>(a.lu_len), 1ull)] = ti;
+    return false;
+  }
   if (st != BTK_ST_OK || n <= 0 || n > R) {
     if (row == 0) write_fail(a, ti, st != BTK_ST_OK ? st : (n > R ? BTK_ST_UNSUPPORTED : BTK_ST_SEARCH_FAILED), 0);
     return false;

@@ -43,7 +43,8 @@ extern "C" {
 #define BTK_ST_OK 0
 #define BTK_ST_SEARCH_FAILED 1 /* fewer than min_samples (EstimError::SearchFailed) */
 #define BTK_ST_SINGULAR 2      /* pivot <= 1e-12 * C(0) (kernel.rs:61) */
-#define BTK_ST_UNSUPPORTED 3   /* more than 64 samples */
+#define BTK_ST_UNSUPPORTED 3   /* more samples than the solve path holds */
+#define BTK_ST_INVALID 4       /* simple kriging with a power structure (EstimError::InvalidParameters, krige.rs:117-124) */
 #define BTK_RULES_CANDIDATES 512 /* candidates a hole / sector rule search sorts per round */
 #define BTK_ST_FP64_FALLBACK 0x10 /* flag: the mixed form re-solved this system in FP64 */
 
@@ -56,7 +57,7 @@ extern "C" {
 #define BTK_CIRCULAR 5
 #define BTK_SINEHOLE 6
 #define BTK_MATERN 7 /* param = order */
-#define BTK_POWER 8  /* param = exponent; not stationary: BTK_EUNSUPPORTED */
+#define BTK_POWER 8  /* param = exponent; not stationary: solved by the dense LU */
 #define BTK_MAX_STRUCT 4
 
 /* ---- kriging kinds (crates/estimation/src/krige.rs:20-27) ---- */
