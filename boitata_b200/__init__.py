@@ -12,6 +12,7 @@ from .errors import InvalidInput, Unsupported
 from .estimation import BlockKriging, CrossValidation, IndicatorKriging, OrdinaryKriging, SimpleKriging
 from .geometry import BlockModel, Geometry
 from .search import Search
+from .table import Table
 from .variogram import Structure, Variogram
 
 __all__ = [
@@ -25,6 +26,7 @@ __all__ = [
     "Search",
     "SimpleKriging",
     "Structure",
+    "Table",
     "Unsupported",
     "Variogram",
 ]

@@ -60,6 +60,11 @@ class OutputsC(ctypes.Structure):
                 ("n_used", ctypes.c_void_p), ("status", ctypes.c_void_p)]
 
 
+class DiagnosticsC(ctypes.Structure):
+    _fields_ = [("negative_weight_sum", ctypes.c_void_p), ("mean_distance", ctypes.c_void_p),
+                ("n_holes", ctypes.c_void_p)]
+
+
 P = ctypes.c_void_p
 SIGNATURES = {
     "btk_version": (ctypes.c_char_p, []),
@@ -76,6 +81,9 @@ SIGNATURES = {
                                                    ctypes.c_int32, ctypes.POINTER(OutputsC), P]),
     "btk_predict_kinds": (ctypes.c_int, [P, ctypes.c_int64, P, P, ctypes.c_double, ctypes.c_int32,
                                          ctypes.POINTER(OutputsC)]),
+    "btk_predict_diagnostics": (ctypes.c_int, [P, ctypes.c_int64, P, ctypes.c_int32, ctypes.c_double,
+                                               ctypes.c_int32, ctypes.POINTER(OutputsC),
+                                               ctypes.POINTER(DiagnosticsC)]),
     "btk_predict_kinds_device": (ctypes.c_int, [P, ctypes.c_int64, P, P, ctypes.c_double, ctypes.c_int32,
                                                 ctypes.POINTER(OutputsC), P]),
     "btk_cross_validate": (ctypes.c_int, [P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32,

@@ -155,7 +155,8 @@ struct btk_ctx {
   DevBuf<uint32_t> nbr;
   DevBuf<int32_t> cnt, o_nused;
   DevBuf<int8_t> sst, o_status, kinds;
-  DevBuf<double> o_value, o_var, o_lag;
+  DevBuf<double> o_value, o_var, o_lag, o_negw, o_mdist;
+  DevBuf<int32_t> o_nholes;
 
   bool timing = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -418,11 +419,12 @@ constexpr int64_t kOrderMin = 2048;
 // Search then solve for m targets whose coordinates are device SoA arrays.
 int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const double* ty, const double* tz,
              const int64_t* perm, int64_t nwork, int loo, int32_t kind, double kparam, int32_t precision,
-             const btk_outputs* o, const int8_t* kinds = nullptr) {
+             const btk_outputs* o, const int8_t* kinds = nullptr, const btk_diagnostics* dg = nullptr) {
   if (kind < BTK_ORDINARY || kind > BTK_INDICATOR) return fail(ctx, BTK_EINVAL, "unknown kriging kind");
   if (precision != BTK_FP64 && precision != BTK_MIXED) return fail(ctx, BTK_EINVAL, "unknown precision");
   if (kind == BTK_SIMPLE && !std::isfinite(kparam)) return fail(ctx, BTK_EINVAL, "simple kriging needs a finite mean");
   if (!o || !o->value) return fail(ctx, BTK_EINVAL, "outputs need a value array");
+  if (dg && !o->status) return fail(ctx, BTK_EINVAL, "diagnostics need the status output");
   int rc = ensure_scratch(ctx, m);
   if (rc) return rc;
   Launch L = ctx->launch(s);
@@ -464,6 +466,16 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
     CK(launch_support_cbb(L, ctx->vgd, ctx->sup.p, ctx->sup_n, ctx->sup_cbb.p));
     a.sup = ctx->sup.p, a.sup_n = ctx->sup_n, a.sup_cbb = ctx->sup_cbb.p;
   }
+  // The diagnostics pass over every work slot, after the solve has set each status.
+  auto diagnose = [&]() -> int {
+    if (!dg) return BTK_OK;
+    SolveDev ad = a;
+    ad.perm = perm, ad.nwork = perm ? nwork : m;
+    ad.negw = dg->negative_weight_sum, ad.mdist = dg->mean_distance, ad.nholes = dg->n_holes;
+    ad.hole = ctx->has_hole ? ctx->hole.p : nullptr;
+    CK(launch_solve_lu(L, ad, int(ctx->search.max_samples), true));
+    return BTK_OK;
+  };
   if (!ctx->vgd.stationary) {
     // A power structure: every system through the dense LU, as the reference
     // sends every non-stationary system to krige_lu (kernel.rs:31).
@@ -472,7 +484,7 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
     ctx->mark(2, L.stream);
     CK(launch_solve_lu(L, al, int(ctx->search.max_samples)));
     ctx->mark(3, L.stream);
-    return BTK_OK;
+    return diagnose();
   }
   const bool big = ctx->search.max_samples > kMaxN;
   if (big) {
@@ -520,7 +532,7 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
     CK(launch_solve_lu(L, al, int(ctx->search.max_samples)));
   }
   ctx->mark(3, L.stream);
-  return BTK_OK;
+  return diagnose();
 }
 
 int need_fit(btk_ctx* ctx) {
@@ -921,7 +933,7 @@ namespace {
 // context's scratch, which the compute stream serialises; chunks write
 // disjoint slices of the staged inputs and outputs.
 int predict_host(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds, int32_t kind, double kparam,
-                 int32_t precision, const btk_outputs* out) {
+                 int32_t precision, const btk_outputs* out, const btk_diagnostics* diag = nullptr) {
   int64_t chunk = ctx->tuning.host_chunk > 0 ? int64_t(ctx->tuning.host_chunk) : m;
   if ((m + chunk - 1) / chunk > 8) chunk = (m + 7) / 8;
   const int64_t nc = (m + chunk - 1) / chunk;
@@ -932,6 +944,11 @@ int predict_host(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds
   btk_outputs d{};
   int rc = host_outputs(ctx, m, out, &d);
   if (rc) return rc;
+  if (diag) {
+    CK(ctx->o_negw.grow(mm));
+    CK(ctx->o_mdist.grow(mm));
+    CK(ctx->o_nholes.grow(mm));
+  }
   if (!ctx->up) CK(cudaStreamCreateWithFlags(&ctx->up, cudaStreamNonBlocking));
   if (!ctx->down) CK(cudaStreamCreateWithFlags(&ctx->down, cudaStreamNonBlocking));
   for (cudaEvent_t& e : ctx->cev)
@@ -955,8 +972,9 @@ int predict_host(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds
     ++ctx->launches;
     CK(cudaGetLastError());
     btk_outputs dc{d.value + off, d.variance + off, d.lagrange + off, d.n_used + off, d.status + off};
+    btk_diagnostics dd{ctx->o_negw.p + off, ctx->o_mdist.p + off, ctx->o_nholes.p + off};
     if ((rc = run_path(ctx, ctx->stream, mc, t + off, t + m + off, t + 2 * m + off, nullptr, mc, 0, kind, kparam,
-                       precision, &dc, kinds ? ctx->kinds.p + off : nullptr)))
+                       precision, &dc, kinds ? ctx->kinds.p + off : nullptr, diag ? &dd : nullptr)))
       return rc;
     CK(cudaEventRecord(out_ready[c], ctx->stream));
     CK(cudaStreamWaitEvent(ctx->down, out_ready[c], 0));
@@ -970,6 +988,14 @@ int predict_host(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds
       CK(cudaMemcpyAsync(out->n_used + off, dc.n_used, n * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->down));
     if (out->status)
       CK(cudaMemcpyAsync(out->status + off, dc.status, n * sizeof(int8_t), cudaMemcpyDeviceToHost, ctx->down));
+    if (diag && diag->negative_weight_sum)
+      CK(cudaMemcpyAsync(diag->negative_weight_sum + off, dd.negative_weight_sum, n * sizeof(double),
+                         cudaMemcpyDeviceToHost, ctx->down));
+    if (diag && diag->mean_distance)
+      CK(cudaMemcpyAsync(diag->mean_distance + off, dd.mean_distance, n * sizeof(double), cudaMemcpyDeviceToHost,
+                         ctx->down));
+    if (diag && diag->n_holes)
+      CK(cudaMemcpyAsync(diag->n_holes + off, dd.n_holes, n * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->down));
   }
   CK(cudaStreamSynchronize(ctx->down));
   CK(cudaStreamSynchronize(ctx->stream));
@@ -987,6 +1013,18 @@ int btk_predict(btk_ctx* ctx, int64_t m, const double* xyz, int32_t kind, double
   if (m == 0) return BTK_OK;
   CK(cudaSetDevice(ctx->device));
   return predict_host(ctx, m, xyz, nullptr, kind, kparam, precision, out);
+}
+
+int btk_predict_diagnostics(btk_ctx* ctx, int64_t m, const double* xyz, int32_t kind, double kparam,
+                            int32_t precision, const btk_outputs* out, const btk_diagnostics* diag) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if (!out || !out->value || !out->status) return fail(ctx, BTK_EINVAL, "outputs need value and status arrays");
+  if (!diag) return fail(ctx, BTK_EINVAL, "diagnostics outputs are required");
+  if (m < 0 || (m > 0 && !xyz)) return fail(ctx, BTK_EINVAL, "targets are required");
+  if (m == 0) return BTK_OK;
+  CK(cudaSetDevice(ctx->device));
+  return predict_host(ctx, m, xyz, nullptr, kind, kparam, precision, out, diag);
 }
 
 int btk_predict_kinds_device(btk_ctx* ctx, int64_t m, const double* d_xyz, const int8_t* d_kinds, double kparam,

@@ -101,6 +101,11 @@ struct SolveDev {
   int64_t *lu, *lu_len;
   const int64_t* perm;
   int64_t nwork;
+  // Diagnostics pass (the LU kernel's `diag` form): per-target columns, and
+  // the fitted samples' hole codes (null: every sample untagged).
+  double *negw, *mdist;
+  int32_t* nholes;
+  const uint32_t* hole;
 };
 
 // Tile-shared solve (btk_tile.cu): the systems of kTileTargets consecutive
@@ -207,7 +212,9 @@ cudaError_t launch_support_cbb(const Launch& L, const VgDev& vg, const double* o
 // FP64 dense LU of the bordered system (btk_lu.cu) for the systems of
 // a.list (or every target, through a.perm / a.nwork when a.list is null),
 // at most kmax (<= kMaxLU) samples each.
-cudaError_t launch_solve_lu(const Launch& L, const SolveDev& a, int kmax);
+// With `diag`, the estimated systems (status OK) are solved again for their
+// weights and only a.negw / a.mdist / a.nholes are written.
+cudaError_t launch_solve_lu(const Launch& L, const SolveDev& a, int kmax, bool diag = false);
 
 // Leave-one-out loss and gradient; sums[stride] receives the column sums.
 cudaError_t launch_loo_grad(const Launch& L, const GradDev& a, double* sums);

@@ -11,6 +11,12 @@
 // unit-lower and upper substitutions, and a zero U diagonal makes the system
 // singular, as LU::solve returning None does. The coincident guard
 // (coincident.rs:27-111) and block support apply as in the other solve paths.
+//
+// The diagnostics form (DIAG) takes every system the solve estimated (status
+// OK) and writes only the table columns that need the samples or weights
+// (crates/py/src/estimation.rs:1046-1105): the negative weight sum of the
+// weights spread over coincident samples as coincident.rs:98-104 spreads them,
+// the mean Euclidean distance to the samples used, and their distinct holes.
 #include "btk_device.cuh"
 
 namespace btk {
@@ -20,6 +26,7 @@ constexpr int kThreads = 128;
 
 struct LuHead {
   int64_t ti;
+  double t[3];
   int n, nn, dim, kind, twin, sing, nperm;
   int best_i[kThreads];
   double best_v[kThreads];
@@ -49,6 +56,7 @@ __host__ __device__ inline LuLayout lu_layout(int kmax) {
   return l;
 }
 
+template <bool DIAG>
 __global__ void __launch_bounds__(kThreads) k_solve_lu(SolveDev a, int kmax) {
   extern __shared__ __align__(16) unsigned char smem[];
   const LuLayout lay = lu_layout(kmax);
@@ -72,9 +80,16 @@ __global__ void __launch_bounds__(kThreads) k_solve_lu(SolveDev a, int kmax) {
       H.ti = ti, H.n = 0, H.twin = 0, H.sing = 0, H.nperm = 0;
       if (ti >= 0) {
         const int n = a.count[ti];
-        const int8_t st = a.sstatus[ti];
+        const int8_t st = DIAG ? int8_t(a.status[ti] & 0x0F) : a.sstatus[ti];
         H.kind = a.kinds ? int(a.kinds[ti]) : a.kind;
-        if (st != BTK_ST_OK) {
+        H.t[0] = a.tx[ti], H.t[1] = a.ty[ti], H.t[2] = a.tz[ti];
+        if (DIAG) {
+          if (a.negw) a.negw[ti] = NAN;
+          if (a.mdist) a.mdist[ti] = NAN;
+          if (a.nholes) a.nholes[ti] = 0;
+          if (st != BTK_ST_OK || n <= 0 || n > kmax) H.ti = -1;
+          else H.n = n;
+        } else if (st != BTK_ST_OK) {
           write_fail(a, ti, st, 0);
           H.ti = -1;
         } else if (n <= 0) {
@@ -104,6 +119,29 @@ __global__ void __launch_bounds__(kThreads) k_solve_lu(SolveDev a, int kmax) {
     }
     __syncthreads();
     if (tid == 0) {
+      if (DIAG) {  // neighborhood_stats over the samples used (neighborhood.rs:76-98)
+        for (int i = 0; i < n; ++i) {  // distances, insertion-sorted ascending (a stable sort)
+          const double dx = P[i] - H.t[0], dy = P[kmax + i] - H.t[1], dz = P[2 * kmax + i] - H.t[2];
+          const double d = sqrt(dx * dx + dy * dy + dz * dz);
+          int q = i;
+          while (q > 0 && B[q - 1] > d) B[q] = B[q - 1], --q;
+          B[q] = d;
+        }
+        double sum = 0.0;
+        for (int i = 0; i < n; ++i) sum += B[i];
+        if (a.mdist) a.mdist[ti] = sum / double(n);
+        int holes = n;
+        if (a.hole) {
+          holes = 0;
+          for (int i = 0; i < n; ++i) {
+            const uint32_t h = a.hole[a.nbr[ti * a.max_samples + i]];
+            bool seen = false;
+            for (int q = 0; q < i && !seen; ++q) seen = a.hole[a.nbr[ti * a.max_samples + q]] == h;
+            holes += seen ? 0 : 1;
+          }
+        }
+        if (a.nholes) a.nholes[ti] = holes;
+      }
       int nn = n;
       if (H.twin) {  // coincident guard, as merge_clusters in btk_solve.cu
         const double eps2 = kEps * kEps;
@@ -145,7 +183,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_lu(SolveDev a, int kmax) {
     }
     __syncthreads();
     const int nn = H.nn, dim = H.dim;
-    const double t0 = a.tx[ti], t1 = a.ty[ti], t2 = a.tz[ti];
+    const double t0 = H.t[0], t1 = H.t[1], t2 = H.t[2];
     // The bordered system (krige.rs:150-166) and its right-hand side.
     for (int e = tid; e < dim * dim; e += kThreads) {
       const int i = e / dim, j = e % dim;
@@ -230,6 +268,17 @@ __global__ void __launch_bounds__(kThreads) k_solve_lu(SolveDev a, int kmax) {
       __syncthreads();
     }
     __syncthreads();
+    if (DIAG) {
+      if (tid == 0 && !H.sing && a.negw) {  // krige.rs:70-75 over the spread weights
+        double neg = -0.0;
+        for (int i = 0; i < n; ++i) {
+          const double w = H.twin ? X[H.cof[i]] / double(H.csize[H.cof[i]]) : X[i];
+          if (w < 0.0) neg += w;
+        }
+        a.negw[ti] = neg;
+      }
+      continue;
+    }
     if (tid == 0) {
       if (H.sing) {
         write_fail(a, ti, BTK_ST_SINGULAR, 0);
@@ -253,19 +302,21 @@ __global__ void __launch_bounds__(kThreads) k_solve_lu(SolveDev a, int kmax) {
 
 }  // namespace
 
-cudaError_t launch_solve_lu(const Launch& L, const SolveDev& a, int kmax) {
+cudaError_t launch_solve_lu(const Launch& L, const SolveDev& a, int kmax, bool diag) {
   if (kmax < 1 || kmax > kMaxLU) return cudaErrorInvalidValue;
+  if (diag && !a.status) return cudaErrorInvalidValue;
   const size_t smem = lu_layout(kmax).total;
-  cudaError_t e = cudaFuncSetAttribute(k_solve_lu, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  auto kern = diag ? k_solve_lu<true> : k_solve_lu<false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_lu, kThreads, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
   if (e != cudaSuccess) return e;
   int64_t blocks = int64_t(L.sm_count) * (per_sm > 0 ? per_sm : 1);
   const int64_t items = a.perm ? a.nwork : a.m;
   if (!a.list && blocks > items) blocks = items;
   if (blocks < 1) blocks = 1;
-  k_solve_lu<<<int(blocks), kThreads, smem, L.stream>>>(a, kmax);
+  kern<<<int(blocks), kThreads, smem, L.stream>>>(a, kmax);
   ++*L.counter;
   return cudaGetLastError();
 }

@@ -22,7 +22,10 @@ from . import _native as N
 from .errors import InvalidInput, Unsupported
 from .geometry import BlockModel, Geometry
 from .search import Search
+from .table import Table
 from .variogram import Variogram
+
+DIAGNOSTICS = ("negative_weight_sum", "mean_distance", "n_holes")
 
 PRECISIONS = {"fp64": N.FP64, "mixed": N.MIXED}
 
@@ -206,19 +209,28 @@ class _Base:
         return self._samples[1].copy()
 
     # -- predict ------------------------------------------------------------
-    def _run(self, xyz, precision):
+    def _run(self, xyz, precision, diagnostics=False):
         m = len(xyz)
         out = {k: np.full(m, np.nan) for k in ("value", "variance", "lagrange")}
         out["n_used"] = np.zeros(m, dtype=np.int32)
         out["status"] = np.zeros(m, dtype=np.int8)
+        if diagnostics:
+            out["negative_weight_sum"] = np.full(m, np.nan)
+            out["mean_distance"] = np.full(m, np.nan)
+            out["n_holes"] = np.zeros(m, dtype=np.int32)
         if m == 0:
             return out
         o = N.OutputsC(out["value"].ctypes.data, out["variance"].ctypes.data, out["lagrange"].ctypes.data,
                        out["n_used"].ctypes.data, out["status"].ctypes.data)
         xyz = np.ascontiguousarray(xyz, dtype=np.float64)
         ctx = self._ctx
-        rc = ctx._lib.btk_predict(ctx.handle, m, xyz.ctypes.data, self._kind, self._kparam, PRECISIONS[precision],
-                                  ctypes.byref(o))
+        if diagnostics:
+            d = N.DiagnosticsC(*(out[k].ctypes.data for k in DIAGNOSTICS))
+            rc = ctx._lib.btk_predict_diagnostics(ctx.handle, m, xyz.ctypes.data, self._kind, self._kparam,
+                                                  PRECISIONS[precision], ctypes.byref(o), ctypes.byref(d))
+        else:
+            rc = ctx._lib.btk_predict(ctx.handle, m, xyz.ctypes.data, self._kind, self._kparam,
+                                      PRECISIONS[precision], ctypes.byref(o))
         ctx.check(rc, "predict")
         return out
 
@@ -232,8 +244,9 @@ class _Base:
         z = locs[0, 2]
         return z if math.isfinite(z) and np.all(locs[:, 2] == z) else None
 
-    def predict_full(self, targets, *, precision=None):
-        """Every output of the engine: value, variance, lagrange, n_used, status and pass (1-based, 0 unfilled)."""
+    def predict_full(self, targets, *, precision=None, diagnostics=False):
+        """Every output of the engine: value, variance, lagrange, n_used, status and pass (1-based, 0 unfilled);
+        with `diagnostics`, also negative_weight_sum, mean_distance and n_holes of the samples used."""
         self._fitted()
         precision = precision or self.precision
         if precision not in PRECISIONS:
@@ -248,13 +261,13 @@ class _Base:
         else:
             xyz = points(targets)
         with self._support(targets):
-            return self._passes(xyz, precision)
+            return self._passes(xyz, precision, diagnostics)
 
     def _support(self, targets):
         """Context manager setting the engine's target support for one prediction (point support here)."""
         return contextlib.nullcontext()
 
-    def _passes(self, xyz, precision):
+    def _passes(self, xyz, precision, diagnostics=False):
         m = len(xyz)
         res = None
         remaining = np.arange(m)
@@ -262,7 +275,7 @@ class _Base:
             if len(remaining) == 0:
                 break
             self._use_pass(p)
-            out = self._run(xyz[remaining], precision)
+            out = self._run(xyz[remaining], precision, diagnostics)
             if res is None:
                 res = {k: v.copy() for k, v in out.items()}
                 res["pass"] = np.where(np.isfinite(out["value"]), 1, 0).astype(np.int32)
@@ -282,11 +295,46 @@ class _Base:
         targets : (n, 2|3) array, Geometry or BlockModel (centroids made on the device).
         """
         if diagnostics:
-            raise Unsupported("diagnostics tables are not produced by this engine; use predict_full")
+            return self._diagnostics(targets, precision)
         res = self.predict_full(targets, precision=precision)
         if return_variance:
             return res["value"], res["variance"]
         return res["value"]
+
+    def _support_variance(self, targets):
+        """C(v, v) of the targets' support: the sill for points (krige.rs:40-42)."""
+        return self.variogram.total_sill()
+
+    def _diagnostics(self, targets, precision):
+        """The diagnostics table (crates/py/src/estimation.rs:1046-1105): NaN where unestimated."""
+        res = self.predict_full(targets, precision=precision, diagnostics=True)
+        est = np.isfinite(res["value"])
+        nan = lambda v: np.where(est, v, np.nan)  # noqa: E731
+        sv = nan(np.full(len(est), self._support_variance(targets)))
+        var, mu = res["variance"], res["lagrange"]
+        cov = sv - var - mu  # Cov(Z, Z*) (krige.rs:58-61)
+        est_var = cov - mu  # Var(Z*) (krige.rs:63-68)
+        passes = np.maximum(res["pass"], 1) - 1
+        full = res["n_used"] >= np.array([s.max_samples for s in self.searches])[passes]
+        with np.errstate(divide="ignore", invalid="ignore"):
+            columns = {
+                "value": res["value"],
+                "variance": var,
+                "efficiency": (sv - var) / sv,
+                "slope": cov / est_var,
+                "n_samples": nan(res["n_used"].astype(np.float64)),
+                "pass": nan(res["pass"].astype(np.float64)),
+                "n_holes": nan(res["n_holes"].astype(np.float64)),
+                "n_other_domain": nan(np.zeros(len(est))),
+                "mean_distance": res["mean_distance"],
+                "negative_weight_sum": res["negative_weight_sum"],
+                "lagrange": mu,
+                "support_variance": sv,
+                "estimate_variance": est_var,
+                "max_samples_reached": nan(full.astype(np.float64)),
+                "target_met": np.full(len(est), np.nan),
+            }
+        return Table(columns)
 
     def predict_kinds(self, targets, kinds, *, mean=0.0, precision=None):
         """Every output at `targets` with a kriging kind per target ("ordinary" / "simple" / "indicator", or
@@ -428,6 +476,9 @@ class BlockKriging(_Base):
             yield
         finally:
             ctx._lib.btk_set_support(ctx.handle, None, None, None)
+
+    def _support_variance(self, targets):
+        return self.support_variance(targets if isinstance(targets, (BlockModel, Geometry)) else None)
 
     def support_variance(self, targets=None):
         """C(B,B), the mean covariance within a block (the reference's support_variance), for blocks turned

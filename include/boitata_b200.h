@@ -161,10 +161,27 @@ int btk_fit(btk_ctx* ctx, int64_t n, const double* xyz, const double* values, co
  * its ellipsoid differs. */
 int btk_set_search(btk_ctx* ctx, const btk_search* search);
 
+/* The per-target columns of the diagnostics table (crates/py/src/estimation.rs:
+ * 1046-1105) that need the samples used or the weights: host arrays of m
+ * entries, any of them NULL; NaN (n_holes 0) where a target is not estimated. */
+typedef struct btk_diagnostics {
+  double* negative_weight_sum; /* sum of the negative weights (Estimate::negative_weight_sum, krige.rs:70-75) */
+  double* mean_distance;       /* mean Euclidean distance to the samples used (neighborhood.rs:94-98) */
+  int32_t* n_holes;            /* distinct holes among the samples used; an untagged sample counts one
+                                  (neighborhood.rs:84-93) */
+} btk_diagnostics;
+
 /* Kriging at m targets given as host arrays (xyz m x 3 row-major); outputs
  * are host arrays of m entries. Host-device copies are part of the call. */
 int btk_predict(btk_ctx* ctx, int64_t m, const double* xyz, int32_t kind, double kparam, int32_t precision,
                 const btk_outputs* out);
+
+/* btk_predict plus the diagnostics columns (the estimator's predict with
+ * diagnostics=True, crates/py/src/estimation.rs:1734-1737). out->status is
+ * required: a second pass re-solves each estimated system for its weights by
+ * the dense LU (the weights of every solve form agree to rounding). */
+int btk_predict_diagnostics(btk_ctx* ctx, int64_t m, const double* xyz, int32_t kind, double kparam,
+                            int32_t precision, const btk_outputs* out, const btk_diagnostics* diag);
 
 /* As btk_predict, with device pointers: d_xyz is 3 arrays (x, y, z) of m
  * doubles laid out back to back; outputs are device arrays; the work is

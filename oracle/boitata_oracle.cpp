@@ -1245,15 +1245,56 @@ int32_t orc_scan_neighbors(int64_t n, const double* xyz, const int64_t* hole, co
   return ok ? 1 : 0;
 }
 
+// The per-target columns of the diagnostics table (crates/py/src/estimation.rs:
+// 1046-1105) that need the samples used or the weights. neighborhood_stats
+// (crates/estimation/src/neighborhood.rs:66-98), called with k = the samples
+// used, radius = inf and no anisotropy (estimation.rs:1041): Euclidean
+// distances (aniso.rs:114-119) sorted ascending (a stable sort), n_within,
+// n_holes (a hole counted once, an untagged sample once each) and their mean;
+// Estimate::negative_weight_sum (krige.rs:70-75). out[4] = {negative weight
+// sum, mean distance, n_holes, n_within}.
+static void diag_of(const double t[3], const std::vector<Sample>& sel, const Estimate& e, double* out) {
+  std::vector<std::pair<double, int64_t>> d;
+  d.reserve(sel.size());
+  for (auto& x : sel) {
+    double dx = x.loc[0] - t[0], dy = x.loc[1] - t[1], dz = x.loc[2] - t[2];
+    d.push_back({std::sqrt(dx * dx + dy * dy + dz * dz), x.hole});
+  }
+  std::stable_sort(d.begin(), d.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+  const double radius = std::numeric_limits<double>::infinity();
+  double within = 0.0, holes = 0.0, sum = 0.0;
+  std::vector<int64_t> seen;
+  for (auto& x : d) {
+    if (!(x.first <= radius)) continue;
+    within += 1.0;
+    if (x.second < 0) {
+      holes += 1.0;
+    } else if (std::find(seen.begin(), seen.end(), x.second) == seen.end()) {
+      seen.push_back(x.second);
+      holes += 1.0;
+    }
+  }
+  for (auto& x : d) sum += x.first;
+  double neg = e.weights.empty() ? NAN : -0.0;
+  for (double w : e.weights)
+    if (w < 0.0) neg = neg + w;
+  out[0] = neg;
+  out[1] = d.empty() ? NAN : sum / double(d.size());
+  out[2] = holes;
+  out[3] = within;
+}
+
 // crates/estimation/src/batch.rs:15-38 (estimate_many) and :165-190
 // (leave_one_out_at, when `loo` is set: targets are the samples themselves,
 // each searched without itself). One result per target; `nbr` (optional,
-// m x max_samples) receives the chosen indices, -1 padded. Threads take
-// static chunks of targets, like rayon's per-target independence.
+// m x max_samples) receives the chosen indices, -1 padded; `diag` (optional,
+// m x 4) the diagnostics columns of diag_of, NaN where a target is not
+// estimated. Threads take static chunks of targets, like rayon's per-target
+// independence.
 int32_t orc_estimate_many(int64_t m, const double* targets, int32_t loo, int64_t n, const double* xyz,
                           const double* v, const double* err, const int64_t* hole, const orc_search* sp,
                           const orc_variogram* vgp, int32_t kind, double kparam, int32_t nthreads,
-                          orc_result* res, int64_t* nbr) {
+                          orc_result* res, int64_t* nbr, double* diag) {
   std::vector<Sample> s = conv_samples(n, xyz, v, err, hole);
   SearchP p = conv_search(sp);
   if (!check(p)) return -1;
@@ -1269,6 +1310,7 @@ int32_t orc_estimate_many(int64_t m, const double* targets, int32_t loo, int64_t
       if (nbr) {
         for (size_t j = 0; j < maxs; ++j) nbr[size_t(k) * maxs + j] = j < chosen.size() ? int64_t(chosen[j]) : -1;
       }
+      if (diag) diag[4 * k] = diag[4 * k + 1] = diag[4 * k + 2] = diag[4 * k + 3] = NAN;
       if (!ok || (loo && chosen.empty())) { Estimate e; put(e, SEARCH_FAILED, &res[k]); continue; }
       std::vector<Sample> sel;
       sel.reserve(chosen.size());
@@ -1276,6 +1318,7 @@ int32_t orc_estimate_many(int64_t m, const double* targets, int32_t loo, int64_t
       Estimate e;
       int st = krige(kind, kparam, t, sel, vg, e);
       put(e, st, &res[k]);
+      if (diag && st == OK) diag_of(t, sel, e, diag + 4 * k);
     }
   };
   int nt = nthreads > 0 ? nthreads : orc_num_threads();

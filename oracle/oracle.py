@@ -92,7 +92,7 @@ def lib():
                                                     ctypes.POINTER(Vario), P, P, P]),
             "orc_estimate_many": (ctypes.c_int32, [ctypes.c_int64, P, ctypes.c_int32, ctypes.c_int64, P, P, P, P,
                                                    ctypes.POINTER(Srch), ctypes.POINTER(Vario), ctypes.c_int32,
-                                                   ctypes.c_double, ctypes.c_int32, P, P]),
+                                                   ctypes.c_double, ctypes.c_int32, P, P, P]),
             "orc_centroids": (None, [P, P, P, P, ctypes.c_int64, ctypes.c_int64, P]),
             "orc_krige_lists": (ctypes.c_int32, [ctypes.c_int64, P, ctypes.c_int64, P, P, P, P, ctypes.c_int64,
                                                  ctypes.POINTER(Vario), ctypes.c_int32, ctypes.c_double,
@@ -272,8 +272,10 @@ def scan_neighbors(target, xyz, s, vg=None, holes=None):
 
 
 def estimate_many(targets, xyz, values, s, vg, *, kind="ordinary", kparam=0.0, err=None, holes=None, loo=False,
-                  threads=0, neighbors=True):
-    """estimate_many / leave_one_out_at (batch.rs:15-38, 165-190) with krige of `kind`."""
+                  threads=0, neighbors=True, diagnostics=False):
+    """estimate_many / leave_one_out_at (batch.rs:15-38, 165-190) with krige of `kind`. With `diagnostics`,
+    also the per-target columns of the diagnostics table that need the samples or weights
+    (crates/py/src/estimation.rs:1046-1105): negative_weight_sum, mean_distance, n_holes, n_within."""
     xyz = _xyz(xyz)
     n = len(xyz)
     t = None if loo else _xyz(targets)
@@ -283,10 +285,11 @@ def estimate_many(targets, xyz, values, s, vg, *, kind="ordinary", kparam=0.0, e
     v = np.ascontiguousarray(values, dtype=np.float64)
     e = None if err is None else np.ascontiguousarray(err, dtype=np.float64)
     h = None if holes is None else np.ascontiguousarray(holes, dtype=np.int64)
+    dg = np.empty((m, 4)) if diagnostics else None
     cs, cv = search(s), variogram(vg)
     rc = lib().orc_estimate_many(m, _ptr(t), 1 if loo else 0, n, xyz.ctypes.data, v.ctypes.data, _ptr(e), _ptr(h),
                                  ctypes.byref(cs), ctypes.byref(cv), KINDS[kind], kparam, threads,
-                                 ctypes.cast(res, P), _ptr(nbr))
+                                 ctypes.cast(res, P), _ptr(nbr), _ptr(dg))
     if rc != 0:
         raise ValueError("oracle: invalid search parameters")
     arr = np.ctypeslib.as_array(ctypes.cast(res, ctypes.POINTER(ctypes.c_byte)), shape=(ctypes.sizeof(Result) * m,))
@@ -296,6 +299,10 @@ def estimate_many(targets, xyz, values, s, vg, *, kind="ordinary", kparam=0.0, e
     out = {k: rec[k].copy() for k in ("value", "variance", "lagrange", "n_used", "status")}
     if neighbors:
         out["neighbors"] = nbr
+    if diagnostics:
+        out["support"] = rec["support"].copy()
+        for j, key in enumerate(("negative_weight_sum", "mean_distance", "n_holes", "n_within")):
+            out[key] = dg[:, j].copy()
     return out
 
 

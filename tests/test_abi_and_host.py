@@ -131,3 +131,36 @@ def test_block_kriging_arguments_are_checked_as_the_reference_does():
             BlockKriging(vg, s, size, discretization=disc)
     b = BlockKriging(vg, s, (10.0, 20.0))
     assert b.size == (10.0, 20.0, 1.0) and b.discretization == (4, 4, 1)
+
+
+def test_table_columns_rows_and_exchange():
+    from boitata_b200 import Table
+
+    t = Table({"value": np.array([1.0, np.nan, 3.0]), "pass": np.array([1.0, np.nan, 2.0])})
+    assert t.column_names == ["value", "pass"] and t.num_rows == 3 and len(t) == 3
+    np.testing.assert_array_equal(t["pass"], [1.0, np.nan, 2.0])
+    f = t.filter(np.isfinite(t["value"]))
+    assert f.num_rows == 2 and f["value"].tolist() == [1.0, 3.0]
+    assert t.with_column("slope", np.ones(3)).column_names == ["value", "pass", "slope"]
+    assert t.to_pyarrow().column_names == ["value", "pass"]
+    assert list(t.to_pandas().columns) == ["value", "pass"]
+    with pytest.raises(KeyError):
+        t["missing"]
+    with pytest.raises(bt.InvalidInput):
+        Table({"a": np.ones(2), "b": np.ones(3)})
+
+
+def test_oracle_diagnostics_columns(oracle):
+    """The oracle's neighborhood_stats restatement on a hand-made case: distances 1, 2 (sorted), two holes."""
+    xyz = np.array([[2.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.5, 0.0]])
+    s = bt.Search(radius=10.0, max_samples=2, min_samples=1)
+    vg = bt.Variogram([bt.Structure("spherical", 1.0, 10.0)])
+    r = oracle.estimate_many(np.zeros((1, 3)), xyz, [1.0, 2.0, 3.0], s, vg, holes=np.array([5, 5, 6]),
+                             neighbors=False, diagnostics=True)
+    assert r["n_used"][0] == 2 and r["n_within"][0] == 2
+    assert r["mean_distance"][0] == pytest.approx((1.0 + 1.5) / 2)
+    assert r["n_holes"][0] == 2
+    r = oracle.estimate_many(np.zeros((1, 3)), xyz, [1.0, 2.0, 3.0], bt.Search(radius=10.0, max_samples=3), vg,
+                             holes=np.array([5, 5, 6]), neighbors=False, diagnostics=True)
+    assert r["n_holes"][0] == 2 and r["mean_distance"][0] == pytest.approx(4.5 / 3)
+    assert r["negative_weight_sum"][0] <= 0.0
