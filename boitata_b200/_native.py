@@ -41,7 +41,8 @@ class SearchC(ctypes.Structure):
                 ("max_per_hole", ctypes.c_int64), ("octant", ctypes.c_int64), ("sectors", ctypes.c_int64),
                 ("max_per_sector", ctypes.c_int64), ("max_per_octant", ctypes.c_int64),
                 ("min_sectors", ctypes.c_int64), ("max_empty_sectors", ctypes.c_int64),
-                ("min_holes", ctypes.c_int64), ("aniso", Aniso)]
+                ("min_holes", ctypes.c_int64), ("aniso", Aniso), ("calibration", ctypes.c_int64),
+                ("calibration_target", ctypes.c_double)]
 
 
 class GeometryC(ctypes.Structure):
@@ -62,7 +63,7 @@ class OutputsC(ctypes.Structure):
 
 class DiagnosticsC(ctypes.Structure):
     _fields_ = [("negative_weight_sum", ctypes.c_void_p), ("mean_distance", ctypes.c_void_p),
-                ("n_holes", ctypes.c_void_p)]
+                ("n_holes", ctypes.c_void_p), ("target_met", ctypes.c_void_p)]
 
 
 P = ctypes.c_void_p

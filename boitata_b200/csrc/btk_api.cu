@@ -157,6 +157,7 @@ struct btk_ctx {
   DevBuf<int8_t> sst, o_status, kinds;
   DevBuf<double> o_value, o_var, o_lag, o_negw, o_mdist;
   DevBuf<int32_t> o_nholes;
+  DevBuf<int8_t> met, o_met;  // calibration: target met per work slot target
 
   bool timing = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -250,6 +251,12 @@ int check_search(btk_ctx* ctx, const btk_search* s) {
     return fail(ctx, BTK_EINVAL, "min_sectors and max_empty_sectors need octant or sectors");
   if (s->min_holes == 0 || s->min_holes > s->max_samples)
     return fail(ctx, BTK_EINVAL, "min_holes must be at least 1 and at most max_samples");
+  if (s->calibration < 0 || s->calibration > 2) return fail(ctx, BTK_EINVAL, "unknown calibration");
+  if (s->calibration == 1 && !(std::isfinite(s->calibration_target) && s->calibration_target > 0.0))
+    return fail(ctx, BTK_EINVAL, "target_slope must be finite and > 0");
+  if (s->calibration == 2 && !(std::isfinite(s->calibration_target) && s->calibration_target <= 1.0))
+    return fail(ctx, BTK_EINVAL, "target_efficiency must be finite and <= 1");
+  if (s->calibration && s->sectors > 360) return fail(ctx, BTK_EINVAL, "at most 360 sectors");
   const btk_aniso& a = s->aniso;
   if (a.on && (!(a.major > 0 && a.semi > 0 && a.minor > 0) || !fin(a.azimuth) || !fin(a.dip) ||
                !fin(a.rake)))
@@ -425,6 +432,9 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
   if (kind == BTK_SIMPLE && !std::isfinite(kparam)) return fail(ctx, BTK_EINVAL, "simple kriging needs a finite mean");
   if (!o || !o->value) return fail(ctx, BTK_EINVAL, "outputs need a value array");
   if (dg && !o->status) return fail(ctx, BTK_EINVAL, "diagnostics need the status output");
+  const btk_search& srch = ctx->search;
+  if (srch.calibration == 1 && kind == BTK_SIMPLE && !kinds)
+    return fail(ctx, BTK_EINVAL, "simple kriging has a slope of regression of 1; calibrate it with target_efficiency");
   int rc = ensure_scratch(ctx, m);
   if (rc) return rc;
   Launch L = ctx->launch(s);
@@ -466,6 +476,17 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
     CK(launch_support_cbb(L, ctx->vgd, ctx->sup.p, ctx->sup_n, ctx->sup_cbb.p));
     a.sup = ctx->sup.p, a.sup_n = ctx->sup_n, a.sup_cbb = ctx->sup_cbb.p;
   }
+  if (srch.calibration) {  // the fewest leading samples that reach the target quality
+    CK(ctx->met.grow(size_t(m > 0 ? m : 1)));
+    SolveDev ac = a;
+    ac.perm = perm, ac.nwork = perm ? nwork : m;
+    CalDev cd{};
+    cd.count = ctx->cnt.p, cd.nbr = ctx->nbr.p, cd.met = ctx->met.p;
+    cd.calibration = int(srch.calibration), cd.target = srch.calibration_target;
+    cd.min_samples = int(srch.min_samples);
+    cd.balance = ctx->spd.balances;
+    CK(launch_calibrate(L, ac, ctx->spd, cd, int(srch.max_samples)));
+  }
   // The diagnostics pass over every work slot, after the solve has set each status.
   auto diagnose = [&]() -> int {
     if (!dg) return BTK_OK;
@@ -474,6 +495,12 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
     ad.negw = dg->negative_weight_sum, ad.mdist = dg->mean_distance, ad.nholes = dg->n_holes;
     ad.hole = ctx->has_hole ? ctx->hole.p : nullptr;
     CK(launch_solve_lu(L, ad, int(ctx->search.max_samples), true));
+    if (dg->target_met) {
+      if (srch.calibration)
+        CK(cudaMemcpyAsync(dg->target_met, ctx->met.p, size_t(m), cudaMemcpyDeviceToDevice, L.stream));
+      else
+        CK(cudaMemsetAsync(dg->target_met, 0xFF, size_t(m), L.stream));
+    }
     return BTK_OK;
   };
   if (!ctx->vgd.stationary) {
@@ -948,6 +975,7 @@ int predict_host(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds
     CK(ctx->o_negw.grow(mm));
     CK(ctx->o_mdist.grow(mm));
     CK(ctx->o_nholes.grow(mm));
+    CK(ctx->o_met.grow(mm));
   }
   if (!ctx->up) CK(cudaStreamCreateWithFlags(&ctx->up, cudaStreamNonBlocking));
   if (!ctx->down) CK(cudaStreamCreateWithFlags(&ctx->down, cudaStreamNonBlocking));
@@ -972,7 +1000,7 @@ int predict_host(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds
     ++ctx->launches;
     CK(cudaGetLastError());
     btk_outputs dc{d.value + off, d.variance + off, d.lagrange + off, d.n_used + off, d.status + off};
-    btk_diagnostics dd{ctx->o_negw.p + off, ctx->o_mdist.p + off, ctx->o_nholes.p + off};
+    btk_diagnostics dd{ctx->o_negw.p + off, ctx->o_mdist.p + off, ctx->o_nholes.p + off, ctx->o_met.p + off};
     if ((rc = run_path(ctx, ctx->stream, mc, t + off, t + m + off, t + 2 * m + off, nullptr, mc, 0, kind, kparam,
                        precision, &dc, kinds ? ctx->kinds.p + off : nullptr, diag ? &dd : nullptr)))
       return rc;
@@ -996,6 +1024,8 @@ int predict_host(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds
                          ctx->down));
     if (diag && diag->n_holes)
       CK(cudaMemcpyAsync(diag->n_holes + off, dd.n_holes, n * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->down));
+    if (diag && diag->target_met)
+      CK(cudaMemcpyAsync(diag->target_met + off, dd.target_met, n, cudaMemcpyDeviceToHost, ctx->down));
   }
   CK(cudaStreamSynchronize(ctx->down));
   CK(cudaStreamSynchronize(ctx->stream));
@@ -1124,6 +1154,8 @@ int btk_loo_freeze(btk_ctx* ctx) {
   if (rc) return rc;
   if (ctx->search.max_samples > 32)
     return fail(ctx, BTK_EUNSUPPORTED, "the leave-one-out gradient takes at most 32 samples per system");
+  if (ctx->search.calibration)
+    return fail(ctx, BTK_EUNSUPPORTED, "the leave-one-out gradient takes an uncalibrated search");
   CK(cudaSetDevice(ctx->device));
   const int64_t n = ctx->n;
   CK(ctx->loo_nbr.grow(size_t(n) * size_t(ctx->search.max_samples)));

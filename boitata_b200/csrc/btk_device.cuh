@@ -42,6 +42,23 @@ __device__ __forceinline__ int sector_of(const double* axes, int planar, const d
   return planar ? (bx << 1) | by : (bx << 2) | (by << 1) | bz;
 }
 
+// Sector of sample w around target t under a search's balancing
+// (search.rs:428-441): plane sectors by the turn of the offset in the search
+// frame, else the octant or quadrant.
+__device__ __forceinline__ int search_sector(const SearchDev& sp, const double w[3], const double t[3]) {
+  if (!sp.plane) return sector_of(sp.axes, sp.planar, w, t);
+  const double v[3] = {xsub(w[0], t[0]), xsub(w[1], t[1]), xsub(w[2], t[2])};
+  double d[3];
+  mulv_exact(sp.axes, v, d);
+  constexpr double kTau = 6.283185307179586;
+  double turn = atan2(-d[0], d[1]);
+  turn = fmod(turn, kTau);
+  if (turn < 0.0) turn += kTau;
+  const double x = turn / kTau * double(sp.plane);
+  const int k = x > 0.0 ? int(x) : 0;  // `as usize`: NaN and negatives to 0
+  return k < sp.plane - 1 ? k : sp.plane - 1;
+}
+
 // ---- variogram (crates/variogram/src/model.rs:76-126, composite.rs:69-85) ----
 // Normalized shape g at t = h / range for the stationary models. Precision
 // here is ordinary FP64 (the solve is compared to the oracle at 1e-10).

@@ -212,6 +212,20 @@ cudaError_t launch_support_cbb(const Launch& L, const VgDev& vg, const double* o
 // FP64 dense LU of the bordered system (btk_lu.cu) for the systems of
 // a.list (or every target, through a.perm / a.nwork when a.list is null),
 // at most kmax (<= kMaxLU) samples each.
+// Search calibration (btk_calibrate.cu): cuts each target's count to the
+// fewest leading samples that reach the target quality, after reordering the
+// list round-robin over the sectors when `balance` is set.
+struct CalDev {
+  int32_t* count;
+  uint32_t* nbr;
+  int8_t* met;      // 1 met, 0 not met, -1 not calibrated (search failed)
+  int calibration;  // 1 slope of regression, 2 kriging efficiency
+  double target;
+  int min_samples;
+  int balance;
+};
+cudaError_t launch_calibrate(const Launch& L, const SolveDev& a, const SearchDev& sp, const CalDev& c, int kmax);
+
 // With `diag`, the estimated systems (status OK) are solved again for their
 // weights and only a.negw / a.mdist / a.nholes are written.
 cudaError_t launch_solve_lu(const Launch& L, const SolveDev& a, int kmax, bool diag = false);

@@ -459,18 +459,6 @@ __device__ void warp_sort(double* d, uint32_t* ix, int n, int lane) {
 
 // Sectors::of (search.rs:427-441): plane sectors by angle in the major /
 // semi-major plane, else octants / quadrants.
-__device__ __forceinline__ int rules_sector(const SearchDev& sp, const double w[3], const double t[3]) {
-  if (!sp.plane) return sector_of(sp.axes, sp.planar, w, t);
-  const double v[3] = {xsub(w[0], t[0]), xsub(w[1], t[1]), xsub(w[2], t[2])};
-  double d[3];
-  mulv_exact(sp.axes, v, d);
-  constexpr double kTau = 6.283185307179586;
-  double turn = atan2(-d[0], d[1]);
-  turn = fmod(turn, kTau);
-  if (turn < 0.0) turn += kTau;
-  const int k = int(turn / kTau * double(sp.plane));
-  return k < sp.plane - 1 ? k : sp.plane - 1;
-}
 
 // Sectors::longest_empty (search.rs:445-467).
 __device__ int longest_empty(const SearchDev& sp, const int* counts) {
@@ -584,7 +572,7 @@ __device__ int rules_scan(const SearchDev& sp, const GridDev& g, RulesSmem& S, c
               if (keep && filter) {
                 if (sp.balances) {
                   const double wv[3] = {sp.sx[idx], sp.sy[idx], sp.sz[idx]};
-                  keep = S.per_sector[rules_sector(sp, wv, t)] < sp.rcap;
+                  keep = S.per_sector[search_sector(sp, wv, t)] < sp.rcap;
                 }
                 if (keep && sp.max_per_hole >= 0 && sp.hole) {
                   const uint32_t h = sp.hole[idx];
@@ -680,7 +668,7 @@ __global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, c
         for (int i = lane; i < n; i += 32) {
           const uint32_t idx = S.ci[i];
           const double wv[3] = {sp.sx[idx], sp.sy[idx], sp.sz[idx]};
-          S.sec[i] = uint16_t(rules_sector(sp, wv, t));
+          S.sec[i] = uint16_t(search_sector(sp, wv, t));
         }
       __syncwarp();
       if (lane == 0)  // Selector::offer (search.rs:535-559)

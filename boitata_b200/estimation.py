@@ -25,7 +25,7 @@ from .search import Search
 from .table import Table
 from .variogram import Variogram
 
-DIAGNOSTICS = ("negative_weight_sum", "mean_distance", "n_holes")
+DIAGNOSTICS = ("negative_weight_sum", "mean_distance", "n_holes", "target_met")
 
 PRECISIONS = {"fp64": N.FP64, "mixed": N.MIXED}
 
@@ -142,6 +142,8 @@ class _Base:
         searches = list(search) if isinstance(search, (list, tuple)) else [search]
         if not searches or not all(isinstance(s, Search) for s in searches):
             raise InvalidInput("search must be a Search or a sequence of Search (passes)")
+        if self._kind == N.SIMPLE and any(s.target_slope is not None for s in searches):
+            raise InvalidInput("simple kriging has a slope of regression of 1; calibrate it with target_efficiency")
         if self._kind == N.SIMPLE and not variogram.is_stationary():
             raise InvalidInput("simple kriging needs a variogram with a sill: every structure must be stationary "
                                "(not power); use ordinary kriging")
@@ -218,6 +220,7 @@ class _Base:
             out["negative_weight_sum"] = np.full(m, np.nan)
             out["mean_distance"] = np.full(m, np.nan)
             out["n_holes"] = np.zeros(m, dtype=np.int32)
+            out["target_met"] = np.full(m, -1, dtype=np.int8)
         if m == 0:
             return out
         o = N.OutputsC(out["value"].ctypes.data, out["variance"].ctypes.data, out["lagrange"].ctypes.data,
@@ -332,7 +335,7 @@ class _Base:
                 "support_variance": sv,
                 "estimate_variance": est_var,
                 "max_samples_reached": nan(full.astype(np.float64)),
-                "target_met": np.full(len(est), np.nan),
+                "target_met": np.where(est & (res["target_met"] >= 0), res["target_met"], np.nan),
             }
         return Table(columns)
 

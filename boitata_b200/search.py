@@ -24,7 +24,18 @@ class Search:
 
     def __init__(self, radius=None, *, max_samples=16, min_samples=1, octant=False, sectors=None,
                  max_per_sector=None, max_per_hole=None, rotation=None, ratios=None, ranges=None,
-                 min_sectors=None, max_empty_sectors=None, min_holes=None):
+                 min_sectors=None, max_empty_sectors=None, min_holes=None, target_slope=None,
+                 target_efficiency=None):
+        # crates/py/src/estimation.rs:458-473: at most one calibration target.
+        if target_slope is not None and target_efficiency is not None:
+            raise InvalidInput("give at most one of target_slope and target_efficiency")
+        if target_slope is not None and not (math.isfinite(float(target_slope)) and float(target_slope) > 0.0):
+            raise InvalidInput("target_slope must be finite and > 0")
+        if target_efficiency is not None and not (math.isfinite(float(target_efficiency)) and
+                                                  float(target_efficiency) <= 1.0):
+            raise InvalidInput("target_efficiency must be finite and <= 1")
+        self.target_slope = None if target_slope is None else float(target_slope)
+        self.target_efficiency = None if target_efficiency is None else float(target_efficiency)
         if radius is not None and ranges is not None:
             raise InvalidInput("give radius or ranges, not both")
         if radius is None and ranges is None:
@@ -122,7 +133,13 @@ class Search:
         s.max_empty_sectors = none if self.max_empty_sectors is None else self.max_empty_sectors
         s.min_holes = none if self.min_holes is None else self.min_holes
         s.aniso = aniso_c(self.anisotropy)
+        s.calibration = 1 if self.target_slope is not None else (2 if self.target_efficiency is not None else 0)
+        s.calibration_target = (self.target_slope if self.target_slope is not None else
+                                self.target_efficiency if self.target_efficiency is not None else 0.0)
         return s
+
+    def calibrated(self):
+        return self.target_slope is not None or self.target_efficiency is not None
 
     def __repr__(self):
         return (f"Search(radius={self.radius}, max_samples={self.max_samples}, min_samples={self.min_samples}, "

@@ -103,6 +103,13 @@ typedef struct {
   int64_t max_empty_sectors; /* -1: none */
   int64_t min_holes;         /* -1: none; a sample without a hole counts as its own */
   btk_aniso aniso;           /* search ellipsoid; on = 0: the variogram's */
+  /* Calibration (search.rs:94-100, crates/py/src/estimation.rs:846-895): each
+   * target keeps the fewest leading samples, from min_samples, whose slope of
+   * regression (1) or kriging efficiency (2) reaches calibration_target; all
+   * of them where none does. With octants or sectors the samples are first
+   * taken round-robin over the sectors (search.rs:913-936). 0: none. */
+  int64_t calibration;
+  double calibration_target;
 } btk_search;
 
 /* Block-model parent grid (crates/core/src/block_model.rs:19-26): corner
@@ -169,6 +176,8 @@ typedef struct btk_diagnostics {
   double* mean_distance;       /* mean Euclidean distance to the samples used (neighborhood.rs:94-98) */
   int32_t* n_holes;            /* distinct holes among the samples used; an untagged sample counts one
                                   (neighborhood.rs:84-93) */
+  int8_t* target_met;          /* calibrated search: 1 where the samples used reach the target, 0 where
+                                  even max_samples fall short; -1 without a calibration or estimate */
 } btk_diagnostics;
 
 /* Kriging at m targets given as host arrays (xyz m x 3 row-major); outputs

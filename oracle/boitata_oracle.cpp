@@ -710,6 +710,8 @@ struct SearchP {
   int64_t sectors = 0, max_per_sector = 0;  // plane sectors; 0 = None
   Aniso aniso;
   int64_t max_per_octant = -1, min_sectors = -1, max_empty_sectors = -1, min_holes = -1;
+  int calibration = 0;  // search.rs:94-100: 0 none, 1 Slope(target), 2 Efficiency(target)
+  double target = 0.0;
   bool balances() const { return octant || sectors > 0; }
 };
 
@@ -1090,6 +1092,104 @@ bool scan_neighbors(const double t[3], const std::vector<Sample>& s, const Searc
   return sel.finish();
 }
 
+// crates/estimation/src/search.rs:913-936 (SearchTree::balanced): with a
+// calibration and octants or sectors, the chosen samples go round-robin over
+// the sectors, each sector in selection order: a stable sort by the rank of
+// each sample within its sector.
+std::vector<size_t> balanced(const Tree& tree, const double t[3], const std::vector<size_t>& chosen) {
+  if (!tree.params.balances() || tree.params.calibration == 0) return chosen;
+  std::vector<size_t> seen(tree.sectors.count(), 0);
+  std::vector<std::pair<size_t, size_t>> ranked;
+  for (size_t i : chosen) {
+    size_t o = tree.sectors.of(t, (*tree.samples)[i].loc);
+    seen[o] += 1;
+    ranked.push_back({seen[o], i});
+  }
+  std::stable_sort(ranked.begin(), ranked.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+  std::vector<size_t> out;
+  for (auto& r : ranked) out.push_back(r.second);
+  return out;
+}
+
+// crates/estimation/src/kriging_algebra.rs:336-395 (prefix_quality) for the
+// drifts of ordinary kriging (one column of ones, x0 = 1) and simple kriging
+// (none). nalgebra's Cholesky (column j from the columns before it by axpy,
+// then sqrt of a positive diagonal and a division) of the covariance matrix
+// serves every leading part; its lower solves are column sweeps. Entry k is
+// the slope and efficiency from the first k + 1 samples; ok[k] = 0 for None.
+void prefix_quality(const std::vector<Sample>& smp, const Variogram& vg, const std::vector<double>& rhs,
+                    bool ordinary, double support, std::vector<double>& slope, std::vector<double>& eff,
+                    std::vector<int>& ok) {
+  const size_t n = smp.size();
+  slope.assign(n, NAN), eff.assign(n, NAN), ok.assign(n, 0);
+  std::vector<double> L(n * n, 0.0);  // column-major, as nalgebra stores it
+  auto at = [&](size_t i, size_t j) -> double& { return L[j * n + i]; };
+  for (size_t j = 0; j < n; ++j)
+    for (size_t i = 0; i < n; ++i) at(i, j) = vg.cov_points(smp[i].loc, smp[j].loc) + (i == j ? smp[i].err : 0.0);
+  for (size_t j = 0; j < n; ++j) {
+    for (size_t k = 0; k < j; ++k) {
+      const double factor = -at(j, k);
+      for (size_t i = j; i < n; ++i) at(i, j) = factor * at(i, k) + at(i, j);
+    }
+    const double diag = at(j, j);
+    if (!(diag > 0.0)) return;  // not positive definite: every entry None
+    const double denom = std::sqrt(diag);
+    at(j, j) = denom;
+    for (size_t i = j + 1; i < n; ++i) at(i, j) = at(i, j) / denom;
+  }
+  std::vector<double> y = rhs, z(n, 1.0);
+  for (size_t i = 0; i < n; ++i) {  // solve_lower_triangular, column by column
+    const double cy = y[i] / at(i, i), cz = z[i] / at(i, i);
+    y[i] = cy, z[i] = cz;
+    for (size_t r = i + 1; r < n; ++r) y[r] = (-cy) * at(r, i) + y[r], z[r] = (-cz) * at(r, i) + z[r];
+  }
+  double sy = 0.0, a = 0.0, b = 0.0;
+  for (size_t k = 0; k < n; ++k) {
+    sy += y[k] * y[k];
+    double cov = sy, mu = 0.0;
+    if (ordinary) {
+      a = a + z[k] * z[k];
+      b = b + z[k] * y[k];
+      if (!(a > 0.0)) continue;
+      const double l = std::sqrt(a);  // the 1 x 1 Cholesky factor and its solve
+      const double m = ((b - 1.0) / l) / l;
+      cov = sy - m * b;
+      mu = m * 1.0;
+    }
+    slope[k] = cov / (cov - mu);
+    eff[k] = (cov + mu) / support;
+    ok[k] = 1;
+  }
+}
+
+// kriging_algebra.rs:397-412 (calibrated_count): the fewest leading samples,
+// from min_samples, whose quality meets the calibration (met = 1), or all.
+size_t calibrated_count(const SearchP& p, const std::vector<double>& slope, const std::vector<double>& eff,
+                        const std::vector<int>& ok, int* met) {
+  const size_t from = std::max<size_t>(p.min_samples, 1);
+  for (size_t k = from - 1; k < ok.size(); ++k) {
+    if (!ok[k]) continue;
+    const bool meets = p.calibration == 1 ? slope[k] >= p.target : eff[k] >= p.target;
+    if (meets) { *met = 1; return k + 1; }
+  }
+  *met = 0;
+  return ok.size();
+}
+
+// crates/py/src/estimation.rs:846-895 (Method::calibrated) for the kriging
+// kinds and block kriging: the samples a calibrated search keeps, in place.
+// `rhs` holds each sample's covariance with the target's support.
+int calibrate(const SearchP& p, const Variogram& vg, int kind, const std::vector<double>& rhs, double support,
+              std::vector<Sample>& sel) {
+  if (p.calibration == 0) return -1;
+  std::vector<double> slope, eff;
+  std::vector<int> ok;
+  prefix_quality(sel, vg, rhs, kind != SIMPLE, support, slope, eff, ok);
+  int met = 0;
+  sel.resize(calibrated_count(p, slope, eff, ok, &met));
+  return met;
+}
+
 }  // namespace
 
 // ===================================================================== C ABI
@@ -1104,6 +1204,8 @@ struct orc_search {
   int64_t max_per_hole, octant, sectors, max_per_sector, max_per_octant, min_sectors,
       max_empty_sectors, min_holes;
   orc_aniso aniso;
+  int64_t calibration;  // 0 none, 1 slope, 2 efficiency
+  double calibration_target;
 };
 struct orc_result { double value, variance, lagrange, support; int64_t n_used; int32_t status; };
 
@@ -1132,6 +1234,8 @@ static SearchP conv_search(const orc_search* s) {
   p.max_empty_sectors = s->max_empty_sectors;
   p.min_holes = s->min_holes;
   p.aniso = conv_aniso(s->aniso);
+  p.calibration = int(s->calibration);
+  p.target = s->calibration_target;
   return p;
 }
 static std::vector<Sample> conv_samples(int64_t n, const double* xyz, const double* v, const double* err,
@@ -1187,6 +1291,20 @@ int32_t orc_krige(int32_t which, int32_t kind, double kparam, const double* t, i
   put(e, st, res);
   if (st == OK && weights) std::copy(e.weights.begin(), e.weights.end(), weights);
   return st;
+}
+
+// prefix_quality (kriging_algebra.rs:336-395) of n samples around t with the
+// ordinary (1) or simple (0) drift and support variance `support`: slope,
+// efficiency and ok (0 for None) per leading part.
+void orc_prefix_quality(int64_t n, const double* xyz, const double* err, const double* t, const orc_variogram* vgp,
+                        int32_t ordinary, double support, double* slope, double* eff, int32_t* ok) {
+  Variogram vg = conv_vg(vgp);
+  std::vector<Sample> s = conv_samples(n, xyz, nullptr, err, nullptr);
+  std::vector<double> rhs, sl, ef;
+  for (auto& x : s) rhs.push_back(vg.cov_points(x.loc, t));
+  std::vector<int> k;
+  prefix_quality(s, vg, rhs, ordinary != 0, support, sl, ef, k);
+  for (int64_t i = 0; i < n; ++i) slope[i] = sl[i], eff[i] = ef[i], ok[i] = k[i];
 }
 
 // Brute-force (d2 bits, index) stream of the grid, for the grid tests:
@@ -1288,8 +1406,9 @@ static void diag_of(const double t[3], const std::vector<Sample>& sel, const Est
 // (leave_one_out_at, when `loo` is set: targets are the samples themselves,
 // each searched without itself). One result per target; `nbr` (optional,
 // m x max_samples) receives the chosen indices, -1 padded; `diag` (optional,
-// m x 4) the diagnostics columns of diag_of, NaN where a target is not
-// estimated. Threads take static chunks of targets, like rayon's per-target
+// m x 5) the diagnostics columns of diag_of and target_met (1, 0; NaN without
+// a calibration), NaN where a target is not estimated. A calibrated search
+// orders the chosen samples with balanced and keeps the calibrated count. Threads take static chunks of targets, like rayon's per-target
 // independence.
 int32_t orc_estimate_many(int64_t m, const double* targets, int32_t loo, int64_t n, const double* xyz,
                           const double* v, const double* err, const int64_t* hole, const orc_search* sp,
@@ -1310,15 +1429,24 @@ int32_t orc_estimate_many(int64_t m, const double* targets, int32_t loo, int64_t
       if (nbr) {
         for (size_t j = 0; j < maxs; ++j) nbr[size_t(k) * maxs + j] = j < chosen.size() ? int64_t(chosen[j]) : -1;
       }
-      if (diag) diag[4 * k] = diag[4 * k + 1] = diag[4 * k + 2] = diag[4 * k + 3] = NAN;
+      if (diag) for (int c = 0; c < 5; ++c) diag[5 * k + c] = NAN;
       if (!ok || (loo && chosen.empty())) { Estimate e; put(e, SEARCH_FAILED, &res[k]); continue; }
       std::vector<Sample> sel;
       sel.reserve(chosen.size());
-      for (size_t i : chosen) sel.push_back(s[i]);
+      for (size_t i : balanced(tree, t, chosen)) sel.push_back(s[i]);
+      int met = -1;
+      if (p.calibration) {
+        std::vector<double> rhs;
+        for (auto& x : sel) rhs.push_back(vg.cov_points(x.loc, t));
+        met = calibrate(p, vg, kind, rhs, vg.total_sill(), sel);
+      }
       Estimate e;
       int st = krige(kind, kparam, t, sel, vg, e);
       put(e, st, &res[k]);
-      if (diag && st == OK) diag_of(t, sel, e, diag + 4 * k);
+      if (diag && st == OK) {
+        diag_of(t, sel, e, diag + 5 * k);
+        diag[5 * k + 4] = met < 0 ? NAN : double(met);
+      }
     }
   };
   int nt = nthreads > 0 ? nthreads : orc_num_threads();
@@ -1399,10 +1527,16 @@ int32_t orc_estimate_block(int64_t m, const double* targets, int64_t n, const do
       bool ok = tree.neighbors(t, -1, chosen);
       if (!ok) { Estimate e; put(e, SEARCH_FAILED, &res[k]); continue; }
       std::vector<Sample> sel;
-      for (size_t i : chosen) sel.push_back(s[i]);
+      for (size_t i : balanced(tree, t, chosen)) sel.push_back(s[i]);
       std::vector<std::array<double, 3>> pts(static_cast<size_t>(np));
       for (int64_t q = 0; q < np; ++q)
         pts[q] = {t[0] + offsets[3 * q], t[1] + offsets[3 * q + 1], t[2] + offsets[3 * q + 2]};
+      if (p.calibration) {  // block.rs block_covariances: the block's rhs and C(B,B)
+        std::vector<double> rhs;
+        double cbb = 0.0;
+        block_rhs(pts, sel, vg, rhs, cbb);
+        calibrate(p, vg, ORDINARY, rhs, cbb, sel);
+      }
       Estimate e;
       int st = block_krige_points(pts, sel, vg, e);
       put(e, st, &res[k]);

@@ -45,7 +45,8 @@ class Srch(ctypes.Structure):
                 ("max_per_hole", ctypes.c_int64), ("octant", ctypes.c_int64), ("sectors", ctypes.c_int64),
                 ("max_per_sector", ctypes.c_int64), ("max_per_octant", ctypes.c_int64),
                 ("min_sectors", ctypes.c_int64), ("max_empty_sectors", ctypes.c_int64),
-                ("min_holes", ctypes.c_int64), ("aniso", Aniso)]
+                ("min_holes", ctypes.c_int64), ("aniso", Aniso), ("calibration", ctypes.c_int64),
+                ("calibration_target", ctypes.c_double)]
 
 
 class Result(ctypes.Structure):
@@ -94,6 +95,8 @@ def lib():
                                                    ctypes.POINTER(Srch), ctypes.POINTER(Vario), ctypes.c_int32,
                                                    ctypes.c_double, ctypes.c_int32, P, P, P]),
             "orc_centroids": (None, [P, P, P, P, ctypes.c_int64, ctypes.c_int64, P]),
+            "orc_prefix_quality": (None, [ctypes.c_int64, P, P, P, ctypes.POINTER(Vario), ctypes.c_int32,
+                                          ctypes.c_double, P, P, P]),
             "orc_krige_lists": (ctypes.c_int32, [ctypes.c_int64, P, ctypes.c_int64, P, P, P, P, ctypes.c_int64,
                                                  ctypes.POINTER(Vario), ctypes.c_int32, ctypes.c_double,
                                                  ctypes.c_int32, P]),
@@ -148,6 +151,9 @@ def search(s):
     c.max_empty_sectors = none(getattr(s, "max_empty_sectors", None))
     c.min_holes = none(getattr(s, "min_holes", None))
     c.aniso = aniso(s.anisotropy)
+    slope, eff = getattr(s, "target_slope", None), getattr(s, "target_efficiency", None)
+    c.calibration = 1 if slope is not None else (2 if eff is not None else 0)
+    c.calibration_target = slope if slope is not None else (eff if eff is not None else 0.0)
     return c
 
 
@@ -271,11 +277,26 @@ def scan_neighbors(target, xyz, s, vg=None, holes=None):
     return bool(ok), out[: n.value].tolist()
 
 
+def prefix_quality(target, xyz, vg, *, ordinary=True, support=None, err=None):
+    """(slope, efficiency, ok) of kriging `target` from each leading part of `xyz`
+    (kriging_algebra.rs:336-395); ok False where the reference gives None."""
+    xyz = _xyz(xyz)
+    n = len(xyz)
+    t = np.ascontiguousarray(target, dtype=np.float64)
+    e = None if err is None else np.ascontiguousarray(err, dtype=np.float64)
+    sl, ef, ok = np.empty(n), np.empty(n), np.empty(n, dtype=np.int32)
+    sv = vg.total_sill() if support is None else float(support)
+    lib().orc_prefix_quality(n, xyz.ctypes.data, _ptr(e), t.ctypes.data, ctypes.byref(variogram(vg)),
+                             1 if ordinary else 0, sv, sl.ctypes.data, ef.ctypes.data, ok.ctypes.data)
+    return sl, ef, ok.astype(bool)
+
+
 def estimate_many(targets, xyz, values, s, vg, *, kind="ordinary", kparam=0.0, err=None, holes=None, loo=False,
                   threads=0, neighbors=True, diagnostics=False):
     """estimate_many / leave_one_out_at (batch.rs:15-38, 165-190) with krige of `kind`. With `diagnostics`,
     also the per-target columns of the diagnostics table that need the samples or weights
-    (crates/py/src/estimation.rs:1046-1105): negative_weight_sum, mean_distance, n_holes, n_within."""
+    (crates/py/src/estimation.rs:1046-1105): negative_weight_sum, mean_distance, n_holes, n_within and
+    target_met (NaN without a calibration)."""
     xyz = _xyz(xyz)
     n = len(xyz)
     t = None if loo else _xyz(targets)
@@ -285,7 +306,7 @@ def estimate_many(targets, xyz, values, s, vg, *, kind="ordinary", kparam=0.0, e
     v = np.ascontiguousarray(values, dtype=np.float64)
     e = None if err is None else np.ascontiguousarray(err, dtype=np.float64)
     h = None if holes is None else np.ascontiguousarray(holes, dtype=np.int64)
-    dg = np.empty((m, 4)) if diagnostics else None
+    dg = np.empty((m, 5)) if diagnostics else None
     cs, cv = search(s), variogram(vg)
     rc = lib().orc_estimate_many(m, _ptr(t), 1 if loo else 0, n, xyz.ctypes.data, v.ctypes.data, _ptr(e), _ptr(h),
                                  ctypes.byref(cs), ctypes.byref(cv), KINDS[kind], kparam, threads,
@@ -301,7 +322,7 @@ def estimate_many(targets, xyz, values, s, vg, *, kind="ordinary", kparam=0.0, e
         out["neighbors"] = nbr
     if diagnostics:
         out["support"] = rec["support"].copy()
-        for j, key in enumerate(("negative_weight_sum", "mean_distance", "n_holes", "n_within")):
+        for j, key in enumerate(("negative_weight_sum", "mean_distance", "n_holes", "n_within", "target_met")):
             out[key] = dg[:, j].copy()
     return out
 

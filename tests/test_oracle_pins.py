@@ -470,3 +470,103 @@ def test_block_with_no_nugget_uses_point_covariances(oracle):
     K = np.block([[C, np.ones((3, 1))], [np.ones((1, 3)), np.zeros((1, 1))]])
     sol = np.linalg.solve(K, np.r_[rhs, 1.0])
     assert np.allclose(w, sol[:3], atol=1e-12) and abs(e["lagrange"] - sol[3]) < 1e-12
+
+
+def scattered_nearest(seed, n, t):
+    """n samples in a 40 m box around t, nearest first (a search's selection order)."""
+    rng = np.random.default_rng(seed)
+    xyz = np.asarray(t) + rng.uniform(-20.0, 20.0, (n, 3)) * [1.0, 1.0, 0.5]
+    return xyz[np.argsort(((xyz - t) ** 2).sum(1), kind="stable")]
+
+
+def test_prefix_quality_matches_direct_solves(oracle):
+    """kriging_algebra.rs:1115-1157: each leading part's slope and efficiency equal those of kriging it."""
+    vg = nested()
+    t = np.array([1.0, 2.0, 5.0])
+    xyz = scattered_nearest(17, 24, t)
+    sill = vg.total_sill()
+    osl, oef, ook = oracle.prefix_quality(t, xyz, vg)
+    ssl, sef, sok = oracle.prefix_quality(t, xyz, vg, ordinary=False)
+    assert ook.all() and sok.all()
+    for n in range(1, 25):
+        _, ok, _ = oracle.krige("ordinary", t, xyz[:n], np.zeros(n), vg)
+        cov = sill - ok["variance"] - ok["lagrange"]
+        assert close(osl[n - 1], cov / (cov - ok["lagrange"]), 1e-9)
+        assert close(oef[n - 1], (sill - ok["variance"]) / sill, 1e-9)
+        _, sk, _ = oracle.krige("simple", t, xyz[:n], np.zeros(n), vg, kparam=1.0)
+        assert close(ssl[n - 1], 1.0, 1e-9) and close(sef[n - 1], (sill - sk["variance"]) / sill, 1e-9)
+
+
+@pytest.mark.parametrize("calibration", [("target_slope", 0.8), ("target_slope", 0.95),
+                                         ("target_efficiency", 0.3), ("target_efficiency", 0.99)])
+def test_calibrated_count_takes_the_fewest_that_meet_the_target(oracle, calibration):
+    """kriging_algebra.rs:1159-1189 through estimate_many: n >= min_samples; where met, the n-sample part
+    meets the target and no shorter part from min_samples does; else every sample is used."""
+    vg = nested()
+    key, target = calibration
+    rng = np.random.default_rng(5)
+    xyz = rng.uniform(0.0, 60.0, (300, 3)) * [1.0, 1.0, 0.3]
+    values = rng.normal(size=300)
+    targets = rng.uniform(5.0, 55.0, (40, 3)) * [1.0, 1.0, 0.3]
+    for trial, t in enumerate(targets):
+        mn = 1 + trial % 4
+        s = Search(radius=1e9, max_samples=20, min_samples=mn, **{key: target})
+        plain = Search(radius=1e9, max_samples=20, min_samples=mn)
+        r = oracle.estimate_many(t[None], xyz, values, s, vg, neighbors=False, diagnostics=True)
+        full = oracle.estimate_many(t[None], xyz, values, plain, vg)
+        chosen = full["neighbors"][0]
+        sl, ef, ok = oracle.prefix_quality(t, xyz[chosen], vg)
+        q = sl if key == "target_slope" else ef
+        n, met = int(r["n_used"][0]), r["target_met"][0]
+        assert mn <= n <= 20
+        if met == 1:
+            assert ok[n - 1] and q[n - 1] >= target
+            assert not any(ok[k - 1] and q[k - 1] >= target for k in range(mn, n))
+        else:
+            assert met == 0 and n == 20
+            assert not any(ok[k - 1] and q[k - 1] >= target for k in range(mn, 21))
+        _, one, w = oracle.krige("ordinary", t, xyz[chosen[:n]], values[chosen[:n]], vg)
+        assert r["value"][0] == one["value"] and abs(w[:n].sum() - 1.0) < 1e-10
+
+
+def test_calibration_balances_octants_round_robin(oracle):
+    """search.rs:913-936: a calibrated octant search krigs its samples taken from the octants in turn."""
+    vg = Variogram([Structure("spherical", 1.0, 50.0)], nugget=0.05)
+    rng = np.random.default_rng(9)
+    xyz = rng.uniform(0.0, 100.0, (400, 3)) * [1.0, 1.0, 0.2]
+    values = rng.normal(size=400)
+    t = np.array([50.0, 50.0, 10.0])
+    plain = Search(radius=60.0, max_samples=24, octant=True, max_per_sector=3)
+    cal = Search(radius=60.0, max_samples=24, octant=True, max_per_sector=3, target_efficiency=-1e9)
+    chosen = oracle.estimate_many(t[None], xyz, values, plain, vg)["neighbors"][0]
+    chosen = chosen[chosen >= 0]
+    d = xyz[chosen] - t
+    octant = (d[:, 0] >= 0) * 4 + (d[:, 1] >= 0) * 2 + (d[:, 2] >= 0)
+    rank = np.array([np.sum(octant[: i + 1] == octant[i]) for i in range(len(chosen))])
+    order = chosen[np.argsort(rank, kind="stable")]
+    r = oracle.estimate_many(t[None], xyz, values, cal, vg, neighbors=False, diagnostics=True)
+    assert r["n_used"][0] == 1 and r["target_met"][0] == 1  # any efficiency meets: the first of the turn
+    _, one, _ = oracle.krige("ordinary", t, xyz[order[:1]], values[order[:1]], vg)
+    assert r["value"][0] == one["value"]
+    cal = Search(radius=60.0, max_samples=24, octant=True, max_per_sector=3, target_efficiency=0.999)
+    r = oracle.estimate_many(t[None], xyz, values, cal, vg, neighbors=False)
+    _, all_, _ = oracle.krige("ordinary", t, xyz[order], values[order], vg)
+    assert r["n_used"][0] == len(order) and close(r["value"][0], all_["value"], 1e-12)
+
+
+def test_calibration_arguments_are_checked_as_the_reference_does():
+    """crates/py/src/estimation.rs:458-473, 819-827."""
+    from boitata_b200 import InvalidInput, OrdinaryKriging, SimpleKriging
+
+    s = Search(radius=60, max_samples=24, min_samples=2, target_slope=0.9)
+    assert (s.target_slope, s.target_efficiency) == (0.9, None)
+    with pytest.raises(InvalidInput, match="at most one"):
+        Search(radius=60, target_slope=0.9, target_efficiency=0.5)
+    with pytest.raises(InvalidInput, match="target_slope"):
+        Search(radius=60, target_slope=0.0)
+    with pytest.raises(InvalidInput, match="target_efficiency"):
+        Search(radius=60, target_efficiency=1.5)
+    with pytest.raises(InvalidInput, match="simple kriging"):
+        SimpleKriging(nested(), s, mean=1.0)
+    OrdinaryKriging(nested(), s)
+    SimpleKriging(nested(), Search(radius=60, target_efficiency=0.5), mean=1.0)
