@@ -9,6 +9,7 @@ include/boitata_b200.h.
 """
 
 from .errors import InvalidInput, Unsupported
+from .persist import FileError
 from .estimation import BlockKriging, CrossValidation, IndicatorKriging, OrdinaryKriging, SimpleKriging
 from .geometry import BlockModel, Geometry
 from .search import Search
@@ -19,6 +20,7 @@ __all__ = [
     "BlockKriging",
     "BlockModel",
     "CrossValidation",
+    "FileError",
     "Geometry",
     "IndicatorKriging",
     "InvalidInput",

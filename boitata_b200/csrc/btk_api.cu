@@ -148,6 +148,8 @@ struct btk_ctx {
   DevBuf<uint32_t> sidx, start, cell_count, cell_of;
   DevBuf<uint8_t> twin;
   DevBuf<int64_t> loo_perm;
+  DevBuf<uint32_t> gsort_keys, gsort_vals;  // stable sort of the samples by cell
+  DevBuf<unsigned char> gsort_temp;
 
   // per-call scratch, grown on demand
   DevBuf<double> txyz, aos;
@@ -388,9 +390,15 @@ int index_samples(btk_ctx* ctx) {
   CK(ctx->swy.grow(n));
   CK(ctx->swz.grow(n));
   CK(ctx->sidx.grow(n));
+  const size_t gtb = grid_sort_temp_bytes(n, g.ncells);
+  if (n > 0 && gtb == 0) return fail(ctx, BTK_ECUDA, "grid sort sizing failed");
+  CK(ctx->gsort_keys.grow(2 * size_t(n > 0 ? n : 1)));
+  CK(ctx->gsort_vals.grow(2 * size_t(n > 0 ? n : 1)));
+  CK(ctx->gsort_temp.grow(gtb > 0 ? gtb : 1));
   CK(launch_grid_build(L, n, ctx->x.p, ctx->y.p, ctx->z.p, ctx->px.p, ctx->py.p, ctx->pz.p, g, ctx->cell_count.p,
                        ctx->start.p, ctx->cell_of.p, ctx->spx.p, ctx->spy.p, ctx->spz.p, ctx->swx.p, ctx->swy.p,
-                       ctx->swz.p, ctx->sidx.p));
+                       ctx->swz.p, ctx->sidx.p, ctx->gsort_keys.p, ctx->gsort_vals.p,
+                       ctx->gsort_temp.p, gtb));
   g.start = ctx->start.p;
   g.px = ctx->spx.p, g.py = ctx->spy.p, g.pz = ctx->spz.p;
   g.wx = ctx->swx.p, g.wy = ctx->swy.p, g.wz = ctx->swz.p;

@@ -9,6 +9,8 @@
 // gives the same (d2, index)-ordered candidates as search/grid.rs.
 #include <cfloat>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "btk_device.cuh"
 
 namespace btk {
@@ -100,17 +102,30 @@ __global__ void k_scan(int64_t ncells, const uint32_t* count, uint32_t* start) {
   if (threadIdx.x == blockDim.x - 1) start[ncells] = sums[threadIdx.x];
 }
 
-__global__ void k_scatter(int64_t n, const double* x, const double* y, const double* z, const double* px,
-                          const double* py, const double* pz, const uint32_t* cell_of, const uint32_t* start,
-                          uint32_t* fill, double* spx, double* spy, double* spz, double* swx, double* swy,
-                          double* swz, uint32_t* sidx) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    uint32_t c = cell_of[i];
-    uint32_t pos = start[c] + atomicAdd(&fill[c], 1u);
+__global__ void k_iota(int64_t n, uint32_t* v) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    v[i] = uint32_t(i);
+}
+
+// Samples in cell order, each cell in sample-index order (`order` is the
+// stable sort of the indices by cell), so the layout, and the leave-one-out
+// walk that follows it, are the same on every run.
+__global__ void k_gather(int64_t n, const double* x, const double* y, const double* z, const double* px,
+                         const double* py, const double* pz, const uint32_t* order, double* spx, double* spy,
+                         double* spz, double* swx, double* swy, double* swz, uint32_t* sidx) {
+  for (int64_t pos = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; pos < n;
+       pos += int64_t(gridDim.x) * blockDim.x) {
+    const uint32_t i = order[pos];
     spx[pos] = px[i], spy[pos] = py[i], spz[pos] = pz[i];
     swx[pos] = x[i], swy[pos] = y[i], swz[pos] = z[i];
-    sidx[pos] = uint32_t(i);
+    sidx[pos] = i;
   }
+}
+
+int cell_bits(int64_t ncells) {
+  int b = 1;
+  while (b < 32 && (int64_t(1) << b) < ncells) ++b;
+  return b;
 }
 
 // twin[i] = 1 when another sample lies within 1e-6 m of sample i, by the
@@ -204,20 +219,31 @@ cudaError_t launch_bounds(const Launch& L, int64_t n, const double* px, const do
   return cudaGetLastError();
 }
 
+size_t grid_sort_temp_bytes(int64_t n, int64_t ncells) {
+  size_t bytes = 0;
+  cub::DoubleBuffer<uint32_t> k(nullptr, nullptr), v(nullptr, nullptr);
+  if (cub::DeviceRadixSort::SortPairs(nullptr, bytes, k, v, int(n), 0, cell_bits(ncells)) != cudaSuccess) return 0;
+  return bytes;
+}
+
 cudaError_t launch_grid_build(const Launch& L, int64_t n, const double* x, const double* y, const double* z,
                               const double* px, const double* py, const double* pz, GridDev g, uint32_t* count,
                               uint32_t* start, uint32_t* cell_of, double* spx, double* spy, double* spz,
-                              double* swx, double* swy, double* swz, uint32_t* sidx) {
+                              double* swx, double* swy, double* swz, uint32_t* sidx, uint32_t* sort_keys,
+                              uint32_t* sort_vals, void* temp, size_t temp_bytes) {
   cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t) * size_t(g.ncells), L.stream);
   if (e != cudaSuccess) return e;
   int nb = grid_blocks(L, n, 256);
   k_cell_count<<<nb, 256, 0, L.stream>>>(n, px, py, pz, g, count, cell_of);
   k_scan<<<1, 1024, 0, L.stream>>>(g.ncells, count, start);
-  e = cudaMemsetAsync(count, 0, sizeof(uint32_t) * size_t(g.ncells), L.stream);
+  k_iota<<<nb, 256, 0, L.stream>>>(n, sort_vals);
+  e = cudaMemcpyAsync(sort_keys, cell_of, sizeof(uint32_t) * size_t(n), cudaMemcpyDeviceToDevice, L.stream);
   if (e != cudaSuccess) return e;
-  k_scatter<<<nb, 256, 0, L.stream>>>(n, x, y, z, px, py, pz, cell_of, start, count, spx, spy, spz, swx, swy, swz,
-                                      sidx);
-  *L.counter += 3;
+  cub::DoubleBuffer<uint32_t> k(sort_keys, sort_keys + n), v(sort_vals, sort_vals + n);
+  e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, k, v, int(n), 0, cell_bits(g.ncells), L.stream);
+  if (e != cudaSuccess) return e;
+  k_gather<<<nb, 256, 0, L.stream>>>(n, x, y, z, px, py, pz, v.Current(), spx, spy, spz, swx, swy, swz, sidx);
+  *L.counter += 5;
   return cudaGetLastError();
 }
 

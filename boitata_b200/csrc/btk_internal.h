@@ -165,10 +165,13 @@ cudaError_t launch_project(const Launch& L, int64_t n, const double* x, const do
                            const double* frame, const double* origin, double* px, double* py, double* pz);
 cudaError_t launch_bounds(const Launch& L, int64_t n, const double* px, const double* py, const double* pz,
                           double* partial /* 6 * 1024 */, double* out6);
+// Temporary bytes of the grid build's stable sort of the samples by cell.
+size_t grid_sort_temp_bytes(int64_t n, int64_t ncells);
 cudaError_t launch_grid_build(const Launch& L, int64_t n, const double* x, const double* y, const double* z,
                               const double* px, const double* py, const double* pz, GridDev g, uint32_t* count,
                               uint32_t* start, uint32_t* cell_of, double* spx, double* spy, double* spz,
-                              double* swx, double* swy, double* swz, uint32_t* sidx);
+                              double* swx, double* swy, double* swz, uint32_t* sidx, uint32_t* sort_keys,
+                              uint32_t* sort_vals, void* temp, size_t temp_bytes);
 cudaError_t launch_twins(const Launch& L, int64_t n, GridDev g, int reach, const double* x, const double* y,
                          const double* z, uint8_t* twin);
 cudaError_t launch_centroids(const Launch& L, btk_geometry g, Frame9 frame_t, int64_t first, int64_t m,

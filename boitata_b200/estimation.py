@@ -184,6 +184,44 @@ class _Base:
         self._use_pass(0)
         return self
 
+    # -- persistence (crates/py/src/persist.rs) ---------------------------------
+    def to_parquet(self, path):
+        """Writes the samples as Parquet columns and the parameters as JSON in the file metadata, in the
+        reference's format (python/boitata/estimation.py:377-383)."""
+        from . import persist
+
+        persist.to_parquet(self, path)
+
+    @classmethod
+    def from_parquet(cls, path):
+        """Reads `to_parquet` output, or a file the reference wrote; predictions match the saved
+        estimator's bit for bit (python/boitata/estimation.py:385-402)."""
+        from . import persist
+
+        return persist.from_parquet(cls, path)
+
+    def __getstate__(self):
+        from . import persist
+
+        cols = persist.columns(self)
+        return {"meta": persist.envelope(self), "columns": cols, "holes": getattr(self, "_holes", None)}
+
+    def __setstate__(self, state):
+        from . import persist
+
+        d = persist._open(type(self).__name__, state["meta"])
+        fitted = d.pop("fitted", None) is True
+        other = persist._build(type(self), d)
+        self.__dict__.update(other.__dict__)
+        self.precision = d.get("precision", self.precision)
+        cols = state["columns"]
+        if fitted and cols is not None:
+            holes = state["holes"]
+            err = cols["error_variance"]
+            self.fit(np.column_stack([cols["x"], cols["y"], cols["z"]]), cols["value"],
+                     holes=None if holes is None else [int(h) for h in holes],
+                     error_variance=None if not err.any() else err)
+
     def _use_pass(self, p):
         if self._pass == p:
             return
