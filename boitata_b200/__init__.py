@@ -13,6 +13,7 @@ from .persist import FileError
 from .estimation import BlockKriging, CrossValidation, IndicatorKriging, OrdinaryKriging, SimpleKriging
 from .geometry import BlockModel, Geometry
 from .search import Search
+from .simulation import SGS, Simulation
 from .table import Table
 from .variogram import Structure, Variogram
 
@@ -25,7 +26,9 @@ __all__ = [
     "IndicatorKriging",
     "InvalidInput",
     "OrdinaryKriging",
+    "SGS",
     "Search",
+    "Simulation",
     "SimpleKriging",
     "Structure",
     "Table",

@@ -82,6 +82,7 @@ SIGNATURES = {
                                                    ctypes.c_int32, ctypes.POINTER(OutputsC), P]),
     "btk_predict_kinds": (ctypes.c_int, [P, ctypes.c_int64, P, P, ctypes.c_double, ctypes.c_int32,
                                          ctypes.POINTER(OutputsC)]),
+    "btk_sgs_simulate": (ctypes.c_int, [P, ctypes.c_int64, P, ctypes.c_int64, P, P, P]),
     "btk_predict_diagnostics": (ctypes.c_int, [P, ctypes.c_int64, P, ctypes.c_int32, ctypes.c_double,
                                                ctypes.c_int32, ctypes.POINTER(OutputsC),
                                                ctypes.POINTER(DiagnosticsC)]),

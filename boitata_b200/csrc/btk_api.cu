@@ -4,6 +4,7 @@
 // Host-side math here is the one-off frame set-up of a call (3x3 matrices);
 // every per-sample and per-target step runs in the CUDA kernels. There is no
 // CPU path for the kriging itself.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -160,6 +161,11 @@ struct btk_ctx {
   DevBuf<double> o_value, o_var, o_lag, o_negw, o_mdist;
   DevBuf<int32_t> o_nholes;
   DevBuf<int8_t> met, o_met;  // calibration: target met per work slot target
+  // sequential simulation
+  DevBuf<double> sg_z, sg_score;
+  DevBuf<uint8_t> sg_done;
+  DevBuf<int8_t> sg_how;
+  DevBuf<int64_t> sg_list, sg_ctl;  // ctl: pending count, first failed node
 
   bool timing = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -320,6 +326,7 @@ void make_searchdev(btk_ctx* ctx) {
   d.rcap = d.plane ? int(s.max_per_sector) : (s.octant ? int(cap) : INT32_MAX);
   d.hole = ctx->has_hole ? ctx->hole.p : nullptr;
   d.sx = ctx->x.p, d.sy = ctx->y.p, d.sz = ctx->z.p;
+  d.sgs = 0, d.sgs_node0 = 0, d.sgs_done = nullptr;
   if (d.nsec == 8) {  // index bx << 2 | by << 1 | bz
     d.bit_axis[2] = ax_x, d.bit_sign[2] = sg_x, d.bit_mask[2] = 0xF0;
     d.bit_axis[1] = ax_y, d.bit_sign[1] = 1, d.bit_mask[1] = 0xCC;
@@ -1111,6 +1118,87 @@ int btk_predict_geometry_device(btk_ctx* ctx, const btk_geometry* g, int32_t kin
   double* t = ctx->txyz.p;
   CK(launch_centroids(L, *g, transposed_frame(*g), 0, nwork, t, t + m, t + 2 * m, ctx->perm.p));
   return run_path(ctx, L.stream, m, t, t + m, t + 2 * m, ctx->perm.p, nwork, 0, kind, kparam, precision, d_out);
+}
+
+int btk_sgs_simulate(btk_ctx* ctx, int64_t n_data, const double* z, int64_t batch, double* score, int8_t* how,
+                     int64_t* rounds) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if (n_data < 1 || n_data > ctx->n) return fail(ctx, BTK_EINVAL, "n_data must be between 1 and the fitted samples");
+  if (!score || (ctx->n > n_data && !z)) return fail(ctx, BTK_EINVAL, "z and score arrays are required");
+  if (batch < 0) return fail(ctx, BTK_EINVAL, "batch must be >= 0 (0: automatic)");
+  if (ctx->search.calibration)
+    return fail(ctx, BTK_EINVAL, "SGS does not take target_slope or target_efficiency");
+  if (!ctx->vgd.stationary)
+    return fail(ctx, BTK_EINVAL, "simple kriging needs a variogram with a sill: every structure must be stationary");
+  if (ctx->sup_n > 0) return fail(ctx, BTK_EINVAL, "SGS simulates points: clear the block support first");
+  const int64_t m = ctx->n - n_data;
+  if (rounds) *rounds = 0;
+  if (m == 0) return BTK_OK;
+  if (ctx->n > int64_t(0xffffffffu)) return fail(ctx, BTK_EINVAL, "too many samples and nodes");
+  CK(cudaSetDevice(ctx->device));
+  Launch L = ctx->launch(nullptr);
+  const size_t mm = size_t(m);
+  CK(ctx->sg_z.grow(mm));
+  CK(ctx->sg_score.grow(mm));
+  CK(ctx->sg_how.grow(mm));
+  CK(ctx->sg_list.grow(mm));
+  CK(ctx->sg_ctl.grow(2));
+  CK(ctx->sg_done.grow(size_t(ctx->n)));
+  btk_outputs d{};
+  if ((rc = host_outputs(ctx, m, nullptr, &d))) return rc;
+  CK(cudaMemcpyAsync(ctx->sg_z.p, z, mm * sizeof(double), cudaMemcpyHostToDevice, L.stream));
+  CK(cudaMemsetAsync(ctx->sg_done.p, 0, size_t(ctx->n), L.stream));
+  CK(cudaMemsetAsync(ctx->sg_how.p, 0, mm, L.stream));
+  CK(cudaMemsetAsync(ctx->sg_ctl.p, 0xFF, 2 * sizeof(int64_t), L.stream));
+  const SearchDev saved = ctx->spd;
+  ctx->spd.rules = 1;  // one warp per node: the selector with the simulation's availability test
+  ctx->spd.sgs = 1, ctx->spd.sgs_node0 = uint32_t(n_data), ctx->spd.sgs_done = ctx->sg_done.p;
+  const uint32_t node0 = uint32_t(n_data);
+  const int64_t most = ctx->search.max_samples;
+  int64_t total_rounds = 0;
+  int64_t ctl[2] = {0, -1};
+  for (int64_t start = 0; start < m && rc == BTK_OK;) {
+    // A window of the path is kriged in parallel against the nodes before it;
+    // about window * most / (2 known) of its nodes go stale (sgs.rs:679-683).
+    const int64_t known = n_data + start;
+    int64_t size = batch > 0 ? batch : known / (2 * (most > 0 ? most : 1));
+    size = std::max<int64_t>(batch > 0 ? 1 : 64, std::min<int64_t>(size, 65536));
+    const int64_t end = std::min(m, start + size);
+    for (int64_t round = 0; round <= size; ++round) {
+      if ((rc = [&]() -> int {
+             CK(launch_sgs_pending(L, start, end, node0, ctx->sg_done.p, ctx->sg_list.p, ctx->sg_ctl.p));
+             CK(cudaMemcpyAsync(ctl, ctx->sg_ctl.p, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, L.stream));
+             CK(cudaStreamSynchronize(L.stream));
+             return BTK_OK;
+           }()))
+        break;
+      if (ctl[1] >= 0) {
+        rc = fail(ctx, BTK_EINVAL, "kriging failed at node " + std::to_string(ctl[1]) + " of the path (singular system)");
+        break;
+      }
+      if (ctl[0] == 0) break;
+      ++total_rounds;
+      if ((rc = run_path(ctx, L.stream, m, ctx->x.p + n_data, ctx->y.p + n_data, ctx->z.p + n_data, ctx->sg_list.p,
+                         ctl[0], 0, BTK_SIMPLE, 0.0, BTK_FP64, &d)))
+        break;
+      cudaError_t e = launch_sgs_commit(L, ctl[0], ctx->sg_list.p, d.value, d.variance, d.status, ctx->sg_z.p, node0,
+                                        ctx->v.p, ctx->sg_done.p, ctx->sg_score.p, ctx->sg_how.p, ctx->sg_ctl.p + 1);
+      if (e != cudaSuccess) {
+        rc = fail(ctx, BTK_ECUDA, cudaGetErrorString(e));
+        break;
+      }
+    }
+    if (rc == BTK_OK && ctl[0] != 0) rc = fail(ctx, BTK_ECUDA, "simulation window did not finish");
+    start = end;
+  }
+  ctx->spd = saved;
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(score, ctx->sg_score.p, mm * sizeof(double), cudaMemcpyDeviceToHost, L.stream));
+  if (how) CK(cudaMemcpyAsync(how, ctx->sg_how.p, mm, cudaMemcpyDeviceToHost, L.stream));
+  CK(cudaStreamSynchronize(L.stream));
+  if (rounds) *rounds = total_rounds;
+  return BTK_OK;
 }
 
 int btk_cross_validate(btk_ctx* ctx, int32_t kind, double kparam, int32_t precision, const btk_outputs* out) {

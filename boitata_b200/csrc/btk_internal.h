@@ -55,7 +55,18 @@ struct SearchDev {
   int rcap;      // samples per sector when balancing
   const uint32_t* hole;        // hole code per sample, original order; null: each sample its own hole
   const double *sx, *sy, *sz;  // sample world coordinates, original order
+  // Sequential simulation (btk_sgs_simulate): samples from sgs_node0 on are
+  // grid nodes in simulation order, and target t is node sgs_node0 + t. A
+  // target sees the data and the earlier nodes already simulated (sgs_done);
+  // an earlier node not yet simulated within the search's reach makes the
+  // target stale (kStStale), to be searched again once that node is done.
+  int sgs;
+  uint32_t sgs_node0;
+  const uint8_t* sgs_done;
 };
+
+// Internal per-target status of a simulation search: searched too early.
+constexpr int8_t kStStale = 5;
 
 // Uniform grid over the projected samples, which are stored sorted by cell.
 struct GridDev {
@@ -228,6 +239,14 @@ struct CalDev {
   int balance;
 };
 cudaError_t launch_calibrate(const Launch& L, const SolveDev& a, const SearchDev& sp, const CalDev& c, int kmax);
+
+// Sequential simulation (btk_sgs.cu): the window's nodes still to simulate,
+// in order, and the commit of a round's kriged nodes.
+cudaError_t launch_sgs_pending(const Launch& L, int64_t first, int64_t last, uint32_t node0, const uint8_t* done,
+                               int64_t* list, int64_t* len);
+cudaError_t launch_sgs_commit(const Launch& L, int64_t nwork, const int64_t* list, const double* mean,
+                              const double* var, const int8_t* status, const double* z, uint32_t node0, double* sv,
+                              uint8_t* done, double* score, int8_t* how, int64_t* failed);
 
 // With `diag`, the estimated systems (status OK) are solved again for their
 // weights and only a.negw / a.mdist / a.nholes are written.

@@ -510,7 +510,7 @@ __device__ __forceinline__ int hole_slot(const RulesSmem& S, uint32_t h) {
 // nearest. Returns the count; *dropped tells whether candidates were cut.
 __device__ int rules_scan(const SearchDev& sp, const GridDev& g, RulesSmem& S, const double q[3], const double t[3],
                           uint32_t left, double after_d, uint32_t after_i, bool filter, unsigned openmask,
-                          bool& dropped, int lane) {
+                          bool& dropped, int lane, uint32_t my, double& d2u) {
   const double glo[3] = {g.lo[0], g.lo[1], g.lo[2]};
   const double ghi[3] = {g.lo[0] + g.dims[0] * g.h, g.lo[1] + g.dims[1] * g.h, g.lo[2] + g.dims[2] * g.h};
   const unsigned all = sp.nsec > 1 ? (1u << sp.nsec) - 1u : 1u;
@@ -569,6 +569,10 @@ __device__ int rules_scan(const SearchDev& sp, const GridDev& g, RulesSmem& S, c
               d2 = d2_exact(g.px[c], g.py[c], g.pz[c], q[0], q[1], q[2]);
               idx = g.idx[c];
               keep = d2 <= thr && idx != left && key_less(after_d, after_i, d2, idx);
+              if (sp.sgs && d2 <= thr && idx >= sp.sgs_node0) {  // a grid node of a simulation
+                if (idx < my && !sp.sgs_done[idx]) d2u = fmin(d2u, d2);
+                keep = keep && idx < my && sp.sgs_done[idx];
+              }
               if (keep && filter) {
                 if (sp.balances) {
                   const double wv[3] = {sp.sx[idx], sp.sy[idx], sp.sz[idx]};
@@ -647,6 +651,8 @@ __global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, c
       mulv_exact(sp.frame, d, q);
     }
     const uint32_t left = loo ? uint32_t(ti) : 0xffffffffu;
+    const uint32_t my = sp.sgs ? sp.sgs_node0 + uint32_t(ti) : 0xffffffffu;
+    double d2u = INFINITY, far = 0.0;  // nearest unsimulated earlier node; farthest accepted
     for (int i = lane; i < kHoleHash; i += 32) S.hkey[i] = kNoHole, S.hcnt[i] = 0;
     for (int i = lane; i < 360; i += 32) S.per_sector[i] = 0;
     __syncwarp();
@@ -662,7 +668,8 @@ __global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, c
     for (int round = 0; round < 1 << 20; ++round) {
       // After a cut, only the K nearest are an exact prefix of the (d2, index)
       // order: entries kept since then can skip cut ones of equal d2.
-      const int nscan = rules_scan(sp, g, S, q, t, left, after_d, after_i, filter, openmask, dropped, lane);
+      const int nscan =
+          rules_scan(sp, g, S, q, t, left, after_d, after_i, filter, openmask, dropped, lane, my, d2u);
       const int n = dropped ? kRulesK : nscan;
       if (sp.balances)
         for (int i = lane; i < n; i += 32) {
@@ -691,6 +698,7 @@ __global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, c
           } else {
             ++untagged;
           }
+          far = S.cd[i];
           S.chosen[nchosen++] = idx;
         }
       nchosen = __shfl_sync(kFull, nchosen, 0);
@@ -715,6 +723,8 @@ __global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, c
       }
       __syncwarp();
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d2u = fmin(d2u, __shfl_xor_sync(kFull, d2u, o));
     if (lane == 0) {  // Selector::finish (search.rs:561-590)
       int8_t st = BTK_ST_OK;
       if (nchosen < sp.min_samples || (loo && nchosen == 0)) {
@@ -727,6 +737,10 @@ __global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, c
       if (st == BTK_ST_OK && sp.max_empty_sectors >= 0 && longest_empty(sp, S.per_sector) > sp.max_empty_sectors)
         st = BTK_ST_SEARCH_FAILED;
       if (st == BTK_ST_OK && sp.min_holes >= 0 && nholes + untagged < sp.min_holes) st = BTK_ST_SEARCH_FAILED;
+      if (sp.sgs) {  // crates/simulation/src/sgs.rs:600-625: reach of the search, with a margin
+        const double reach2 = (st == BTK_ST_OK && nchosen >= sp.max_samples) ? far : sp.radius2;
+        if (d2u < INFINITY && d2u <= reach2 * (1.0 + 1e-8)) st = kStStale;  // an unsimulated node was seen
+      }
       count[ti] = nchosen;
       status[ti] = st;
     }

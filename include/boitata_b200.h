@@ -185,6 +185,23 @@ typedef struct btk_diagnostics {
 int btk_predict(btk_ctx* ctx, int64_t m, const double* xyz, int32_t kind, double kparam, int32_t precision,
                 const btk_outputs* out);
 
+/* Sequential Gaussian simulation of grid nodes (crates/simulation/src/sgs.rs:
+ * 586-760, `sequential`): the fitted samples are the n_data conditioning data
+ * (values = normal scores) followed by the grid nodes in simulation-path
+ * order (their fitted values are overwritten). Node j, in that order, is
+ * simple-kriged (mean 0, the fitted variogram, which the caller scales to a
+ * unit sill) from the data and the nodes before it, and draws
+ * score = mean + sqrt(variance) * z[j]; a node whose search finds fewer than
+ * min_samples draws z[j]. Nodes run in parallel windows of `batch` (0: sized
+ * from the data) whose nodes are searched again when an earlier node of the
+ * window was still unsimulated within their reach, so the result is the
+ * sequential one for any batch. Outputs (host, one per node): score, and
+ * how (1 kriged, 2 marginal; may be NULL); *rounds (may be NULL) counts the
+ * parallel rounds. Nodes on a datum (they take its value and draw nothing)
+ * and the normal-score transform and its back-transform are the caller's. */
+int btk_sgs_simulate(btk_ctx* ctx, int64_t n_data, const double* z, int64_t batch, double* score, int8_t* how,
+                     int64_t* rounds);
+
 /* btk_predict plus the diagnostics columns (the estimator's predict with
  * diagnostics=True, crates/py/src/estimation.rs:1734-1737). out->status is
  * required: a second pass re-solves each estimated system for its weights by

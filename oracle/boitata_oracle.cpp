@@ -1460,6 +1460,45 @@ int32_t orc_estimate_many(int64_t m, const double* targets, int32_t loo, int64_t
   return 0;
 }
 
+// crates/simulation/src/sgs.rs:586-760 (`sequential`), one node at a time:
+// node j (in simulation order) is searched among the data and the nodes
+// before it (a linear scan, which selects as the tree does, search.rs:647-
+// 687), simple-kriged with mean 0 from their scores, and draws
+// mean + sqrt(variance) * z[j]; a failed search draws z[j]. The node then
+// joins the conditioning set as sample n_data + j, with no hole. how[j] = 1
+// kriged, 2 marginal. Returns -1 - j when kriging node j fails.
+int64_t orc_sgs(int64_t n_data, const double* xyz, const double* scores, const int64_t* hole, int64_t m,
+                const double* nodes, const double* z, const orc_search* sp, const orc_variogram* vgp, double* out,
+                int8_t* how) {
+  std::vector<Sample> s = conv_samples(n_data, xyz, scores, nullptr, hole);
+  SearchP p = conv_search(sp);
+  Variogram vg = conv_vg(vgp);
+  s.reserve(size_t(n_data + m));
+  for (int64_t j = 0; j < m; ++j) {
+    const double* t = &nodes[3 * j];
+    std::vector<size_t> chosen;
+    const bool ok = scan_neighbors(t, s, p, &vg, chosen);
+    double score;
+    if (!ok || chosen.empty()) {
+      score = z[j];
+      how[j] = 2;
+    } else {
+      std::vector<Sample> sel;
+      for (size_t i : chosen) sel.push_back(s[i]);
+      Estimate e;
+      if (krige(SIMPLE, 0.0, t, sel, vg, e) != OK) return -1 - j;
+      score = e.value + std::sqrt(std::fmax(e.variance, 0.0)) * z[j];
+      how[j] = 1;
+    }
+    out[j] = score;
+    Sample node;
+    node.loc[0] = t[0], node.loc[1] = t[1], node.loc[2] = t[2];
+    node.value = score, node.err = 0.0, node.hole = -1;
+    s.push_back(node);
+  }
+  return 0;
+}
+
 // krige (krige.rs:83-95) of m targets from given neighbour lists (m x k,
 // -1 padded): frozen neighbourhoods for the leave-one-out gradient checks.
 // With skip_coincident, a system holding two samples within 1e-6 m gets

@@ -95,6 +95,8 @@ def lib():
                                                    ctypes.POINTER(Srch), ctypes.POINTER(Vario), ctypes.c_int32,
                                                    ctypes.c_double, ctypes.c_int32, P, P, P]),
             "orc_centroids": (None, [P, P, P, P, ctypes.c_int64, ctypes.c_int64, P]),
+            "orc_sgs": (ctypes.c_int64, [ctypes.c_int64, P, P, P, ctypes.c_int64, P, P, ctypes.POINTER(Srch),
+                                         ctypes.POINTER(Vario), P, P]),
             "orc_prefix_quality": (None, [ctypes.c_int64, P, P, P, ctypes.POINTER(Vario), ctypes.c_int32,
                                           ctypes.c_double, P, P, P]),
             "orc_krige_lists": (ctypes.c_int32, [ctypes.c_int64, P, ctypes.c_int64, P, P, P, P, ctypes.c_int64,
@@ -289,6 +291,22 @@ def prefix_quality(target, xyz, vg, *, ordinary=True, support=None, err=None):
     lib().orc_prefix_quality(n, xyz.ctypes.data, _ptr(e), t.ctypes.data, ctypes.byref(variogram(vg)),
                              1 if ordinary else 0, sv, sl.ctypes.data, ef.ctypes.data, ok.ctypes.data)
     return sl, ef, ok.astype(bool)
+
+
+def sgs(xyz, scores, nodes, z, s, vg, *, holes=None):
+    """Sequential simulation of `nodes` (in simulation order) from data `xyz` with normal `scores`
+    (crates/simulation/src/sgs.rs:586-760): (node scores, how: 1 kriged, 2 marginal)."""
+    xyz, nodes = _xyz(xyz), _xyz(nodes)
+    sc = np.ascontiguousarray(scores, dtype=np.float64)
+    zz = np.ascontiguousarray(z, dtype=np.float64)
+    h = None if holes is None else np.ascontiguousarray(holes, dtype=np.int64)
+    m = len(nodes)
+    out, how = np.empty(m), np.zeros(m, dtype=np.int8)
+    rc = lib().orc_sgs(len(xyz), xyz.ctypes.data, sc.ctypes.data, _ptr(h), m, nodes.ctypes.data, zz.ctypes.data,
+                       ctypes.byref(search(s)), ctypes.byref(variogram(vg)), out.ctypes.data, how.ctypes.data)
+    if rc < 0:
+        raise ValueError(f"oracle: kriging failed at node {-1 - rc}")
+    return out, how
 
 
 def estimate_many(targets, xyz, values, s, vg, *, kind="ordinary", kparam=0.0, err=None, holes=None, loo=False,
