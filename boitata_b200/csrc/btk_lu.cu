@@ -22,14 +22,14 @@
 namespace btk {
 namespace {
 
-constexpr int kThreads = 128;
+constexpr unsigned kFull = 0xffffffffu;
 
 struct LuHead {
   int64_t ti;
   double t[3];
   int n, nn, dim, kind, twin, sing, nperm;
-  int best_i[kThreads];
-  double best_v[kThreads];
+  int piv[2];        // pivot row of the column, double-buffered by column parity
+  double pv[2];      // and its value
   int cof[kMaxLU], cfirst[kMaxLU], csize[kMaxLU];
 };
 
@@ -56,8 +56,11 @@ __host__ __device__ inline LuLayout lu_layout(int kmax) {
   return l;
 }
 
-template <bool DIAG>
-__global__ void __launch_bounds__(kThreads) k_solve_lu(SolveDev a, int kmax) {
+// NT threads per system: 128 up to 64 samples, 512 beyond (one system per SM
+// then, its matrix filling most of the shared memory).
+template <bool DIAG, int NT>
+__global__ void __launch_bounds__(NT) k_solve_lu(SolveDev a, int kmax) {
+  constexpr int kThreads = NT, kWarps = NT / 32;
   extern __shared__ __align__(16) unsigned char smem[];
   const LuLayout lay = lu_layout(kmax);
   LuHead& H = *reinterpret_cast<LuHead*>(smem + lay.head);
@@ -70,7 +73,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_lu(SolveDev a, int kmax) {
   int* pb = pa + kmax + 1;
   double* A = reinterpret_cast<double*>(smem + lay.a);
   const int S = lay.stride;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t nitems = a.list ? *a.list_len : (a.perm ? a.nwork : a.m);
   const VgDev& vg = a.vg;
   for (int64_t item = blockIdx.x; item < nitems; item += gridDim.x) {
@@ -200,29 +203,30 @@ __global__ void __launch_bounds__(kThreads) k_solve_lu(SolveDev a, int kmax) {
       B[i] = v, X[i] = v;
     }
     __syncthreads();
-    // LU with partial pivoting (nalgebra lu.rs).
+    // LU with partial pivoting (nalgebra lu.rs). Per column: warp 0 finds the
+    // first largest |a_rk| (r >= k); rows k and the pivot swap; each warp
+    // scales and updates its rows below k (row k is only read meanwhile).
     for (int k = 0; k < dim; ++k) {
-      double bv = -1.0;
-      int bi = k;
-      for (int r = k + tid; r < dim; r += kThreads) {
-        const double v = fabs(A[r * S + k]);
-        if (v > bv) bv = v, bi = r;
-      }
-      H.best_v[tid] = bv, H.best_i[tid] = bi;
-      __syncthreads();
-      for (int w = kThreads / 2; w > 0; w >>= 1) {
-        if (tid < w) {
-          const double v2 = H.best_v[tid + w];
-          const int i2 = H.best_i[tid + w];
-          if (v2 > H.best_v[tid] || (v2 == H.best_v[tid] && i2 < H.best_i[tid]))
-            H.best_v[tid] = v2, H.best_i[tid] = i2;
+      const int b = k & 1;
+      if (warp == 0) {
+        double bv = -1.0;
+        int bi = k;
+        for (int r = k + lane; r < dim; r += 32) {
+          const double v = fabs(A[r * S + k]);
+          if (v > bv) bv = v, bi = r;
         }
-        __syncthreads();
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const double v2 = __shfl_xor_sync(kFull, bv, o);
+          const int i2 = __shfl_xor_sync(kFull, bi, o);
+          if (v2 > bv || (v2 == bv && i2 < bi)) bv = v2, bi = i2;
+        }
+        if (lane == 0) H.piv[b] = bi, H.pv[b] = A[bi * S + k];
       }
-      const int piv = H.best_i[0];
-      const double diag = A[piv * S + k];
       __syncthreads();
-      if (diag == 0.0) continue;  // uniform: every thread read the same pivot
+      const int piv = H.piv[b];
+      const double diag = H.pv[b];
+      if (diag == 0.0) continue;  // uniform: a zero column is skipped
       if (piv != k) {
         for (int j = tid; j < dim; j += kThreads) {
           const double tmp = A[k * S + j];
@@ -230,42 +234,43 @@ __global__ void __launch_bounds__(kThreads) k_solve_lu(SolveDev a, int kmax) {
           A[piv * S + j] = tmp;
         }
         if (tid == 0) pa[H.nperm] = k, pb[H.nperm] = piv, ++H.nperm;
+        __syncthreads();
       }
-      __syncthreads();
       const double inv = 1.0 / diag;
-      for (int r = k + 1 + tid; r < dim; r += kThreads) A[r * S + k] *= inv;
-      __syncthreads();
-      const int rest = dim - k - 1;
-      for (int e = tid; e < rest * rest; e += kThreads) {
-        const int r = k + 1 + e / rest, c = k + 1 + e % rest;
-        A[r * S + c] = fma(-A[k * S + c], A[r * S + k], A[r * S + c]);
+      for (int r = k + 1 + warp; r < dim; r += kWarps) {
+        const double l = A[r * S + k] * inv;
+        __syncwarp();
+        if (lane == 0) A[r * S + k] = l;
+        for (int c = k + 1 + lane; c < dim; c += 32) A[r * S + c] = fma(-A[k * S + c], l, A[r * S + c]);
       }
       __syncthreads();
     }
-    // LU::solve: row swaps, then L (unit lower) and U substitutions.
-    if (tid == 0)
-      for (int q = 0; q < H.nperm; ++q) {
-        const double tmp = X[pa[q]];
-        X[pa[q]] = X[pb[q]];
-        X[pb[q]] = tmp;
+    // LU::solve by warp 0: row swaps, then L (unit lower) and U substitutions.
+    if (warp == 0) {
+      if (lane == 0)
+        for (int q = 0; q < H.nperm; ++q) {
+          const double tmp = X[pa[q]];
+          X[pa[q]] = X[pb[q]];
+          X[pb[q]] = tmp;
+        }
+      __syncwarp();
+      for (int i = 0; i < dim; ++i) {
+        const double coeff = X[i];
+        for (int r = i + 1 + lane; r < dim; r += 32) X[r] = fma(-coeff, A[r * S + i], X[r]);
+        __syncwarp();
       }
-    __syncthreads();
-    for (int i = 0; i < dim; ++i) {
-      const double coeff = X[i];
-      for (int r = i + 1 + tid; r < dim; r += kThreads) X[r] = fma(-coeff, A[r * S + i], X[r]);
-      __syncthreads();
-    }
-    for (int i = dim - 1; i >= 0; --i) {
-      const double diag = A[i * S + i];
-      if (diag == 0.0) {  // uniform
-        if (tid == 0) H.sing = 1;
-        break;
+      for (int i = dim - 1; i >= 0; --i) {
+        const double d = A[i * S + i];
+        if (d == 0.0) {  // uniform over the warp
+          if (lane == 0) H.sing = 1;
+          break;
+        }
+        const double coeff = X[i] / d;
+        __syncwarp();
+        if (lane == 0) X[i] = coeff;
+        for (int r = lane; r < i; r += 32) X[r] = fma(-coeff, A[r * S + i], X[r]);
+        __syncwarp();
       }
-      const double coeff = X[i] / diag;
-      __syncthreads();
-      if (tid == 0) X[i] = coeff;
-      for (int r = tid; r < i; r += kThreads) X[r] = fma(-coeff, A[r * S + i], X[r]);
-      __syncthreads();
     }
     __syncthreads();
     if (DIAG) {
@@ -306,17 +311,20 @@ cudaError_t launch_solve_lu(const Launch& L, const SolveDev& a, int kmax, bool d
   if (kmax < 1 || kmax > kMaxLU) return cudaErrorInvalidValue;
   if (diag && !a.status) return cudaErrorInvalidValue;
   const size_t smem = lu_layout(kmax).total;
-  auto kern = diag ? k_solve_lu<true> : k_solve_lu<false>;
+  const bool wide = kmax > 64;
+  const int threads = wide ? 512 : 128;
+  auto kern = diag ? (wide ? k_solve_lu<true, 512> : k_solve_lu<true, 128>)
+                   : (wide ? k_solve_lu<false, 512> : k_solve_lu<false, 128>);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
   if (e != cudaSuccess) return e;
   int64_t blocks = int64_t(L.sm_count) * (per_sm > 0 ? per_sm : 1);
   const int64_t items = a.perm ? a.nwork : a.m;
   if (!a.list && blocks > items) blocks = items;
   if (blocks < 1) blocks = 1;
-  kern<<<int(blocks), kThreads, smem, L.stream>>>(a, kmax);
+  kern<<<int(blocks), threads, smem, L.stream>>>(a, kmax);
   ++*L.counter;
   return cudaGetLastError();
 }
