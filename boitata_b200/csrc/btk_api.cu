@@ -1152,7 +1152,10 @@ int btk_sgs_simulate(btk_ctx* ctx, int64_t n_data, const double* z, int64_t batc
   CK(cudaMemsetAsync(ctx->sg_how.p, 0, mm, L.stream));
   CK(cudaMemsetAsync(ctx->sg_ctl.p, 0xFF, 2 * sizeof(int64_t), L.stream));
   const SearchDev saved = ctx->spd;
-  ctx->spd.rules = 1;  // one warp per node: the selector with the simulation's availability test
+  // One warp per node (the rules kernel): a window's nodes lie anywhere on the
+  // path, so the tile search, which grows one box around 32 targets, does not
+  // fit them.
+  ctx->spd.rules = 1;
   ctx->spd.sgs = 1, ctx->spd.sgs_node0 = uint32_t(n_data), ctx->spd.sgs_done = ctx->sg_done.p;
   const uint32_t node0 = uint32_t(n_data);
   const int64_t most = ctx->search.max_samples;
@@ -1162,8 +1165,8 @@ int btk_sgs_simulate(btk_ctx* ctx, int64_t n_data, const double* z, int64_t batc
     // A window of the path is kriged in parallel against the nodes before it;
     // about window * most / (2 known) of its nodes go stale (sgs.rs:679-683).
     const int64_t known = n_data + start;
-    int64_t size = batch > 0 ? batch : known / (2 * (most > 0 ? most : 1));
-    size = std::max<int64_t>(batch > 0 ? 1 : 64, std::min<int64_t>(size, 65536));
+    int64_t size = batch > 0 ? batch : known / (most > 0 ? most : 1);
+    size = std::max<int64_t>(batch > 0 ? 1 : 1024, std::min<int64_t>(size, batch > 0 ? 65536 : 8192));
     const int64_t end = std::min(m, start + size);
     for (int64_t round = 0; round <= size; ++round) {
       if ((rc = [&]() -> int {
