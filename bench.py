@@ -52,6 +52,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-grad", action="store_true")
     p.add_argument("--no-tune", action="store_true")
+    p.add_argument("--no-callers", action="store_true", help="skip the dense-LU, calibration and SGS lines")
     p.add_argument("--grid", default=None, help="block counts NXxNYxNZ in place of 200x200x80 (profiling cases)")
     p.add_argument("--profile", action="store_true",
                    help="profiling case: warm-up and two steps of each form, no timing, no JSON line")
@@ -208,6 +209,58 @@ def loo_gradient(args, dev, ws=1, rank=0):
                                  "frozen at theta0, gradient w.r.t. nugget, 2 sills, 2 ranges, 2 ratios, "
                                  "3 angles (FP64 adjoint, one kernel with the forward); samples split over the "
                                  "ranks, partial sums all-reduced"}}
+
+
+def callers(dev):
+    """The paths around the headline one, each timed once warm (wall clock around the host call, inputs on
+    the host): the dense LU of 128-sample and power-model systems and a calibrated search over c1's 50,000
+    blocks, and one sequential Gaussian simulation of 400,000 nodes conditioned on c2's 50,000 composites."""
+    import torch
+
+    import boitata_b200 as bt
+    from boitata_b200 import workloads
+    from boitata_b200.simulation import sgs_scores, unit_sill
+    from boitata_b200.transforms import normal_score
+
+    out = {}
+    w = workloads.c1()
+    g = w.geometry
+    cases = {
+        "dense_lu_128": (w.variogram, bt.Search(ranges=(300.0, 300.0, 100.0), max_samples=128, min_samples=1)),
+        "power_model_32": (bt.Variogram([bt.Structure("power", 0.02, 100.0, exponent=1.5)], nugget=0.1,
+                                        ratios=(1.0, 1.0 / 3.0)),
+                           bt.Search(ranges=(300.0, 300.0, 100.0), max_samples=32, min_samples=1)),
+        "calibrated_slope_0.9": (w.variogram, bt.Search(ranges=(300.0, 300.0, 100.0), max_samples=48, min_samples=4,
+                                                         target_slope=0.9)),
+    }
+    for name, (vg, s) in cases.items():
+        ok = bt.OrdinaryKriging(vg, s).fit(w.coords, w.values)
+        ok.predict_full(g)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            ok.predict_full(g)
+            ts.append(time.perf_counter() - t0)
+        out[name] = {"blocks_per_s": g.cells() / float(np.median(ts)), "blocks": g.cells(),
+                     "workload": "c1 samples and block model, " + name.replace("_", " ")}
+    w2 = workloads.c2()
+    scores, _ = normal_score(w2.values)
+    sim_grid = bt.Geometry((0.0, 0.0, 0.0), (5.0, 5.0, 6.25), (100, 100, 40))
+    ctx = bt._native.Context(0)
+    nodes = bt.BlockModel(sim_grid).centroids(ctx)
+    rng = np.random.default_rng(1)
+    order, z = rng.permutation(len(nodes)), rng.standard_normal(len(nodes))
+    vg = unit_sill(w2.variogram)
+    sgs_scores(w2.coords, scores, None, nodes[order][:4096], z[:4096], w2.search, vg, context=ctx)
+    t0 = time.perf_counter()
+    _, how, rounds = sgs_scores(w2.coords, scores, None, nodes[order], z, w2.search, vg, context=ctx)
+    dt = time.perf_counter() - t0
+    out["sgs"] = {"nodes_per_s": len(nodes) / dt, "nodes": len(nodes), "seconds": dt, "rounds": rounds,
+                  "kriged": int((how == 1).sum()),
+                  "workload": "c2 composites (normal scores) conditioning a 100x100x40 grid of 5x5x6.25 m nodes, "
+                              "one realization, c2's octant search, FP64"}
+    return out
 
 
 def run_reference(args, ws, rank):
@@ -430,6 +483,8 @@ def main():
     if not args.no_grad:
         line.update(loo_gradient(args, dev, ws, rank))
 
+    if rank == 0 and ws == 1 and not args.no_callers:
+        line["callers"] = callers(dev)
     if rank == 0 and ws == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(w, args.cpu_sample)
     if rank == 0:
