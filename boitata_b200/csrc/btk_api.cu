@@ -453,7 +453,7 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
   int rc = ensure_scratch(ctx, m);
   if (rc) return rc;
   Launch L = ctx->launch(s);
-  if (!perm && m >= kOrderMin) {  // caller's order: sort into Morton order so warps and tiles are compact
+  if (!perm && m >= kOrderMin) {  // caller's order: sort into Hilbert order so warps and tiles are compact
     const size_t tb = morton_temp_bytes(m);
     if (tb == 0) return fail(ctx, BTK_ECUDA, "radix sort sizing failed");
     CK(ctx->ord_keys.grow(2 * size_t(m)));

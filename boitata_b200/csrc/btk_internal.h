@@ -209,7 +209,7 @@ cudaError_t launch_solve_redo_pairs(const Launch& L, const SolveDev& a);
 // (and, mixed, a.redo) for the per-system kernels. Counts must start at 0.
 cudaError_t launch_tile(const Launch& L, const TileDev& a, bool mixed);
 
-// Work-slot permutation of m caller-supplied targets in Morton order of
+// Work-slot permutation of m caller-supplied targets in Hilbert order of
 // their positions, axis d weighted by w[d] (btk_order.cu). keys and vals
 // hold 2m entries each; temp holds morton_temp_bytes(m). *perm points into
 // vals on return.
