@@ -30,6 +30,8 @@
 // residuals. The Lagrange multiplier and the variance are then formed in
 // FP64. A system whose FP32 pivots fall below 1e-5 C0 or whose residual is
 // large goes to an FP64 re-solve list (status flag BTK_ST_FP64_FALLBACK).
+#include <cstddef>
+
 #include "btk_device.cuh"
 
 namespace btk {
@@ -37,12 +39,14 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+// 16-byte aligned, with a size a multiple of 16, so every group's column line
+// takes 16-byte (double2) loads.
 template <int NW>
-struct SolveSmem {
+struct alignas(16) SolveSmem {
   static constexpr int R = 32 * NW;
   double P[R][3];
   double T[R * (R - 1) / 2];
-  double col[2][R];
+  alignas(16) double col[2][R + 2];  // column below the pivot (0 .. R-2), the pivot (R), a sink (R+1)
   double rhs[2][4];
   double red[NW][8];
   int ired[NW];
@@ -50,11 +54,16 @@ struct SolveSmem {
   int cof[R], cfirst[R], csize[R];
 };
 
+static_assert(sizeof(SolveSmem<1>) % 16 == 0 && sizeof(SolveSmem<2>) % 16 == 0, "group stride");
+static_assert(offsetof(SolveSmem<1>, col) % 16 == 0 && offsetof(SolveSmem<2>, col) % 16 == 0, "column line");
+static_assert((sizeof(double) * (32 + 2)) % 16 == 0 && (sizeof(double) * (64 + 2)) % 16 == 0, "line stride");
+static_assert((sizeof(float) * (32 + 4)) % 16 == 0 && (sizeof(float) * (64 + 4)) % 16 == 0, "FP32 line stride");
+
 template <int NW>
 struct MixedSmem {
   static constexpr int R = 32 * NW;
   SolveSmem<NW> base;
-  float colf[2][R];
+  alignas(16) float colf[2][R + 4];  // column below the pivot (0 .. R-2), the pivot (R), a sink (R+1)
   float rhsf[2][4];
   float L[R][R + 1];
   double xs[3][R];
@@ -236,6 +245,41 @@ __device__ __forceinline__ bool assemble(const SolveDev& a, SolveSmem<NW>& S, in
   return true;
 }
 
+// Pivots k0 .. k1-1 of the FP64 right-looking LDL^T with the forward
+// substitution of y fused in, the row kept shifted so that slot 0 holds the
+// current pivot column: a step writes it to the group's line, then
+// A[q] <- A[q+1] - f col[q] over the W slots that can still hold live
+// columns. The loop body is the same for every k, so it is a runtime loop
+// and A stays in registers.
+template <int NW, int W>
+__device__ __forceinline__ void eliminate_rows(double (&A)[32 * NW], int k0, int k1, int row, SolveSmem<NW>& S,
+                                               int gid, double& y0, double& y1, double& y2, double& dme, bool& sing,
+                                               double thr) {
+  constexpr int R = 32 * NW;
+  for (int k = k0; k < k1; ++k) {
+    const int b = k & 1;
+    S.col[b][row > k ? row - k - 1 : (row == k ? R : R + 1)] = A[0];
+    if (row == k) S.rhs[b][0] = y0, S.rhs[b][1] = y1, S.rhs[b][2] = y2;
+    gsync<NW>(gid);
+    const double d = S.col[b][R];
+    if (!(d > thr)) {  // NaN or at most 1e-12 C0 (kernel.rs:61); uniform over the group
+      sing = true;
+      return;
+    }
+    if (row == k) dme = d;
+    const double f = row > k ? A[0] * (1.0 / d) : 0.0;
+#pragma unroll
+    for (int q = 0; q < W; q += 2) {
+      const double2 cv = *reinterpret_cast<const double2*>(&S.col[b][q]);
+      A[q] = fma(-f, cv.x, A[q + 1]);
+      A[q + 1] = q + 2 < R ? fma(-f, cv.y, A[q + 2]) : 0.0;
+    }
+    y0 = fma(-f, S.rhs[b][0], y0);
+    y1 = fma(-f, S.rhs[b][1], y1);
+    y2 = fma(-f, S.rhs[b][2], y2);
+  }
+}
+
 template <int NW, bool kPairs = false>
 __global__ void __launch_bounds__(128) k_solve64(SolveDev a, int8_t flag) {
   constexpr int R = 32 * NW;
@@ -261,29 +305,14 @@ __global__ void __launch_bounds__(128) k_solve64(SolveDev a, int8_t flag) {
     double y0 = have ? c : 0.0, y1 = have ? 1.0 : 0.0, y2 = have ? zf : 0.0;
     double dme = 1.0;
     bool sing = false;
-#pragma unroll
-    for (int k = 0; k < R; ++k) {
-      if (k >= nn) break;
-      const int b = k & 1;
-      S.col[b][row] = A[k];
-      if (row == k) S.rhs[b][0] = y0, S.rhs[b][1] = y1, S.rhs[b][2] = y2;
-      gsync<NW>(gid);
-      const double d = S.col[b][k];
-      if (!(d > kPivot * c0)) {  // NaN or at most 1e-12 C0 (kernel.rs:61)
-        sing = true;
-        break;
-      }
-      if (row == k) dme = d;
-      if (row > k) {
-        const double f = A[k] * (1.0 / d);
-#pragma unroll
-        for (int q = k + 1; q < R; ++q) A[q] = fma(-f, S.col[b][q], A[q]);
-        y0 = fma(-f, S.rhs[b][0], y0);
-        y1 = fma(-f, S.rhs[b][1], y1);
-        y2 = fma(-f, S.rhs[b][2], y2);
-        A[k] = f;
-      }
-    }
+    const double thr = kPivot * c0;
+    // Four stages of R/4 pivots over windows of R, 3R/4, R/2 and R/4 slots.
+    constexpr int Q = R / 4;
+    const int n1 = min(nn, Q), n2 = min(nn, 2 * Q), n3 = min(nn, 3 * Q);
+    eliminate_rows<NW, R>(A, 0, n1, row, S, gid, y0, y1, y2, dme, sing, thr);
+    if (!sing) eliminate_rows<NW, 3 * Q>(A, n1, n2, row, S, gid, y0, y1, y2, dme, sing, thr);
+    if (!sing) eliminate_rows<NW, 2 * Q>(A, n2, n3, row, S, gid, y0, y1, y2, dme, sing, thr);
+    if (!sing) eliminate_rows<NW, Q>(A, n3, nn, row, S, gid, y0, y1, y2, dme, sing, thr);
     if (sing) {
       if (row == 0) write_fail(a, ti, BTK_ST_SINGULAR, 0);
       continue;
@@ -292,6 +321,41 @@ __global__ void __launch_bounds__(128) k_solve64(SolveDev a, int8_t flag) {
     double s[5] = {y1 * y0 * wt, y1 * y1 * wt, y2 * y0 * wt, y2 * y1 * wt, y0 * y0 * wt};
     group_sum5<NW>(S, gid, wig, s);
     if (row == 0) epilogue(a, kind, ti, s, n, flag);
+  }
+}
+
+// The FP32 form of eliminate_rows: the multiplier of row i at step k goes to
+// L[i][k] for the back substitution, and a pivot at most thr (1e-5 C0) or NaN
+// leaves the system to the FP64 form.
+template <int NW, int W>
+__device__ __forceinline__ void eliminate_rows_f32(float (&A)[32 * NW], int k0, int k1, int row, MixedSmem<NW>& X,
+                                                   int gid, float& y0, float& y1, float& y2, float& dme, bool& weak,
+                                                   float thr) {
+  constexpr int R = 32 * NW;
+  for (int k = k0; k < k1; ++k) {
+    const int b = k & 1;
+    X.colf[b][row > k ? row - k - 1 : (row == k ? R : R + 1)] = A[0];
+    if (row == k) X.rhsf[b][0] = y0, X.rhsf[b][1] = y1, X.rhsf[b][2] = y2;
+    gsync<NW>(gid);
+    const float d = X.colf[b][R];
+    if (!(d > thr)) {  // uniform over the group
+      weak = true;
+      return;
+    }
+    if (row == k) dme = d;
+    const float f = row > k ? A[0] * __frcp_rn(d) : 0.f;
+    if (row > k) X.L[row][k] = f;
+#pragma unroll
+    for (int q = 0; q < W; q += 4) {
+      const float4 cv = *reinterpret_cast<const float4*>(&X.colf[b][q]);
+      A[q] = fmaf(-f, cv.x, A[q + 1]);
+      A[q + 1] = fmaf(-f, cv.y, A[q + 2]);
+      A[q + 2] = fmaf(-f, cv.z, A[q + 3]);
+      A[q + 3] = q + 4 < R ? fmaf(-f, cv.w, A[q + 4]) : 0.f;
+    }
+    y0 = fmaf(-f, X.rhsf[b][0], y0);
+    y1 = fmaf(-f, X.rhsf[b][1], y1);
+    y2 = fmaf(-f, X.rhsf[b][2], y2);
   }
 }
 
@@ -324,36 +388,19 @@ __global__ void __launch_bounds__(128) k_solve_mixed(SolveDev a, int64_t* redo, 
     float y0 = have ? float(c) : 0.f, y1 = have ? 1.f : 0.f, y2 = have ? float(zf) : 0.f;
     float dme = 1.f;
     bool weak = false;
-#pragma unroll
-    for (int k = 0; k < R; ++k) {
-      if (k >= nn) break;
-      const int b = k & 1;
-      X.colf[b][row] = A[k];
-      if (row == k) X.rhsf[b][0] = y0, X.rhsf[b][1] = y1, X.rhsf[b][2] = y2;
-      gsync<NW>(gid);
-      const float d = X.colf[b][k];
-      if (!(d > 1e-5f * c0f)) {
-        weak = true;
-        break;
-      }
-      if (row == k) dme = d;
-      if (row > k) {
-        const float f = A[k] * __frcp_rn(d);
-#pragma unroll
-        for (int q = k + 1; q < R; ++q) A[q] = fmaf(-f, X.colf[b][q], A[q]);
-        y0 = fmaf(-f, X.rhsf[b][0], y0);
-        y1 = fmaf(-f, X.rhsf[b][1], y1);
-        y2 = fmaf(-f, X.rhsf[b][2], y2);
-        A[k] = f;
-      }
-    }
+    const float thr = 1e-5f * c0f;
+    constexpr int Q = R / 4;
+    const int n1 = min(nn, Q), n2 = min(nn, 2 * Q), n3 = min(nn, 3 * Q);
+    eliminate_rows_f32<NW, R>(A, 0, n1, row, X, gid, y0, y1, y2, dme, weak, thr);
+    if (!weak) eliminate_rows_f32<NW, 3 * Q>(A, n1, n2, row, X, gid, y0, y1, y2, dme, weak, thr);
+    if (!weak) eliminate_rows_f32<NW, 2 * Q>(A, n2, n3, row, X, gid, y0, y1, y2, dme, weak, thr);
+    if (!weak) eliminate_rows_f32<NW, Q>(A, n3, nn, row, X, gid, y0, y1, y2, dme, weak, thr);
     if (weak) {  // leave it to the FP64 form, which also takes the singular decision
       if (row == 0) redo[atomicAdd(reinterpret_cast<unsigned long long*>(redo_len), 1ull)] = ti;
       continue;
     }
-    // Back substitution L^T x = D^-1 y, column by column from the last row.
-#pragma unroll
-    for (int q = 0; q < R; ++q) X.L[row][q] = A[q];
+    // Back substitution L^T x = D^-1 y, column by column from the last row
+    // (L[i][k], i > k, written during the elimination).
     float u0 = y0 / dme, u1 = y1 / dme, u2 = y2 / dme;
     gsync<NW>(gid);
     for (int k = nn - 1; k >= 0; --k) {
