@@ -244,6 +244,29 @@ def callers(dev):
             ts.append(time.perf_counter() - t0)
         out[name] = {"blocks_per_s": g.cells() / float(np.median(ts)), "blocks": g.cells(),
                      "workload": "c1 samples and block model, " + name.replace("_", " ")}
+    # C5: 220k clustered composites (10% near-twins 0.01 m away), Gaussian model with a 1e-4 nugget, octant
+    # search with up to 64 samples, 10.24M blocks; FP64 (every system is ill-conditioned, so the mixed form
+    # re-solves all of them in FP64), device outputs, one timed step after a warm one.
+    w5 = workloads.c5()
+    est = bt.OrdinaryKriging(w5.variogram, w5.search).fit(w5.coords, w5.values)
+    c5ctx = est._ctx
+    m5 = w5.geometry.cells()
+    g5 = w5.geometry.to_c()
+    v5 = torch.empty(m5, dtype=torch.float64, device=dev)
+    s5 = torch.empty(m5, dtype=torch.float64, device=dev)
+    o5 = bt._native.OutputsC(v5.data_ptr(), s5.data_ptr(), None, None, None)
+    ts = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        c5ctx.check(c5ctx._lib.btk_predict_geometry_device(c5ctx.handle, ctypes.byref(g5), bt._native.ORDINARY, 0.0,
+                                                           bt._native.FP64, ctypes.byref(o5), None), "c5")
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    out["c5_fp64"] = {"blocks_per_s": m5 / ts[-1], "blocks": m5, "samples": int(len(w5.coords)),
+                      "seconds": ts[-1], "finite": int(torch.isfinite(v5).sum().item()),
+                      "workload": "C5: 10.24M blocks, octant search up to 64 samples, FP64, device outputs"}
+    del est, v5, s5
     w2 = workloads.c2()
     scores, _ = normal_score(w2.values)
     sim_grid = bt.Geometry((0.0, 0.0, 0.0), (5.0, 5.0, 6.25), (100, 100, 40))
