@@ -136,6 +136,10 @@ struct btk_ctx {
   double ppc = 2.0;  // samples per grid cell
 
   bool fitted = false;
+  // A host call in the mixed form that saw most of its systems go to the FP64
+  // re-solve (an ill-conditioned model) makes later host calls of this fit and
+  // search run the FP64 form directly (see mixed_precision_for).
+  bool mixed_to_fp64 = false;
   int64_t n = 0;
   bool has_err = false, planar = false;
   btk_search search{};
@@ -896,6 +900,7 @@ int btk_fit(btk_ctx* ctx, int64_t n, const double* xyz, const double* values, co
             const int64_t* holes, const btk_search* search, const btk_variogram* vg) {
   if (!ctx) return BTK_EINVAL;
   ctx->fitted = false;
+  ctx->mixed_to_fp64 = false;
   if (n <= 0 || !xyz || !values) return fail(ctx, BTK_EINVAL, "fit needs at least one sample with coordinates and values");
   if (n >= int64_t(0xffffffffu)) return fail(ctx, BTK_EINVAL, "too many samples");
   int rc = check_vg(ctx, vg);
@@ -950,6 +955,7 @@ int btk_set_search(btk_ctx* ctx, const btk_search* search) {
   if ((rc = check_search(ctx, search))) return rc;
   CK(cudaSetDevice(ctx->device));
   ctx->search = *search;
+  ctx->mixed_to_fp64 = false;
   ctx->frozen = false;
   if ((rc = index_samples(ctx))) return rc;
   CK(cudaStreamSynchronize(ctx->stream));
@@ -974,8 +980,28 @@ namespace {
 // out overlap chunk c's search and solve. Each chunk is a run_path of its own over the
 // context's scratch, which the compute stream serialises; chunks write
 // disjoint slices of the staged inputs and outputs.
+// On an ill-conditioned model the FP32 factor fails for most systems, and the
+// mixed form then pays for the FP32 attempt and the FP64 re-solve of each. A
+// host call of the mixed form whose re-solves exceeded half of its m targets
+// marks the context, and its later host calls (until the next fit or search)
+// take the FP64 form: the re-solve is that form, so those systems get the
+// same bits, and the rest get FP64 results in place of mixed ones. Device
+// calls and captured graphs keep the precision they are given.
+int32_t mixed_precision_for(btk_ctx* ctx, int32_t precision) {
+  return precision == BTK_MIXED && ctx->mixed_to_fp64 ? BTK_FP64 : precision;
+}
+
+int note_mixed_outcome(btk_ctx* ctx, int32_t precision, int64_t m) {
+  if (precision != BTK_MIXED || m <= 0) return BTK_OK;
+  int64_t redo[2] = {0, 0};
+  CK(cudaMemcpy(redo, ctx->redo_len.p, sizeof(redo), cudaMemcpyDeviceToHost));
+  if (2 * (redo[0] + redo[1]) > m) ctx->mixed_to_fp64 = true;
+  return BTK_OK;
+}
+
 int predict_host(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds, int32_t kind, double kparam,
                  int32_t precision, const btk_outputs* out, const btk_diagnostics* diag = nullptr) {
+  precision = mixed_precision_for(ctx, precision);
   int64_t chunk = ctx->tuning.host_chunk > 0 ? int64_t(ctx->tuning.host_chunk) : m;
   if ((m + chunk - 1) / chunk > 8) chunk = (m + 7) / 8;
   const int64_t nc = (m + chunk - 1) / chunk;
@@ -1044,7 +1070,7 @@ int predict_host(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds
   }
   CK(cudaStreamSynchronize(ctx->down));
   CK(cudaStreamSynchronize(ctx->stream));
-  return BTK_OK;
+  return nc == 1 ? note_mixed_outcome(ctx, precision, m) : BTK_OK;
 }
 
 }  // namespace
@@ -1211,10 +1237,12 @@ int btk_cross_validate(btk_ctx* ctx, int32_t kind, double kparam, int32_t precis
   CK(cudaSetDevice(ctx->device));
   btk_outputs d{};
   if ((rc = host_outputs(ctx, ctx->n, out, &d))) return rc;
+  precision = mixed_precision_for(ctx, precision);
   if ((rc = run_path(ctx, nullptr, ctx->n, ctx->x.p, ctx->y.p, ctx->z.p, ctx->loo_perm.p, ctx->n, 1, kind, kparam,
                      precision, &d)))
     return rc;
-  return copy_out(ctx, ctx->n, &d, out);
+  if ((rc = copy_out(ctx, ctx->n, &d, out))) return rc;
+  return note_mixed_outcome(ctx, precision, ctx->n);
 }
 
 int btk_neighbors(btk_ctx* ctx, int64_t m, const double* xyz, int32_t loo, int64_t* idx, int32_t* count, int8_t* ok) {

@@ -295,3 +295,21 @@ def test_ill_conditioned_systems(oracle):
     assert np.all((mixed["status"][fin] & 0x10) != 0)
     for k in ("value", "variance", "lagrange"):
         np.testing.assert_array_equal(mixed[k], got[k])
+
+
+def test_mixed_calls_after_a_mostly_fp64_call_take_the_fp64_form():
+    """A mixed host call whose systems mostly went to the FP64 re-solve makes the next calls of the same fit
+    run the FP64 form directly: the same bits, no FP32 attempt (no fallback flags); a new fit starts over."""
+    w = W.c5(holes=160)
+    rng = np.random.default_rng(1)
+    targets = np.column_stack([rng.uniform(0, 1000, 1500), rng.uniform(0, 1000, 1500), rng.uniform(0, 250, 1500)])
+    fp64 = OrdinaryKriging(w.variogram, w.search).fit(w.coords, w.values).predict_full(targets)
+    est = OrdinaryKriging(w.variogram, w.search, precision="mixed").fit(w.coords, w.values)
+    first, second = est.predict_full(targets), est.predict_full(targets)
+    fin = np.isfinite(fp64["value"])
+    assert np.mean((first["status"][fin] & 0x10) != 0) > 0.5
+    assert np.all((second["status"] & 0x10) == 0)
+    for k in ("value", "variance", "lagrange"):
+        np.testing.assert_array_equal(second[k], fp64[k])
+    again = est.fit(w.coords, w.values).predict_full(targets)
+    np.testing.assert_array_equal(again["status"], first["status"])
