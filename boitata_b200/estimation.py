@@ -7,7 +7,11 @@ sharing a location keep the first one with a warning (args.rs:318-376),
 targets a search cannot fill are NaN, several searches run as passes on the
 targets earlier passes left (batch.rs:132-147). The kriging itself runs in
 the CUDA engine through its C ABI; `precision` selects the FP64 form
-(default, the reference's arithmetic) or the mixed FP32/FP64 form.
+(default, the reference's arithmetic) or the mixed FP32/FP64 form. In the
+mixed form a system whose FP32 factor is too weak is re-solved in FP64; once
+one call of an estimator re-solved most of its systems that way (an
+ill-conditioned model), its later calls until the next fit run the FP64 form
+directly, with the same results for those systems.
 """
 
 import contextlib
