@@ -420,13 +420,18 @@ cudaError_t run(const Launch& L, const SearchDev& sp, const GridDev& g, const do
 // selection is full, no sector is open or the radius is exhausted: the
 // result is the reference's for any number of candidates.
 constexpr int kRulesK = BTK_RULES_CANDIDATES;
+// A simulation's plain or octant search of at most 64 samples keeps fewer
+// candidates per round: its candidate set grows with every simulated node,
+// and the K-nearest cut, not the selection, dominates the search.
+constexpr int kSgsK = 128, kSgsK32 = 64;  // at most 64 / at most 32 samples
 constexpr int kHoleHash = 128;  // > 2 x 64 accepted holes
 constexpr uint32_t kNoHole = 0xffffffffu;
 
+template <int K>
 struct RulesSmem {
-  double cd[2 * kRulesK];
-  uint32_t ci[2 * kRulesK];
-  uint16_t sec[2 * kRulesK];
+  double cd[2 * K];
+  uint32_t ci[2 * K];
+  uint16_t sec[2 * K];
   uint32_t hkey[kHoleHash];
   int hcnt[kHoleHash];
   int per_sector[360];
@@ -494,7 +499,8 @@ __device__ int longest_empty(const SearchDev& sp, const int* counts) {
 
 // Hole slot of h in the warp's table of accepted holes (the free slot where
 // it would go when absent).
-__device__ __forceinline__ int hole_slot(const RulesSmem& S, uint32_t h) {
+template <int K>
+__device__ __forceinline__ int hole_slot(const RulesSmem<K>& S, uint32_t h) {
   int k = int((h * 2654435761u) >> 25);  // 7 bits
   for (int probe = 0; probe < kHoleHash; ++probe) {
     if (S.hkey[k] == h || S.hkey[k] == kNoHole) break;
@@ -508,7 +514,8 @@ __device__ __forceinline__ int hole_slot(const RulesSmem& S, uint32_t h) {
 // an open sector (per_sector below the cap) from a hole below its cap, goes
 // into the warp's buffer; above 2K - 32 candidates the buffer keeps its K
 // nearest. Returns the count; *dropped tells whether candidates were cut.
-__device__ int rules_scan(const SearchDev& sp, const GridDev& g, RulesSmem& S, const double q[3], const double t[3],
+template <int K>
+__device__ int rules_scan(const SearchDev& sp, const GridDev& g, RulesSmem<K>& S, const double q[3], const double t[3],
                           uint32_t left, double after_d, uint32_t after_i, bool filter, unsigned openmask,
                           bool& dropped, int lane, uint32_t my, double& d2u) {
   const double glo[3] = {g.lo[0], g.lo[1], g.lo[2]};
@@ -591,11 +598,11 @@ __device__ int rules_scan(const SearchDev& sp, const GridDev& g, RulesSmem& S, c
               S.cd[pos] = d2, S.ci[pos] = idx;
             }
             n += __popc(bal);
-            if (n > 2 * kRulesK - 32) {  // keep the K nearest
+            if (n > 2 * K - 32) {  // keep the K nearest
               __syncwarp();
               warp_sort(S.cd, S.ci, n, lane);
-              n = kRulesK;
-              thr = S.cd[kRulesK - 1];
+              n = K;
+              thr = S.cd[K - 1];
               dropped = true;
             }
             __syncwarp();
@@ -632,6 +639,7 @@ __device__ int rules_scan(const SearchDev& sp, const GridDev& g, RulesSmem& S, c
   return n;
 }
 
+template <int K>
 __global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, const double* __restrict__ tx,
                                                       const double* __restrict__ ty, const double* __restrict__ tz,
                                                       const int64_t* __restrict__ perm, int64_t m, int loo,
@@ -639,7 +647,7 @@ __global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, c
                                                       int8_t* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
-  RulesSmem& S = reinterpret_cast<RulesSmem*>(smem_raw)[threadIdx.x >> 5];
+  RulesSmem<K>& S = reinterpret_cast<RulesSmem<K>*>(smem_raw)[threadIdx.x >> 5];
   const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
   for (int64_t w = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); w < m; w += warps) {
     const int64_t ti = perm ? perm[w] : w;
@@ -670,7 +678,7 @@ __global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, c
       // order: entries kept since then can skip cut ones of equal d2.
       const int nscan =
           rules_scan(sp, g, S, q, t, left, after_d, after_i, filter, openmask, dropped, lane, my, d2u);
-      const int n = dropped ? kRulesK : nscan;
+      const int n = dropped ? K : nscan;
       if (sp.balances)
         for (int i = lane; i < n; i += 32) {
           const uint32_t idx = S.ci[i];
@@ -757,17 +765,22 @@ cudaError_t launch_search(const Launch& L, const SearchDev& sp, const GridDev& g
                           uint32_t* nbr, int32_t* count, int8_t* status) {
   if (sp.rules) {
     constexpr int kWarps = 4;
-    const size_t smem = sizeof(RulesSmem) * kWarps;
-    cudaError_t e = cudaFuncSetAttribute(k_search_rules, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    const bool small = sp.sgs && sp.max_samples <= 64 && sp.max_per_hole < 0 && !sp.plane && sp.min_sectors < 0 &&
+                       sp.max_empty_sectors < 0 && sp.min_holes < 0;
+    const bool tiny = small && sp.max_samples <= 32;
+    const size_t smem =
+        (tiny ? sizeof(RulesSmem<kSgsK32>) : small ? sizeof(RulesSmem<kSgsK>) : sizeof(RulesSmem<kRulesK>)) * kWarps;
+    auto kern = tiny ? k_search_rules<kSgsK32> : small ? k_search_rules<kSgsK> : k_search_rules<kRulesK>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search_rules, kWarps * 32, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWarps * 32, smem);
     if (e != cudaSuccess) return e;
     int64_t blocks = int64_t(L.sm_count) * (per_sm > 0 ? per_sm : 1);
     const int64_t need = (m + kWarps - 1) / kWarps;
     if (blocks > need) blocks = need;
     if (blocks < 1) blocks = 1;
-    k_search_rules<<<int(blocks), kWarps * 32, smem, L.stream>>>(sp, g, tx, ty, tz, perm, m, loo, nbr, count, status);
+    kern<<<int(blocks), kWarps * 32, smem, L.stream>>>(sp, g, tx, ty, tz, perm, m, loo, nbr, count, status);
     ++*L.counter;
     return cudaGetLastError();
   }
