@@ -33,9 +33,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM bytes per system of k_tile<mixed>: (132,788,224 read + 13,551,104 written) / 800,000 systems in the
+# DRAM bytes per system of k_tile<mixed>: (132,862,720 read + 12,793,344 written) / 800,000 systems in the
 # ncu capture of profiles/k_tile_c2_800k_blocks.md.
-TILE_DRAM_BYTES_PER_SYSTEM = (132788224 + 13551104) / 800000
+TILE_DRAM_BYTES_PER_SYSTEM = (132862720 + 12793344) / 800000
 
 METRIC = "OK blocks/s @3.2M blocks n≤32: mixed vs FP64 GPU at ≤1e-6 rel; LOO-grad ms"
 UNIT = "blocks/s"
@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--grid", default=None, help="block counts NXxNYxNZ in place of 200x200x80 (profiling cases)")
     p.add_argument("--profile", action="store_true",
                    help="profiling case: warm-up and two steps of each form, no timing, no JSON line")
+    p.add_argument("--tile-union", type=int, default=None,
+                   help="profiling case: the tile table size (the autotuner's choice otherwise)")
     return p.parse_args()
 
 
@@ -345,12 +347,23 @@ def main():
     torch.cuda.set_stream(stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
+    tunings = {}
+
+    def use(prec):
+        """Each form runs at its own tuned launch configuration (set outside the timed region)."""
+        if tunings:
+            from boitata_b200.autotune import set_tuning
+
+            set_tuning(ctx, tunings[prec])
+
     def step(prec):
+        use(prec)
         rc = lib.btk_predict_geometry_device(h, ctypes.byref(gc), N.ORDINARY, 0.0, prec, ctypes.byref(oc),
                                              ctypes.c_void_p(stream.cuda_stream))
         ctx.check(rc, "predict")
 
     def capture(prec):
+        use(prec)
         ctx.check(lib.btk_graph_capture_geometry(h, ctypes.byref(gc), N.ORDINARY, 0.0, prec, ctypes.byref(oc)),
                   "capture")
 
@@ -363,12 +376,20 @@ def main():
 
             dist.barrier()
 
-    tuning = None
+    tuning = {}
+    if args.profile and args.tile_union is not None:
+        from boitata_b200.autotune import get_tuning
+
+        for prec in (N.FP64, N.MIXED):
+            tunings[prec] = dict(get_tuning(ctx), tile_union=args.tile_union)
     if not args.profile and not args.no_tune:
         from boitata_b200.autotune import autotune_geometry
 
-        tuned = autotune_geometry(est, geo, precision="mixed", steps=2)
-        tuning = {**tuned["best"], "tile": list(tuned["best"]["tile"]), "ms": tuned["ms"], "cached": tuned["cached"]}
+        for prec, name in ((N.FP64, "fp64"), (N.MIXED, "mixed")):
+            tuned = autotune_geometry(est, geo, precision=name, steps=2)
+            tunings[prec] = dict(tuned["best"])
+            tuning[name] = {**tuned["best"], "tile": list(tuned["best"]["tile"]), "ms": tuned["ms"],
+                            "cached": tuned["cached"]}
     for _ in range(args.warmup):
         step(N.MIXED)
         step(N.FP64)
@@ -483,6 +504,7 @@ def main():
         hv = torch.empty(m, dtype=torch.float64).pin_memory()
         hs = torch.empty(m, dtype=torch.float64).pin_memory()
         ho = N.OutputsC(hv.data_ptr(), hs.data_ptr(), None, None, None)
+        use(N.MIXED)
         e2e = []
         for i in range(args.warmup + args.steps):
             flush.zero_()
