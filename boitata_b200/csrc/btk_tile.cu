@@ -115,9 +115,16 @@ __device__ __forceinline__ float rcp_approx(float d) {
   return r;
 }
 
-// The tile's targets, union and covariance table; false when nothing is left
-// for the solve phase. Ends with the block synchronised.
-__device__ bool build_tile(const TileDev& a, int64_t tile, unsigned char* smem, const Layout& lay) {
+enum TileBuild { kTileEmpty = 0, kTileReady = 1, kTileOverflow = 2 };
+
+// The union and covariance table of the tile's targets lo .. hi-1. The first
+// pass (lo = 0, hi = kT) also reads the tile's targets and routes failed
+// searches and n > 32; if its union exceeds the table it returns
+// kTileOverflow and the caller retries the two halves, each with a union of
+// its own, before a half that still does not fit goes to the per-system
+// kernels. kTileEmpty: nothing left for the solve phase. Ends with the block
+// synchronised.
+__device__ int build_tile(const TileDev& a, int64_t tile, unsigned char* smem, const Layout& lay, int lo, int hi) {
   const SolveDev& s = a.s;
   TileHead& H = *reinterpret_cast<TileHead*>(smem + lay.head);
   uint32_t* ukey = reinterpret_cast<uint32_t*>(smem + lay.ukey);
@@ -129,8 +136,9 @@ __device__ bool build_tile(const TileDev& a, int64_t tile, unsigned char* smem, 
   uint8_t* uidx = reinterpret_cast<uint8_t*>(keys + kHash);
   const int tid = threadIdx.x;
   const int umax = a.umax, S = a.stride;
+  const bool first = lo == 0 && hi == kT;
 
-  if (tid < kT) {
+  if (first && tid < kT) {
     const int64_t w = tile * kT + tid;
     int64_t ti = w < a.nwork ? (a.perm ? a.perm[w] : w) : -1;
     int n = 0, kd = s.kind;
@@ -152,8 +160,8 @@ __device__ bool build_tile(const TileDev& a, int64_t tile, unsigned char* smem, 
     H.ti[tid] = ti;
     H.n[tid] = ti >= 0 ? n : 0;
     H.kind[tid] = kd;
-    H.twin[tid] = 0;
   }
+  if (tid < kT) H.twin[tid] = 0;
   if (tid == 0) H.nu = 0;
   for (int i = tid; i < kHash; i += kThreads) keys[i] = kEmpty;
   __syncthreads();
@@ -162,7 +170,7 @@ __device__ bool build_tile(const TileDev& a, int64_t tile, unsigned char* smem, 
   for (int e = tid; e < kT * 32; e += kThreads) {
     const int t = e >> 5, r = e & 31;
     const int64_t ti = H.ti[t];
-    if (ti < 0 || r >= H.n[t]) continue;
+    if (ti < 0 || r >= H.n[t] || t < lo || t >= hi) continue;
     const uint32_t key = s.nbr[ti * s.max_samples + r];
     if (s.twin && s.twin[key]) H.twin[t] = 1;
     uint32_t h = (key * 2654435761u) >> 22;  // multiplicative hash, 10 bits
@@ -190,28 +198,32 @@ __device__ bool build_tile(const TileDev& a, int64_t tile, unsigned char* smem, 
   }
   __syncthreads();
   const int nu = H.nu;
-  if (nu > umax) {  // the table would not hold this tile: per-system kernels
-    if (tid < kT && H.ti[tid] >= 0) a.small[atomicAdd(reinterpret_cast<unsigned long long*>(a.small_len), 1ull)] = H.ti[tid];
+  if (nu > umax) {  // the table would not hold these targets: halves, then per-system kernels
+    if (first) return kTileOverflow;  // uniform: every thread read the same H.nu
+    if (tid >= lo && tid < hi && H.ti[tid] >= 0)
+      a.small[atomicAdd(reinterpret_cast<unsigned long long*>(a.small_len), 1ull)] = H.ti[tid];
     __syncthreads();
-    return false;
+    return kTileEmpty;
   }
   for (int e = tid; e < kT * 32; e += kThreads) {
     const int t = e >> 5, r = e & 31;
-    H.map[t][r] = (H.ti[t] >= 0 && r < H.n[t]) ? uidx[H.slot[t][r]] : uint8_t(0);
+    // 0 outside lo .. hi: a map entry always indexes this pass's table
+    H.map[t][r] = (H.ti[t] >= 0 && r < H.n[t] && t >= lo && t < hi) ? uidx[H.slot[t][r]] : uint8_t(0);
   }
   if (tid < kT) {
     const int64_t ti = H.ti[tid];
-    const bool go = ti >= 0 && !H.twin[tid];
-    if (ti >= 0 && !go) a.small[atomicAdd(reinterpret_cast<unsigned long long*>(a.small_len), 1ull)] = ti;
+    const bool in = ti >= 0 && tid >= lo && tid < hi;
+    const bool go = in && !H.twin[tid];
+    if (in && !go) a.small[atomicAdd(reinterpret_cast<unsigned long long*>(a.small_len), 1ull)] = ti;
     H.go[tid] = go;
   }
   if (tid == 0) {
     int any = 0;
-    for (int t = 0; t < kT; ++t) any |= H.ti[t] >= 0 && !H.twin[t];
+    for (int t = lo; t < hi; ++t) any |= H.ti[t] >= 0 && !H.twin[t];
     H.any = any;
   }
   __syncthreads();
-  if (!H.any) return false;  // uniform: every thread read the same H.any
+  if (!H.any) return kTileEmpty;  // uniform: every thread read the same H.any
 
   // 2. Union coordinates (world) and the covariance table.
   for (int u = tid; u < nu; u += kThreads) {
@@ -231,7 +243,7 @@ __device__ bool build_tile(const TileDev& a, int64_t tile, unsigned char* smem, 
   }
   for (int u = tid; u < nu; u += kThreads) UU[u * S + u] = s.vg.c0 + E[u];
   __syncthreads();
-  return true;
+  return kTileReady;
 }
 
 // C(target, union sample u).
@@ -497,9 +509,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(TileDev a) {
   const double* UU = reinterpret_cast<const double*>(smem + lay.table);
   const int warp = threadIdx.x >> 5;
   const int64_t ntiles = (a.nwork + kT - 1) / kT;
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    __syncthreads();  // the previous tile's systems are done with the table
-    if (!build_tile(a, tile, smem, lay)) continue;
+  // Systems whose go flag is set; a half tile (an even number of targets)
+  // leaves the other half's flags clear, so the mixed form's pairs stay whole.
+  auto solve_all = [&]() {
     if (MIXED) {
       WarpMixed& W = reinterpret_cast<WarpMixed*>(smem + lay.warp)[warp];
       for (int p = warp; p < kT / 2; p += kThreads / 32)
@@ -508,6 +520,18 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(TileDev a) {
       WarpFp64& W = reinterpret_cast<WarpFp64*>(smem + lay.warp)[warp];
       for (int t = warp; t < kT; t += kThreads / 32)
         if (H.go[t]) solve_fp64(a, H, P, Z, UU, a.umax, a.stride, W, t);
+    }
+  };
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    __syncthreads();  // the previous tile's systems are done with the table
+    const int built = build_tile(a, tile, smem, lay, 0, kT);
+    if (built == kTileReady) {
+      solve_all();
+    } else if (built == kTileOverflow) {
+      for (int h = 0; h < 2; ++h) {
+        __syncthreads();  // the previous half is done with the table and the head
+        if (build_tile(a, tile, smem, lay, h * (kT / 2), (h + 1) * (kT / 2)) == kTileReady) solve_all();
+      }
     }
   }
 }

@@ -40,8 +40,9 @@ def test_results_do_not_depend_on_the_tuning():
     base = predict(est, geo, N.FP64, outs, oc)
     cfg = get_tuning(est._ctx)
     assert cfg["tile_union"] > 0  # the tile-shared solve is the default
+    # Tables of 32 and 40 samples: tiles overflow and are retried as halves, some of which overflow too.
     for ppc, tile, sw, sb, tu in [(1.0, (8, 4, 1), 2, 2, 0), (4.0, (2, 2, 8), 8, 3, 64), (2.0, (4, 4, 2), 0, 0, 96),
-                                  (2.0, (4, 4, 2), 0, 0, 32)]:
+                                  (2.0, (4, 4, 2), 0, 0, 32), (2.0, (4, 4, 2), 0, 0, 40)]:
         set_tuning(est._ctx, dict(cfg, samples_per_cell=ppc, tile=tile, search_warps=sw, solve_blocks_per_sm=sb,
                                   tile_union=tu))
         got = predict(est, geo, N.FP64, outs, oc)
@@ -61,12 +62,18 @@ def test_tile_and_per_system_mixed_forms_agree():
     exact = predict(est, geo, N.FP64, outs, oc)
     set_tuning(est._ctx, dict(cfg, tile_union=0))
     per_system = predict(est, geo, N.MIXED, outs, oc)
+    # A 40-sample table: most tiles overflow it and are retried as two halves of 8 targets, and halves
+    # that still do not fit go to the per-system kernel.
+    set_tuning(est._ctx, dict(cfg, tile_union=40))
+    halves = predict(est, geo, N.MIXED, outs, oc)
     for k in (0, 1):
         scale = 1.0 + np.maximum(np.abs(exact[k]), np.abs(tiled[k]))
         assert np.nanmax(np.abs(tiled[k] - exact[k]) / scale) < 1e-9
         assert np.nanmax(np.abs(tiled[k] - per_system[k]) / scale) < 1e-9
-    np.testing.assert_array_equal(tiled[3], per_system[3])
-    np.testing.assert_array_equal(tiled[4] & 0x0F, per_system[4] & 0x0F)
+        assert np.nanmax(np.abs(halves[k] - exact[k]) / scale) < 1e-9
+    for got in (per_system, halves):
+        np.testing.assert_array_equal(tiled[3], got[3])
+        np.testing.assert_array_equal(tiled[4] & 0x0F, got[4] & 0x0F)
 
 
 def test_graph_replay_matches_the_call_and_autotune_keeps_results():
