@@ -1,10 +1,10 @@
-"""Seeded synthetic workloads with the shapes of the five kriging configurations.
+"""Five seeded synthetic kriging workloads, c1 to c5 (described below).
 
 No public dataset is named for this path, so every input is generated here
 with the reference tests' 64-bit LCG (crates/estimation/src/kernel.rs:132-137:
 state = state * 6364136223846793005 + 1442695040888963407, u = (state >> 11)
 / 2^53, one step before each draw) and its Box-Muller normals
-(batch.rs:639-642). Draws are taken in the order documented per config, so
+(batch.rs:639-642). Draws are taken in the order documented per workload, so
 another implementation can regenerate the same inputs.
 
   c1  2,000 samples uniform in 1000 x 1000 x 200 m, lognormal values
@@ -125,7 +125,7 @@ def c3(seed=3):
     return Workload("c3", xyz, values, vg, search, geo, kind="mixed-sk", mean=1.0)
 
 
-CONFIGS = {"c1": c1, "c2": c2, "c3": c3}
+WORKLOADS = {"c1": c1, "c2": c2, "c3": c3}
 
 
 def gaussian_field(xyz, normals, rng=150.0, device=None):
@@ -161,7 +161,7 @@ def c4(n=20000, seed=4, device=None):
     return Workload("c4", xyz, values, vg, search, None)
 
 
-CONFIGS["c4"] = c4
+WORKLOADS["c4"] = c4
 
 
 def c5(holes=1600, seed=5):
@@ -188,4 +188,4 @@ def c5(holes=1600, seed=5):
     return Workload("c5", xyz, values, vg, search, geo)
 
 
-CONFIGS["c5"] = c5
+WORKLOADS["c5"] = c5
