@@ -56,8 +56,6 @@ def parse():
     p.add_argument("--grid", default=None, help="block counts NXxNYxNZ in place of 200x200x80 (profiling cases)")
     p.add_argument("--profile", action="store_true",
                    help="profiling case: warm-up and two steps of each form, no timing, no JSON line")
-    p.add_argument("--tile-union", type=int, default=None,
-                   help="profiling case: the tile table size (the autotuner's choice otherwise)")
     p.add_argument("--tuning", default=None,
                    help="launch configuration per form as JSON, the bench line's config.tuning "
                         "({\"fp64\": {...}, \"mixed\": {...}}); skips the autotuner")
@@ -387,11 +385,6 @@ def main():
         for prec, name in ((N.FP64, "fp64"), (N.MIXED, "mixed")):
             tunings[prec] = {**get_tuning(ctx), **{k: v for k, v in given[name].items() if k not in ("ms", "cached")}}
             tuning[name] = {**tunings[prec], "tile": list(tunings[prec]["tile"]), "given": True}
-    elif args.profile and args.tile_union is not None:
-        from boitata_b200.autotune import get_tuning
-
-        for prec in (N.FP64, N.MIXED):
-            tunings[prec] = dict(get_tuning(ctx), tile_union=args.tile_union)
     if not args.profile and not args.no_tune and not args.tuning:
         from boitata_b200.autotune import autotune_geometry
 
