@@ -120,3 +120,34 @@ def test_caller_order_does_not_change_results():
     inv[perm] = np.arange(len(perm))
     for k in a:
         np.testing.assert_array_equal(np.asarray(b[k])[inv], np.asarray(a[k]))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_host_chunks_give_the_unchunked_results(precision):
+    """A host call in chunks of tuning.host_chunk targets (the copies of chunks c - 1 out and c + 1 in overlap
+    chunk c's kernels; each chunk is ordered and solved on its own) gives the one-chunk results: FP64 bit for
+    bit, with the diagnostics; the mixed form far inside its 1e-6 tolerance."""
+    w = W.c2()
+    t = np.random.default_rng(8).uniform(0.0, 1.0, (150_000, 3)) * [500.0, 500.0, 250.0]
+    kinds = np.where(np.arange(len(t)) % 7 == 0, "simple", "ordinary")
+    est = OrdinaryKriging(w.variogram, w.search, precision=precision).fit(w.coords, w.values)
+    whole = est.predict_full(t, diagnostics=True)
+    whole_kinds = est.predict_kinds(t, kinds, mean=1.0)
+    set_tuning(est._ctx, dict(get_tuning(est._ctx), host_chunk=40_000))  # four chunks
+    parts = est.predict_full(t, diagnostics=True)
+    parts_kinds = est.predict_kinds(t, kinds, mean=1.0)
+    if precision == "fp64":
+        for k in ("value", "variance", "lagrange", "n_used", "status"):
+            np.testing.assert_array_equal(parts_kinds[k], whole_kinds[k])
+    for k in ("n_used", "n_holes", "negative_weight_sum", "mean_distance"):
+        np.testing.assert_array_equal(parts[k], whole[k])
+    np.testing.assert_array_equal(parts["status"] & 0x0F, whole["status"] & 0x0F)
+    assert np.isfinite(whole["value"]).mean() > 0.5
+    for k in ("value", "variance", "lagrange"):
+        if precision == "fp64":
+            np.testing.assert_array_equal(parts[k], whole[k])
+        else:
+            fin = np.isfinite(whole[k])
+            np.testing.assert_array_equal(fin, np.isfinite(parts[k]))
+            scale = 1.0 + np.maximum(np.abs(whole[k][fin]), np.abs(parts[k][fin]))
+            assert np.max(np.abs(parts[k][fin] - whole[k][fin]) / scale) < 1e-9, k
