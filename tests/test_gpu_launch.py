@@ -151,3 +151,34 @@ def test_host_chunks_give_the_unchunked_results(precision):
             np.testing.assert_array_equal(fin, np.isfinite(parts[k]))
             scale = 1.0 + np.maximum(np.abs(whole[k][fin]), np.abs(parts[k][fin]))
             assert np.max(np.abs(parts[k][fin] - whole[k][fin]) / scale) < 1e-9, k
+
+
+def test_device_calls_match_the_host_calls():
+    """btk_predict_device and btk_predict_kinds_device (device x, y, z arrays and outputs, queued on a torch
+    stream) give the host calls' results bit for bit: the same targets take the same order and tiles."""
+    import torch
+
+    w = W.c2()
+    t = np.random.default_rng(10).uniform(0.0, 1.0, (60_000, 3)) * [500.0, 500.0, 250.0]
+    kinds = np.where(np.arange(len(t)) % 5 == 0, N.SIMPLE, N.ORDINARY).astype(np.int8)
+    keys = ("value", "variance", "lagrange", "n_used", "status")
+    dxyz = torch.from_numpy(np.ascontiguousarray(t.T)).cuda()
+    dkinds = torch.from_numpy(kinds).cuda()
+    stream = torch.cuda.Stream()
+    for precision, code in (("fp64", N.FP64), ("mixed", N.MIXED)):
+        est = OrdinaryKriging(w.variogram, w.search, precision=precision).fit(w.coords, w.values)
+        ctx = est._ctx
+        host, host_kinds = est.predict_full(t), est.predict_kinds(t, kinds, mean=1.0)
+        assert np.isfinite(host["value"]).mean() > 0.5
+        outs, oc = device_outputs(len(t))
+        ctx.check(ctx._lib.btk_predict_device(ctx.handle, len(t), ctypes.c_void_p(dxyz.data_ptr()), N.ORDINARY, 0.0,
+                                              code, ctypes.byref(oc), ctypes.c_void_p(stream.cuda_stream)), "device")
+        stream.synchronize()
+        for got, k in zip(outs, keys):
+            np.testing.assert_array_equal(got.cpu().numpy(), host[k])
+        ctx.check(ctx._lib.btk_predict_kinds_device(ctx.handle, len(t), ctypes.c_void_p(dxyz.data_ptr()),
+                                                    ctypes.c_void_p(dkinds.data_ptr()), 1.0, code, ctypes.byref(oc),
+                                                    ctypes.c_void_p(stream.cuda_stream)), "kinds")
+        stream.synchronize()
+        for got, k in zip(outs, keys):
+            np.testing.assert_array_equal(got.cpu().numpy(), host_kinds[k])
