@@ -278,7 +278,8 @@ def callers(dev):
     rng = np.random.default_rng(1)
     order, z = rng.permutation(len(nodes)), rng.standard_normal(len(nodes))
     vg = unit_sill(w2.variogram)
-    sgs_scores(w2.coords, scores, None, nodes[order][:4096], z[:4096], w2.search, vg, context=ctx)
+    # Warm at full size: the first run grows the context's buffers to 400k nodes (device allocations).
+    sgs_scores(w2.coords, scores, None, nodes[order], z, w2.search, vg, context=ctx)
     t0 = time.perf_counter()
     _, how, rounds = sgs_scores(w2.coords, scores, None, nodes[order], z, w2.search, vg, context=ctx)
     dt = time.perf_counter() - t0

@@ -47,7 +47,7 @@ def set_tuning(ctx, cfg):
         t.tile[a] = int(cfg["tile"][a])
     t.search_warps = int(cfg["search_warps"])
     t.solve_blocks_per_sm = int(cfg["solve_blocks_per_sm"])
-    t.tile_union = int(cfg.get("tile_union", 72))
+    t.tile_union = int(cfg.get("tile_union", 64))
     t.host_chunk = int(cfg.get("host_chunk", 0))
     ctx.check(ctx._lib.btk_set_tuning(ctx.handle, ctypes.byref(t)), "tuning")
 

@@ -157,7 +157,8 @@ struct Tuning {
   int tile[3] = {4, 4, 2};       // block-model tile of one search warp (product 32)
   int search_warps = 0;          // warps per search CTA; 0: 4 (2 with 64 list slots)
   int solve_blocks_per_sm = 0;   // resident solve CTAs per SM; 0: as many as fit
-  int tile_union = 72;           // tile-shared solve: most distinct samples per tile; 0: per-system solve
+  int tile_union = 64;           // tile-shared solve: most distinct samples per tile; 0: per-system solve
+                                 // (64 lets four mixed-form CTAs share an SM; a tile above it is split)
   int host_chunk = 0;            // host-buffer calls: targets per pipelined chunk; 0: one chunk
 };
 

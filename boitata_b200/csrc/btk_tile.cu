@@ -199,7 +199,9 @@ __device__ int build_tile(const TileDev& a, int64_t tile, unsigned char* smem, c
   __syncthreads();
   const int nu = H.nu;
   if (nu > umax) {  // the table would not hold these targets: halves, then per-system kernels
-    if (first) return kTileOverflow;  // uniform: every thread read the same H.nu
+    // Halves only when both could fit: above 2 umax one of them holds more
+    // than umax samples (scattered targets, a simulation's path order).
+    if (first && nu <= 2 * umax) return kTileOverflow;  // uniform: every thread read the same H.nu
     if (tid >= lo && tid < hi && H.ti[tid] >= 0)
       a.small[atomicAdd(reinterpret_cast<unsigned long long*>(a.small_len), 1ull)] = H.ti[tid];
     __syncthreads();
