@@ -190,6 +190,7 @@ struct btk_ctx {
   DevBuf<int64_t> ord_vals;
   DevBuf<uint8_t> ord_temp;
   DevBuf<double> ord_part, ord_b6;
+  DevBuf<unsigned long long> ord_lat;  // lattice steps of caller targets and their off flag
 
   // hole codes of the fitted samples (btk_fit), for the search's hole rules
   DevBuf<uint32_t> hole;
@@ -465,6 +466,7 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
     CK(ctx->ord_temp.grow(tb));
     CK(ctx->ord_part.grow(6 * 1024));
     CK(ctx->ord_b6.grow(6));
+    CK(ctx->ord_lat.grow(4));
     // World axes weighted by the search metric's stretch along each (column
     // norms of the search frame): key cells stay aligned with a block lattice
     // but are as long, in search distance, along every axis.
@@ -472,8 +474,8 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
     for (int d = 0; d < 3; ++d)
       wgt[d] = std::sqrt(ctx->spd.frame[d] * ctx->spd.frame[d] + ctx->spd.frame[3 + d] * ctx->spd.frame[3 + d] +
                          ctx->spd.frame[6 + d] * ctx->spd.frame[6 + d]);
-    CK(launch_morton_order(L, m, tx, ty, tz, wgt, ctx->ord_part.p, ctx->ord_b6.p, ctx->ord_keys.p, ctx->ord_vals.p,
-                           ctx->ord_temp.p, tb, &perm));
+    CK(launch_morton_order(L, m, tx, ty, tz, wgt, ctx->ord_part.p, ctx->ord_b6.p, ctx->ord_lat.p, ctx->ord_keys.p,
+                           ctx->ord_vals.p, ctx->ord_temp.p, tb, &perm));
     nwork = m;
   }
   ctx->mark(0, L.stream);

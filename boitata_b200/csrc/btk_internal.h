@@ -215,9 +215,12 @@ cudaError_t launch_tile(const Launch& L, const TileDev& a, bool mixed);
 // hold 2m entries each; temp holds morton_temp_bytes(m). *perm points into
 // vals on return.
 size_t morton_temp_bytes(int64_t m);
+// lat: 4 scratch words (the lattice steps and its off flag): targets on an
+// axis-aligned lattice take the block-model path's order, tiles of
+// L.tuning.tile in Hilbert order.
 cudaError_t launch_morton_order(const Launch& L, int64_t m, const double* x, const double* y, const double* z,
-                                const double w[3], double* partial, double* b6, uint64_t* keys, int64_t* vals,
-                                void* temp, size_t temp_bytes, const int64_t** perm);
+                                const double w[3], double* partial, double* b6, unsigned long long* lat,
+                                uint64_t* keys, int64_t* vals, void* temp, size_t temp_bytes, const int64_t** perm);
 
 // C(B,B) of a block discretized by nd offsets (x, y, z triples) into *cbb:
 // the mean over pairs of point covariances with the nugget left out at zero

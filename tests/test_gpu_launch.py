@@ -182,3 +182,21 @@ def test_device_calls_match_the_host_calls():
         stream.synchronize()
         for got, k in zip(outs, keys):
             np.testing.assert_array_equal(got.cpu().numpy(), host_kinds[k])
+
+
+def test_lattice_targets_in_any_order_match_the_block_model():
+    """Block centroids passed as coordinates, in the model's order and shuffled, are found to be a lattice and
+    take the block-model path's tile order; either way the FP64 results are the block-model call's, bit for
+    bit."""
+    from boitata_b200 import BlockModel
+
+    w = W.c2()
+    geo = Geometry((0.0, 0.0, 0.0), (2.5, 2.5, 3.125), (60, 60, 30))
+    est = OrdinaryKriging(w.variogram, w.search).fit(w.coords, w.values)
+    want = est.predict_full(geo)
+    cent = BlockModel(geo).centroids(est._ctx)
+    perm = np.random.default_rng(3).permutation(len(cent))
+    for t, back in ((cent, np.arange(len(cent))), (cent[perm], np.argsort(perm))):
+        got = est.predict_full(t)
+        for k in ("value", "variance", "lagrange", "n_used", "status"):
+            np.testing.assert_array_equal(got[k][back], want[k])
