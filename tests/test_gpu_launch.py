@@ -200,3 +200,46 @@ def test_lattice_targets_in_any_order_match_the_block_model():
         got = est.predict_full(t)
         for k in ("value", "variance", "lagrange", "n_used", "status"):
             np.testing.assert_array_equal(got[k][back], want[k])
+
+
+def test_target_order_never_changes_results():
+    """The order the engine gives caller targets (the lattice tile order, or Hilbert when they are not a
+    lattice) is invisible: FP64 results are the same bits for every permutation of the targets. Cases: a
+    flat lattice (one z), a lattice with blocks missing, a lattice too long for the tile keys (Hilbert) and a
+    rotated lattice (Hilbert). A NaN target, which only the C ABI takes, turns the lattice order off and
+    gets NaN; the other targets keep their results."""
+    w = W.c2()
+    est = OrdinaryKriging(w.variogram, w.search).fit(w.coords, w.values)
+    rng = np.random.default_rng(21)
+    g = np.stack(np.meshgrid(np.arange(40), np.arange(30), np.arange(6), indexing="ij"), -1).reshape(-1, 3)
+    lattice = g * [5.0, 5.0, 6.25] + [100.0, 120.0, 10.0]
+    a = np.deg2rad(30.0)
+    rot = np.array([[np.cos(a), -np.sin(a), 0.0], [np.sin(a), np.cos(a), 0.0], [0.0, 0.0, 1.0]])
+    g2 = np.stack(np.meshgrid(np.arange(60), np.arange(50), indexing="ij"), -1).reshape(-1, 2)
+    flat = np.column_stack([g2 * 5.0 + [100.0, 120.0], np.full(len(g2), 10.0)])  # 3,000: ordered (2,048 up)
+    holed = lattice[rng.random(len(lattice)) > 0.3]
+    long = np.vstack([lattice, [[100.0 + 5.0 * 600_000, 120.0, 10.0]]])
+    rotated = (lattice - 250.0) @ rot.T + 250.0
+    keys = ("value", "variance", "lagrange", "n_used", "status")
+    for t in (flat, holed, long, rotated):
+        want = est.predict_full(t)
+        perm = rng.permutation(len(t))
+        got = est.predict_full(t[perm])
+        back = np.argsort(perm)
+        for k in keys:
+            np.testing.assert_array_equal(got[k][back], want[k])
+        assert np.isfinite(want["value"]).sum() >= len(t) - 1
+    want = est.predict_full(lattice)
+    nan = np.ascontiguousarray(lattice.copy())
+    nan[17, 1] = np.nan
+    out = {k: np.full(len(nan), np.nan) for k in ("value", "variance", "lagrange")}
+    out["n_used"] = np.zeros(len(nan), dtype=np.int32)
+    out["status"] = np.zeros(len(nan), dtype=np.int8)
+    oc = N.OutputsC(*(out[k].ctypes.data for k in keys))
+    ctx = est._ctx
+    ctx.check(ctx._lib.btk_predict(ctx.handle, len(nan), nan.ctypes.data, N.ORDINARY, 0.0, N.FP64,
+                                   ctypes.byref(oc)), "predict")
+    assert np.isnan(out["value"][17])
+    keep = np.arange(len(nan)) != 17
+    for k in keys:
+        np.testing.assert_array_equal(out[k][keep], want[k][keep])
