@@ -56,6 +56,7 @@ struct TileHead {
   int go[kT];
   int nu;
   int any;
+  int wsum[kThreads / 32];
   uint8_t map[kT][32];
   uint16_t slot[kT][32];
 };
@@ -102,7 +103,7 @@ __host__ __device__ inline Layout layout(int umax, int stride, bool mixed) {
   l.e = l.z + sizeof(double) * umax;
   l.table = align16(l.e + sizeof(double) * umax);
   size_t tb = sizeof(double) * size_t(umax) * stride;
-  const size_t hash = sizeof(uint32_t) * kHash + sizeof(uint8_t) * kHash;
+  const size_t hash = sizeof(uint32_t) * 2 * kHash + sizeof(uint8_t) * kHash;  // keys, first entries, uidx
   if (tb < hash) tb = hash;
   l.warp = align16(l.table + tb);
   l.total = l.warp + (kThreads / 32) * (mixed ? sizeof(WarpMixed) : sizeof(WarpFp64));
@@ -133,7 +134,8 @@ __device__ int build_tile(const TileDev& a, int64_t tile, unsigned char* smem, c
   double* E = reinterpret_cast<double*>(smem + lay.e);
   double* UU = reinterpret_cast<double*>(smem + lay.table);
   uint32_t* keys = reinterpret_cast<uint32_t*>(smem + lay.table);  // phase 1 only
-  uint8_t* uidx = reinterpret_cast<uint8_t*>(keys + kHash);
+  uint32_t* lowest = keys + kHash;  // per slot: the lowest entry t * 32 + r holding its key
+  uint8_t* uidx = reinterpret_cast<uint8_t*>(lowest + kHash);
   const int tid = threadIdx.x;
   const int umax = a.umax, S = a.stride;
   const bool first = lo == 0 && hi == kT;
@@ -163,7 +165,7 @@ __device__ int build_tile(const TileDev& a, int64_t tile, unsigned char* smem, c
   }
   if (tid < kT) H.twin[tid] = 0;
   if (tid == 0) H.nu = 0;
-  for (int i = tid; i < kHash; i += kThreads) keys[i] = kEmpty;
+  for (int i = tid; i < kHash; i += kThreads) keys[i] = kEmpty, lowest[i] = kEmpty;
   __syncthreads();
 
   // 1. Union of the neighbour lists.
@@ -180,20 +182,43 @@ __device__ int build_tile(const TileDev& a, int64_t tile, unsigned char* smem, c
       h = (h + 1) & (kHash - 1);
     }
     H.slot[t][r] = uint16_t(h);
+    atomicMin(&lowest[h], uint32_t(e));
   }
   __syncthreads();
-  for (int i = tid; i < kHash; i += kThreads) {  // one atomic per warp and round
-    const uint32_t k = keys[i];
-    const bool occ = k != kEmpty;
-    const unsigned bal = __ballot_sync(kFull, occ);
-    const int lane = tid & 31;
-    int base = 0;
-    if (lane == 0 && bal) base = atomicAdd(&H.nu, __popc(bal));
-    base = __shfl_sync(kFull, base, 0);
-    if (occ) {
-      const int u = base + __popc(bal & ((1u << lane) - 1u));
-      uidx[i] = uint8_t(u < 255 ? u : 255);
-      if (u < umax) ukey[u] = k;
+  // Union indices in order of first appearance, target by target and each
+  // target's list in (d2, index) order: a system's rows then take nearby
+  // indices, which spread its row gathers over the shared-memory banks (the
+  // table's values do not depend on the indices). Thread tid takes entries
+  // 4 tid .. 4 tid + 3; a block scan of their first-appearance counts gives
+  // each new sample its index.
+  {
+    uint32_t fl = 0;  // bit j: entry 4 tid + j is its key's first
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int e = 4 * tid + j, t = e >> 5, r = e & 31;
+      if (H.ti[t] >= 0 && r < H.n[t] && t >= lo && t < hi && lowest[H.slot[t][r]] == uint32_t(e)) fl |= 1u << j;
+    }
+    const int cnt = __popc(fl);
+    const int lane = tid & 31, warp = tid >> 5;
+    int inc = cnt;  // inclusive warp scan
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(kFull, inc, o);
+      if (lane >= o) inc += v;
+    }
+    if (lane == 31) H.wsum[warp] = inc;
+    __syncthreads();
+    int base = inc - cnt;
+    for (int w = 0; w < warp; ++w) base += H.wsum[w];
+    if (tid == kThreads - 1) H.nu = base + cnt;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (!((fl >> j) & 1u)) continue;
+      const int e = 4 * tid + j, t = e >> 5, r = e & 31;
+      const int h = H.slot[t][r];
+      uidx[h] = uint8_t(base < 255 ? base : 255);
+      if (base < umax) ukey[base] = keys[h];
+      ++base;
     }
   }
   __syncthreads();
