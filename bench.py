@@ -33,9 +33,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM bytes per system of k_tile<mixed>: (132,831,744 read + 14,383,872 written) / 800,000 systems in the
+# DRAM bytes per system of k_tile<mixed>: (132,827,648 read + 16,656,896 written) / 800,000 systems in the
 # ncu capture of profiles/k_tile_c2_800k_blocks.md.
-TILE_DRAM_BYTES_PER_SYSTEM = (132831744 + 14383872) / 800000
+TILE_DRAM_BYTES_PER_SYSTEM = (132827648 + 16656896) / 800000
 
 METRIC = "OK blocks/s @3.2M blocks n≤32: mixed vs FP64 GPU at ≤1e-6 rel; LOO-grad ms"
 UNIT = "blocks/s"
