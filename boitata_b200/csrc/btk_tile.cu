@@ -466,7 +466,9 @@ __device__ void solve_mixed(const TileDev& a, const TileHead& H, const double* P
       z[v].y = __shfl_sync(kFull, w.y, k);
     }
     if (lane == k) x[0] = z[0], x[1] = z[1], x[2] = z[2];
-    const float2 l = my_col[k];
+    // Rows below k take no more terms: their lanes skip the load, which
+    // would only add bank conflicts (the columns' starts fall on few banks).
+    const float2 l = lane < k ? my_col[k] : make_float2(0.f, 0.f);
 #pragma unroll
     for (int v = 0; v < 3; ++v) acc[v] = __ffma2_rn(l, z[v], acc[v]);
   }
