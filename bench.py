@@ -37,6 +37,16 @@ sys.path.insert(0, ROOT)
 # ncu capture of profiles/k_tile_c2_800k_blocks.md.
 TILE_DRAM_BYTES_PER_SYSTEM = (132827648 + 16656896) / 800000
 
+def hbm_peak():
+    """Measured HBM copy bandwidth of this pool's B200s (GB/s) and where it came from."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, a STREAM-style copy)"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback (an earlier copy measurement on this pool)"
+
+
 METRIC = "OK blocks/s @3.2M blocks n≤32: mixed vs FP64 GPU at ≤1e-6 rel; LOO-grad ms"
 UNIT = "blocks/s"
 
@@ -496,7 +506,13 @@ def main():
                                        "the systems per launch (the per-target streams grow in proportion)",
                      "peak_source": "measured in this run: CUDA-core FP64 FMA loop (btk_peak_flops)",
                      "fp32_peak": peak32 / 1e12,
-                     "algorithmic_flops_per_step": flops},
+                     "algorithmic_flops_per_step": flops,
+                     # The same launches against HBM: the tile solve reads the neighbour table and targets
+                     # and writes the outputs; its tables live in shared memory, so HBM is far from bound.
+                     "hbm_view": {"achieved_gbs": TILE_DRAM_BYTES_PER_SYSTEM * m / (solve_ms * 1e-3) / 1e9,
+                                  "peak_gbs": hbm_peak()[0],
+                                  "frac": TILE_DRAM_BYTES_PER_SYSTEM * m / (solve_ms * 1e-3) / 1e9 / hbm_peak()[0],
+                                  "peak_source": hbm_peak()[1]}},
         "gpu_launches": int(launches[N.MIXED]),
         "clocks": clocks,
     }
