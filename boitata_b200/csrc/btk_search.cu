@@ -104,13 +104,6 @@ struct Need {
   }
 };
 
-template <int SLOTS, bool OCT>
-__device__ __forceinline__ double max_root(const WarpSmem<SLOTS, OCT>& S, int lane, int nsec, int cap) {
-  double m = S.hd[0][lane];
-  for (int s = 1; s < nsec; ++s) m = fmax(m, S.hd[s * cap][lane]);
-  return m;
-}
-
 __device__ __forceinline__ void set_root(Need& nd, int sec, double v) {
 #pragma unroll
   for (int s = 0; s < 8; ++s)
@@ -185,7 +178,12 @@ __device__ __forceinline__ void consider(WarpSmem<SLOTS, OCT>& S, int lane, int 
   if (c + 1 >= cap) {  // full (now or before): the root bounds what the sector still takes
     nd.open &= ~(1u << sec);
     set_root(nd, sec, root);
-    if (nd.open == 0) thr = max_root(S, lane, nsec, cap);
+    if (nd.open == 0) {  // every sector full: the largest root, from the register copies
+      double m = nd.root[0];
+#pragma unroll
+      for (int s = 1; s < 8; ++s) m = fmax(m, nd.root[s]);
+      thr = m;
+    }
   }
 }
 
