@@ -314,16 +314,18 @@ __global__ void __launch_bounds__(256, SLOTS > 32 ? 1 : 2) k_search(SearchDev sp
               }
               __syncwarp();
               if (need) {
-                // The next candidate's coordinates load while this one is
-                // offered (the heaps' stores never touch the staged arrays).
+                // The next candidate's coordinates and index load while this
+                // one is offered (the heaps' stores never touch the staged
+                // arrays).
                 double nx = S.cp[0][0], ny = S.cp[1][0], nz = S.cp[2][0];
+                uint32_t ni = S.ci[0];
 #pragma unroll 1
                 for (int c = 0; c < nc; ++c) {
                   const double cx = nx, cy = ny, cz = nz;
-                  if (c + 1 < nc) nx = S.cp[0][c + 1], ny = S.cp[1][c + 1], nz = S.cp[2][c + 1];
+                  const uint32_t idx = ni;
+                  if (c + 1 < nc) nx = S.cp[0][c + 1], ny = S.cp[1][c + 1], nz = S.cp[2][c + 1], ni = S.ci[c + 1];
                   const double d2 = d2_exact(cx, cy, cz, q[0], q[1], q[2]);
                   if (d2 <= thr) {
-                    const uint32_t idx = S.ci[c];
                     if (idx == left) continue;
                     int sec = 0;
                     if (OCT) {
