@@ -13,30 +13,34 @@
 //
 // Per tile (one CTA of 128 threads):
 //   1. the union of the tile's neighbour lists through a shared-memory hash
-//      (open addressing, 1024 slots for at most 16 x 32 keys);
+//      (open addressing, 1024 slots for at most 16 x 32 keys), its samples
+//      numbered in order of first appearance (target by target, each list
+//      nearest first), so that a system's rows sit at nearby indices and
+//      their gathers spread over the shared-memory banks;
 //   2. the union's world coordinates and the table C[u][v] (FP64, full
 //      square, diagonal C0 + the sample's error variance), every lag from
 //      lag_world, so an entry is bit for bit the one the per-system kernels
 //      assemble and results do not depend on the tiling;
 //   3. the systems: FP64 form one per warp, lane = row, the right-looking
-//      LDL^T of btk_solve.cu; mixed form two per warp (a half-warp each, lane l
-//      holding rows l and l + 16 in FP32 registers), LDL^T with packed FP32
-//      FMA (fma.rn.f32x2), a register-only backward sweep for x = C^-1 v, FP64
+//      LDL^T of btk_solve.cu with the row kept shifted (slot 0 = the pivot
+//      column) and windows of 32, 24, 16 and 8 slots; mixed form two per
+//      warp, lane = row of both as a float2 (system a in .x, b in .y), the
+//      same elimination with packed FP32 FMA (__ffma2_rn) writing each pivot
+//      column to a packed per-warp triangle in shared memory, a
+//      column-oriented backward sweep over that triangle for x = C^-1 v, FP64
 //      residuals r = v - C x from the FP64 table and the corrected forms
 //      u'x_v + x_u'r_v, as in btk_solve.cu's mixed kernel.
-// Each row keeps the full symmetric row (not only its lower part). After the
-// elimination, lane i's slots q > i then hold D_i L[q][i], the i-th column of
-// L, which is what the backward sweep needs, so no transpose goes through
-// shared memory.
 //
 // Systems the tile does not take: a failed search (outputs written here),
-// n > 32 (appended to `large`), a sample flagged coincident at fit time or a
-// tile whose union exceeds the table (appended to `small`), and, in the mixed
-// form, systems whose FP32 pivots or residuals fail the refinement tests
-// (appended to `redo`). The per-system kernels of btk_solve.cu take those.
-// The table entries do not depend on the order in which samples enter the
-// union or on the tile (each is a function of its sample pair alone), so the
-// FP64 form gives bit for bit the per-system kernel's results.
+// n > 32 (appended to `large`) and a sample flagged coincident at fit time
+// (appended to `small`). A tile whose union exceeds the table, but not twice
+// the table, is retried as two halves of 8 targets, each with a union of its
+// own; what still does not fit goes to `small`. In the mixed form, systems
+// whose FP32 pivots or residuals fail the refinement tests go to `redo`. The
+// per-system kernels of btk_solve.cu take those. The table entries do not
+// depend on the order in which samples enter the union or on the tile (each
+// is a function of its sample pair alone), so the FP64 form gives bit for bit
+// the per-system kernel's results.
 #include "btk_device.cuh"
 
 namespace btk {
