@@ -6,7 +6,12 @@ most) in a rotated ellipsoid, nested spherical + exponential variogram. One
 step = the whole kriging path over the block model (centroids, neighbour
 search, assembly, solve, estimate and variance) with the samples resident
 on the device. `value` is the mixed FP32/FP64 form; the FP64 form is
-timed beside it, with the error of mixed against FP64 over every block.
+timed beside it, with the error of mixed against FP64 over every block and
+of both forms against the FP64 oracle over the CPU baseline's sample of
+blocks. The line also measures the other configurations: c3 (uneven
+neighbour counts with simple kriging in the same launch) and c5 (10.24M
+ill-conditioned blocks), each against the oracle, the c4 leave-one-out
+gradient and the paths around the headline one.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -20,6 +25,7 @@ blocks, with every host thread.
 
 import argparse
 import ctypes
+import hashlib
 import json
 import os
 import statistics
@@ -33,9 +39,21 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM bytes per system of k_tile<mixed>: (132,827,648 read + 16,656,896 written) / 800,000 systems in the
-# ncu capture of profiles/k_tile_c2_800k_blocks.md.
+# DRAM bytes per system of k_tile<mixed> from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum over
+# the systems of the launch), valid for the tile kernel's sources whose hash is TILE_TRAFFIC_SOURCE: when they
+# change, the line reports no traffic until a new capture is made.
 TILE_DRAM_BYTES_PER_SYSTEM = (132827648 + 16656896) / 800000
+TILE_TRAFFIC_SOURCE = ""
+TILE_SOURCES = ("boitata_b200/csrc/btk_tile.cu", "boitata_b200/csrc/btk_device.cuh", "boitata_b200/csrc/btk_internal.h")
+
+
+def tile_source_hash():
+    h = hashlib.sha256()
+    for f in TILE_SOURCES:
+        with open(os.path.join(ROOT, f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
 
 def hbm_peak():
     """Measured HBM copy bandwidth of this pool's B200s (GB/s) and where it came from."""
@@ -63,6 +81,7 @@ def parse():
     p.add_argument("--no-grad", action="store_true")
     p.add_argument("--no-tune", action="store_true")
     p.add_argument("--no-callers", action="store_true", help="skip the dense-LU, calibration and SGS lines")
+    p.add_argument("--no-configs", action="store_true", help="skip the c3 and c5 configurations")
     p.add_argument("--grid", default=None, help="block counts NXxNYxNZ in place of 200x200x80 (profiling cases)")
     p.add_argument("--profile", action="store_true",
                    help="profiling case: warm-up and two steps of each form, no timing, no JSON line")
@@ -99,20 +118,46 @@ def workload_config(w, blocks):
 
 
 def cpu_baseline(w, sample_blocks, threads=0):
-    """The oracle (CPU restatement of the reference path) on every host thread over a fixed sample of blocks."""
+    """The oracle (CPU restatement of the reference path) on every host thread over a fixed sample of blocks:
+    (the baseline record, the oracle's per-block results, the sampled cell indices)."""
     from oracle import oracle
 
     g = w.geometry
     cent = oracle.centroids(g.origin, g.size, g.count, g.rotation)
     step = max(1, len(cent) // sample_blocks)
-    targets = np.ascontiguousarray(cent[::step][:sample_blocks])
+    cells = np.arange(0, len(cent), step)[:sample_blocks]
+    targets = np.ascontiguousarray(cent[cells])
     cores = threads or oracle.num_threads()
     t0 = time.perf_counter()
-    oracle.estimate_many(targets, w.coords, w.values, w.search, w.variogram, threads=cores, neighbors=False)
+    ref = oracle.estimate_many(targets, w.coords, w.values, w.search, w.variogram, threads=cores, neighbors=False)
     dt = time.perf_counter() - t0
-    return {"value": len(targets) / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"every {step}th block of the 3.2M-block model ({len(targets)} blocks), "
-                      f"{dt:.2f} s on {cores} threads"}
+    return ({"value": len(targets) / dt, "unit": UNIT, "cores": cores, "kind": "port",
+             "sample": f"every {step}th block of the {len(cent)}-block model ({len(targets)} blocks), "
+                       f"{dt:.2f} s on {cores} threads"}, ref, cells)
+
+
+ORACLE_STATUS = {0: 0, 1: 1, 2: 2, 3: 3, 4: 4}  # oracle status -> engine status
+
+
+def oracle_error(got, ref, cells=None):
+    """Error of one GPU form against the FP64 oracle, per result, in the reference tests' convention
+    |a - b| / (1 + max(|a|, |b|)) (crates/estimation/src/kernel.rs:178-180), over value, variance and
+    lagrange; with the NaN pattern and the status (fallback flag masked) compared block for block."""
+    pick = (lambda a: a) if cells is None else (lambda a: a[cells])
+    errs = []
+    fin = np.isfinite(ref["value"])
+    for key in ("value", "variance", "lagrange"):
+        a, b = pick(got[key])[fin], ref[key][fin]
+        errs.append(np.abs(a - b) / (1.0 + np.maximum(np.abs(a), np.abs(b))))
+    e = np.concatenate(errs)
+    st = pick(got["status"]) & 0x0F
+    want = np.vectorize(ORACLE_STATUS.get)(ref["status"]).astype(np.int8)
+    nan_same = np.isfinite(pick(got["value"])) == fin
+    return {"max": float(e.max()) if len(e) else None, "p99": float(np.percentile(e, 99)) if len(e) else None,
+            "nan_pattern_equal": bool(nan_same.all()), "nan_pattern_differs": int((~nan_same).sum()),
+            "status_equal": bool(np.array_equal(st, want)), "status_differs": int((st != want).sum()),
+            "n_used_equal": bool(np.array_equal(pick(got["n_used"])[fin], ref["n_used"][fin])),
+            "blocks": int(len(fin))}
 
 
 class Clocks:
@@ -176,32 +221,23 @@ def rel_err(a, b):
     return e
 
 
-def loo_gradient(args, dev, ws=1, rank=0):
-    """c4: leave-one-out loss of 20,000 samples (32 neighbours, frozen) and its 10-parameter gradient;
-    kernel times from CUDA events on the launch stream, forward alone and forward with the adjoint. With
-    several ranks the samples are split over them (boitata_b200.shard) and the partial sums are
-    all-reduced; the time is the slowest rank's kernel time."""
+def objective_times(obj, theta, first, count, warmup, steps, dev, ws=1):
+    """Kernel times (ms, CUDA events on the launch stream, median over steps, max over ranks) of the objective
+    alone and with its gradient, over systems first .. first + count - 1; and the summed partial sums."""
     import torch
 
-    from boitata_b200 import OrdinaryKriging, shard, workloads
-    from boitata_b200.gradient import LeaveOneOut, theta_of
+    from boitata_b200 import shard
 
-    w = workloads.c4(device=dev)
-    torch.cuda.empty_cache()
-    est = OrdinaryKriging(w.variogram, w.search).fit(w.coords, w.values)
-    loo = LeaveOneOut(est)
-    theta = theta_of(w.variogram)
-    first, count = shard.split(loo.n, ws)[rank]
-    ctx = est._ctx
+    ctx = obj.estimator._ctx
     ctx._lib.btk_set_timing(ctx.handle, 1)
-    times = {}
+    times, sums = {}, None
     for grad in (False, True):
         ms = []
-        for i in range(args.warmup + max(args.steps, 3)):
-            sums = shard.loo_sums(loo, theta, first, count, grad)
+        for i in range(warmup + max(steps, 3)):
+            sums = shard.loo_sums(obj, theta, first, count, grad)
             p3 = (ctypes.c_float * 3)()
             ctx.check(ctx._lib.btk_phase_ms(ctx.handle, p3), "phase timing")
-            if i >= args.warmup:
+            if i >= warmup:
                 ms.append(p3[0])
         t = np.array([float(np.median(ms))])
         if ws > 1:
@@ -211,16 +247,46 @@ def loo_gradient(args, dev, ws=1, rank=0):
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             t = tt.cpu().numpy()
         times[grad] = float(t[0])
-    loss, g, _ = shard.finish(shard.all_reduce_sum(sums))
     ctx._lib.btk_set_timing(ctx.handle, 0)
-    return {"loo_grad_ms": times[True],
-            "loo_grad": {"samples": int(len(w.coords)), "parameters": int(len(theta)), "loss": loss,
-                         "forward_ms": times[False], "forward_and_adjoint_ms": times[True],
-                         "adjoint_over_forward": (times[True] - times[False]) / times[False],
-                         "grad_norm": float(np.linalg.norm(g)), "ranks": ws,
+    return times, sums
+
+
+def loo_gradient(args, dev, ws=1, rank=0):
+    """c4: leave-one-out loss of 20,000 samples (32 neighbours, frozen) and its 10-parameter gradient, in the
+    FP64 form and the mixed form (FP32 factorisation, FP64 refinement and gradient sums); kernel times from
+    CUDA events on the launch stream, forward alone and forward with the adjoint. With several ranks the
+    samples are split over them (boitata_b200.shard) and the partial sums are all-reduced; the time is the
+    slowest rank's kernel time. loo_grad_ms is the faster form's forward with the adjoint."""
+    import torch
+
+    from boitata_b200 import OrdinaryKriging, shard, workloads
+    from boitata_b200.gradient import LeaveOneOut, theta_of
+
+    w = workloads.c4(device=dev)
+    torch.cuda.empty_cache()
+    est = OrdinaryKriging(w.variogram, w.search).fit(w.coords, w.values)
+    theta = theta_of(w.variogram)
+    forms = {}
+    for precision in ("fp64", "mixed"):
+        loo = LeaveOneOut(est, precision=precision)
+        first, count = shard.split(loo.n, ws)[rank]
+        times, sums = objective_times(loo, theta, first, count, args.warmup, args.steps, dev, ws)
+        loss, g, cnt = shard.finish(shard.all_reduce_sum(sums))
+        forms[precision] = {"forward_ms": times[False], "forward_and_adjoint_ms": times[True],
+                            "adjoint_over_forward": (times[True] - times[False]) / times[False],
+                            "loss": loss, "grad": [float(x) for x in g], "systems": cnt}
+    gd = np.array(forms["mixed"]["grad"]) - np.array(forms["fp64"]["grad"])
+    best = min(forms, key=lambda k: forms[k]["forward_and_adjoint_ms"])
+    return {"loo_grad_ms": forms[best]["forward_and_adjoint_ms"],
+            "loo_grad": {"samples": int(len(w.coords)), "parameters": int(len(theta)), "form": best,
+                         "forms": forms, "ranks": ws,
+                         "mixed_vs_fp64": {"loss": abs(forms["mixed"]["loss"] - forms["fp64"]["loss"]) /
+                                           abs(forms["fp64"]["loss"]),
+                                           "grad_max_rel": float(np.max(np.abs(gd) / np.maximum(
+                                               np.abs(forms["fp64"]["grad"]), 1e-12)))},
                          "what": "c4: mean squared leave-one-out error of ordinary kriging, 32 nearest samples "
                                  "frozen at theta0, gradient w.r.t. nugget, 2 sills, 2 ranges, 2 ratios, "
-                                 "3 angles (FP64 adjoint, one kernel with the forward); samples split over the "
+                                 "3 angles (adjoint in the same kernel as the forward); samples split over the "
                                  "ranks, partial sums all-reduced"}}
 
 
@@ -257,29 +323,6 @@ def callers(dev):
             ts.append(time.perf_counter() - t0)
         out[name] = {"blocks_per_s": g.cells() / float(np.median(ts)), "blocks": g.cells(),
                      "workload": "c1 samples and block model, " + name.replace("_", " ")}
-    # C5: 220k clustered composites (10% near-twins 0.01 m away), Gaussian model with a 1e-4 nugget, octant
-    # search with up to 64 samples, 10.24M blocks; FP64 (every system is ill-conditioned, so the mixed form
-    # re-solves all of them in FP64), device outputs, one timed step after a warm one.
-    w5 = workloads.c5()
-    est = bt.OrdinaryKriging(w5.variogram, w5.search).fit(w5.coords, w5.values)
-    c5ctx = est._ctx
-    m5 = w5.geometry.cells()
-    g5 = w5.geometry.to_c()
-    v5 = torch.empty(m5, dtype=torch.float64, device=dev)
-    s5 = torch.empty(m5, dtype=torch.float64, device=dev)
-    o5 = bt._native.OutputsC(v5.data_ptr(), s5.data_ptr(), None, None, None)
-    ts = []
-    for _ in range(2):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        c5ctx.check(c5ctx._lib.btk_predict_geometry_device(c5ctx.handle, ctypes.byref(g5), bt._native.ORDINARY, 0.0,
-                                                           bt._native.FP64, ctypes.byref(o5), None), "c5")
-        torch.cuda.synchronize()
-        ts.append(time.perf_counter() - t0)
-    out["c5_fp64"] = {"blocks_per_s": m5 / ts[-1], "blocks": m5, "samples": int(len(w5.coords)),
-                      "seconds": ts[-1], "finite": int(torch.isfinite(v5).sum().item()),
-                      "workload": "C5: 10.24M blocks, octant search up to 64 samples, FP64, device outputs"}
-    del est, v5, s5
     w2 = workloads.c2()
     scores, _ = normal_score(w2.values)
     sim_grid = bt.Geometry((0.0, 0.0, 0.0), (5.0, 5.0, 6.25), (100, 100, 40))
@@ -300,6 +343,169 @@ def callers(dev):
     return out
 
 
+class Replay:
+    """One captured CUDA graph of a prediction on a context, replayed on `stream` with CUDA events around
+    each replay and L2 flushed between replays (outside the events)."""
+
+    def __init__(self, ctx, stream, flush):
+        self.ctx, self.stream, self.flush = ctx, stream, flush
+
+    def time(self, warmup, steps):
+        import torch
+
+        lib, h = self.ctx._lib, self.ctx.handle
+        for _ in range(warmup):
+            self.ctx.check(lib.btk_graph_launch(h, ctypes.c_void_p(self.stream.cuda_stream)), "replay")
+        torch.cuda.synchronize()
+        before = self.ctx.launches()
+        ms = []
+        for _ in range(steps):
+            self.flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(self.stream)
+            self.ctx.check(lib.btk_graph_launch(h, ctypes.c_void_p(self.stream.cuda_stream)), "replay")
+            e1.record(self.stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.mean(ms)), self.ctx.launches() - before
+
+
+def device_outputs(m, dev):
+    import torch
+
+    from boitata_b200 import _native as N
+
+    outs = {k: torch.empty(m, dtype=torch.float64, device=dev) for k in ("value", "variance", "lagrange")}
+    outs["n_used"] = torch.empty(m, dtype=torch.int32, device=dev)
+    outs["status"] = torch.empty(m, dtype=torch.int8, device=dev)
+    oc = N.OutputsC(*(outs[k].data_ptr() for k in ("value", "variance", "lagrange", "n_used", "status")))
+    return outs, oc
+
+
+def host_copy(outs):
+    return {k: v.cpu().numpy() for k, v in outs.items()}
+
+
+def config_c3(args, dev, stream, flush, tune=True):
+    """c3: c1's box with a 10x sample-density gradient along x (2,000 samples), the 50,000 block centroids
+    of c1's model as device targets, neighbour counts 4 to 64, simple kriging (mean 1.0) on every 10th target
+    and ordinary kriging on the rest in the same call; each form autotuned, captured into one CUDA graph and
+    replayed; every block checked against the FP64 oracle (ordinary and simple kriging per block)."""
+    import torch
+
+    from boitata_b200 import OrdinaryKriging, workloads
+    from boitata_b200 import _native as N
+    from boitata_b200.autotune import autotune_device
+    from oracle import oracle
+
+    w = workloads.c3()
+    g = w.geometry
+    targets = oracle.centroids(g.origin, g.size, g.count, g.rotation)
+    m = len(targets)
+    sk = np.arange(m) % 10 == 0
+    kinds = np.where(sk, N.SIMPLE, N.ORDINARY).astype(np.int8)
+    est = OrdinaryKriging(w.variogram, w.search).fit(w.coords, w.values)
+    ctx = est._ctx
+    lib, h = ctx._lib, ctx.handle
+    d_xyz = torch.from_numpy(np.ascontiguousarray(targets.T).ravel()).to(dev)
+    d_kinds = torch.from_numpy(kinds).to(dev)
+    outs, oc = device_outputs(m, dev)
+    out = {"workload": "c3: 2,000 samples with density rising 10x along x in 1000x1000x200 m, 50x50x20 block "
+                       "centroids (50,000 device targets), Search(radius=150, min_samples=4, max_samples=64), "
+                       "simple kriging (mean 1.0) on every 10th target in the same launch",
+           "blocks": m}
+    got = {}
+    for prec, name in ((N.FP64, "fp64"), (N.MIXED, "mixed")):
+        if tune:
+            t = autotune_device(est, m, d_xyz.data_ptr(), d_kinds.data_ptr(), kparam=1.0, precision=name, steps=2,
+                                tag="c3 block centroids, every 10th simple")
+            out.setdefault("tuning", {})[name] = {**t["best"], "tile": list(t["best"]["tile"])}
+        ctx.check(lib.btk_graph_capture_device(h, m, d_xyz.data_ptr(), d_kinds.data_ptr(), N.ORDINARY, 1.0, prec,
+                                               ctypes.byref(oc)), "capture")
+        ms, launches = Replay(ctx, stream, flush).time(args.warmup, max(args.steps, 5))
+        got[name] = host_copy(outs)
+        out[name] = {"blocks_per_s": m / (ms * 1e-3), "ms_per_step": ms, "gpu_launches_per_step":
+                     launches / max(args.steps, 5)}
+    n_used = got["fp64"]["n_used"]
+    ok = (got["fp64"]["status"] & 0x0F) == 0
+    out["n_used"] = {"min": int(n_used[ok].min()), "max": int(n_used[ok].max()), "mean": float(n_used[ok].mean())}
+    out["mixed_over_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    out["fp64_fallback_systems"] = int(np.sum((got["mixed"]["status"] & 0x10) != 0))
+    ref = {}
+    for kind, sel in (("ordinary", ~sk), ("simple", sk)):
+        r = oracle.estimate_many(targets[sel], w.coords, w.values, w.search, w.variogram, kind=kind, kparam=1.0,
+                                 neighbors=False)
+        for k, v in r.items():
+            ref.setdefault(k, np.empty(m, dtype=v.dtype))[sel] = v
+    out["oracle_error"] = {name: oracle_error(got[name], ref) for name in ("fp64", "mixed")}
+    out["launch"] = "btk_graph_capture_device (btk_predict_kinds_device: Hilbert order, search, tile solve, " \
+                    "per-system kernels, FP64 re-solve) replayed per step; L2 flushed between steps"
+    del est
+    return out
+
+
+def config_c5(args, dev, stream, flush, sample=20_000):
+    """c5: 220,000 clustered composites (10 % copied 0.01 m away), Gaussian variogram with a 1e-4 nugget,
+    octant search of up to 64 samples, 10.24M blocks; each form captured into one CUDA graph (centroids,
+    search, solves, FP64 re-solves) and replayed; the mixed form's fallback fraction; a sample of blocks
+    checked against the FP64 oracle."""
+    from boitata_b200 import OrdinaryKriging, workloads
+    from boitata_b200 import _native as N
+    from oracle import oracle
+
+    w = workloads.c5()
+    est = OrdinaryKriging(w.variogram, w.search).fit(w.coords, w.values)
+    ctx = est._ctx
+    lib, h = ctx._lib, ctx.handle
+    m = w.geometry.cells()
+    gc = w.geometry.to_c()
+    outs, oc = device_outputs(m, dev)
+    out = {"workload": "c5: 220,000 composites (1,600 holes in 40 clusters, 125 x 2 m, plus 10% copied 0.01 m away), "
+                       "Gaussian variogram (nugget 1e-4, range 200 m), 400x400x64 blocks (10.24M), octant search "
+                       "8 per octant / 64 max, radius 300 m", "blocks": m, "samples": int(len(w.coords))}
+    got = {}
+    steps = max(2, min(args.steps, 3))
+    for prec, name in ((N.FP64, "fp64"), (N.MIXED, "mixed")):
+        ctx.check(lib.btk_graph_capture_geometry(h, ctypes.byref(gc), N.ORDINARY, 0.0, prec, ctypes.byref(oc)),
+                  "capture")
+        ms, _ = Replay(ctx, stream, flush).time(1, steps)
+        st = outs["status"].cpu().numpy()
+        got[name] = {k: v.cpu().numpy() for k, v in outs.items()}
+        out[name] = {"blocks_per_s": m / (ms * 1e-3), "ms_per_step": ms}
+        if name == "mixed":
+            fin = (st & 0x0F) == 0
+            out[name]["fp64_fallback_fraction"] = float(np.mean((st[fin] & 0x10) != 0))
+    out["mixed_over_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    # The gradient of the global mean estimate with respect to the variogram (nugget, sill, range, 2 ratios,
+    # 3 angles), neighbourhoods frozen at theta0, covariances recomputed in the adjoint; against one forward
+    # step of the same form (the captured prediction above).
+    from boitata_b200.gradient import BlockMean, theta_of
+
+    del outs, oc
+    theta = theta_of(w.variogram)
+    grad = {}
+    for precision in ("fp64", "mixed"):
+        bm = BlockMean(est, w.geometry, precision=precision)
+        times, sums = objective_times(bm, theta, 0, bm.n, 1, 3, dev)
+        grad[precision] = {"objective_ms": times[False], "objective_and_gradient_ms": times[True],
+                           "over_forward_step": times[True] / out[precision]["ms_per_step"],
+                           "mean": float(sums[0] / sums[1]), "systems": int(sums[1]),
+                           "grad": [float(x) for x in sums[2:] / sums[1]]}
+    out["mean_gradient"] = grad
+    out["c5_grad_ms"] = min(v["objective_and_gradient_ms"] for v in grad.values())
+    out["c5_forward_ms"] = min(out["fp64"]["ms_per_step"], out["mixed"]["ms_per_step"])
+    g = w.geometry
+    cells = np.arange(0, m, m // sample)[:sample]
+    cent = oracle.centroids(g.origin, g.size, g.count, g.rotation)[cells]
+    ref = oracle.estimate_many(cent, w.coords, w.values, w.search, w.variogram, neighbors=False)
+    out["oracle_error"] = {name: oracle_error(got[name], ref, cells) for name in ("fp64", "mixed")}
+    out["oracle_error"]["sample"] = f"every {m // sample}th block ({len(cells)} blocks)"
+    out["oracle_error"]["note"] = ("condition numbers reach ~5e5 here, so two FP64 evaluation orders differ by up "
+                                   "to ~1e-15 x cond (about 1e-10) on their own")
+    del est
+    return out
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return
@@ -309,7 +515,7 @@ def run_reference(args, ws, rank):
     vals = []
     sample = min(args.cpu_sample, 60_000)
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(w, sample)
+        r, _, _ = cpu_baseline(w, sample)
         if i >= args.warmup:
             vals.append(r["value"])
     v = float(statistics.mean(vals))
@@ -418,7 +624,7 @@ def main():
     for prec in (N.FP64, N.MIXED):
         step(prec)
         torch.cuda.synchronize()
-        results[prec] = {k: v.clone() for k, v in outs.items()}
+        results[prec] = host_copy(outs)
 
     timed = {}
     launches = {}
@@ -467,16 +673,23 @@ def main():
     peak32 = lib.btk_peak_flops(h, 0)
 
     mixed, fp64 = results[N.MIXED], results[N.FP64]
-    v64, vmx = fp64["value"].cpu().numpy(), mixed["value"].cpu().numpy()
-    s64, smx = fp64["variance"].cpu().numpy(), mixed["variance"].cpu().numpy()
-    n_used = fp64["n_used"].cpu().numpy()
-    st64 = fp64["status"].cpu().numpy()
+    v64, vmx = fp64["value"], mixed["value"]
+    s64, smx = fp64["variance"], mixed["variance"]
+    n_used = fp64["n_used"]
+    st64 = fp64["status"]
     err = np.concatenate([rel_err(vmx, v64), rel_err(smx, s64)])
     nan_same = int(np.sum(np.isfinite(vmx) == np.isfinite(v64)))
-    fallback = int(np.sum((mixed["status"].cpu().numpy() & 0x10) != 0))
+    fallback = int(np.sum((mixed["status"] & 0x10) != 0))
     flops = float(np.sum(flops_per_system(n_used[st64 == 0], [s.model for s in w.variogram.structures])))
 
     ms_mixed, ms_fp64 = timed[N.MIXED][0], timed[N.FP64][0]
+    if TILE_TRAFFIC_SOURCE == tile_source_hash():
+        traffic = TILE_DRAM_BYTES_PER_SYSTEM * m
+        traffic_source = ("dram__bytes_read.sum + dram__bytes_write.sum of k_tile<mixed> per system from one ncu "
+                          "capture of these kernel sources (hash " + TILE_TRAFFIC_SOURCE + "), times the systems "
+                          "of one launch (the per-target streams grow in proportion)")
+    else:
+        traffic, traffic_source = None, "no ncu capture of the current tile kernel sources"
     value = ws * m / (ms_mixed * 1e-3)
     solve_ms = phases[N.MIXED][1]
     line = {
@@ -500,19 +713,16 @@ def main():
                                                "FP64 refinement) and the per-system kernels for its leftovers",
                      "achieved": flops / (solve_ms * 1e-3) / 1e12, "peak": peak64 / 1e12, "unit": "TFLOP/s",
                      "frac": (flops / (solve_ms * 1e-3)) / peak64,
-                     "traffic": TILE_DRAM_BYTES_PER_SYSTEM * m,
-                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of k_tile<mixed> from one ncu "
-                                       "capture at 800,000 blocks (profiles/k_tile_c2_800k_blocks.md), scaled by "
-                                       "the systems per launch (the per-target streams grow in proportion)",
+                     "traffic": traffic,
+                     "traffic_source": traffic_source,
                      "peak_source": "measured in this run: CUDA-core FP64 FMA loop (btk_peak_flops)",
                      "fp32_peak": peak32 / 1e12,
                      "algorithmic_flops_per_step": flops,
                      # The same launches against HBM: the tile solve reads the neighbour table and targets
                      # and writes the outputs; its tables live in shared memory, so HBM is far from bound.
-                     "hbm_view": {"achieved_gbs": TILE_DRAM_BYTES_PER_SYSTEM * m / (solve_ms * 1e-3) / 1e9,
-                                  "peak_gbs": hbm_peak()[0],
-                                  "frac": TILE_DRAM_BYTES_PER_SYSTEM * m / (solve_ms * 1e-3) / 1e9 / hbm_peak()[0],
-                                  "peak_source": hbm_peak()[1]}},
+                     "hbm_view": None if traffic is None else {
+                         "achieved_gbs": traffic / (solve_ms * 1e-3) / 1e9, "peak_gbs": hbm_peak()[0],
+                         "frac": traffic / (solve_ms * 1e-3) / 1e9 / hbm_peak()[0], "peak_source": hbm_peak()[1]}},
         "gpu_launches": int(launches[N.MIXED]),
         "clocks": clocks,
     }
@@ -550,8 +760,17 @@ def main():
 
     if rank == 0 and ws == 1 and not args.no_callers:
         line["callers"] = callers(dev)
+    if rank == 0 and ws == 1 and not args.no_configs:
+        line["configs"] = {"c3": config_c3(args, dev, stream, flush, tune=not args.no_tune),
+                           "c5": config_c5(args, dev, stream, flush)}
     if rank == 0 and ws == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(w, args.cpu_sample)
+        base, ref, cells = cpu_baseline(w, args.cpu_sample)
+        line["cpu_baseline"] = base
+        line["oracle_error"] = {"fp64": oracle_error(fp64, ref, cells), "mixed": oracle_error(mixed, ref, cells),
+                                "sample": base["sample"],
+                                "metric": "|a-b| / (1 + max(|a|, |b|)) over value, variance and lagrange against "
+                                          "the FP64 oracle (crates/estimation/src/kernel.rs:178-180)",
+                                "tolerance": {"fp64": 1e-10, "mixed": 1e-6}}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -99,16 +99,24 @@ SIGNATURES = {
     "btk_set_tuning": (ctypes.c_int, [P, ctypes.POINTER(TuningC)]),
     "btk_graph_capture_geometry": (ctypes.c_int, [P, ctypes.POINTER(GeometryC), ctypes.c_int32, ctypes.c_double,
                                                   ctypes.c_int32, ctypes.POINTER(OutputsC)]),
+    "btk_graph_capture_device": (ctypes.c_int, [P, ctypes.c_int64, P, P, ctypes.c_int32, ctypes.c_double,
+                                                ctypes.c_int32, ctypes.POINTER(OutputsC)]),
     "btk_graph_launch": (ctypes.c_int, [P, P]),
     "btk_set_timing": (ctypes.c_int, [P, ctypes.c_int32]),
     "btk_phase_ms": (ctypes.c_int, [P, P]),
     "btk_peak_flops": (ctypes.c_double, [P, ctypes.c_int32]),
     "btk_loo_freeze": (ctypes.c_int, [P]),
-    "btk_loo_gradient": (ctypes.c_int, [P, ctypes.POINTER(VariogramC), ctypes.c_int32, P, P, P, P]),
+    "btk_loo_gradient": (ctypes.c_int, [P, ctypes.POINTER(VariogramC), ctypes.c_int32, ctypes.c_int32, P, P, P, P]),
     "btk_loo_gradient_range": (ctypes.c_int, [P, ctypes.POINTER(VariogramC), ctypes.c_int64, ctypes.c_int64,
-                                              ctypes.c_int32, P]),
+                                              ctypes.c_int32, ctypes.c_int32, P]),
+    "btk_mean_freeze": (ctypes.c_int, [P, ctypes.POINTER(GeometryC)]),
+    "btk_mean_gradient": (ctypes.c_int, [P, ctypes.POINTER(VariogramC), ctypes.c_int32, ctypes.c_int32, P, P, P,
+                                         P]),
+    "btk_mean_gradient_range": (ctypes.c_int, [P, ctypes.POINTER(VariogramC), ctypes.c_int64, ctypes.c_int64,
+                                               ctypes.c_int32, ctypes.c_int32, P]),
     "btk_solve_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(VariogramC), ctypes.c_int32, ctypes.c_double,
-                                         P, P, P, P, P, ctypes.c_int64, P, P, P, P, ctypes.c_int32, P, P,
+                                         P, P, P, P, P, ctypes.c_int64, ctypes.c_int64, P, P, P, P, ctypes.c_int32,
+                                         P, P,
                                          ctypes.POINTER(OutputsC), P, ctypes.c_char_p, ctypes.c_size_t]),
 }
 

@@ -9,7 +9,9 @@ The tunables (btk_tuning in include/boitata_b200.h):
 
 They are picked by timing the real workload. The time is the sum of the search and solve kernels, taken
 with CUDA events on the launch stream. Three stages run, each at the best of the one before: cell size x
-tile, then search CTA warps, then table size x solve CTAs per SM. The choice is cached per workload signature in a JSON file (BTK_TUNING_CACHE, or
+tile, then search CTA warps, then table size x solve CTAs per SM. Block models (autotune_geometry) and
+device target arrays (autotune_device, e.g. uneven neighbour counts with per-target kinds in one launch)
+are tuned alike. The choice is cached per workload signature in a JSON file (BTK_TUNING_CACHE, or
 ~/.cache/boitata_b200/tuning.json) and applied to the context.
 """
 
@@ -56,7 +58,8 @@ def signature(estimator, geometry, precision):
     s = estimator.searches[0]
     return json.dumps({"n": int(len(estimator._samples[0])), "max": s.max_samples, "octant": s.octant,
                        "radius": s.radius, "anisotropy": s.anisotropy or estimator.variogram.anisotropy,
-                       "models": [x.model for x in estimator.variogram.structures], "count": geometry.count,
+                       "models": [x.model for x in estimator.variogram.structures],
+                       "count": None if geometry is None else geometry.count,
                        "precision": precision}, sort_keys=True, default=str)
 
 
@@ -88,13 +91,76 @@ def time_geometry(estimator, geometry, precision, steps=2):
     return float(np.median(times))
 
 
-def autotune_geometry(estimator, geometry, *, precision="mixed", steps=2, use_cache=True):
-    """Picks and applies the fastest tuning for kriging `geometry` with `estimator` (fitted, first pass).
-    Returns {"best": config, "ms": time, "table": [(config, ms), ...], "cached": bool}."""
+def time_device(estimator, m, d_xyz, d_kinds=None, *, kparam=0.0, precision="mixed", steps=2):
+    """Median search + solve kernel time (ms) of one prediction at m device targets (d_xyz: x, y, z arrays of
+    m doubles back to back; d_kinds: one int8 kind per target, or None for the estimator's kind)."""
+    import torch
+
+    ctx = estimator._ctx
+    dev = torch.device("cuda", estimator._device)
+    outs = [torch.empty(m, dtype=torch.float64, device=dev) for _ in range(3)]
+    outs += [torch.empty(m, dtype=torch.int32, device=dev), torch.empty(m, dtype=torch.int8, device=dev)]
+    oc = N.OutputsC(*(t.data_ptr() for t in outs))
+    prec = {"fp64": N.FP64, "mixed": N.MIXED}[precision]
+    ctx.check(ctx._lib.btk_set_timing(ctx.handle, 1), "timing")
+    times = []
+    try:
+        for i in range(steps + 1):
+            if d_kinds is None:
+                rc = ctx._lib.btk_predict_device(ctx.handle, m, d_xyz, estimator._kind, estimator._kparam, prec,
+                                                 ctypes.byref(oc), None)
+            else:
+                rc = ctx._lib.btk_predict_kinds_device(ctx.handle, m, d_xyz, d_kinds, kparam, prec, ctypes.byref(oc),
+                                                       None)
+            ctx.check(rc, "predict")
+            p = (ctypes.c_float * 3)()
+            ctx.check(ctx._lib.btk_phase_ms(ctx.handle, p), "timing")
+            if i > 0:
+                times.append(sum(p))
+    finally:
+        ctx._lib.btk_set_timing(ctx.handle, 0)
+    return float(np.median(times))
+
+
+def _search(ctx, base, timer, table):
+    """The three stages over the tunables, each at the best of the one before; returns (best, ms)."""
+    best, best_ms = dict(base), float("inf")
+    for ppc in SAMPLES_PER_CELL:
+        for tile in TILES:
+            cfg = dict(base, samples_per_cell=ppc, tile=tile)
+            set_tuning(ctx, cfg)
+            ms = timer()
+            table.append((dict(cfg), ms))
+            if ms < best_ms:
+                best, best_ms = dict(cfg), ms
+    stage1 = dict(best)
+    for sw in SEARCH_WARPS:
+        cfg = dict(stage1, search_warps=sw)
+        if cfg == stage1:
+            continue
+        set_tuning(ctx, cfg)
+        ms = timer()
+        table.append((dict(cfg), ms))
+        if ms < best_ms:
+            best, best_ms = dict(cfg), ms
+    stage2 = dict(best)
+    for tu in TILE_UNION:
+        for sb in SOLVE_BLOCKS:
+            cfg = dict(stage2, tile_union=tu, solve_blocks_per_sm=sb)
+            if cfg == stage2:
+                continue
+            set_tuning(ctx, cfg)
+            ms = timer()
+            table.append((dict(cfg), ms))
+            if ms < best_ms:
+                best, best_ms = dict(cfg), ms
+    return best, best_ms
+
+
+def _tune(estimator, key, timer, use_cache):
     estimator._fitted()
     estimator._use_pass(0)
     ctx = estimator._ctx
-    key = signature(estimator, geometry, precision)
     path = cache_path()
     cache = {}
     if use_cache and os.path.exists(path):
@@ -108,38 +174,8 @@ def autotune_geometry(estimator, geometry, *, precision="mixed", steps=2, use_ca
         cfg["tile"] = tuple(cfg["tile"])
         set_tuning(ctx, cfg)
         return {"best": cfg, "ms": cache[key]["ms"], "table": [], "cached": True}
-    base = get_tuning(ctx)
     table = []
-    best, best_ms = dict(base), float("inf")
-    for ppc in SAMPLES_PER_CELL:
-        for tile in TILES:
-            cfg = dict(base, samples_per_cell=ppc, tile=tile)
-            set_tuning(ctx, cfg)
-            ms = time_geometry(estimator, geometry, precision, steps)
-            table.append((dict(cfg), ms))
-            if ms < best_ms:
-                best, best_ms = dict(cfg), ms
-    stage1 = dict(best)
-    for sw in SEARCH_WARPS:
-        cfg = dict(stage1, search_warps=sw)
-        if cfg == stage1:
-            continue
-        set_tuning(ctx, cfg)
-        ms = time_geometry(estimator, geometry, precision, steps)
-        table.append((dict(cfg), ms))
-        if ms < best_ms:
-            best, best_ms = dict(cfg), ms
-    stage2 = dict(best)
-    for tu in TILE_UNION:
-        for sb in SOLVE_BLOCKS:
-            cfg = dict(stage2, tile_union=tu, solve_blocks_per_sm=sb)
-            if cfg == stage2:
-                continue
-            set_tuning(ctx, cfg)
-            ms = time_geometry(estimator, geometry, precision, steps)
-            table.append((dict(cfg), ms))
-            if ms < best_ms:
-                best, best_ms = dict(cfg), ms
+    best, best_ms = _search(ctx, get_tuning(ctx), timer, table)
     set_tuning(ctx, best)
     if use_cache:
         cache[key] = {"best": {**best, "tile": list(best["tile"])}, "ms": best_ms}
@@ -150,3 +186,21 @@ def autotune_geometry(estimator, geometry, *, precision="mixed", steps=2, use_ca
         except OSError:
             pass
     return {"best": best, "ms": best_ms, "table": table, "cached": False}
+
+
+def autotune_geometry(estimator, geometry, *, precision="mixed", steps=2, use_cache=True):
+    """Picks and applies the fastest tuning for kriging `geometry` with `estimator` (fitted, first pass).
+    Returns {"best": config, "ms": time, "table": [(config, ms), ...], "cached": bool}."""
+    key = signature(estimator, geometry, precision)
+    return _tune(estimator, key, lambda: time_geometry(estimator, geometry, precision, steps), use_cache)
+
+
+def autotune_device(estimator, m, d_xyz, d_kinds=None, *, kparam=0.0, precision="mixed", steps=2, use_cache=True,
+                    tag=""):
+    """As autotune_geometry for m device targets (btk_predict_device, or btk_predict_kinds_device with
+    d_kinds); `tag` names the target set in the cache key (the targets themselves are not hashed)."""
+    key = signature(estimator, None, precision)[:-1] + f', "targets": {m}, "kinds": {d_kinds is not None}, ' \
+        f'"tag": {json.dumps(tag)}}}'
+    return _tune(estimator, key,
+                 lambda: time_device(estimator, m, d_xyz, d_kinds, kparam=kparam, precision=precision, steps=steps),
+                 use_cache)

@@ -1,59 +1,96 @@
-// Leave-one-out loss and its gradient with respect to the variogram (K5).
+// A kriging objective and its gradient with respect to the variogram (K5),
+// over frozen neighbourhoods: the leave-one-out loss or the mean estimate of
+// a block model.
 //
-// Loss: L = (1/N) sum_i (z*_i - z_i)^2 over the samples whose leave-one-out
-// ordinary-kriging estimate z*_i (crates/estimation/src/batch.rs:165-190 with
-// kernel.rs:24-123) exists, with each sample's neighbourhood frozen (the
-// lists the leave-one-out search gave at fit). Parameters theta: nugget,
-// each structure's sill, each structure's major range, the semi/major and
-// minor/major ratios and the azimuth, dip and rake (degrees) of the shared
-// anisotropy (crates/variogram/src/{composite,aniso}.rs).
+// Objectives (ordinary kriging, crates/estimation/src/kernel.rs:24-123):
+//   - leave-one-out: L = (1/N) sum_i (z*_i - z_i)^2 over the samples whose
+//     leave-one-out estimate z*_i (crates/estimation/src/batch.rs:165-190)
+//     exists, each from the list the leave-one-out search gave at fit;
+//   - block-model mean: J = (1/N) sum_t z*_t over the targets t whose
+//     estimate exists, each from the list the search gave when frozen.
+// Systems holding coincident samples (the reference merges them, coincident.rs)
+// are left out of both. Parameters theta: nugget, each structure's sill, each
+// structure's major range, the semi/major and minor/major ratios and the
+// azimuth, dip and rake (degrees) of the shared anisotropy
+// (crates/variogram/src/{composite,aniso}.rs).
 //
 // For one system with bordered matrix K = [C 1; 1' 0], K [w; mu] = [c; 1]
 // and z* = z'w, the adjoint K [lambda; nu] = [z; 0] gives
 //   dz*/dtheta = lambda' dc/dtheta - lambda' dC/dtheta w,
-// so with a = 2 (z* - z_i) lambda the system adds
-//   sum_j a_j dc_j/dtheta - sum_jk a_j w_k dC_jk/dtheta
-// to the gradient. C = L D L' is factored once (the forward's
-// factorisation); w and lambda come from three solves (c, 1, z) on it. The
-// covariance derivatives are recomputed pair by pair, never stored:
-// C(h) = sum_s sill_s (1 - g_s(h / r_s)) for h > 0 and C(0) = C0, so
-//   dC/dsill_s = 1 - g_s,  dC/dr_s = sill_s g_s'(t) h / r_s^2,
-//   dC/dh = -sum_s sill_s g_s'(t) / r_s,  dh/dphi = (M d)' (dM/dphi d) / h
-// for the lag h = |M d| of world offset d, M = diag(1, 1/semi, 1/minor) R.
+// so with a = 2 (z* - z_i) lambda (leave-one-out) or a = lambda (mean) the
+// system adds sum_j a_j dc_j/dtheta - sum_jk a_j w_k dC_jk/dtheta to the
+// gradient sum. w and lambda come from x_v = C^-1 v for v = c, 1, z:
+// mu = (1'x_c - 1) / 1'x_1, w = x_c - mu x_1, nu = 1'x_z / 1'x_1 and
+// lambda = x_z - nu x_1. The covariance derivatives are recomputed pair by
+// pair, never stored: C(h) = sum_s sill_s (1 - g_s(h / r_s)) for h > 0 and
+// C(0) = C0, so dC/dsill_s = 1 - g_s, dC/dr_s = sill_s g_s'(t) h / r_s^2,
+// dC/dh = -sum_s sill_s g_s'(t) / r_s and dh/dphi = (M d)'(dM/dphi d) / h for
+// the lag h = |M d| of world offset d, M = diag(1, 1/semi, 1/minor) R, with
+// the shape derivatives of crates/variogram/src/model.rs:181-312.
 //
-// One warp per system (n <= 32), FP64 throughout, per-system partial sums
-// written to a buffer and reduced in a fixed order (deterministic).
+// One group of NW warps per system (n <= 32 NW), lane = row. Every lag comes
+// from lag_world, as in the prediction kernels, so the FP64 objective is the
+// prediction path's estimate to the bit. Two forms:
+//   - FP64: the shifted, windowed right-looking LDL^T of the prediction
+//     kernels with the forward substitutions fused in, the multipliers kept
+//     in place of the covariance triangle, and one backward sweep for x;
+//   - mixed: the FP32 LDL^T with its multipliers in shared memory, then FP64
+//     iterative refinement (residuals from the FP64 triangle, corrections
+//     from the FP32 factors) until x is good to about 1e-8 relative; the
+//     systems it does not converge on are redone by the FP64 form.
+// Gradient terms are accumulated in FP64. Per-system partial sums go to a
+// buffer that is reduced in a fixed order, so results are deterministic.
+#include <type_traits>
+
 #include "btk_device.cuh"
+#include "btk_group.cuh"
 
 namespace btk {
 namespace {
 
-constexpr unsigned kFull = 0xffffffffu;
-constexpr int R = 32;
 constexpr int kMaxTheta = 1 + 2 * BTK_MAX_STRUCT + 5;
+constexpr int kRefine = 4;  // most FP64 refinement steps of the mixed form
 
-struct AdjSmem {
-  double W[R][3];  // world coordinates of the samples
-  double P[R][3];  // M (s - t)
-  double T[R * (R - 1) / 2];
-  double L[R][R + 1];
-  double col[2][R];
+template <int NW>
+struct alignas(16) GradSmem {
+  static constexpr int R = 32 * NW;
+  double W[R][3];             // world coordinates of the samples
+  double T[R * (R - 1) / 2];  // covariances, strictly lower, packed; the FP64 form's multipliers after the load
+  alignas(16) double col[2][R + 2];
   double rhs[2][4];
+  double red[NW][8];
+  int ired[NW];
   double w[R], adj[R];
+  double xs[3][R];
 };
 
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-  return v;
+template <int NW>
+struct alignas(16) GradSmemMixed {
+  static constexpr int R = 32 * NW;
+  GradSmem<NW> base;
+  alignas(16) float colf[2][R + 4];
+  float rhsf[2][4];
+  float L[R][R + 1];
+};
+
+template <int NW>
+__device__ __forceinline__ GradSmem<NW>& base_of(GradSmem<NW>& s) {
+  return s;
+}
+template <int NW>
+__device__ __forceinline__ GradSmem<NW>& base_of(GradSmemMixed<NW>& s) {
+  return s.base;
 }
 
-__device__ __forceinline__ void tri_ij(int e, int& i, int& j) {
-  int r = int((1.0f + sqrtf(8.0f * float(e) + 1.0f)) * 0.5f);
-  while (r * (r - 1) / 2 > e) --r;
-  while ((r + 1) * r / 2 <= e) ++r;
-  i = r, j = e - r * (r - 1) / 2;
+// M d for the lag frame M (row-major), in lag_world's operation order.
+__device__ __forceinline__ void frame_apply(const VgDev& vg, const double d[3], double md[3]) {
+  const double* M = vg.frame;
+  md[0] = fma(M[2], d[2], fma(M[1], d[1], M[0] * d[0]));
+  md[1] = fma(M[5], d[2], fma(M[4], d[1], M[3] * d[0]));
+  md[2] = fma(M[8], d[2], fma(M[7], d[1], M[6] * d[0]));
 }
+
+__device__ __forceinline__ double norm3(const double v[3]) { return sqrt(fma(v[2], v[2], fma(v[1], v[1], v[0] * v[0]))); }
 
 // Adds coef * dC(h)/dtheta for a lag h > 0 with projected offset Md and world
 // offset d to g (theta order: nugget, sills, ranges, semi, minor, az, dip, rake).
@@ -81,134 +118,196 @@ __device__ __forceinline__ void add_lag_terms(const GradDev& a, double coef, dou
   }
 }
 
-__global__ void __launch_bounds__(128) k_loo_grad(GradDev a) {
+// FP64 backward sweep x = L^-T D^-1 y with the multipliers L[k][row] packed
+// at T[k (k - 1) / 2 + row].
+template <int NW>
+__device__ __forceinline__ void sweep_back64(GradSmem<NW>& S, int gid, int row, int nn, double dme, double& u0,
+                                             double& u1, double& u2) {
+  u0 /= dme, u1 /= dme, u2 /= dme;
+  gsync<NW>(gid);
+  for (int k = nn - 1; k >= 0; --k) {
+    const int b = k & 1;
+    if (row == k) S.rhs[b][0] = u0, S.rhs[b][1] = u1, S.rhs[b][2] = u2;
+    gsync<NW>(gid);
+    if (row < k) {
+      const double l = S.T[k * (k - 1) / 2 + row];
+      u0 = fma(-l, S.rhs[b][0], u0);
+      u1 = fma(-l, S.rhs[b][1], u1);
+      u2 = fma(-l, S.rhs[b][2], u2);
+    }
+  }
+}
+
+template <int NW, bool MIXED>
+__global__ void __launch_bounds__(128) k_grad(GradDev a) {
+  constexpr int R = 32 * NW;
+  constexpr int GROUPS = 128 / R;
+  constexpr int Q = R / 4;
+  using Sx = typename std::conditional<MIXED, GradSmemMixed<NW>, GradSmem<NW>>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int lane = threadIdx.x & 31;
-  AdjSmem& S = reinterpret_cast<AdjSmem*>(smem_raw)[threadIdx.x >> 5];
+  const int gid = threadIdx.x / R, row = threadIdx.x % R, wig = row >> 5;
+  Sx& X = reinterpret_cast<Sx*>(smem_raw)[gid];
+  GradSmem<NW>& S = base_of<NW>(X);
   const int ns = a.vg.nstruct;
   const int ntheta = 1 + 2 * ns + 5;
   const double c0 = a.vg.c0;
-  const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
-  for (int64_t i = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); i < a.n; i += warps) {
-    __syncwarp();
+  const bool mean = a.tx != nullptr;
+  const int64_t nitems = a.list ? *a.list_len : a.n;
+  for (int64_t item = int64_t(blockIdx.x) * GROUPS + gid; item < nitems; item += int64_t(gridDim.x) * GROUPS) {
+    const int64_t i = a.list ? a.list[item] : item;
+    const int64_t si = a.first + i;  // the left-out sample, or the target
     double* out = a.part + i * a.stride;
-    const int64_t si = a.first + i;  // the left-out sample
+    gsync<NW>(gid);
     const int n = a.count[si];
-    bool skip = a.sstatus[si] != BTK_ST_OK || n <= 0 || n > R;
-    const bool have = !skip && lane < n;
-    const double t[3] = {a.sx[si], a.sy[si], a.sz[si]};
-    double w0 = 0, w1 = 0, w2 = 0, z = 0, err = 0;
+    const bool solvable = a.sstatus[si] == BTK_ST_OK && n > 0 && n <= R;
+    const bool have = solvable && row < n;
+    const double t[3] = {mean ? a.tx[si] : a.sx[si], mean ? a.ty[si] : a.sy[si], mean ? a.tz[si] : a.sz[si]};
+    double w[3] = {0.0, 0.0, 0.0}, z = 0.0, err = 0.0;
     int tw = 0;
     if (have) {
-      const uint32_t j = a.nbr[si * a.max_samples + lane];
-      w0 = a.sx[j], w1 = a.sy[j], w2 = a.sz[j], z = a.sv[j];
+      const uint32_t j = a.nbr[si * a.max_samples + row];
+      w[0] = a.sx[j], w[1] = a.sy[j], w[2] = a.sz[j], z = a.sv[j];
       if (a.se) err = a.se[j];
-      tw = a.twin[j];
+      tw = a.twin ? a.twin[j] : 0;
     }
-    // Systems holding coincident samples (merged by the reference's guard)
-    // are left out of the loss and the gradient.
-    skip = skip || __any_sync(kFull, tw != 0);
-    if (skip) {
-      if (lane == 0) {
+    // uniform over the group: `solvable` depends on the system alone
+    if (!solvable || group_any<NW>(S, gid, wig, tw != 0)) {
+      if (row == 0) {
         for (int k = 0; k < a.stride; ++k) out[k] = 0.0;
         if (a.value) a.value[si] = NAN;
       }
       continue;
     }
-    double p[3] = {w0 - t[0], w1 - t[1], w2 - t[2]};
-    {
-      const double* M = a.vg.frame;
-      const double r0 = M[0] * p[0] + M[1] * p[1] + M[2] * p[2];
-      const double r1 = M[3] * p[0] + M[4] * p[1] + M[5] * p[2];
-      const double r2 = M[6] * p[0] + M[7] * p[1] + M[8] * p[2];
-      p[0] = r0, p[1] = r1, p[2] = r2;
-    }
-    if (have) {
-      S.P[lane][0] = p[0], S.P[lane][1] = p[1], S.P[lane][2] = p[2];
-      S.W[lane][0] = w0, S.W[lane][1] = w1, S.W[lane][2] = w2;
-    }
-    __syncwarp();
+    if (have) S.W[row][0] = w[0], S.W[row][1] = w[1], S.W[row][2] = w[2];
+    gsync<NW>(gid);
     const int E = n * (n - 1) / 2;
-    for (int e = lane; e < E; e += R) {
-      int r, q;
-      tri_ij(e, r, q);
-      const double dx = S.P[r][0] - S.P[q][0], dy = S.P[r][1] - S.P[q][1], dz = S.P[r][2] - S.P[q][2];
-      S.T[e] = cov64(a.vg, sqrt(dx * dx + dy * dy + dz * dz));
+    for (int e = row; e < E; e += R) {
+      int p, q;
+      tri_index(e, p, q);
+      S.T[e] = cov64(a.vg, lag_world(a.vg, S.W[q][0], S.W[q][1], S.W[q][2], S.W[p][0], S.W[p][1], S.W[p][2]));
     }
-    const double hc = sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+    const double dt[3] = {w[0] - t[0], w[1] - t[1], w[2] - t[2]};  // lag_world(t, w)'s offset
+    double pt[3];
+    frame_apply(a.vg, dt, pt);
+    const double hc = norm3(pt);
     const double c = have ? cov64(a.vg, hc) : 0.0;
-    __syncwarp();
+    const double diag = have ? c0 + err : 1.0;
+    const int tri = row * (row - 1) / 2;
+    gsync<NW>(gid);
 
-    // LDL' with the forward substitutions of c, 1 and z fused in.
-    double A[R];
-    const int tri = lane * (lane - 1) / 2;
+    double x0 = 0.0, x1 = 0.0, x2 = 0.0;
+    double estimate = 0.0;  // the FP64 form's, from the same forms as the prediction epilogue
+    bool redo = false;
+    const int n1 = min(n, Q), n2 = min(n, 2 * Q), n3 = min(n, 3 * Q);
+    if constexpr (MIXED) {
+      float A[R];
 #pragma unroll
-    for (int q = 0; q < R; ++q) A[q] = q < lane ? (have ? S.T[tri + q] : 0.0) : (q == lane ? (have ? c0 + err : 1.0) : 0.0);
-    double y0 = have ? c : 0.0, y1 = have ? 1.0 : 0.0, y2 = have ? z : 0.0, dme = 1.0;
-    bool sing = false;
-#pragma unroll
-    for (int k = 0; k < R; ++k) {
-      if (k >= n) break;
-      const int b = k & 1;
-      S.col[b][lane] = A[k];
-      if (lane == k) S.rhs[b][0] = y0, S.rhs[b][1] = y1, S.rhs[b][2] = y2;
-      __syncwarp();
-      const double dk = S.col[b][k];
-      if (!(dk > kPivot * c0)) {
-        sing = true;
-        break;
+      for (int q = 0; q < R; ++q)
+        A[q] = q < row ? (have ? float(S.T[tri + q]) : 0.f) : (q == row ? float(diag) : 0.f);
+      float y0 = have ? float(c) : 0.f, y1 = have ? 1.f : 0.f, y2 = have ? float(z) : 0.f;
+      float dme = 1.f;
+      bool weak = false;
+      // A pivot at most n ulp(C0) is not resolved in FP32: the FP64 form takes the system.
+      const float thr = float(n) * 1.1920929e-7f * float(c0);
+      eliminate_rows_f32<NW, R>(A, 0, n1, row, X, gid, y0, y1, y2, dme, weak, thr);
+      if (!weak) eliminate_rows_f32<NW, 3 * Q>(A, n1, n2, row, X, gid, y0, y1, y2, dme, weak, thr);
+      if (!weak) eliminate_rows_f32<NW, 2 * Q>(A, n2, n3, row, X, gid, y0, y1, y2, dme, weak, thr);
+      if (!weak) eliminate_rows_f32<NW, Q>(A, n3, n, row, X, gid, y0, y1, y2, dme, weak, thr);
+      redo = weak;
+      if (!weak) {
+        float u0 = y0, u1 = y1, u2 = y2;
+        sweep_f32<NW>(X, gid, row, n, dme, false, u0, u1, u2);
+        x0 = have ? double(u0) : 0.0, x1 = have ? double(u1) : 0.0, x2 = have ? double(u2) : 0.0;
+        const double cmax = fmax(group_max<NW>(S, gid, wig, have ? fabs(c) : 0.0), 1e-300);
+        const double zmax = fmax(group_max<NW>(S, gid, wig, have ? fabs(z) : 0.0), 1e-300);
+        const double dmin = -group_max<NW>(S, gid, wig, have ? -double(dme) : -1e300);
+        // x errs by about rho C0 / D_min (rho the relative residual): refine
+        // until that is at most 1e-8, as long as each step halves rho.
+        double rho = 0.0;
+        for (int it = 0;; ++it) {
+          S.xs[0][row] = x0, S.xs[1][row] = x1, S.xs[2][row] = x2;
+          gsync<NW>(gid);
+          double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+          if (have) {
+            double a0 = diag * x0, a1 = diag * x1, a2 = diag * x2;
+            for (int j = 0; j < n; ++j) {
+              if (j == row) continue;
+              const double cij = j < row ? S.T[tri + j] : S.T[j * (j - 1) / 2 + row];
+              a0 = fma(cij, S.xs[0][j], a0);
+              a1 = fma(cij, S.xs[1][j], a1);
+              a2 = fma(cij, S.xs[2][j], a2);
+            }
+            r0 = c - a0, r1 = 1.0 - a1, r2 = z - a2;
+          }
+          const double prev = rho;
+          rho = group_max<NW>(S, gid, wig, have ? fmax(fmax(fabs(r0) / cmax, fabs(r1)), fabs(r2) / zmax) : 0.0);
+          if (rho * c0 / dmin <= 1e-8) break;
+          if (it == kRefine || !(rho < 1.0) || (it > 0 && !(rho < 0.5 * prev))) {
+            redo = true;
+            break;
+          }
+          float v0 = float(r0), v1 = float(r1), v2 = float(r2);
+          sweep_f32<NW>(X, gid, row, n, dme, true, v0, v1, v2);
+          if (have) x0 += double(v0), x1 += double(v1), x2 += double(v2);
+          gsync<NW>(gid);  // every row has read xs
+        }
       }
-      if (lane == k) dme = dk;
-      if (lane > k) {
-        const double f = A[k] * (1.0 / dk);
-#pragma unroll
-        for (int q = k + 1; q < R; ++q) A[q] = fma(-f, S.col[b][q], A[q]);
-        y0 = fma(-f, S.rhs[b][0], y0);
-        y1 = fma(-f, S.rhs[b][1], y1);
-        y2 = fma(-f, S.rhs[b][2], y2);
-        A[k] = f;
+      if (redo) {  // uniform over the group
+        if (row == 0) a.redo[atomicAdd(reinterpret_cast<unsigned long long*>(a.redo_len), 1ull)] = i;
+        continue;
       }
+    } else {
+      double A[R];
+#pragma unroll
+      for (int q = 0; q < R; ++q) A[q] = q < row ? (have ? S.T[tri + q] : 0.0) : (q == row ? diag : 0.0);
+      double y0 = have ? c : 0.0, y1 = have ? 1.0 : 0.0, y2 = have ? z : 0.0, dme = 1.0;
+      bool sing = false;
+      const double thr = kPivot * c0;
+      gsync<NW>(gid);  // every row has its covariances: the triangle now takes the multipliers
+      double* Lrow = S.T + tri;
+      eliminate_rows<NW, R, true>(A, 0, n1, row, S, gid, y0, y1, y2, dme, sing, thr, Lrow);
+      if (!sing) eliminate_rows<NW, 3 * Q, true>(A, n1, n2, row, S, gid, y0, y1, y2, dme, sing, thr, Lrow);
+      if (!sing) eliminate_rows<NW, 2 * Q, true>(A, n2, n3, row, S, gid, y0, y1, y2, dme, sing, thr, Lrow);
+      if (!sing) eliminate_rows<NW, Q, true>(A, n3, n, row, S, gid, y0, y1, y2, dme, sing, thr, Lrow);
+      if (sing) {  // a pivot at most 1e-12 C0 (kernel.rs:61): no estimate
+        if (row == 0) {
+          for (int k = 0; k < a.stride; ++k) out[k] = 0.0;
+          if (a.value) a.value[si] = NAN;
+        }
+        continue;
+      }
+      // The estimate as the prediction kernels form it (u'C^-1 v = sum y_u y_v / D),
+      // so the objective is their value to the bit.
+      const double wt = have ? 1.0 / dme : 0.0;
+      double f5[5] = {y1 * y0 * wt, y1 * y1 * wt, y2 * y0 * wt, y2 * y1 * wt, y0 * y0 * wt};
+      group_sum5<NW>(S, gid, wig, f5);
+      const double mu5 = (f5[0] - 1.0) / f5[1];
+      estimate = f5[2] - mu5 * f5[3];
+      double u0 = y0, u1 = y1, u2 = y2;
+      sweep_back64<NW>(S, gid, row, n, dme, u0, u1, u2);
+      x0 = have ? u0 : 0.0, x1 = have ? u1 : 0.0, x2 = have ? u2 : 0.0;
     }
-    if (sing) {
-      if (lane == 0) {
-        for (int k = 0; k < a.stride; ++k) out[k] = 0.0;
-        if (a.value) a.value[si] = NAN;
-      }
-      continue;
-    }
-    // Back substitution L' x = D^-1 y: x_c = C^-1 c, x_1 = C^-1 1, x_z = C^-1 z.
-#pragma unroll
-    for (int q = 0; q < R; ++q) S.L[lane][q] = A[q];
-    double u0 = y0 / dme, u1 = y1 / dme, u2 = y2 / dme;
-    __syncwarp();
-    for (int k = n - 1; k >= 0; --k) {
-      const int b = k & 1;
-      if (lane == k) S.rhs[b][0] = u0, S.rhs[b][1] = u1, S.rhs[b][2] = u2;
-      __syncwarp();
-      if (lane < k) {
-        const double l = S.L[k][lane];
-        u0 = fma(-l, S.rhs[b][0], u0);
-        u1 = fma(-l, S.rhs[b][1], u1);
-        u2 = fma(-l, S.rhs[b][2], u2);
-      }
-    }
-    if (!have) u0 = u1 = u2 = 0.0;
-    const double sa = warp_sum(u0), sb = warp_sum(u1), se = warp_sum(u2);
-    const double mu = (sa - 1.0) / sb;  // kernel.rs:93
-    const double wl = u0 - mu * u1;     // weights
-    const double est = warp_sum(have ? wl * z : 0.0);
-    const double nu = se / sb;
-    const double lam = u2 - nu * u1;  // adjoint weights
-    const double resid = est - a.sv[si];
-    const double adj = have ? 2.0 * resid * lam : 0.0;
-    if (lane == 0) {
-      out[0] = resid * resid;
+    double sums[3] = {x0, x1, x2};
+    group_sum<NW, 3>(S, gid, wig, sums);
+    const double mu = (sums[0] - 1.0) / sums[1];  // kernel.rs:93
+    const double wl = x0 - mu * x1;               // weights
+    const double nu = sums[2] / sums[1];
+    const double lam = x2 - nu * x1;              // adjoint weights
+    double est[1] = {have ? wl * z : 0.0};
+    if (MIXED)
+      group_sum<NW, 1>(S, gid, wig, est);
+    else
+      est[0] = estimate;
+    const double resid = est[0] - (mean ? 0.0 : a.sv[si]);
+    const double adj = have ? (mean ? lam : 2.0 * resid * lam) : 0.0;
+    if (row == 0) {
+      out[0] = mean ? est[0] : resid * resid;
       out[1] = 1.0;
-      if (a.value) a.value[si] = est;
+      if (a.value) a.value[si] = est[0];
     }
     if (!a.want_grad) continue;
-    S.w[lane] = have ? wl : 0.0, S.adj[lane] = adj;
-    __syncwarp();
+    S.w[row] = have ? wl : 0.0, S.adj[row] = adj;
+    gsync<NW>(gid);
     double g[kMaxTheta];
 #pragma unroll
     for (int k = 0; k < kMaxTheta; ++k) g[k] = 0.0;
@@ -219,26 +318,26 @@ __global__ void __launch_bounds__(128) k_loo_grad(GradDev a) {
       for (int s = 0; s < ns; ++s) g[1 + s] += f;
       // Right-hand side c_j = C(|M (s_j - t)|).
       if (hc > 0.0) {
-        const double d[3] = {w0 - t[0], w1 - t[1], w2 - t[2]};
-        add_lag_terms(a, adj, hc, p, d, g);
+        add_lag_terms(a, adj, hc, pt, dt, g);
       } else {
         g[0] += adj;
         for (int s = 0; s < ns; ++s) g[1 + s] += adj;
       }
     }
-    for (int e = lane; e < E; e += R) {  // sample pairs (r > q)
-      int r, q;
-      tri_ij(e, r, q);
-      const double coef = -(S.adj[r] * S.w[q] + S.adj[q] * S.w[r]);
-      const double Md[3] = {S.P[r][0] - S.P[q][0], S.P[r][1] - S.P[q][1], S.P[r][2] - S.P[q][2]};
-      const double d[3] = {S.W[r][0] - S.W[q][0], S.W[r][1] - S.W[q][1], S.W[r][2] - S.W[q][2]};
-      const double h = sqrt(Md[0] * Md[0] + Md[1] * Md[1] + Md[2] * Md[2]);
-      if (h > 0.0) add_lag_terms(a, coef, h, Md, d, g);
+    for (int e = row; e < E; e += R) {  // sample pairs (p > q)
+      int p, q;
+      tri_index(e, p, q);
+      const double coef = -(S.adj[p] * S.w[q] + S.adj[q] * S.w[p]);
+      const double d[3] = {S.W[p][0] - S.W[q][0], S.W[p][1] - S.W[q][1], S.W[p][2] - S.W[q][2]};
+      double md[3];
+      frame_apply(a.vg, d, md);
+      const double h = norm3(md);
+      if (h > 0.0) add_lag_terms(a, coef, h, md, d, g);
     }
-    for (int k = 0; k < ntheta; ++k) {
-      const double v = warp_sum(g[k]);
-      if (lane == 0) out[2 + k] = v;
-    }
+    group_sum<NW, 8>(S, gid, wig, g);
+    group_sum<NW, kMaxTheta - 8>(S, gid, wig, g + 8);
+    if (row == 0)
+      for (int k = 0; k < ntheta; ++k) out[2 + k] = g[k];
   }
 }
 
@@ -256,22 +355,41 @@ __global__ void k_col_sums(int64_t n, int stride, const double* part, double* su
   if (threadIdx.x == 0) sums[blockIdx.x] = s[0];
 }
 
-}  // namespace
-
-cudaError_t launch_loo_grad(const Launch& L, const GradDev& a, double* sums) {
-  const size_t smem = sizeof(AdjSmem) * 4;
-  cudaError_t e = cudaFuncSetAttribute(k_loo_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+template <int NW, bool MIXED>
+cudaError_t run_grad(const Launch& L, const GradDev& a) {
+  using Sx = typename std::conditional<MIXED, GradSmemMixed<NW>, GradSmem<NW>>::type;
+  const size_t smem = sizeof(Sx) * (128 / (32 * NW));
+  auto kern = k_grad<NW, MIXED>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_loo_grad, 128, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem);
   if (e != cudaSuccess) return e;
   int64_t blocks = int64_t(L.sm_count) * (per_sm > 0 ? per_sm : 1);
-  const int64_t need = (a.n + 3) / 4;
+  const int64_t need = (a.n + (128 / (32 * NW)) - 1) / (128 / (32 * NW));
   if (blocks > need) blocks = need;
   if (blocks < 1) blocks = 1;
-  k_loo_grad<<<int(blocks), 128, smem, L.stream>>>(a);
+  kern<<<int(blocks), 128, smem, L.stream>>>(a);
+  ++*L.counter;
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_grad(const Launch& L, const GradDev& a0, double* sums, int rows, bool mixed) {
+  if (a0.n <= 0) return cudaSuccess;
+  GradDev a = a0;
+  a.list = nullptr, a.list_len = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (mixed) {
+    e = cudaMemsetAsync(a.redo_len, 0, sizeof(int64_t), L.stream);
+    if (e == cudaSuccess) e = rows > 32 ? run_grad<2, true>(L, a) : run_grad<1, true>(L, a);
+    a.list = a.redo, a.list_len = a.redo_len;  // what the mixed pass left, in FP64
+  }
+  if (e == cudaSuccess) e = rows > 32 ? run_grad<2, false>(L, a) : run_grad<1, false>(L, a);
+  if (e != cudaSuccess) return e;
   k_col_sums<<<a.stride, 256, 0, L.stream>>>(a.n, a.stride, a.part, sums);
-  *L.counter += 2;
+  ++*L.counter;
   return cudaGetLastError();
 }
 

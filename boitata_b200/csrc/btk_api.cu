@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "boitata_b200_measure.h"
 #include "btk_internal.h"
 
 namespace {
@@ -136,10 +137,6 @@ struct btk_ctx {
   double ppc = 2.0;  // samples per grid cell
 
   bool fitted = false;
-  // A host call in the mixed form that saw most of its systems go to the FP64
-  // re-solve (an ill-conditioned model) makes later host calls of this fit and
-  // search run the FP64 form directly (see mixed_precision_for).
-  bool mixed_to_fp64 = false;
   int64_t n = 0;
   bool has_err = false, planar = false;
   btk_search search{};
@@ -180,6 +177,13 @@ struct btk_ctx {
   DevBuf<int32_t> loo_cnt;
   DevBuf<int8_t> loo_sst;
   DevBuf<double> g_part, g_sums, g_val;
+  DevBuf<int64_t> g_redo;  // mixed form: systems left to the FP64 pass, and their count
+  // block-model neighbourhoods frozen for the mean-estimate gradient
+  int64_t mean_m = 0;
+  DevBuf<double> mean_txyz;
+  DevBuf<uint32_t> mean_nbr;
+  DevBuf<int32_t> mean_cnt;
+  DevBuf<int8_t> mean_sst;
 
   // pipelined host calls: copies in and out on their own streams
   cudaStream_t up = nullptr, down = nullptr;
@@ -818,6 +822,7 @@ int btk_set_tuning(btk_ctx* ctx, const btk_tuning* t) {
     if (ctx->fitted) {
       CK(cudaSetDevice(ctx->device));
       ctx->frozen = false;
+      ctx->mean_m = 0;
       int rc = index_samples(ctx);
       if (rc) return rc;
       CK(cudaStreamSynchronize(ctx->stream));
@@ -826,13 +831,19 @@ int btk_set_tuning(btk_ctx* ctx, const btk_tuning* t) {
   return BTK_OK;
 }
 
-int btk_graph_capture_geometry(btk_ctx* ctx, const btk_geometry* g, int32_t kind, double kparam,
-                               int32_t precision, const btk_outputs* d_out) {
-  int rc = need_fit(ctx);
-  if (rc) return rc;
+}  // extern "C"
+
+namespace {
+
+// Captures `call(stream)` (one prediction on the context's stream) into the
+// context's CUDA graph, replacing any earlier one. One plain call first sizes
+// every buffer and sets every kernel attribute, so the captured call
+// allocates nothing.
+template <class Call>
+int capture_graph(btk_ctx* ctx, Call call) {
   CK(cudaSetDevice(ctx->device));
-  // One plain call sizes every buffer and sets every kernel attribute first.
-  if ((rc = btk_predict_geometry_device(ctx, g, kind, kparam, precision, d_out, ctx->stream))) return rc;
+  int rc = call(ctx->stream);
+  if (rc) return rc;
   CK(cudaStreamSynchronize(ctx->stream));
   if (ctx->graph_exec) {
     CK(cudaGraphExecDestroy(ctx->graph_exec));
@@ -846,7 +857,7 @@ int btk_graph_capture_geometry(btk_ctx* ctx, const btk_geometry* g, int32_t kind
   ctx->timing = false;
   const int64_t before = ctx->launches;
   CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
-  rc = btk_predict_geometry_device(ctx, g, kind, kparam, precision, d_out, ctx->stream);
+  rc = call(ctx->stream);
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
   ctx->timing = timing;
@@ -860,6 +871,30 @@ int btk_graph_capture_geometry(btk_ctx* ctx, const btk_geometry* g, int32_t kind
   ctx->launches = before;
   CK(cudaGraphInstantiate(&ctx->graph_exec, graph, 0));
   return BTK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int btk_graph_capture_geometry(btk_ctx* ctx, const btk_geometry* g, int32_t kind, double kparam,
+                               int32_t precision, const btk_outputs* d_out) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  return capture_graph(ctx, [&](cudaStream_t s) {
+    return btk_predict_geometry_device(ctx, g, kind, kparam, precision, d_out, s);
+  });
+}
+
+int btk_graph_capture_device(btk_ctx* ctx, int64_t m, const double* d_xyz, const int8_t* d_kinds, int32_t kind,
+                             double kparam, int32_t precision, const btk_outputs* d_out) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if (m <= 0 || !d_xyz) return fail(ctx, BTK_EINVAL, "a captured prediction needs targets");
+  return capture_graph(ctx, [&](cudaStream_t s) {
+    return d_kinds ? btk_predict_kinds_device(ctx, m, d_xyz, d_kinds, kparam, precision, d_out, s)
+                   : btk_predict_device(ctx, m, d_xyz, kind, kparam, precision, d_out, s);
+  });
 }
 
 int btk_graph_launch(btk_ctx* ctx, void* stream) {
@@ -902,7 +937,6 @@ int btk_fit(btk_ctx* ctx, int64_t n, const double* xyz, const double* values, co
             const int64_t* holes, const btk_search* search, const btk_variogram* vg) {
   if (!ctx) return BTK_EINVAL;
   ctx->fitted = false;
-  ctx->mixed_to_fp64 = false;
   if (n <= 0 || !xyz || !values) return fail(ctx, BTK_EINVAL, "fit needs at least one sample with coordinates and values");
   if (n >= int64_t(0xffffffffu)) return fail(ctx, BTK_EINVAL, "too many samples");
   int rc = check_vg(ctx, vg);
@@ -919,6 +953,7 @@ int btk_fit(btk_ctx* ctx, int64_t n, const double* xyz, const double* values, co
   CK(cudaSetDevice(ctx->device));
   ctx->n = n;
   ctx->frozen = false;
+  ctx->mean_m = 0;
   ctx->search = *search;
   ctx->vg = *vg;
   ctx->has_err = err_var != nullptr;
@@ -957,8 +992,8 @@ int btk_set_search(btk_ctx* ctx, const btk_search* search) {
   if ((rc = check_search(ctx, search))) return rc;
   CK(cudaSetDevice(ctx->device));
   ctx->search = *search;
-  ctx->mixed_to_fp64 = false;
   ctx->frozen = false;
+  ctx->mean_m = 0;
   if ((rc = index_samples(ctx))) return rc;
   CK(cudaStreamSynchronize(ctx->stream));
   return BTK_OK;
@@ -982,28 +1017,8 @@ namespace {
 // out overlap chunk c's search and solve. Each chunk is a run_path of its own over the
 // context's scratch, which the compute stream serialises; chunks write
 // disjoint slices of the staged inputs and outputs.
-// On an ill-conditioned model the FP32 factor fails for most systems, and the
-// mixed form then pays for the FP32 attempt and the FP64 re-solve of each. A
-// host call of the mixed form whose re-solves exceeded half of its m targets
-// marks the context, and its later host calls (until the next fit or search)
-// take the FP64 form: the re-solve is that form, so those systems get the
-// same bits, and the rest get FP64 results in place of mixed ones. Device
-// calls and captured graphs keep the precision they are given.
-int32_t mixed_precision_for(btk_ctx* ctx, int32_t precision) {
-  return precision == BTK_MIXED && ctx->mixed_to_fp64 ? BTK_FP64 : precision;
-}
-
-int note_mixed_outcome(btk_ctx* ctx, int32_t precision, int64_t m) {
-  if (precision != BTK_MIXED || m <= 0) return BTK_OK;
-  int64_t redo[2] = {0, 0};
-  CK(cudaMemcpy(redo, ctx->redo_len.p, sizeof(redo), cudaMemcpyDeviceToHost));
-  if (2 * (redo[0] + redo[1]) > m) ctx->mixed_to_fp64 = true;
-  return BTK_OK;
-}
-
 int predict_host(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds, int32_t kind, double kparam,
                  int32_t precision, const btk_outputs* out, const btk_diagnostics* diag = nullptr) {
-  precision = mixed_precision_for(ctx, precision);
   int64_t chunk = ctx->tuning.host_chunk > 0 ? int64_t(ctx->tuning.host_chunk) : m;
   if ((m + chunk - 1) / chunk > 8) chunk = (m + 7) / 8;
   const int64_t nc = (m + chunk - 1) / chunk;
@@ -1072,7 +1087,7 @@ int predict_host(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds
   }
   CK(cudaStreamSynchronize(ctx->down));
   CK(cudaStreamSynchronize(ctx->stream));
-  return nc == 1 ? note_mixed_outcome(ctx, precision, m) : BTK_OK;
+  return BTK_OK;
 }
 
 }  // namespace
@@ -1239,12 +1254,10 @@ int btk_cross_validate(btk_ctx* ctx, int32_t kind, double kparam, int32_t precis
   CK(cudaSetDevice(ctx->device));
   btk_outputs d{};
   if ((rc = host_outputs(ctx, ctx->n, out, &d))) return rc;
-  precision = mixed_precision_for(ctx, precision);
   if ((rc = run_path(ctx, nullptr, ctx->n, ctx->x.p, ctx->y.p, ctx->z.p, ctx->loo_perm.p, ctx->n, 1, kind, kparam,
                      precision, &d)))
     return rc;
-  if ((rc = copy_out(ctx, ctx->n, &d, out))) return rc;
-  return note_mixed_outcome(ctx, precision, ctx->n);
+  return copy_out(ctx, ctx->n, &d, out);
 }
 
 int btk_neighbors(btk_ctx* ctx, int64_t m, const double* xyz, int32_t loo, int64_t* idx, int32_t* count, int8_t* ok) {
@@ -1281,8 +1294,8 @@ int btk_neighbors(btk_ctx* ctx, int64_t m, const double* xyz, int32_t loo, int64
 int btk_loo_freeze(btk_ctx* ctx) {
   int rc = need_fit(ctx);
   if (rc) return rc;
-  if (ctx->search.max_samples > 32)
-    return fail(ctx, BTK_EUNSUPPORTED, "the leave-one-out gradient takes at most 32 samples per system");
+  if (ctx->search.max_samples > kMaxN)
+    return fail(ctx, BTK_EUNSUPPORTED, "the leave-one-out gradient takes at most 64 samples per system");
   if (ctx->search.calibration)
     return fail(ctx, BTK_EUNSUPPORTED, "the leave-one-out gradient takes an uncalibrated search");
   CK(cudaSetDevice(ctx->device));
@@ -1300,21 +1313,29 @@ int btk_loo_freeze(btk_ctx* ctx) {
 
 namespace {
 
-// Sums over the frozen leave-one-out systems first .. first + count - 1:
-// sums[0] = squared-error sum, sums[1] = systems in the loss, sums[2 + k] =
-// gradient sum of parameter k. values (full length n, or null) gets the
-// range's leave-one-out estimates.
-int loo_sums(btk_ctx* ctx, const btk_variogram* vg, int64_t first, int64_t count, int32_t want_grad,
-             std::vector<double>& sums, double* values) {
+enum Objective { kLeaveOneOut = 0, kBlockMean = 1 };
+
+// Sums over the frozen systems first .. first + count - 1 of an objective
+// (leave-one-out loss or block-model mean estimate): sums[0] = objective sum,
+// sums[1] = systems in it, sums[2 + k] = gradient sum of parameter k.
+// values (full length, or null) gets the range's estimates.
+int objective_sums(btk_ctx* ctx, Objective which, const btk_variogram* vg, int64_t first, int64_t count,
+                   int32_t want_grad, int32_t precision, std::vector<double>& sums, double* values) {
   int rc = need_fit(ctx);
   if (rc) return rc;
-  if (!ctx->frozen) return fail(ctx, BTK_EINVAL, "call btk_loo_freeze first");
+  const bool mean = which == kBlockMean;
+  const char* what = mean ? "the mean-estimate gradient" : "the leave-one-out gradient";
+  if (mean ? ctx->mean_m <= 0 : !ctx->frozen)
+    return fail(ctx, BTK_EINVAL, mean ? "call btk_mean_freeze first" : "call btk_loo_freeze first");
+  if (precision != BTK_FP64 && precision != BTK_MIXED) return fail(ctx, BTK_EINVAL, "unknown precision");
   if ((rc = check_vg(ctx, vg))) return rc;
   for (int k = 0; k < vg->nstruct; ++k)
     if (vg->s[k].model == BTK_POWER)
-      return fail(ctx, BTK_EUNSUPPORTED, "the leave-one-out gradient takes stationary variograms (no power structure)");
-  if (first < 0 || count < 0 || first + count > ctx->n)
-    return fail(ctx, BTK_EINVAL, "the range must lie within the fitted samples");
+      return fail(ctx, BTK_EUNSUPPORTED, std::string(what) + " takes stationary variograms (no power structure)");
+  const int64_t total = mean ? ctx->mean_m : ctx->n;
+  if (first < 0 || count < 0 || first + count > total)
+    return fail(ctx, BTK_EINVAL, mean ? "the range must lie within the frozen targets"
+                                      : "the range must lie within the fitted samples");
   CK(cudaSetDevice(ctx->device));
   btk_variogram v = *vg;
   if (!v.aniso.on) v.aniso = btk_aniso{1, 0.0, 0.0, 0.0, 1.0, 1.0, 1.0};  // isotropic, as a point of theta
@@ -1324,7 +1345,12 @@ int loo_sums(btk_ctx* ctx, const btk_variogram* vg, int64_t first, int64_t count
   const int ntheta = 1 + 2 * v.nstruct + 5;
   a.sx = ctx->x.p, a.sy = ctx->y.p, a.sz = ctx->z.p, a.sv = ctx->v.p, a.se = ctx->has_err ? ctx->e.p : nullptr;
   a.twin = ctx->twin.p;
-  a.nbr = ctx->loo_nbr.p, a.count = ctx->loo_cnt.p, a.sstatus = ctx->loo_sst.p;
+  if (mean) {
+    a.tx = ctx->mean_txyz.p, a.ty = ctx->mean_txyz.p + total, a.tz = ctx->mean_txyz.p + 2 * total;
+    a.nbr = ctx->mean_nbr.p, a.count = ctx->mean_cnt.p, a.sstatus = ctx->mean_sst.p;
+  } else {
+    a.nbr = ctx->loo_nbr.p, a.count = ctx->loo_cnt.p, a.sstatus = ctx->loo_sst.p;
+  }
   a.max_samples = int(ctx->search.max_samples);
   a.first = first;
   a.n = count;
@@ -1335,13 +1361,17 @@ int loo_sums(btk_ctx* ctx, const btk_variogram* vg, int64_t first, int64_t count
   CK(ctx->g_part.grow(size_t(count) * size_t(a.stride)));
   CK(ctx->g_sums.grow(size_t(a.stride)));
   a.part = ctx->g_part.p;
+  if (precision == BTK_MIXED) {
+    CK(ctx->g_redo.grow(size_t(count) + 1));
+    a.redo_len = ctx->g_redo.p, a.redo = ctx->g_redo.p + 1;
+  }
   if (values) {
-    CK(ctx->g_val.grow(size_t(ctx->n)));
+    CK(ctx->g_val.grow(size_t(total)));
     a.value = ctx->g_val.p;
   }
   Launch L = ctx->launch(nullptr);
   ctx->mark(0, L.stream);
-  CK(launch_loo_grad(L, a, ctx->g_sums.p));
+  CK(launch_grad(L, a, ctx->g_sums.p, ctx->search.max_samples > 32 ? 64 : 32, precision == BTK_MIXED));
   ctx->mark(1, L.stream);
   ctx->mark(2, L.stream);
   ctx->mark(3, L.stream);
@@ -1353,28 +1383,88 @@ int loo_sums(btk_ctx* ctx, const btk_variogram* vg, int64_t first, int64_t count
   return BTK_OK;
 }
 
-}  // namespace
-
-int btk_loo_gradient(btk_ctx* ctx, const btk_variogram* vg, int32_t want_grad, double* loss, double* grad,
-                     int64_t* n_valid, double* values) {
-  if (!loss) return fail(ctx, BTK_EINVAL, "loss is required");
-  std::vector<double> sums;
-  const int rc = loo_sums(ctx, vg, 0, ctx ? ctx->n : 0, want_grad, sums, values);
-  if (rc) return rc;
+int finish_objective(const std::vector<double>& sums, int32_t want_grad, double* obj, double* grad,
+                     int64_t* n_valid) {
   const int ntheta = int(sums.size()) - 2;
   const double cnt = sums[1];
-  *loss = cnt > 0 ? sums[0] / cnt : NAN;
+  *obj = cnt > 0 ? sums[0] / cnt : NAN;
   if (n_valid) *n_valid = int64_t(cnt);
   if (grad && want_grad)
     for (int k = 0; k < ntheta; ++k) grad[k] = cnt > 0 ? sums[2 + k] / cnt : NAN;
   return BTK_OK;
 }
 
+}  // namespace
+
+int btk_loo_gradient(btk_ctx* ctx, const btk_variogram* vg, int32_t want_grad, int32_t precision, double* loss,
+                     double* grad, int64_t* n_valid, double* values) {
+  if (!loss) return fail(ctx, BTK_EINVAL, "loss is required");
+  std::vector<double> sums;
+  const int rc = objective_sums(ctx, kLeaveOneOut, vg, 0, ctx ? ctx->n : 0, want_grad, precision, sums, values);
+  if (rc) return rc;
+  return finish_objective(sums, want_grad, loss, grad, n_valid);
+}
+
 int btk_loo_gradient_range(btk_ctx* ctx, const btk_variogram* vg, int64_t first, int64_t count, int32_t want_grad,
-                           double* sums) {
+                           int32_t precision, double* sums) {
   if (!sums) return fail(ctx, BTK_EINVAL, "sums is required");
   std::vector<double> s;
-  const int rc = loo_sums(ctx, vg, first, count, want_grad, s, nullptr);
+  const int rc = objective_sums(ctx, kLeaveOneOut, vg, first, count, want_grad, precision, s, nullptr);
+  if (rc) return rc;
+  for (size_t k = 0; k < s.size(); ++k) sums[k] = (k < 2 || want_grad) ? s[k] : 0.0;
+  return BTK_OK;
+}
+
+int btk_mean_freeze(btk_ctx* ctx, const btk_geometry* g) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if (!g) return fail(ctx, BTK_EINVAL, "geometry is required");
+  for (int a = 0; a < 3; ++a) {
+    if (!(g->size[a] > 0.0 && fin(g->size[a]))) return fail(ctx, BTK_EINVAL, "cell sizes must be positive");
+    if (g->count[a] <= 0) return fail(ctx, BTK_EINVAL, "cell counts must be positive");
+    if (!fin(g->origin[a]) || !fin(g->rotation[a])) return fail(ctx, BTK_EINVAL, "origin and rotation must be finite");
+  }
+  if (ctx->search.max_samples > kMaxN)
+    return fail(ctx, BTK_EUNSUPPORTED, "the mean-estimate gradient takes at most 64 samples per system");
+  if (ctx->search.calibration)
+    return fail(ctx, BTK_EUNSUPPORTED, "the mean-estimate gradient takes an uncalibrated search");
+  CK(cudaSetDevice(ctx->device));
+  const int64_t m = g->count[0] * g->count[1] * g->count[2];
+  const int* tw = ctx->tuning.tile;
+  const int64_t tiles = ((g->count[0] + tw[0] - 1) / tw[0]) * ((g->count[1] + tw[1] - 1) / tw[1]) *
+                        ((g->count[2] + tw[2] - 1) / tw[2]);
+  const int64_t nwork = tiles * 32;
+  ctx->mean_m = 0;
+  CK(ctx->mean_txyz.grow(3 * size_t(m)));
+  CK(ctx->mean_nbr.grow(size_t(m) * size_t(ctx->search.max_samples)));
+  CK(ctx->mean_cnt.grow(size_t(m)));
+  CK(ctx->mean_sst.grow(size_t(m)));
+  CK(ctx->perm.grow(size_t(nwork)));
+  Launch L = ctx->launch(nullptr);
+  double* t = ctx->mean_txyz.p;
+  CK(launch_centroids(L, *g, transposed_frame(*g), 0, nwork, t, t + m, t + 2 * m, ctx->perm.p));
+  CK(launch_search(L, ctx->spd, ctx->gd, t, t + m, t + 2 * m, ctx->perm.p, nwork, 0, ctx->mean_nbr.p,
+                   ctx->mean_cnt.p, ctx->mean_sst.p));
+  CK(cudaStreamSynchronize(L.stream));
+  ctx->mean_m = m;
+  return BTK_OK;
+}
+
+int btk_mean_gradient(btk_ctx* ctx, const btk_variogram* vg, int32_t want_grad, int32_t precision, double* mean,
+                      double* grad, int64_t* n_valid, double* values) {
+  if (!mean) return fail(ctx, BTK_EINVAL, "mean is required");
+  std::vector<double> sums;
+  const int rc =
+      objective_sums(ctx, kBlockMean, vg, 0, ctx ? ctx->mean_m : 0, want_grad, precision, sums, values);
+  if (rc) return rc;
+  return finish_objective(sums, want_grad, mean, grad, n_valid);
+}
+
+int btk_mean_gradient_range(btk_ctx* ctx, const btk_variogram* vg, int64_t first, int64_t count, int32_t want_grad,
+                            int32_t precision, double* sums) {
+  if (!sums) return fail(ctx, BTK_EINVAL, "sums is required");
+  std::vector<double> s;
+  const int rc = objective_sums(ctx, kBlockMean, vg, first, count, want_grad, precision, s, nullptr);
   if (rc) return rc;
   for (size_t k = 0; k < s.size(); ++k) sums[k] = (k < 2 || want_grad) ? s[k] : 0.0;
   return BTK_OK;

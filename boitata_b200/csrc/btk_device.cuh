@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "btk_internal.h"
+#include "btk_turn.cuh"
 
 namespace btk {
 
@@ -44,19 +45,15 @@ __device__ __forceinline__ int sector_of(const double* axes, int planar, const d
 
 // Sector of sample w around target t under a search's balancing
 // (search.rs:428-441): plane sectors by the turn of the offset in the search
-// frame, else the octant or quadrant.
+// frame (btk_turn.cuh: the reference's arithmetic, with a correctly rounded
+// atan2 where the last bit could move the sample across a boundary), else
+// the octant or quadrant.
 __device__ __forceinline__ int search_sector(const SearchDev& sp, const double w[3], const double t[3]) {
   if (!sp.plane) return sector_of(sp.axes, sp.planar, w, t);
   const double v[3] = {xsub(w[0], t[0]), xsub(w[1], t[1]), xsub(w[2], t[2])};
   double d[3];
   mulv_exact(sp.axes, v, d);
-  constexpr double kTau = 6.283185307179586;
-  double turn = atan2(-d[0], d[1]);
-  turn = fmod(turn, kTau);
-  if (turn < 0.0) turn += kTau;
-  const double x = turn / kTau * double(sp.plane);
-  const int k = x > 0.0 ? int(x) : 0;  // `as usize`: NaN and negatives to 0
-  return k < sp.plane - 1 ? k : sp.plane - 1;
+  return turn::plane_sector(d[0], d[1], sp.plane);
 }
 
 // ---- variogram (crates/variogram/src/model.rs:76-126, composite.rs:69-85) ----

@@ -94,6 +94,11 @@ struct SolveDev {
   const uint32_t* nbr;                   // [target][max_samples]
   const int32_t* count;
   const int8_t* sstatus;
+  // Caller-supplied lists (btk_solve_noalloc): > 0, the number of samples;
+  // the pair-testing kernels then check every neighbour index against it and
+  // every count against max_samples, and fail the system (BTK_ST_INVALID)
+  // instead of reading past the caller's buffers. 0: lists from the search.
+  int64_t nsamples;
   const int64_t* list;      // systems of this bucket (target indices), or null for 0..m-1
   const int64_t* list_len;  // device count of `list`
   int64_t m;
@@ -133,22 +138,29 @@ struct TileDev {
   int64_t *redo, *redo_len;    // mixed form: systems left to the FP64 re-solve
 };
 
-// Leave-one-out loss and gradient over frozen neighbourhoods (btk_adjoint.cu).
+// A kriging objective and its gradient over frozen neighbourhoods
+// (btk_adjoint.cu): the leave-one-out loss (system i is the fitted sample
+// first + i, kriged from its leave-one-out list) or the mean estimate of a
+// block model (system i is the target first + i).
 struct GradDev {
   VgDev vg;         // the variogram at theta; vg.frame = M(theta), always set
   double dM[5][9];  // dM/d(semi, minor, azimuth, dip, rake), degrees for angles
   const double *sx, *sy, *sz, *sv, *se;
   const uint8_t* twin;
+  const double *tx, *ty, *tz;  // mean objective: the targets; null: leave-one-out
   const uint32_t* nbr;
   const int32_t* count;
   const int8_t* sstatus;
   int max_samples;
-  int64_t first;  // systems first .. first + n - 1 (the left-out samples)
+  int64_t first;  // systems first .. first + n - 1
   int64_t n;
+  const int64_t* list;      // FP64 pass over the systems the mixed pass left (offsets i), or null: all n
+  const int64_t* list_len;
+  int64_t *redo, *redo_len;  // mixed pass: systems left to the FP64 pass
   int want_grad;
   int stride;     // 2 + number of parameters
-  double* part;   // [n][stride]: loss term, valid flag, gradient terms
-  double* value;  // leave-one-out estimates, or null
+  double* part;   // [n][stride]: objective term, valid flag, gradient terms
+  double* value;  // the systems' estimates (indexed first + i), or null
 };
 
 // ---- launchers (each returns the launch's error, if any) ----
@@ -256,8 +268,11 @@ cudaError_t launch_sgs_commit(const Launch& L, int64_t nwork, const int64_t* lis
 // weights and only a.negw / a.mdist / a.nholes are written.
 cudaError_t launch_solve_lu(const Launch& L, const SolveDev& a, int kmax, bool diag = false);
 
-// Leave-one-out loss and gradient; sums[stride] receives the column sums.
-cudaError_t launch_loo_grad(const Launch& L, const GradDev& a, double* sums);
+// Objective and gradient of systems of at most `rows` (32 or 64) samples,
+// FP64 or mixed (FP32 factorisation with FP64 refinement; the systems it
+// does not converge on are redone in FP64, so a.redo must hold a.n entries
+// and a.redo_len one); sums[stride] receives the column sums of a.part.
+cudaError_t launch_grad(const Launch& L, const GradDev& a, double* sums, int rows, bool mixed);
 
 // Checks a variogram as btk_fit does and fills its device form; on failure
 // returns a BTK_E* code with the reason in *why.

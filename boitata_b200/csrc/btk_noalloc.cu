@@ -7,7 +7,6 @@
 // factorisation leaves to FP64 and its count, lives in the static device
 // array below instead of a cudaMalloc'd buffer.
 #include <cstdio>
-#include <mutex>
 #include <string>
 
 #include "btk_internal.h"
@@ -23,23 +22,19 @@ using btk::VgDev;
 // library, held until the process exits; every call shares it.
 static __device__ __align__(256) int64_t g_redo[BTK_NOALLOC_MAX_SYSTEMS + 1];
 
-constexpr int kMaxDevices = 256;
-std::mutex g_lock;
-int64_t* g_redo_addr[kMaxDevices] = {};
-
-// Device address of g_redo on the current device, looked up once per device.
-// In host code g_redo names a host-side stand-in, not device memory, so the
-// kernels only ever receive the address from cudaGetSymbolAddress.
-cudaError_t scratch_on(int device, int64_t** out) {
-  std::lock_guard<std::mutex> hold(g_lock);
-  if (!g_redo_addr[device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_redo);
-    if (e != cudaSuccess) return e;
-    g_redo_addr[device] = static_cast<int64_t*>(p);
-  }
-  *out = g_redo_addr[device];
-  return cudaSuccess;
+// Device address of g_redo in the current context. In host code g_redo names
+// a host-side stand-in, not device memory, so the kernels only ever receive
+// the address cudaGetSymbolAddress gives. The address belongs to one CUDA
+// context (one load of this module), so it is looked up on every call rather
+// than cached: a call from another context on the same device, or after a
+// cudaDeviceReset, gets that context's own array. The lookup is cheap once
+// the module is loaded; the first one in a context loads it, which is why the
+// first call there should come before any stream capture.
+cudaError_t scratch_here(int64_t** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_redo);
+  if (e == cudaSuccess) *out = static_cast<int64_t*>(p);
+  return e;
 }
 
 int say(char* err, size_t errlen, int code, const std::string& msg) {
@@ -51,8 +46,8 @@ int say(char* err, size_t errlen, int code, const std::string& msg) {
 
 extern "C" int btk_solve_noalloc(int device, const btk_variogram* vg, int32_t kind, double kparam,
                                  const double* d_x, const double* d_y, const double* d_z, const double* d_values,
-                                 const double* d_err, int64_t m, const double* d_tx, const double* d_ty,
-                                 const double* d_tz, const uint32_t* d_nbr, int32_t max_samples,
+                                 const double* d_err, int64_t n_samples, int64_t m, const double* d_tx,
+                                 const double* d_ty, const double* d_tz, const uint32_t* d_nbr, int32_t max_samples,
                                  const int32_t* d_count, const int8_t* d_status, const btk_outputs* d_out,
                                  void* stream, char* err, size_t errlen) {
   if (m < 0 || m > BTK_NOALLOC_MAX_SYSTEMS)
@@ -65,7 +60,10 @@ extern "C" int btk_solve_noalloc(int device, const btk_variogram* vg, int32_t ki
   if (!d_x || !d_y || !d_z || !d_values || !d_nbr || !d_count || !d_status || !d_out || !d_out->value ||
       (m > 0 && (!d_tx || !d_ty || !d_tz)))
     return say(err, errlen, BTK_EINVAL, "every input and the value output must be device pointers");
-  if (device < 0 || device >= kMaxDevices) return say(err, errlen, BTK_EINVAL, "device index out of range");
+  if (n_samples < 1 || n_samples > int64_t(UINT32_MAX))
+    return say(err, errlen, BTK_EINVAL,
+               "n_samples must be the number of samples behind d_x .. d_values (1 .. 2^32 - 1)");
+  if (device < 0) return say(err, errlen, BTK_EINVAL, "device index out of range");
   VgDev vgd{};
   std::string why;
   int rc = btk::prepare_variogram(vg, &vgd, &why);
@@ -78,7 +76,7 @@ extern "C" int btk_solve_noalloc(int device, const btk_variogram* vg, int32_t ki
   cudaError_t e = cudaGetDevice(&before);
   if (e == cudaSuccess && before != device) e = cudaSetDevice(device);
   int64_t* scratch = nullptr;
-  if (e == cudaSuccess) e = scratch_on(device, &scratch);
+  if (e == cudaSuccess) e = scratch_here(&scratch);
   int sm = 0;
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, device);
   int64_t launches = 0;
@@ -92,6 +90,7 @@ extern "C" int btk_solve_noalloc(int device, const btk_variogram* vg, int32_t ki
   a.twin = nullptr;  // the pair-testing kernels check each system themselves
   a.tx = d_tx, a.ty = d_ty, a.tz = d_tz;
   a.nbr = d_nbr, a.count = d_count, a.sstatus = d_status;
+  a.nsamples = n_samples;  // every index and count is checked against the caller's buffers
   a.m = m;
   a.value = d_out->value, a.variance = d_out->variance, a.lagrange = d_out->lagrange;
   a.n_used = d_out->n_used, a.status = d_out->status;

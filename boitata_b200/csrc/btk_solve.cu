@@ -25,19 +25,21 @@
 //
 // Mixed form: the same assembly (FP64), an FP32 LDL^T with fused forward
 // substitution and an FP32 back substitution give approximate solutions
-// x_v; FP64 residuals r_v = v - C x_v (C from the FP64 triangle) correct the
-// forms to u^T x_v + x_u^T r_v, whose error is second order in the
-// residuals. The Lagrange multiplier and the variance are then formed in
-// FP64. A system whose FP32 pivots fall below 1e-5 C0 or whose residual is
-// large goes to an FP64 re-solve list (status flag BTK_ST_FP64_FALLBACK).
+// x_v; FP64 residuals r_v = v - C x_v (C from the FP64 triangle) drive up to
+// three steps of iterative refinement (x_v += C~^-1 r_v with the stored FP32
+// factors) until the corrected forms u^T x_v + x_u^T r_v, whose error is
+// second order in the residuals, are good to about 1e-8 C0. The Lagrange
+// multiplier and the variance are then formed in FP64. A system whose FP32
+// factorisation breaks down (a pivot NaN or not positive) or whose
+// refinement does not converge goes to an FP64 re-solve list (status flag
+// BTK_ST_FP64_FALLBACK), which also takes the singular decision.
 #include <cstddef>
 
 #include "btk_device.cuh"
+#include "btk_group.cuh"
 
 namespace btk {
 namespace {
-
-constexpr unsigned kFull = 0xffffffffu;
 
 // 16-byte aligned, with a size a multiple of 16, so every group's column line
 // takes 16-byte (double2) loads.
@@ -68,64 +70,6 @@ struct MixedSmem {
   float L[R][R + 1];
   double xs[3][R];
 };
-
-template <int NW>
-__device__ __forceinline__ void gsync(int gid) {
-  if (NW == 1)
-    __syncwarp();
-  else
-    asm volatile("bar.sync %0, %1;" ::"r"(gid + 1), "r"(NW * 32) : "memory");
-}
-
-template <int NW>
-__device__ __forceinline__ bool group_any(SolveSmem<NW>& S, int gid, int wig, bool pred) {
-  int v = __any_sync(kFull, pred);
-  if (NW == 1) return v != 0;
-  if ((threadIdx.x & 31) == 0) S.ired[wig] = v;
-  gsync<NW>(gid);
-  int all = 0;
-#pragma unroll
-  for (int w = 0; w < NW; ++w) all |= S.ired[w];
-  gsync<NW>(gid);
-  return all != 0;
-}
-
-// Sums of five values over the group, returned on every lane.
-template <int NW>
-__device__ __forceinline__ void group_sum5(SolveSmem<NW>& S, int gid, int wig, double v[5]) {
-#pragma unroll
-  for (int q = 0; q < 5; ++q)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(kFull, v[q], o);
-  if (NW == 1) return;
-  if ((threadIdx.x & 31) == 0)
-#pragma unroll
-    for (int q = 0; q < 5; ++q) S.red[wig][q] = v[q];
-  gsync<NW>(gid);
-#pragma unroll
-  for (int q = 0; q < 5; ++q) {
-    double s = 0.0;
-#pragma unroll
-    for (int w = 0; w < NW; ++w) s += S.red[w][q];
-    v[q] = s;
-  }
-  gsync<NW>(gid);
-}
-
-// Maximum of one value over the group, on every lane.
-template <int NW>
-__device__ __forceinline__ double group_max(SolveSmem<NW>& S, int gid, int wig, double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o));
-  if (NW == 1) return v;
-  if ((threadIdx.x & 31) == 0) S.red[wig][7] = v;
-  gsync<NW>(gid);
-  double m = S.red[0][7];
-#pragma unroll
-  for (int w = 1; w < NW; ++w) m = fmax(m, S.red[w][7]);
-  gsync<NW>(gid);
-  return m;
-}
 
 // Coincident guard on one lane (coincident.rs:27-82): samples within 1e-6 m
 // of a cluster's first member join it; each cluster becomes one datum at the
@@ -195,18 +139,31 @@ __device__ __forceinline__ bool assemble(const SolveDev& a, SolveSmem<NW>& S, in
     if (row == 0) write_fail(a, ti, st != BTK_ST_OK ? st : (n > R ? BTK_ST_UNSUPPORTED : BTK_ST_SEARCH_FAILED), 0);
     return false;
   }
+  // A caller's list longer than its row: nothing of it is read.
+  if (kPairs && a.nsamples > 0 && n > a.max_samples) {
+    if (row == 0) write_fail(a, ti, BTK_ST_INVALID, 0);
+    return false;
+  }
   const double t[3] = {a.tx[ti], a.ty[ti], a.tz[ti]};
   have = row < n;
   double w[3] = {0, 0, 0};
   double z = 0.0;
   err = 0.0;
   int tw = 0;
+  bool bad = false;
   if (have) {
     const uint32_t j = a.nbr[ti * a.max_samples + row];
-    w[0] = a.sx[j], w[1] = a.sy[j], w[2] = a.sz[j];
-    z = a.sv[j];
-    if (a.se) err = a.se[j];
-    if (!kPairs) tw = a.twin[j];
+    bad = kPairs && a.nsamples > 0 && int64_t(j) >= a.nsamples;
+    if (!bad) {
+      w[0] = a.sx[j], w[1] = a.sy[j], w[2] = a.sz[j];
+      z = a.sv[j];
+      if (a.se) err = a.se[j];
+      if (!kPairs) tw = a.twin[j];
+    }
+  }
+  if (kPairs && a.nsamples > 0 && group_any<NW>(S, gid, wig, bad)) {  // an index past the caller's samples
+    if (row == 0) write_fail(a, ti, BTK_ST_INVALID, 0);
+    return false;
   }
   zf = kind_f(kind, a.kparam, z);
   nn = n;
@@ -245,40 +202,6 @@ __device__ __forceinline__ bool assemble(const SolveDev& a, SolveSmem<NW>& S, in
   return true;
 }
 
-// Pivots k0 .. k1-1 of the FP64 right-looking LDL^T with the forward
-// substitution of y fused in, the row kept shifted so that slot 0 holds the
-// current pivot column: a step writes it to the group's line, then
-// A[q] <- A[q+1] - f col[q] over the W slots that can still hold live
-// columns. The loop body is the same for every k, so it is a runtime loop
-// and A stays in registers.
-template <int NW, int W>
-__device__ __forceinline__ void eliminate_rows(double (&A)[32 * NW], int k0, int k1, int row, SolveSmem<NW>& S,
-                                               int gid, double& y0, double& y1, double& y2, double& dme, bool& sing,
-                                               double thr) {
-  constexpr int R = 32 * NW;
-  for (int k = k0; k < k1; ++k) {
-    const int b = k & 1;
-    S.col[b][row > k ? row - k - 1 : (row == k ? R : R + 1)] = A[0];
-    if (row == k) S.rhs[b][0] = y0, S.rhs[b][1] = y1, S.rhs[b][2] = y2;
-    gsync<NW>(gid);
-    const double d = S.col[b][R];
-    if (!(d > thr)) {  // NaN or at most 1e-12 C0 (kernel.rs:61); uniform over the group
-      sing = true;
-      return;
-    }
-    if (row == k) dme = d;
-    const double f = row > k ? A[0] * (1.0 / d) : 0.0;
-#pragma unroll
-    for (int q = 0; q < W; q += 2) {
-      const double2 cv = *reinterpret_cast<const double2*>(&S.col[b][q]);
-      A[q] = fma(-f, cv.x, A[q + 1]);
-      A[q + 1] = q + 2 < R ? fma(-f, cv.y, A[q + 2]) : 0.0;
-    }
-    y0 = fma(-f, S.rhs[b][0], y0);
-    y1 = fma(-f, S.rhs[b][1], y1);
-    y2 = fma(-f, S.rhs[b][2], y2);
-  }
-}
 
 template <int NW, bool kPairs = false>
 __global__ void __launch_bounds__(128) k_solve64(SolveDev a, int8_t flag) {
@@ -324,40 +247,11 @@ __global__ void __launch_bounds__(128) k_solve64(SolveDev a, int8_t flag) {
   }
 }
 
-// The FP32 form of eliminate_rows: the multiplier of row i at step k goes to
-// L[i][k] for the back substitution, and a pivot at most thr (1e-5 C0) or NaN
-// leaves the system to the FP64 form.
-template <int NW, int W>
-__device__ __forceinline__ void eliminate_rows_f32(float (&A)[32 * NW], int k0, int k1, int row, MixedSmem<NW>& X,
-                                                   int gid, float& y0, float& y1, float& y2, float& dme, bool& weak,
-                                                   float thr) {
-  constexpr int R = 32 * NW;
-  for (int k = k0; k < k1; ++k) {
-    const int b = k & 1;
-    X.colf[b][row > k ? row - k - 1 : (row == k ? R : R + 1)] = A[0];
-    if (row == k) X.rhsf[b][0] = y0, X.rhsf[b][1] = y1, X.rhsf[b][2] = y2;
-    gsync<NW>(gid);
-    const float d = X.colf[b][R];
-    if (!(d > thr)) {  // uniform over the group
-      weak = true;
-      return;
-    }
-    if (row == k) dme = d;
-    const float f = row > k ? A[0] * __frcp_rn(d) : 0.f;
-    if (row > k) X.L[row][k] = f;
-#pragma unroll
-    for (int q = 0; q < W; q += 4) {
-      const float4 cv = *reinterpret_cast<const float4*>(&X.colf[b][q]);
-      A[q] = fmaf(-f, cv.x, A[q + 1]);
-      A[q + 1] = fmaf(-f, cv.y, A[q + 2]);
-      A[q + 2] = fmaf(-f, cv.z, A[q + 3]);
-      A[q + 3] = q + 4 < R ? fmaf(-f, cv.w, A[q + 4]) : 0.f;
-    }
-    y0 = fmaf(-f, X.rhsf[b][0], y0);
-    y1 = fmaf(-f, X.rhsf[b][1], y1);
-    y2 = fmaf(-f, X.rhsf[b][2], y2);
-  }
-}
+
+
+// Iterative refinement: at most this many FP32 corrections after the first
+// solve; each takes its residual in FP64 from the FP64 triangle.
+constexpr int kRefineSteps = 3;
 
 template <int NW, bool kPairs = false>
 __global__ void __launch_bounds__(128) k_solve_mixed(SolveDev a, int64_t* redo, int64_t* redo_len) {
@@ -369,7 +263,6 @@ __global__ void __launch_bounds__(128) k_solve_mixed(SolveDev a, int64_t* redo, 
   SolveSmem<NW>& S = X.base;
   const int64_t nitems = a.list ? *a.list_len : a.m;
   const double c0 = a.vg.c0;
-  const float c0f = float(c0);
   for (int64_t item = int64_t(blockIdx.x) * GROUPS + gid; item < nitems; item += int64_t(gridDim.x) * GROUPS) {
     const int64_t ti = a.list ? a.list[item] : item;
     gsync<NW>(gid);
@@ -388,56 +281,61 @@ __global__ void __launch_bounds__(128) k_solve_mixed(SolveDev a, int64_t* redo, 
     float y0 = have ? float(c) : 0.f, y1 = have ? 1.f : 0.f, y2 = have ? float(zf) : 0.f;
     float dme = 1.f;
     bool weak = false;
-    const float thr = 1e-5f * c0f;
     constexpr int Q = R / 4;
     const int n1 = min(nn, Q), n2 = min(nn, 2 * Q), n3 = min(nn, 3 * Q);
+    // An FP32 pivot at most nn ulp(C0) is not resolved from the rounding of
+    // its row, so it leaves no factorisation to refine with (nor a trustworthy
+    // smallest pivot for the error test below): the FP64 form takes the
+    // system, and with it the singular decision (a pivot at most 1e-12 C0,
+    // kernel.rs:61). The FP32 form never declares a system singular.
+    const float thr = float(nn) * 1.1920929e-7f * float(c0);
     eliminate_rows_f32<NW, R>(A, 0, n1, row, X, gid, y0, y1, y2, dme, weak, thr);
     if (!weak) eliminate_rows_f32<NW, 3 * Q>(A, n1, n2, row, X, gid, y0, y1, y2, dme, weak, thr);
     if (!weak) eliminate_rows_f32<NW, 2 * Q>(A, n2, n3, row, X, gid, y0, y1, y2, dme, weak, thr);
     if (!weak) eliminate_rows_f32<NW, Q>(A, n3, nn, row, X, gid, y0, y1, y2, dme, weak, thr);
-    if (weak) {  // leave it to the FP64 form, which also takes the singular decision
+    if (weak) {
       if (row == 0) redo[atomicAdd(reinterpret_cast<unsigned long long*>(redo_len), 1ull)] = ti;
       continue;
     }
-    // Back substitution L^T x = D^-1 y, column by column from the last row
-    // (L[i][k], i > k, written during the elimination).
-    float u0 = y0 / dme, u1 = y1 / dme, u2 = y2 / dme;
-    gsync<NW>(gid);
-    for (int k = nn - 1; k >= 0; --k) {
-      const int b = k & 1;
-      if (row == k) X.rhsf[b][0] = u0, X.rhsf[b][1] = u1, X.rhsf[b][2] = u2;
-      gsync<NW>(gid);
-      if (row < k) {
-        const float l = X.L[k][row];
-        u0 = fmaf(-l, X.rhsf[b][0], u0);
-        u1 = fmaf(-l, X.rhsf[b][1], u1);
-        u2 = fmaf(-l, X.rhsf[b][2], u2);
-      }
-    }
-    // FP64 residuals r_v = v - C x_v with C from the FP64 triangle.
-    const double x0 = have ? double(u0) : 0.0, x1 = have ? double(u1) : 0.0, x2 = have ? double(u2) : 0.0;
-    X.xs[0][row] = x0, X.xs[1][row] = x1, X.xs[2][row] = x2;
-    gsync<NW>(gid);
-    double r0 = 0.0, r1 = 0.0, r2 = 0.0;
-    if (have) {
-      double a0 = diag * x0, a1 = diag * x1, a2 = diag * x2;
-      for (int j = 0; j < nn; ++j) {
-        if (j == row) continue;
-        const double cij = j < row ? S.T[tri + j] : S.T[j * (j - 1) / 2 + row];
-        a0 = fma(cij, X.xs[0][j], a0);
-        a1 = fma(cij, X.xs[1][j], a1);
-        a2 = fma(cij, X.xs[2][j], a2);
-      }
-      r0 = c - a0, r1 = 1.0 - a1, r2 = zf - a2;
-    }
-    // Refinement residual test: the corrected forms below err by about
-    // rho^2 C0 / D_min (rho the FP32 solve's relative residual, D_min its
-    // smallest pivot); above 1e-8 the system is re-solved in FP64.
+    // First solve x = C~^-1 v (y is already L^-1 v).
+    float u0 = y0, u1 = y1, u2 = y2;
+    sweep_f32<NW>(X, gid, row, nn, dme, false, u0, u1, u2);
+    double x0 = have ? double(u0) : 0.0, x1 = have ? double(u1) : 0.0, x2 = have ? double(u2) : 0.0;
     const double cmax = group_max<NW>(S, gid, wig, have ? fabs(c) : 0.0);
     const double zmax = group_max<NW>(S, gid, wig, have ? fabs(zf) : 0.0);
-    const double rho = group_max<NW>(S, gid, wig, have ? fmax(fmax(fabs(r0) / fmax(cmax, 1e-300), fabs(r1)),
-                                                              fabs(r2) / fmax(zmax, 1e-300)) : 0.0);
     const double dmin = -group_max<NW>(S, gid, wig, have ? -double(dme) : -1e300);
+    double r0 = 0.0, r1 = 0.0, r2 = 0.0, rho = 0.0;
+    for (int it = 0;; ++it) {
+      // FP64 residuals r_v = v - C x_v with C from the FP64 triangle.
+      X.xs[0][row] = x0, X.xs[1][row] = x1, X.xs[2][row] = x2;
+      gsync<NW>(gid);
+      r0 = r1 = r2 = 0.0;
+      if (have) {
+        double a0 = diag * x0, a1 = diag * x1, a2 = diag * x2;
+        for (int j = 0; j < nn; ++j) {
+          if (j == row) continue;
+          const double cij = j < row ? S.T[tri + j] : S.T[j * (j - 1) / 2 + row];
+          a0 = fma(cij, X.xs[0][j], a0);
+          a1 = fma(cij, X.xs[1][j], a1);
+          a2 = fma(cij, X.xs[2][j], a2);
+        }
+        r0 = c - a0, r1 = 1.0 - a1, r2 = zf - a2;
+      }
+      // The corrected forms below err by about rho^2 C0 / D_min (rho the
+      // relative residual, D_min the smallest FP32 pivot): refine until that
+      // is at most 1e-8, or give the system to the FP64 form.
+      const double prev = rho;
+      rho = group_max<NW>(S, gid, wig, have ? fmax(fmax(fabs(r0) / fmax(cmax, 1e-300), fabs(r1)),
+                                                   fabs(r2) / fmax(zmax, 1e-300)) : 0.0);
+      if (rho * rho * c0 / dmin <= 1e-8) break;
+      // Out of steps, no factorisation worth the name (rho >= 1), or a step
+      // that did not halve the residual: refinement will not converge.
+      if (it == kRefineSteps || !(rho < 1.0) || (it > 0 && !(rho < 0.5 * prev))) break;
+      u0 = float(r0), u1 = float(r1), u2 = float(r2);
+      sweep_f32<NW>(X, gid, row, nn, dme, true, u0, u1, u2);
+      if (have) x0 += double(u0), x1 += double(u1), x2 += double(u2);
+      gsync<NW>(gid);  // every row has read xs
+    }
     // Corrected forms u'x_v + x_u'r_v (error second order in the residuals).
     double s[5] = {x0 + x1 * r0, x1 + x1 * r1, zf * x0 + x2 * r0, zf * x1 + x2 * r1, c * x0 + x0 * r0};
     if (!have) s[0] = s[1] = s[2] = s[3] = s[4] = 0.0;

@@ -35,12 +35,15 @@
 // n > 32 (appended to `large`) and a sample flagged coincident at fit time
 // (appended to `small`). A tile whose union exceeds the table, but not twice
 // the table, is retried as two halves of 8 targets, each with a union of its
-// own; what still does not fit goes to `small`. In the mixed form, systems
-// whose FP32 pivots or residuals fail the refinement tests go to `redo`. The
-// per-system kernels of btk_solve.cu take those. The table entries do not
-// depend on the order in which samples enter the union or on the tile (each
-// is a function of its sample pair alone), so the FP64 form gives bit for bit
-// the per-system kernel's results.
+// own; what still does not fit goes to `small`. In the mixed form, a system
+// whose FP32 factorisation breaks down goes to `redo` (FP64), and one whose
+// corrected forms fail the residual test goes to `small`, where the
+// per-system mixed kernel refines it iteratively (and hands it to `redo` if
+// that does not converge). The per-system kernels of btk_solve.cu take
+// those lists. The table entries do not depend on the order in which
+// samples enter the union or on the tile (each is a function of its sample
+// pair alone), so the FP64 form gives bit for bit the per-system kernel's
+// results.
 #include "btk_device.cuh"
 
 namespace btk {
@@ -450,9 +453,11 @@ __device__ void solve_mixed(const TileDev& a, const TileHead& H, const double* P
   eliminate2<24>(A, n1, n2, lane, W, y, dme, pmin);
   eliminate2<16>(A, n2, n3, lane, W, y, dme, pmin);
   eliminate2<8>(A, n3, nmax, lane, W, y, dme, pmin);
-  // NaN or at most 1e-5 C0 among the FP32 pivots: the FP64 form takes it.
-  const float thr = 1e-5f * float(c0);
-  const bool weak_a = !(pmin.x > thr), weak_b = !(pmin.y > thr);
+  // An FP32 pivot that is NaN or at most n ulp(C0) is not resolved from the
+  // rounding of its row: the FP64 form takes the system (and with it the
+  // singular decision, kernel.rs:61).
+  const bool weak_a = !(pmin.x > float(na) * 1.1920929e-7f * float(c0));
+  const bool weak_b = !(pmin.y > float(nb) * 1.1920929e-7f * float(c0));
   __syncwarp();
   // Backward sweep L^T x = D^-1 y, column-oriented: once x_k is known every
   // row i < k takes D_i L[k][i] x_k (column i of the triangle) into acc_i,
@@ -519,8 +524,10 @@ __device__ void solve_mixed(const TileDev& a, const TileHead& H, const double* P
       const double* v = is_a ? va : vb;
       const double rho = is_a ? rho_a : rho_b, dmin = is_a ? dmin_a : dmin_b;
       const bool weak = is_a ? weak_a : weak_b;
-      if (weak || !(rho * rho * c0 / dmin <= 1e-8) || !(v[1] > 0.0) || !(fabs(v[0]) < 1e30))
+      if (weak)
         a.redo[atomicAdd(reinterpret_cast<unsigned long long*>(a.redo_len), 1ull)] = ti;
+      else if (!(rho * rho * c0 / dmin <= 1e-8) || !(v[1] > 0.0) || !(fabs(v[0]) < 1e30))
+        a.small[atomicAdd(reinterpret_cast<unsigned long long*>(a.small_len), 1ull)] = ti;  // refined there
       else
         epilogue(s, H.kind[is_a ? ta : tb], ti, v, is_a ? na : nb, 0);
     }

@@ -7,10 +7,11 @@ exchanged on the data path. A slab is a range of cell indices of the whole
 model (row index i + nx (j + ny k), block_model.rs:62-86), so each rank's
 centroids, and its FP64 results, are bit for bit those of the unsharded run.
 
-The leave-one-out loss and gradient split over the left-out samples: each
-rank sums its range's squared errors, count and gradient terms
-(btk_loo_gradient_range) and one all-reduce of those 2 + p FP64 values
-gives every rank the same loss and gradient.
+The leave-one-out loss and gradient split over the left-out samples, and the
+block-model mean over the cells: each rank sums its range's objective
+terms, count and gradient terms (btk_loo_gradient_range,
+btk_mean_gradient_range) and one all-reduce of those 2 + p FP64 values
+gives every rank the same value and gradient.
 
 `group` is a torch.distributed process group (None: the default group when
 torch.distributed is initialised, else a single rank).
@@ -108,18 +109,9 @@ def predict_sharded(estimator, geometry, *, group=None, precision=None, keys=("v
 
 
 def loo_sums(loo, theta, first, count, grad=True):
-    """Partial sums of a LeaveOneOut over left-out samples first .. first + count - 1: [squared-error sum,
+    """Partial sums of a LeaveOneOut (or BlockMean) over systems first .. first + count - 1: [objective sum,
     systems counted, gradient sums...]."""
-    from .gradient import _variogram_c, variogram_of
-
-    vg = variogram_of(loo.template, theta)
-    c = _variogram_c(vg)
-    out = np.zeros(2 + 1 + 2 * len(vg.structures) + 5)
-    ctx = loo.estimator._ctx
-    rc = ctx._lib.btk_loo_gradient_range(ctx.handle, ctypes.byref(c), int(first), int(count), 1 if grad else 0,
-                                         out.ctypes.data)
-    ctx.check(rc, "leave-one-out range")
-    return out
+    return loo.range_sums(theta, first, count, grad)
 
 
 def finish(sums):
@@ -131,14 +123,17 @@ def finish(sums):
     return float(sums[0] / cnt), sums[2:] / cnt, int(round(cnt))
 
 
-def loo_loss_sharded(loo, theta, *, group=None, grad=True):
-    """Leave-one-out loss and gradient with the samples split over the ranks: (loss, gradient or None,
-    systems), the same on every rank."""
+def objective_sharded(obj, theta, *, group=None, grad=True):
+    """A LeaveOneOut's loss or a BlockMean's mean, and its gradient, with the systems split over the ranks:
+    (value, gradient or None, systems), the same on every rank."""
     rank, world = rank_world(group)
-    first, count = split(loo.n, world)[rank]
-    loss, g, cnt = finish(all_reduce_sum(loo_sums(loo, theta, first, count, grad), group))
-    return loss, (g if grad else None), cnt
+    first, count = split(obj.n, world)[rank]
+    value, g, cnt = finish(all_reduce_sum(loo_sums(obj, theta, first, count, grad), group))
+    return value, (g if grad else None), cnt
+
+
+loo_loss_sharded = objective_sharded
 
 
 __all__ = ["rank_world", "split", "slab", "all_reduce_sum", "all_gather_rows", "predict_slab", "predict_sharded",
-           "loo_sums", "finish", "loo_loss_sharded"]
+           "loo_sums", "finish", "objective_sharded", "loo_loss_sharded"]

@@ -44,7 +44,8 @@ extern "C" {
 #define BTK_ST_SEARCH_FAILED 1 /* fewer than min_samples (EstimError::SearchFailed) */
 #define BTK_ST_SINGULAR 2      /* pivot <= 1e-12 * C(0) (kernel.rs:61) */
 #define BTK_ST_UNSUPPORTED 3   /* more samples than the solve path holds */
-#define BTK_ST_INVALID 4       /* simple kriging with a power structure (EstimError::InvalidParameters, krige.rs:117-124) */
+#define BTK_ST_INVALID 4       /* simple kriging with a power structure (EstimError::InvalidParameters, krige.rs:117-124),
+                                  or a caller's neighbour list out of bounds (btk_solve_noalloc) */
 #define BTK_RULES_CANDIDATES 512 /* candidates a hole / sector rule search sorts per round */
 #define BTK_ST_FP64_FALLBACK 0x10 /* flag: the mixed form re-solved this system in FP64 */
 
@@ -248,7 +249,7 @@ int btk_centroids(btk_ctx* ctx, const btk_geometry* g, int64_t first, int64_t m,
  * has no counterpart in the reference, which computes leave-one-out
  * estimates (batch.rs:165-190) but no gradient of them.
  * btk_loo_freeze runs the leave-one-out search of the fitted samples once
- * and keeps each sample's neighbour list (at most 32), so every later loss
+ * and keeps each sample's neighbour list (at most 64), so every later loss
  * and gradient uses those neighbourhoods, whatever variogram it is given.
  * btk_loo_gradient evaluates, for the variogram `vg` (same structure count
  * and models as needed, any parameters), the mean squared leave-one-out
@@ -258,10 +259,13 @@ int btk_centroids(btk_ctx* ctx, const btk_geometry* g, int64_t first, int64_t m,
  * range of each structure, semi/major ratio, minor/major ratio, azimuth,
  * dip, rake (degrees); 1 + 2 nstruct + 5 values. A variogram without
  * anisotropy is taken as ratios 1, 1 and angles 0. `values` (n, or NULL)
- * receives the leave-one-out estimates. */
+ * receives the leave-one-out estimates. `precision`: BTK_FP64 (FP64
+ * factorisation), or BTK_MIXED (FP32 factorisation refined in FP64 until the
+ * solutions are good to about 1e-8, FP64 gradient accumulation; systems
+ * whose refinement does not converge are solved in FP64). */
 int btk_loo_freeze(btk_ctx* ctx);
-int btk_loo_gradient(btk_ctx* ctx, const btk_variogram* vg, int32_t want_grad, double* loss, double* grad,
-                     int64_t* n_valid, double* values);
+int btk_loo_gradient(btk_ctx* ctx, const btk_variogram* vg, int32_t want_grad, int32_t precision, double* loss,
+                     double* grad, int64_t* n_valid, double* values);
 
 /* The same over the left-out samples first .. first + count - 1 only, as
  * sums for a reduction across ranks: sums[0] = sum of squared errors,
@@ -270,7 +274,26 @@ int btk_loo_gradient(btk_ctx* ctx, const btk_variogram* vg, int32_t want_grad, d
  * partition of the samples is sum(sums[0]) / sum(sums[1]), and the gradient
  * sum(sums[2 + k]) / sum(sums[1]). */
 int btk_loo_gradient_range(btk_ctx* ctx, const btk_variogram* vg, int64_t first, int64_t count, int32_t want_grad,
-                           double* sums);
+                           int32_t precision, double* sums);
+
+/* The mean ordinary-kriging estimate of a block model and its gradient with
+ * respect to the variogram; no counterpart in the reference. btk_mean_freeze
+ * runs the search at every centroid of `g` (cell order, as
+ * btk_predict_geometry_device) once and keeps each list (at most 64
+ * samples), so later calls krige from those neighbourhoods whatever
+ * variogram they are given. btk_mean_gradient gives the mean of the point
+ * estimates over the centroids whose system is solvable and holds no
+ * coincident samples (*n_valid), its gradient (the parameter order of
+ * btk_loo_gradient) when want_grad is set, and the estimates themselves in
+ * `values` (one per cell, NaN where none, or NULL). The FP64 objective
+ * equals the mean of btk_predict_geometry_device's FP64 values to the bit.
+ * btk_mean_gradient_range gives the sums over cells first .. first + count
+ * - 1, as btk_loo_gradient_range does (sums[0] = sum of the estimates). */
+int btk_mean_freeze(btk_ctx* ctx, const btk_geometry* g);
+int btk_mean_gradient(btk_ctx* ctx, const btk_variogram* vg, int32_t want_grad, int32_t precision, double* mean,
+                      double* grad, int64_t* n_valid, double* values);
+int btk_mean_gradient_range(btk_ctx* ctx, const btk_variogram* vg, int64_t first, int64_t count, int32_t want_grad,
+                            int32_t precision, double* sums);
 
 /* Kernel launches issued by this context since it was created. */
 int64_t btk_launch_count(const btk_ctx* ctx);
@@ -302,24 +325,21 @@ int btk_set_tuning(btk_ctx* ctx, const btk_tuning* tuning);
  * writing the same d_out. No counterpart in the reference. */
 int btk_graph_capture_geometry(btk_ctx* ctx, const btk_geometry* g, int32_t kind, double kparam,
                                int32_t precision, const btk_outputs* d_out);
+/* The same for m device targets d_xyz (as btk_predict_device): with d_kinds
+ * (one int8 kind per target, device) btk_predict_kinds_device is captured,
+ * else btk_predict_device with `kind`. The graph reads d_xyz and d_kinds on
+ * every replay, so the caller may change their contents between replays. */
+int btk_graph_capture_device(btk_ctx* ctx, int64_t m, const double* d_xyz, const int8_t* d_kinds, int32_t kind,
+                             double kparam, int32_t precision, const btk_outputs* d_out);
 int btk_graph_launch(btk_ctx* ctx, void* stream);
-
-/* Diagnostics with no counterpart in the reference. btk_set_timing records
- * CUDA events around the phases of every prediction on this context;
- * btk_phase_ms waits for the last one and gives its search, solve and FP64
- * re-solve times in milliseconds. btk_peak_flops runs a CUDA-core FMA loop
- * and returns the FLOP/s reached (fp64 != 0: double, else float), the
- * denominator of the solve kernels' roofline. */
-int btk_set_timing(btk_ctx* ctx, int32_t on);
-int btk_phase_ms(btk_ctx* ctx, float* out3);
-double btk_peak_flops(btk_ctx* ctx, int32_t fp64);
 
 /* Kriging without any allocation. This entry point has no counterpart in the
  * reference. It is for callers that cannot call cudaMalloc: a host that owns
  * every device allocation (its own arena or pool allocator, a fixed device
  * memory budget) or a plugin running inside another program's CUDA context.
  * The caller passes device buffers for every input and output:
- *   - samples d_x, d_y, d_z, d_values and d_err (NULL: no measurement error);
+ *   - n_samples samples d_x, d_y, d_z, d_values and d_err (NULL: no
+ *     measurement error);
  *   - m targets d_tx, d_ty, d_tz;
  *   - each target's neighbour list d_nbr (m x max_samples sample indices, as
  *     btk_neighbors gives them), its length d_count and its search status
@@ -327,20 +347,23 @@ double btk_peak_flops(btk_ctx* ctx, int32_t fp64);
  *   - outputs d_out, as for btk_predict_device.
  * It solves the systems in the mixed form (BTK_MIXED, FP64 re-solve where
  * needed) on `stream`, with the results of btk_predict_device; coincident
- * samples are detected within each system.
+ * samples are detected within each system. The lists are checked on the
+ * device: a count above max_samples, or an index at or past n_samples, fails
+ * that target with BTK_ST_INVALID and nothing past the buffers is read.
  * Its only scratch is a static device array of BTK_NOALLOC_MAX_SYSTEMS + 1
  * int64 (2 MiB), held by every GPU that loads the library until the process
  * exits. Limits: at most BTK_NOALLOC_MAX_SYSTEMS systems per call (more
- * return BTK_EINVAL: split the call) and at most 32 samples per system. The
- * first call on a device looks the array's address up (cudaGetSymbolAddress),
- * so make it before capturing a stream. Every call shares the array, so calls
- * that overlap on the GPU race: serialise them on one stream. `device` is
- * made current for the call and the caller's device restored afterwards;
- * `err` (may be NULL) receives the reason of a failure. */
+ * return BTK_EINVAL: split the call) and at most 32 samples per system. Each
+ * call looks the array's address up in the current CUDA context
+ * (cudaGetSymbolAddress); the first lookup in a context loads the module, so
+ * make the first call there before capturing a stream. Every call shares the
+ * array, so calls that overlap on the GPU race: serialise them on one stream.
+ * `device` is made current for the call and the caller's device restored
+ * afterwards; `err` (may be NULL) receives the reason of a failure. */
 #define BTK_NOALLOC_MAX_SYSTEMS 262144
 int btk_solve_noalloc(int device, const btk_variogram* vg, int32_t kind, double kparam, const double* d_x,
                       const double* d_y, const double* d_z, const double* d_values, const double* d_err,
-                      int64_t m, const double* d_tx, const double* d_ty, const double* d_tz,
+                      int64_t n_samples, int64_t m, const double* d_tx, const double* d_ty, const double* d_tz,
                       const uint32_t* d_nbr, int32_t max_samples, const int32_t* d_count,
                       const int8_t* d_status, const btk_outputs* d_out, void* stream, char* err,
                       size_t errlen);

@@ -86,3 +86,46 @@ def test_quadrants_with_a_hole_cap_on_planar_data(oracle):
     est = OrdinaryKriging(w.variogram, s).fit(xyz, vals, holes=labels)
     t = np.column_stack([rng.uniform(0, 500, 300), rng.uniform(0, 500, 300), np.full(300, 10.0)])
     assert_same_neighbors(est, oracle, xyz, s, w.variogram, t, hole_codes(labels))
+
+
+def boundary_clusters(P, axes, rng, targets=40):
+    """Per target (1 km apart, so no search sees another's samples): for each boundary of P plane sectors, two
+    samples within a few ulps of it in the search frame (near, 10-20 m), and one inside each sector (50-60 m).
+    Samples whose offset's host-libm atan2 is not correctly rounded are left out: at those the reference's
+    sector depends on its platform's libm (tests/test_sector_angles.py), and the oracle shares this host's."""
+    from test_sector_angles import libm_misrounds
+
+    M = np.asarray(axes)
+    T = np.column_stack([1000.0 * np.arange(targets), np.zeros(targets), np.full(targets, 100.0)])
+    pts = []
+    for t in T:
+        for k in range(P):
+            for r, th in ((rng.uniform(10, 20), 2 * np.pi * k / P), (rng.uniform(10, 20), 2 * np.pi * k / P),
+                          (rng.uniform(50, 60), 2 * np.pi * (k + 0.5) / P)):
+                d = np.array([-r * np.sin(th), r * np.cos(th), rng.uniform(-3, 3)])
+                d[0] = np.nextafter(d[0], np.inf if rng.random() < 0.5 else -np.inf)
+                s = t + M.T @ d
+                v = s - t
+                # the search frame's offset as the reference computes it (nalgebra column order, no FMA)
+                dd = [(M[r_, 0] * v[0] + M[r_, 1] * v[1]) + M[r_, 2] * v[2] for r_ in range(3)]
+                if dd[0] != 0.0 and dd[1] != 0.0 and libm_misrounds(-dd[0], dd[1]):
+                    continue
+                pts.append(s)
+    return T, np.array(pts)
+
+
+@pytest.mark.parametrize("P", [4, 6, 12])
+@pytest.mark.parametrize("rotation", [None, (30.0, 20.0, 10.0)])
+def test_plane_sectors_at_their_boundaries(oracle, P, rotation):
+    """Samples within a few ulps of every plane-sector boundary (search.rs:428-434), one per sector taken:
+    the lists are the oracle's index for index."""
+    from boitata_b200 import Structure, Variogram
+
+    rng = np.random.default_rng(P)
+    kw = {} if rotation is None else dict(rotation=rotation, ratios=(1.0, 1.0))
+    s = Search(radius=100.0, sectors=P, max_per_sector=1, max_samples=P, min_samples=1, **kw)
+    axes = oracle.block_frame(*(rotation or (0.0, 0.0, 0.0)))
+    T, X = boundary_clusters(P, axes, rng)
+    vg = Variogram([Structure("spherical", 1.0, 200.0)], nugget=0.1)
+    est = OrdinaryKriging(vg, s).fit(X, rng.uniform(0, 1, len(X)))
+    assert_same_neighbors(est, oracle, X, s, vg, T, None)
