@@ -90,7 +90,12 @@ SIGNATURES = {
                                                 ctypes.POINTER(OutputsC), P]),
     "btk_cross_validate": (ctypes.c_int, [P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
                                           ctypes.POINTER(OutputsC)]),
-    "btk_neighbors": (ctypes.c_int, [P, ctypes.c_int64, P, ctypes.c_int32, P, P, P]),
+    "btk_neighbors": (ctypes.c_int, [P, ctypes.c_int64, P, ctypes.c_int32, P, P, P, P]),
+    "btk_set_domains": (ctypes.c_int, [P, P]),
+    "btk_predict_ex": (ctypes.c_int, [P, ctypes.c_int64, P, P, P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
+                                      ctypes.POINTER(OutputsC), P]),
+    "btk_predict_ex_device": (ctypes.c_int, [P, ctypes.c_int64, P, P, P, ctypes.c_int32, ctypes.c_double,
+                                             ctypes.c_int32, ctypes.POINTER(OutputsC), P]),
     "btk_centroids": (ctypes.c_int, [P, ctypes.POINTER(GeometryC), ctypes.c_int64, ctypes.c_int64, P]),
     "btk_launch_count": (ctypes.c_int64, [P]),
     "btk_set_support": (ctypes.c_int, [P, P, P, P]),

@@ -200,6 +200,10 @@ struct btk_ctx {
   DevBuf<uint32_t> hole;
   bool has_hole = false;
 
+  // domain codes of the fitted samples (btk_set_domains) and of a call's targets
+  DevBuf<int32_t> dom, tdom;
+  bool has_dom = false;
+
   // block support (btk_set_support): discretization offsets, C(B,B)
   DevBuf<double> sup, sup_cbb;
   int sup_n = 0;
@@ -448,9 +452,32 @@ int ensure_scratch(btk_ctx* ctx, int64_t m) {
 constexpr int64_t kOrderMin = 2048;
 
 // Search then solve for m targets whose coordinates are device SoA arrays.
+// The fitted search, restricted by hard domains when the samples have them:
+// the rules kernel then takes each target's own domain only, tdom[t] for a
+// prediction and the left-out sample's for leave-one-out (loo).
+SearchDev search_for(const btk_ctx* ctx, const int32_t* tdom, bool loo) {
+  SearchDev sp = ctx->spd;
+  if (ctx->has_dom) {
+    sp.rules = 1;
+    sp.sdom = ctx->dom.p;
+    sp.tdom = loo ? ctx->dom.p : tdom;
+  }
+  return sp;
+}
+
+// A call's target domains against the fit's: both or neither.
+int check_domains(btk_ctx* ctx, const int32_t* tdom, bool loo) {
+  if (loo) return BTK_OK;
+  if (ctx->has_dom && !tdom) return fail(ctx, BTK_EINVAL, "fitted with domains; predict needs domains too");
+  if (!ctx->has_dom && tdom) return fail(ctx, BTK_EINVAL, "fitted without domains; predict takes none");
+  return BTK_OK;
+}
+
 int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const double* ty, const double* tz,
              const int64_t* perm, int64_t nwork, int loo, int32_t kind, double kparam, int32_t precision,
-             const btk_outputs* o, const int8_t* kinds = nullptr, const btk_diagnostics* dg = nullptr) {
+             const btk_outputs* o, const int8_t* kinds = nullptr, const btk_diagnostics* dg = nullptr,
+             const int32_t* tdom = nullptr) {
+  if (int rc = check_domains(ctx, tdom, loo != 0)) return rc;
   if (kind < BTK_ORDINARY || kind > BTK_INDICATOR) return fail(ctx, BTK_EINVAL, "unknown kriging kind");
   if (precision != BTK_FP64 && precision != BTK_MIXED) return fail(ctx, BTK_EINVAL, "unknown precision");
   if (kind == BTK_SIMPLE && !std::isfinite(kparam)) return fail(ctx, BTK_EINVAL, "simple kriging needs a finite mean");
@@ -483,7 +510,8 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
     nwork = m;
   }
   ctx->mark(0, L.stream);
-  CK(launch_search(L, ctx->spd, ctx->gd, tx, ty, tz, perm, nwork, loo, ctx->nbr.p, ctx->cnt.p, ctx->sst.p));
+  CK(launch_search(L, search_for(ctx, tdom, loo != 0), ctx->gd, tx, ty, tz, perm, nwork, loo, ctx->nbr.p, ctx->cnt.p,
+                   ctx->sst.p));
   ctx->mark(1, L.stream);
   SolveDev a{};
   a.vg = ctx->vgd;
@@ -937,6 +965,7 @@ int btk_fit(btk_ctx* ctx, int64_t n, const double* xyz, const double* values, co
             const int64_t* holes, const btk_search* search, const btk_variogram* vg) {
   if (!ctx) return BTK_EINVAL;
   ctx->fitted = false;
+  ctx->has_dom = false;
   if (n <= 0 || !xyz || !values) return fail(ctx, BTK_EINVAL, "fit needs at least one sample with coordinates and values");
   if (n >= int64_t(0xffffffffu)) return fail(ctx, BTK_EINVAL, "too many samples");
   int rc = check_vg(ctx, vg);
@@ -1018,7 +1047,9 @@ namespace {
 // context's scratch, which the compute stream serialises; chunks write
 // disjoint slices of the staged inputs and outputs.
 int predict_host(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds, int32_t kind, double kparam,
-                 int32_t precision, const btk_outputs* out, const btk_diagnostics* diag = nullptr) {
+                 int32_t precision, const btk_outputs* out, const btk_diagnostics* diag = nullptr,
+                 const int32_t* domains = nullptr) {
+  if (int rc = check_domains(ctx, domains, false)) return rc;
   int64_t chunk = ctx->tuning.host_chunk > 0 ? int64_t(ctx->tuning.host_chunk) : m;
   if ((m + chunk - 1) / chunk > 8) chunk = (m + 7) / 8;
   const int64_t nc = (m + chunk - 1) / chunk;
@@ -1026,6 +1057,7 @@ int predict_host(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds
   CK(ctx->aos.grow(3 * mm));
   CK(ctx->txyz.grow(3 * mm));
   if (kinds) CK(ctx->kinds.grow(mm));
+  if (domains) CK(ctx->tdom.grow(mm));
   btk_outputs d{};
   int rc = host_outputs(ctx, m, out, &d);
   if (rc) return rc;
@@ -1046,6 +1078,9 @@ int predict_host(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds
     CK(cudaMemcpyAsync(ctx->aos.p + 3 * off, xyz + 3 * off, 3 * size_t(mc) * sizeof(double), cudaMemcpyHostToDevice,
                        ctx->up));
     if (kinds) CK(cudaMemcpyAsync(ctx->kinds.p + off, kinds + off, size_t(mc), cudaMemcpyHostToDevice, ctx->up));
+    if (domains)
+      CK(cudaMemcpyAsync(ctx->tdom.p + off, domains + off, size_t(mc) * sizeof(int32_t), cudaMemcpyHostToDevice,
+                         ctx->up));
     CK(cudaEventRecord(in_done[c], ctx->up));
   }
   double* t = ctx->txyz.p;
@@ -1060,7 +1095,8 @@ int predict_host(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds
     btk_outputs dc{d.value + off, d.variance + off, d.lagrange + off, d.n_used + off, d.status + off};
     btk_diagnostics dd{ctx->o_negw.p + off, ctx->o_mdist.p + off, ctx->o_nholes.p + off, ctx->o_met.p + off};
     if ((rc = run_path(ctx, ctx->stream, mc, t + off, t + m + off, t + 2 * m + off, nullptr, mc, 0, kind, kparam,
-                       precision, &dc, kinds ? ctx->kinds.p + off : nullptr, diag ? &dd : nullptr)))
+                       precision, &dc, kinds ? ctx->kinds.p + off : nullptr, diag ? &dd : nullptr,
+                       domains ? ctx->tdom.p + off : nullptr)))
       return rc;
     CK(cudaEventRecord(out_ready[c], ctx->stream));
     CK(cudaStreamWaitEvent(ctx->down, out_ready[c], 0));
@@ -1137,6 +1173,54 @@ int btk_predict_kinds(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* 
   if (m == 0) return BTK_OK;
   CK(cudaSetDevice(ctx->device));
   return predict_host(ctx, m, xyz, kinds, BTK_ORDINARY, kparam, precision, out);
+}
+
+int btk_set_domains(btk_ctx* ctx, const int32_t* codes) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  ctx->frozen = false;
+  ctx->mean_m = 0;
+  if (!codes) {
+    ctx->has_dom = false;
+    return BTK_OK;
+  }
+  for (int64_t i = 0; i < ctx->n; ++i)
+    if (codes[i] < 0) return fail(ctx, BTK_EINVAL, "every sample needs a domain code (>= 0)");
+  CK(cudaSetDevice(ctx->device));
+  CK(ctx->dom.grow(size_t(ctx->n)));
+  CK(cudaMemcpy(ctx->dom.p, codes, size_t(ctx->n) * sizeof(int32_t), cudaMemcpyHostToDevice));
+  ctx->has_dom = true;
+  return BTK_OK;
+}
+
+int btk_predict_ex(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds, const int32_t* domains,
+                   int32_t kind, double kparam, int32_t precision, const btk_outputs* out,
+                   const btk_diagnostics* diag) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if (!out || !out->value) return fail(ctx, BTK_EINVAL, "outputs need a value array");
+  if (diag && !out->status) return fail(ctx, BTK_EINVAL, "diagnostics need the status output");
+  if (m < 0 || (m > 0 && !xyz)) return fail(ctx, BTK_EINVAL, "targets are required");
+  if (kinds)
+    for (int64_t i = 0; i < m; ++i)
+      if (kinds[i] < BTK_ORDINARY || kinds[i] > BTK_INDICATOR) return fail(ctx, BTK_EINVAL, "unknown kriging kind");
+  if ((rc = check_domains(ctx, domains, false))) return rc;
+  if (m == 0) return BTK_OK;
+  CK(cudaSetDevice(ctx->device));
+  return predict_host(ctx, m, xyz, kinds, kinds ? BTK_ORDINARY : kind, kparam, precision, out, diag, domains);
+}
+
+int btk_predict_ex_device(btk_ctx* ctx, int64_t m, const double* d_xyz, const int8_t* d_kinds,
+                          const int32_t* d_domains, int32_t kind, double kparam, int32_t precision,
+                          const btk_outputs* d_out, void* stream) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if (m < 0 || (m > 0 && !d_xyz)) return fail(ctx, BTK_EINVAL, "targets are required");
+  if ((rc = check_domains(ctx, d_domains, false))) return rc;
+  if (m == 0) return BTK_OK;
+  CK(cudaSetDevice(ctx->device));
+  return run_path(ctx, static_cast<cudaStream_t>(stream), m, d_xyz, d_xyz + m, d_xyz + 2 * m, nullptr, m, 0,
+                  d_kinds ? BTK_ORDINARY : kind, kparam, precision, d_out, d_kinds, nullptr, d_domains);
 }
 
 int btk_predict_geometry_device(btk_ctx* ctx, const btk_geometry* g, int32_t kind, double kparam, int32_t precision,
@@ -1260,9 +1344,11 @@ int btk_cross_validate(btk_ctx* ctx, int32_t kind, double kparam, int32_t precis
   return copy_out(ctx, ctx->n, &d, out);
 }
 
-int btk_neighbors(btk_ctx* ctx, int64_t m, const double* xyz, int32_t loo, int64_t* idx, int32_t* count, int8_t* ok) {
+int btk_neighbors(btk_ctx* ctx, int64_t m, const double* xyz, int32_t loo, const int32_t* domains, int64_t* idx,
+                  int32_t* count, int8_t* ok) {
   int rc = need_fit(ctx);
   if (rc) return rc;
+  if ((rc = check_domains(ctx, domains, loo != 0))) return rc;
   CK(cudaSetDevice(ctx->device));
   const double* t;
   const int64_t* perm = nullptr;
@@ -1278,7 +1364,12 @@ int btk_neighbors(btk_ctx* ctx, int64_t m, const double* xyz, int32_t loo, int64
   if ((rc = ensure_scratch(ctx, m))) return rc;
   Launch L = ctx->launch(nullptr);
   const double *tx = loo ? ctx->x.p : t, *ty = loo ? ctx->y.p : t + m, *tz = loo ? ctx->z.p : t + 2 * m;
-  CK(launch_search(L, ctx->spd, ctx->gd, tx, ty, tz, perm, m, loo ? 1 : 0, ctx->nbr.p, ctx->cnt.p, ctx->sst.p));
+  if (domains && !loo) {
+    CK(ctx->tdom.grow(size_t(m)));
+    CK(cudaMemcpyAsync(ctx->tdom.p, domains, size_t(m) * sizeof(int32_t), cudaMemcpyHostToDevice, L.stream));
+  }
+  CK(launch_search(L, search_for(ctx, domains ? ctx->tdom.p : nullptr, loo != 0), ctx->gd, tx, ty, tz, perm, m,
+                   loo ? 1 : 0, ctx->nbr.p, ctx->cnt.p, ctx->sst.p));
   const size_t k = size_t(ctx->search.max_samples);
   std::vector<uint32_t> nb(size_t(m) * k);
   std::vector<int8_t> st(m);
@@ -1298,6 +1389,7 @@ int btk_loo_freeze(btk_ctx* ctx) {
     return fail(ctx, BTK_EUNSUPPORTED, "the leave-one-out gradient takes at most 64 samples per system");
   if (ctx->search.calibration)
     return fail(ctx, BTK_EUNSUPPORTED, "the leave-one-out gradient takes an uncalibrated search");
+  if (ctx->has_dom) return fail(ctx, BTK_EUNSUPPORTED, "the leave-one-out gradient takes samples without domains");
   CK(cudaSetDevice(ctx->device));
   const int64_t n = ctx->n;
   CK(ctx->loo_nbr.grow(size_t(n) * size_t(ctx->search.max_samples)));
@@ -1428,6 +1520,7 @@ int btk_mean_freeze(btk_ctx* ctx, const btk_geometry* g) {
     return fail(ctx, BTK_EUNSUPPORTED, "the mean-estimate gradient takes at most 64 samples per system");
   if (ctx->search.calibration)
     return fail(ctx, BTK_EUNSUPPORTED, "the mean-estimate gradient takes an uncalibrated search");
+  if (ctx->has_dom) return fail(ctx, BTK_EUNSUPPORTED, "the mean-estimate gradient takes samples without domains");
   CK(cudaSetDevice(ctx->device));
   const int64_t m = g->count[0] * g->count[1] * g->count[2];
   const int* tw = ctx->tuning.tile;

@@ -63,6 +63,12 @@ struct SearchDev {
   int sgs;
   uint32_t sgs_node0;
   const uint8_t* sgs_done;
+  // Hard domains (search.rs:269-288 with no soft boundary): a target of
+  // domain tdom[t] takes only samples of its own domain sdom[i] (codes >= 0;
+  // a target code < 0, a domain without samples, takes none). Run by
+  // k_search_rules. Null: no domains.
+  const int32_t* sdom;
+  const int32_t* tdom;
 };
 
 // Internal per-target status of a simulation search: searched too early.

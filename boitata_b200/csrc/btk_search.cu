@@ -539,7 +539,7 @@ __device__ __forceinline__ int hole_slot(const RulesSmem<K>& S, uint32_t h) {
 template <int K>
 __device__ int rules_scan(const SearchDev& sp, const GridDev& g, RulesSmem<K>& S, const double q[3], const double t[3],
                           uint32_t left, double after_d, uint32_t after_i, bool filter, unsigned openmask,
-                          bool& dropped, int lane, uint32_t my, double& d2u) {
+                          bool& dropped, int lane, uint32_t my, double& d2u, int32_t dom) {
   const double glo[3] = {g.lo[0], g.lo[1], g.lo[2]};
   const double ghi[3] = {g.lo[0] + g.dims[0] * g.h, g.lo[1] + g.dims[1] * g.h, g.lo[2] + g.dims[2] * g.h};
   const unsigned all = sp.nsec > 1 ? (1u << sp.nsec) - 1u : 1u;
@@ -598,6 +598,7 @@ __device__ int rules_scan(const SearchDev& sp, const GridDev& g, RulesSmem<K>& S
               d2 = d2_exact(g.px[c], g.py[c], g.pz[c], q[0], q[1], q[2]);
               idx = g.idx[c];
               keep = d2 <= thr && idx != left && key_less(after_d, after_i, d2, idx);
+              if (sp.sdom) keep = keep && sp.sdom[idx] == dom;  // samples of the target's domain only
               if (sp.sgs && d2 <= thr && idx >= sp.sgs_node0) {  // a grid node of a simulation
                 if (idx < my && !sp.sgs_done[idx]) d2u = fmin(d2u, d2);
                 keep = keep && idx < my && sp.sgs_done[idx];
@@ -682,6 +683,7 @@ __global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, c
     }
     const uint32_t left = loo ? uint32_t(ti) : 0xffffffffu;
     const uint32_t my = sp.sgs ? sp.sgs_node0 + uint32_t(ti) : 0xffffffffu;
+    const int32_t dom = sp.sdom ? sp.tdom[ti] : 0;  // the target's domain (hard boundaries)
     double d2u = INFINITY, far = 0.0;  // nearest unsimulated earlier node; farthest accepted
     for (int i = lane; i < kHoleHash; i += 32) S.hkey[i] = kNoHole, S.hcnt[i] = 0;
     for (int i = lane; i < 360; i += 32) S.per_sector[i] = 0;
@@ -699,7 +701,7 @@ __global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, c
       // After a cut, only the K nearest are an exact prefix of the (d2, index)
       // order: entries kept since then can skip cut ones of equal d2.
       const int nscan =
-          rules_scan(sp, g, S, q, t, left, after_d, after_i, filter, openmask, dropped, lane, my, d2u);
+          rules_scan(sp, g, S, q, t, left, after_d, after_i, filter, openmask, dropped, lane, my, d2u, dom);
       const int n = dropped ? K : nscan;
       if (sp.balances)
         for (int i = lane; i < n; i += 32) {

@@ -7,11 +7,11 @@ sharing a location keep the first one with a warning (args.rs:318-376),
 targets a search cannot fill are NaN, several searches run as passes on the
 targets earlier passes left (batch.rs:132-147). The kriging itself runs in
 the CUDA engine through its C ABI; `precision` selects the FP64 form
-(default, the reference's arithmetic) or the mixed FP32/FP64 form. In the
-mixed form a system whose FP32 factor is too weak is re-solved in FP64; once
-one call of an estimator re-solved most of its systems that way (an
-ill-conditioned model), its later calls until the next fit run the FP64 form
-directly, with the same results for those systems.
+(default, the reference's arithmetic) or the mixed form (FP32 factorisation
+refined in FP64; a system whose refinement does not converge is re-solved in
+FP64). Hard domains (`fit(domains=)`, `predict(domains=)`) restrict each
+target to its own domain's samples; `cross_validate(folds=k)` runs the
+reference's k-fold scheme (batch.rs:197-243).
 """
 
 import contextlib
@@ -77,11 +77,79 @@ def hole_codes(labels):
     return out
 
 
-def distinct(locs, holes=None):
-    """Rows to keep so no two samples share a location: the first of each group,
-    with a UserWarning naming the dropped groups (args.rs:318-376 over
-    eda::duplicates with tolerance 0, which treats -0 as 0)."""
+def _label_key(v):
+    """A domain label as the reference keys it (crates/py/src/args.rs:16-37): strings, booleans, integral
+    numbers as integers, other finite numbers; None for a missing label (None or NaN)."""
+    if v is None:
+        return None
+    if isinstance(v, (bool, np.bool_)):
+        return ("bool", bool(v))
+    if isinstance(v, str):
+        return ("str", v)
+    if isinstance(v, (int, np.integer)):
+        return ("num", int(v))
+    try:
+        f = float(v)
+    except (TypeError, ValueError):
+        f = None
+    if f is None or math.isinf(f):
+        raise InvalidInput(f"domain labels must be strings, finite numbers or booleans, not {v!r}")
+    if math.isnan(f):
+        return None
+    return ("num", int(f)) if f == int(f) and abs(f) < 9e15 else ("num", f)
+
+
+def _labels(obj, n):
+    """A sequence of n labels, or one label for all (crates/py/src/estimation.rs:250-265)."""
+    if isinstance(obj, (str, bool, int, float, np.generic)) or not hasattr(obj, "__len__"):
+        return [obj] * n
+    labels = list(obj)
+    if len(labels) != n:
+        raise InvalidInput(f"domains: expected {n} values, got {len(labels)}")
+    return labels
+
+
+def domain_codes(obj, n):
+    """(fitted labels by code, int32 codes of the n samples): one code per distinct label in order of first
+    appearance (crates/py/src/estimation.rs:1321-1333); every sample needs a label."""
+    fitted, code, out = [], {}, np.empty(n, dtype=np.int32)
+    for i, v in enumerate(_labels(obj, n)):
+        k = _label_key(v)
+        if k is None:
+            raise InvalidInput(f"domain labels must be strings, finite numbers or booleans, not {v!r}")
+        if k not in code:
+            code[k] = len(fitted)
+            fitted.append(v)
+        out[i] = code[k]
+    return fitted, out
+
+
+def target_codes(fitted, obj, n, method="predict"):
+    """Codes of n target labels among the fitted ones, -1 for a domain without samples
+    (crates/py/src/estimation.rs:1337-1360)."""
+    if fitted is None and obj is None:
+        return None
+    if fitted is not None and obj is None:
+        raise InvalidInput(f"fitted with domains; {method} needs domains too")
+    if fitted is None:
+        raise InvalidInput(f"fitted without domains; {method} takes none")
+    code = {_label_key(v): c for c, v in enumerate(fitted)}
+    out = np.empty(n, dtype=np.int32)
+    for i, v in enumerate(_labels(obj, n)):
+        k = _label_key(v)
+        if k is None:
+            raise InvalidInput(f"domain labels must be strings, finite numbers or booleans, not {v!r}")
+        out[i] = code.get(k, -1)
+    return out
+
+
+def distinct(locs, holes=None, domains=None):
+    """Rows to keep so no two samples share a location (within a domain, with domains): the first of each
+    group, with a UserWarning naming the dropped groups (args.rs:318-376 over eda::duplicates with
+    tolerance 0, which treats -0 as 0)."""
     key = np.ascontiguousarray(locs + 0.0)
+    if domains is not None:
+        key = np.column_stack([key, np.asarray(domains, dtype=np.float64)])
     _, first, inverse, counts = np.unique(key, axis=0, return_index=True, return_inverse=True, return_counts=True)
     inverse = inverse.ravel()
     if np.all(counts == 1):
@@ -163,8 +231,11 @@ class _Base:
         self._samples = None
 
     # -- fit --------------------------------------------------------------
-    def fit(self, coords, values, *, holes=None, error_variance=None):
-        """Stores the samples; samples sharing a location keep the first one, with a warning."""
+    def fit(self, coords, values, *, holes=None, error_variance=None, domains=None):
+        """Stores the samples; samples sharing a location keep the first one, with a warning. With
+        `domains` (one label per sample: strings, finite numbers or booleans) a target is estimated from
+        the samples of its own domain only (hard boundaries), shared locations are dropped within a domain
+        only, and predict needs the targets' domains too (python/boitata/estimation.py:226-250)."""
         locs = points(coords)
         n = len(locs)
         vals = finite(values, "values", n)
@@ -177,10 +248,13 @@ class _Base:
             holes = list(holes)
             if len(holes) != n:
                 raise InvalidInput(f"holes: expected {n} values, got {len(holes)}")
-        keep = distinct(locs, holes)
+        fitted, codes = (None, None) if domains is None else domain_codes(domains, n)
+        keep = distinct(locs, holes, codes)
         locs, vals = np.ascontiguousarray(locs[keep]), np.ascontiguousarray(vals[keep])
         err = None if err is None else np.ascontiguousarray(err[keep])
         self._holes = None if holes is None else np.ascontiguousarray(hole_codes(holes)[keep])
+        self._domain_labels = fitted
+        self._domains = None if codes is None else np.ascontiguousarray(codes[keep])
         self._samples = (locs, vals, err)
         if self._ctx is None:
             self._ctx = N.Context(self._device)
@@ -208,7 +282,10 @@ class _Base:
         from . import persist
 
         cols = persist.columns(self)
-        return {"meta": persist.envelope(self), "columns": cols, "holes": getattr(self, "_holes", None)}
+        doms = getattr(self, "_domains", None)
+        labels = getattr(self, "_domain_labels", None)
+        return {"meta": persist.envelope(self), "columns": cols, "holes": getattr(self, "_holes", None),
+                "domains": None if doms is None else [labels[c] for c in doms]}
 
     def __setstate__(self, state):
         from . import persist
@@ -224,7 +301,7 @@ class _Base:
             err = cols["error_variance"]
             self.fit(np.column_stack([cols["x"], cols["y"], cols["z"]]), cols["value"],
                      holes=None if holes is None else [int(h) for h in holes],
-                     error_variance=None if not err.any() else err)
+                     error_variance=None if not err.any() else err, domains=state.get("domains"))
 
     def _use_pass(self, p):
         if self._pass == p:
@@ -239,6 +316,9 @@ class _Base:
                                   None if err is None else err.ctypes.data,
                                   None if holes is None else holes.ctypes.data, ctypes.byref(s), ctypes.byref(vg))
             ctx.check(rc, "fit")
+            doms = getattr(self, "_domains", None)
+            if doms is not None:
+                ctx.check(ctx._lib.btk_set_domains(ctx.handle, doms.ctypes.data), "domains")
         else:
             ctx.check(ctx._lib.btk_set_search(ctx.handle, ctypes.byref(s)), "search")
         self._pass = p
@@ -253,7 +333,7 @@ class _Base:
         return self._samples[1].copy()
 
     # -- predict ------------------------------------------------------------
-    def _run(self, xyz, precision, diagnostics=False):
+    def _run(self, xyz, precision, diagnostics=False, domains=None):
         m = len(xyz)
         out = {k: np.full(m, np.nan) for k in ("value", "variance", "lagrange")}
         out["n_used"] = np.zeros(m, dtype=np.int32)
@@ -269,13 +349,11 @@ class _Base:
                        out["n_used"].ctypes.data, out["status"].ctypes.data)
         xyz = np.ascontiguousarray(xyz, dtype=np.float64)
         ctx = self._ctx
-        if diagnostics:
-            d = N.DiagnosticsC(*(out[k].ctypes.data for k in DIAGNOSTICS))
-            rc = ctx._lib.btk_predict_diagnostics(ctx.handle, m, xyz.ctypes.data, self._kind, self._kparam,
-                                                  PRECISIONS[precision], ctypes.byref(o), ctypes.byref(d))
-        else:
-            rc = ctx._lib.btk_predict(ctx.handle, m, xyz.ctypes.data, self._kind, self._kparam,
-                                      PRECISIONS[precision], ctypes.byref(o))
+        d = N.DiagnosticsC(*(out[k].ctypes.data for k in DIAGNOSTICS)) if diagnostics else None
+        dom = None if domains is None else np.ascontiguousarray(domains, dtype=np.int32)
+        rc = ctx._lib.btk_predict_ex(ctx.handle, m, xyz.ctypes.data, None, None if dom is None else dom.ctypes.data,
+                                     self._kind, self._kparam, PRECISIONS[precision], ctypes.byref(o),
+                                     None if d is None else ctypes.byref(d))
         ctx.check(rc, "predict")
         return out
 
@@ -289,9 +367,10 @@ class _Base:
         z = locs[0, 2]
         return z if math.isfinite(z) and np.all(locs[:, 2] == z) else None
 
-    def predict_full(self, targets, *, precision=None, diagnostics=False):
+    def predict_full(self, targets, *, precision=None, diagnostics=False, domains=None):
         """Every output of the engine: value, variance, lagrange, n_used, status and pass (1-based, 0 unfilled);
-        with `diagnostics`, also negative_weight_sum, mean_distance and n_holes of the samples used."""
+        with `diagnostics`, also negative_weight_sum, mean_distance and n_holes of the samples used.
+        `domains`: the targets' domain labels (one per target, or one for all) when fitted with domains."""
         self._fitted()
         precision = precision or self.precision
         if precision not in PRECISIONS:
@@ -305,14 +384,15 @@ class _Base:
                 xyz[:, 2] = z
         else:
             xyz = points(targets)
+        codes = target_codes(getattr(self, "_domain_labels", None), domains, len(xyz))
         with self._support(targets):
-            return self._passes(xyz, precision, diagnostics)
+            return self._passes(xyz, precision, diagnostics, codes)
 
     def _support(self, targets):
         """Context manager setting the engine's target support for one prediction (point support here)."""
         return contextlib.nullcontext()
 
-    def _passes(self, xyz, precision, diagnostics=False):
+    def _passes(self, xyz, precision, diagnostics=False, codes=None):
         m = len(xyz)
         res = None
         remaining = np.arange(m)
@@ -320,7 +400,7 @@ class _Base:
             if len(remaining) == 0:
                 break
             self._use_pass(p)
-            out = self._run(xyz[remaining], precision, diagnostics)
+            out = self._run(xyz[remaining], precision, diagnostics, None if codes is None else codes[remaining])
             if res is None:
                 res = {k: v.copy() for k, v in out.items()}
                 res["pass"] = np.where(np.isfinite(out["value"]), 1, 0).astype(np.int32)
@@ -334,14 +414,16 @@ class _Base:
             remaining = np.nonzero(~np.isfinite(res["value"]))[0]
         return res
 
-    def predict(self, targets, *, return_variance=False, diagnostics=False, precision=None):
+    def predict(self, targets, *, return_variance=False, diagnostics=False, precision=None, domains=None):
         """Estimates at targets; NaN where the search found too few samples (estimation.py:273-335).
 
         targets : (n, 2|3) array, Geometry or BlockModel (centroids made on the device).
+        domains : the targets' domain labels (one per target, or one for all), when fitted with domains; a
+            target of a domain without samples is NaN.
         """
         if diagnostics:
-            return self._diagnostics(targets, precision)
-        res = self.predict_full(targets, precision=precision)
+            return self._diagnostics(targets, precision, domains)
+        res = self.predict_full(targets, precision=precision, domains=domains)
         if return_variance:
             return res["value"], res["variance"]
         return res["value"]
@@ -350,9 +432,10 @@ class _Base:
         """C(v, v) of the targets' support: the sill for points (krige.rs:40-42)."""
         return self.variogram.total_sill()
 
-    def _diagnostics(self, targets, precision):
-        """The diagnostics table (crates/py/src/estimation.rs:1046-1105): NaN where unestimated."""
-        res = self.predict_full(targets, precision=precision, diagnostics=True)
+    def _diagnostics(self, targets, precision, domains=None):
+        """The diagnostics table (crates/py/src/estimation.rs:1046-1105): NaN where unestimated. With hard
+        domains every sample used is of the target's domain, so n_other_domain is 0."""
+        res = self.predict_full(targets, precision=precision, diagnostics=True, domains=domains)
         est = np.isfinite(res["value"])
         nan = lambda v: np.where(est, v, np.nan)  # noqa: E731
         sv = nan(np.full(len(est), self._support_variance(targets)))
@@ -405,29 +488,85 @@ class _Base:
         return out
 
     def cross_validate(self, *, folds=None, precision=None):
-        """Re-estimates every sample from the others, through the same passes (estimation.py:337-355)."""
+        """Re-estimates every sample from the others, through the same passes (estimation.py:337-355):
+        leave-one-out when `folds` is None, else k-fold (batch.rs:197-243): each sample estimated without the
+        samples of its fold, where the j-th of the sorted hole ids goes to fold j % k (holes stay whole) and
+        an untagged sample i to fold i % k; each held-out sample in its own domain."""
         self._fitted()
-        if folds is not None:
-            raise Unsupported("k-fold cross-validation is not run by this engine; use folds=None (leave-one-out)")
         precision = precision or self.precision
         n = len(self._samples[0])
         est = np.full(n, np.nan)
         var = np.full(n, np.nan)
+        if folds is not None:
+            k = int(folds)
+            if k != folds or k < 2:
+                raise InvalidInput("k must be ≥ 2")
+            fold = self._folds(k)
         for p in range(len(self.searches)):
-            self._use_pass(p)
-            value, variance = np.full(n, np.nan), np.full(n, np.nan)
-            o = N.OutputsC(value.ctypes.data, variance.ctypes.data, None, None, None)
-            ctx = self._ctx
-            ctx.check(ctx._lib.btk_cross_validate(ctx.handle, self._kind, self._kparam, PRECISIONS[precision],
-                                                  ctypes.byref(o)), "cross_validate")
+            remaining = np.nonzero(~np.isfinite(est))[0]
+            if len(remaining) == 0:
+                break
+            if folds is None:
+                self._use_pass(p)
+                value, variance = np.full(n, np.nan), np.full(n, np.nan)
+                o = N.OutputsC(value.ctypes.data, variance.ctypes.data, None, None, None)
+                ctx = self._ctx
+                ctx.check(ctx._lib.btk_cross_validate(ctx.handle, self._kind, self._kparam, PRECISIONS[precision],
+                                                      ctypes.byref(o)), "cross_validate")
+            else:
+                value, variance = self._k_fold(fold, k, remaining, p, precision)
             fill = ~np.isfinite(est) & np.isfinite(value)
             est[fill], var[fill] = value[fill], variance[fill]
-            if np.all(np.isfinite(est)):
-                break
         return CrossValidation(self._samples[1].copy(), est, var)
 
-    def neighbors(self, targets, *, loo=False, search_pass=0):
-        """Neighbour lists (selection order, -1 padded), counts and success flags of the search."""
+    def _folds(self, k):
+        """Fold of each fitted sample (batch.rs:210-220): rank of its hole id among the sorted ids, or its
+        index when untagged, modulo k."""
+        n = len(self._samples[0])
+        holes = getattr(self, "_holes", None)
+        if holes is None:
+            return np.arange(n) % k
+        ids = np.unique(holes)
+        return np.searchsorted(ids, holes) % k
+
+    def _k_fold(self, fold, k, which, p, precision):
+        """Estimates at samples `which` with search pass p, each from a fit of the samples outside its fold
+        (a new index per fold, as the reference builds a new tree over the training samples)."""
+        n = len(self._samples[0])
+        value, variance = np.full(n, np.nan), np.full(n, np.nan)
+        locs, vals, err = self._samples
+        holes, doms = getattr(self, "_holes", None), getattr(self, "_domains", None)
+        s = self.searches[p].to_c()
+        vg = self.variogram.to_c()
+        for f in range(k):
+            test = which[fold[which] == f]
+            if len(test) == 0:
+                continue
+            train = np.nonzero(fold != f)[0]
+            ctx = N.Context(self._device)
+            sub = lambda a: None if a is None else np.ascontiguousarray(a[train])  # noqa: E731
+            tl, tv, te, th, td = sub(locs), sub(vals), sub(err), sub(holes), sub(doms)
+            rc = ctx._lib.btk_fit(ctx.handle, len(train), tl.ctypes.data, tv.ctypes.data,
+                                  None if te is None else te.ctypes.data, None if th is None else th.ctypes.data,
+                                  ctypes.byref(s), ctypes.byref(vg))
+            ctx.check(rc, "fit")
+            if td is not None:
+                ctx.check(ctx._lib.btk_set_domains(ctx.handle, td.ctypes.data), "domains")
+            m = len(test)
+            xyz = np.ascontiguousarray(locs[test])
+            v, sv = np.full(m, np.nan), np.full(m, np.nan)
+            o = N.OutputsC(v.ctypes.data, sv.ctypes.data, None, None, None)
+            dom = None if doms is None else np.ascontiguousarray(doms[test])
+            ctx.check(ctx._lib.btk_predict_ex(ctx.handle, m, xyz.ctypes.data, None,
+                                              None if dom is None else dom.ctypes.data, self._kind, self._kparam,
+                                              PRECISIONS[precision], ctypes.byref(o), None), "k-fold predict")
+            value[test], variance[test] = v, sv
+            del ctx
+        return value, variance
+
+    def neighbors(self, targets, *, loo=False, search_pass=0, domains=None):
+        """Neighbour lists (selection order, -1 padded), counts and success flags of the search; `domains`
+        as for predict when fitted with domains."""
         self._fitted()
         self._use_pass(search_pass)
         k = self.searches[search_pass].max_samples
@@ -441,8 +580,10 @@ class _Base:
         cnt = np.empty(m, dtype=np.int32)
         ok = np.empty(m, dtype=np.int8)
         ctx = self._ctx
+        codes = None if loo else target_codes(getattr(self, "_domain_labels", None), domains, m, "neighbors")
         rc = ctx._lib.btk_neighbors(ctx.handle, m, None if xyz is None else xyz.ctypes.data, 1 if loo else 0,
-                                    idx.ctypes.data, cnt.ctypes.data, ok.ctypes.data)
+                                    None if codes is None else codes.ctypes.data, idx.ctypes.data, cnt.ctypes.data,
+                                    ok.ctypes.data)
         ctx.check(rc, "neighbors")
         return idx, cnt, ok.astype(bool)
 

@@ -16,7 +16,7 @@ model,aniso}.rs) and each search pass (crates/estimation/src/search.rs:31-
 may be infinite or NaN are written as "inf", "-inf", "NaN"
 (crates/core/src/nonfinite.rs). A file the reference wrote loads here and
 predicts as the saved estimator did; options this engine does not run
-(domains, high-grade, soft boundaries, external drift) raise Unsupported.
+(high-grade, soft boundaries, external drift) raise Unsupported.
 """
 
 import json
@@ -181,7 +181,20 @@ def envelope(est):
               "method": method_json(est), "variogram": variogram_json(est.variogram),
               "search": [search_json(s) for s in est.searches], "drift_data": [], "units": [None, None, None],
               "precision": est.precision}  # this engine's own field; serde ignores unknown fields
+    labels = getattr(est, "_domain_labels", None)
+    if labels is not None:  # the fitted domain labels, indexed by the domain column's codes
+        fields["domains"] = [_label_json(v) for v in labels]
     return json.dumps(fields, separators=(",", ":"), allow_nan=False)
+
+
+def _label_json(v):
+    """A domain label as JSON: string, boolean, or number (integral numbers as integers)."""
+    if isinstance(v, (bool, np.bool_)):
+        return bool(v)
+    if isinstance(v, str):
+        return v
+    f = float(v)
+    return int(f) if f == int(f) and abs(f) < 9e15 else f
 
 
 def columns(est):
@@ -195,7 +208,8 @@ def columns(est):
             "z": locs[:, 2].astype(np.float64), "value": np.asarray(vals, dtype=np.float64),
             "hole": None if holes is None else np.asarray(holes, dtype=np.float64),
             "error_variance": np.zeros(n) if err is None else np.asarray(err, dtype=np.float64),
-            "domain": None, "_rows": n}
+            "domain": None if getattr(est, "_domains", None) is None else np.asarray(est._domains, dtype=np.float64),
+            "_rows": n}
 
 
 def to_parquet(est, path):
@@ -253,8 +267,7 @@ def from_parquet(cls, path):
         raise InvalidInput("no boitata metadata")
     d = _open(cls.__name__, meta.decode())
     fitted = d.pop("fitted", None) is True
-    if d.get("domains"):
-        raise Unsupported("estimators fitted with domains are not run by this engine")
+    labels = d.get("domains")
     if d.get("drift_data"):
         raise Unsupported("external-drift estimators are not run by this engine")
     est = _build(cls, d)
@@ -273,18 +286,24 @@ def from_parquet(cls, path):
         for name in ("x", "y", "z", "value", "error_variance"):
             if np.isnan(got[name]).any() and table.column(name).null_count:
                 raise InvalidInput(f"null in column {name}")
-        if (~np.isnan(got["domain"])).any():
-            raise Unsupported("estimators fitted with domains are not run by this engine")
+        doms = None
+        if labels:
+            codes = got["domain"]
+            if np.isnan(codes).any() or np.any((codes < 0) | (codes >= len(labels)) | (codes != np.floor(codes))):
+                raise InvalidInput("domain codes must index the fitted domains")
+            doms = [labels[int(c)] for c in codes]
+        elif (~np.isnan(got["domain"])).any():
+            raise InvalidInput("domain codes without fitted domains")
         holes = got["hole"]
         has = ~np.isnan(holes)
         if has.any():
             h = holes[has]
             if np.any((h < 0) | (h != np.floor(h)) | (h >= 2.0 ** 32 - 1)):
                 raise InvalidInput("hole codes must be indices")
-        labels = None if not has.any() else [int(v) if ok else None for v, ok in zip(holes, has)]
+        hole_labels = None if not has.any() else [int(v) if ok else None for v, ok in zip(holes, has)]
         err = got["error_variance"]
-        est.fit(np.column_stack([got["x"], got["y"], got["z"]]), got["value"], holes=labels,
-                error_variance=None if not err.any() else err)
+        est.fit(np.column_stack([got["x"], got["y"], got["z"]]), got["value"], holes=hole_labels,
+                error_variance=None if not err.any() else err, domains=doms)
     return est
 
 

@@ -238,9 +238,38 @@ int btk_cross_validate(btk_ctx* ctx, int32_t kind, double kparam, int32_t precis
 /* Neighbour lists of m host targets: `idx` (m x max_samples, -1 padded) in
  * selection order, `count` per target, `ok` 1 where the search succeeds.
  * With `loo` set the targets are the n fitted samples themselves (xyz and m
- * ignored), each searched as if it were absent (search.rs:951-982). */
-int btk_neighbors(btk_ctx* ctx, int64_t m, const double* xyz, int32_t loo, int64_t* idx, int32_t* count,
-                  int8_t* ok);
+ * ignored), each searched as if it were absent (search.rs:951-982).
+ * `domains`: the targets' domain codes when the samples have domains
+ * (btk_set_domains), else NULL; ignored with `loo`. */
+int btk_neighbors(btk_ctx* ctx, int64_t m, const double* xyz, int32_t loo, const int32_t* domains, int64_t* idx,
+                  int32_t* count, int8_t* ok);
+
+/* Hard domains (crates/estimation/src/search.rs:269-288 with no soft
+ * boundary; batch.rs:15-38 `domains`): after btk_fit, `codes` gives each
+ * fitted sample's domain (n codes >= 0, host; NULL removes the domains).
+ * Every later search of a target of domain d then takes only samples of
+ * domain d, and leave-one-out takes each sample's own domain. Predictions
+ * must then give each target's domain code (btk_predict_ex), a code < 0
+ * (a domain without samples) leaving the target unestimated (status
+ * BTK_ST_SEARCH_FAILED); the calls without target domains return BTK_EINVAL,
+ * as the reference refuses them. The caller drops exact duplicates within a
+ * domain only (crates/py/src/estimation.rs:1273-1308); samples of different
+ * domains at one location never meet in a search. The gradients and the
+ * simulation take samples without domains. */
+int btk_set_domains(btk_ctx* ctx, const int32_t* codes);
+
+/* Prediction at m host targets with every option of the reference's
+ * estimator call: `kinds` (one int8 kind per target, or NULL for `kind`),
+ * `domains` (one domain code per target, required exactly when the samples
+ * have domains), outputs as btk_predict and, when `diag` is given (out->status
+ * then required), the diagnostics columns as btk_predict_diagnostics. */
+int btk_predict_ex(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds, const int32_t* domains,
+                   int32_t kind, double kparam, int32_t precision, const btk_outputs* out,
+                   const btk_diagnostics* diag);
+/* The same with device arrays (d_xyz as btk_predict_device), queued on `stream`. */
+int btk_predict_ex_device(btk_ctx* ctx, int64_t m, const double* d_xyz, const int8_t* d_kinds,
+                          const int32_t* d_domains, int32_t kind, double kparam, int32_t precision,
+                          const btk_outputs* d_out, void* stream);
 
 /* Centroids of cells [first, first + m) of `g` into host xyz (m x 3). */
 int btk_centroids(btk_ctx* ctx, const btk_geometry* g, int64_t first, int64_t m, double* xyz);

@@ -310,7 +310,7 @@ struct Variogram {
 enum Kind { ORDINARY = 0, SIMPLE = 1, INDICATOR = 2 };
 enum Status { OK = 0, SEARCH_FAILED = 1, SINGULAR = 2, INSUFFICIENT = 3, INVALID = 4, NONE = -1 };
 
-struct Sample { double loc[3]; double value; int64_t hole; double err; };
+struct Sample { double loc[3]; double value; int64_t hole; double err; int64_t domain = -1; };
 
 struct Estimate {
   double value = NAN, variance = NAN, lagrange = NAN, support = NAN;
@@ -1051,18 +1051,68 @@ struct Tree {
     grid.build(points);
   }
 
-  // neighbors_around with domain None and no high-grade / soft rules: every
-  // sample is admitted and one_per_location is the identity, so the group
-  // logic offers the (d2, index) stream in order.
-  bool neighbors(const double t[3], int64_t left_out, std::vector<size_t>& out) const {
+  // search.rs:269-288 (Search::admits) with hard domain boundaries (no soft
+  // distance) and no high-grade rule: a sample of another domain than the
+  // target's never informs it; an untagged target or sample is admitted.
+  static bool admits(int64_t tdomain, int64_t sdomain) { return tdomain < 0 || sdomain < 0 || tdomain == sdomain; }
+
+  // search.rs:597-632 (one_per_location): samples at one location (the
+  // coordinates' bits, -0 as 0) reduced to the first, replaced by the first
+  // one of the target's domain if it is not; nothing changes without a
+  // target domain.
+  std::vector<size_t> one_per_location(const std::vector<size_t>& ordered, int64_t tdomain) const {
+    if (tdomain < 0) return ordered;
+    std::vector<size_t> out;
+    std::vector<std::array<uint64_t, 3>> keys;
+    for (size_t i : ordered) {
+      std::array<uint64_t, 3> k;
+      for (int a = 0; a < 3; ++a) {
+        const double v = (*samples)[i].loc[a] + 0.0;
+        std::memcpy(&k[a], &v, sizeof(double));
+      }
+      size_t at = keys.size();
+      for (size_t j = 0; j < keys.size(); ++j)
+        if (keys[j] == k) { at = j; break; }
+      if (at == keys.size()) {
+        keys.push_back(k);
+        out.push_back(i);
+      } else if ((*samples)[out[at]].domain != tdomain && (*samples)[i].domain == tdomain) {
+        out[at] = i;
+      }
+    }
+    return out;
+  }
+
+  // search.rs:951-1005 (neighbors_around): the (d2, index) stream of the grid
+  // is offered in groups of equal d2, each reduced to the admitted samples
+  // (without `left_out`) and one per location.
+  bool neighbors(const double t[3], int64_t left_out, std::vector<size_t>& out, int64_t tdomain = -1) const {
     Selector sel(t, params, sectors);
     if (!samples->empty() && params.max_samples > 0) {
       double q[3];
       space.project(t, q);
-      grid.nearest(q, params.radius * params.radius, [&](double, size_t i) {
-        if (int64_t(i) == left_out) return false;
-        return sel.offer(i, (*samples)[i].loc, (*samples)[i].hole);
+      std::vector<size_t> group;
+      double at = NAN;
+      bool full = false;
+      auto offer = [&]() {
+        std::vector<size_t> admitted;
+        for (size_t i : group)
+          if (int64_t(i) != left_out && admits(tdomain, (*samples)[i].domain)) admitted.push_back(i);
+        group.clear();
+        for (size_t i : one_per_location(admitted, tdomain))
+          if (sel.offer(i, (*samples)[i].loc, (*samples)[i].hole)) return true;
+        return false;
+      };
+      grid.nearest(q, params.radius * params.radius, [&](double d2, size_t i) {
+        if (d2 != at && !group.empty()) {
+          full = offer();
+          if (full) return true;
+        }
+        at = d2;
+        group.push_back(i);
+        return false;
       });
+      if (!full) offer();
     }
     out = sel.chosen;
     return sel.finish();
@@ -1410,11 +1460,19 @@ static void diag_of(const double t[3], const std::vector<Sample>& sel, const Est
 // a calibration), NaN where a target is not estimated. A calibrated search
 // orders the chosen samples with balanced and keeps the calibrated count. Threads take static chunks of targets, like rayon's per-target
 // independence.
+// With `sdomain` (the samples' domain codes, or null) each target krigs from
+// its own domain, tdomain[k] (batch.rs:15-38 `domains`; the left-out
+// sample's own with `loo`); a target code < 0 is a domain without samples,
+// which the reference leaves unestimated (crates/py/src/estimation.rs:1655-
+// 1657), here SEARCH_FAILED.
 int32_t orc_estimate_many(int64_t m, const double* targets, int32_t loo, int64_t n, const double* xyz,
                           const double* v, const double* err, const int64_t* hole, const orc_search* sp,
                           const orc_variogram* vgp, int32_t kind, double kparam, int32_t nthreads,
-                          orc_result* res, int64_t* nbr, double* diag) {
+                          orc_result* res, int64_t* nbr, double* diag, const int64_t* sdomain,
+                          const int64_t* tdomain) {
   std::vector<Sample> s = conv_samples(n, xyz, v, err, hole);
+  if (sdomain)
+    for (int64_t i = 0; i < n; ++i) s[size_t(i)].domain = sdomain[i];
   SearchP p = conv_search(sp);
   if (!check(p)) return -1;
   Variogram vg = conv_vg(vgp);
@@ -1424,8 +1482,9 @@ int32_t orc_estimate_many(int64_t m, const double* targets, int32_t loo, int64_t
   auto work = [&](int64_t k0, int64_t k1) {
     for (int64_t k = k0; k < k1; ++k) {
       const double* t = loo ? s[size_t(k)].loc : &targets[3 * k];
+      const int64_t dom = !sdomain ? -1 : (loo ? sdomain[k] : tdomain[k]);
       std::vector<size_t> chosen;
-      bool ok = tree.neighbors(t, loo ? k : -1, chosen);
+      bool ok = sdomain && dom < 0 ? false : tree.neighbors(t, loo ? k : -1, chosen, dom);
       if (nbr) {
         for (size_t j = 0; j < maxs; ++j) nbr[size_t(k) * maxs + j] = j < chosen.size() ? int64_t(chosen[j]) : -1;
       }
@@ -1457,6 +1516,58 @@ int32_t orc_estimate_many(int64_t m, const double* targets, int32_t loo, int64_t
     if (k0 < k1) pool.emplace_back(work, k0, k1);
   }
   for (auto& th : pool) th.join();
+  return 0;
+}
+
+// crates/estimation/src/batch.rs:197-243 (k_fold_at over every sample): the
+// j-th of the sorted hole ids goes to fold j % k and an untagged sample i to
+// fold i % k; each fold's samples are kriged, each in its own domain, from a
+// tree over the samples outside the fold (a new space, so a new origin).
+int32_t orc_k_fold(int64_t k, int64_t n, const double* xyz, const double* v, const double* err, const int64_t* hole,
+                   const int64_t* sdomain, const orc_search* sp, const orc_variogram* vgp, int32_t kind,
+                   double kparam, orc_result* res) {
+  if (k < 2) return -2;
+  std::vector<Sample> s = conv_samples(n, xyz, v, err, hole);
+  if (sdomain)
+    for (int64_t i = 0; i < n; ++i) s[size_t(i)].domain = sdomain[i];
+  SearchP p = conv_search(sp);
+  if (!check(p)) return -1;
+  Variogram vg = conv_vg(vgp);
+  std::vector<int64_t> ids;
+  for (auto& x : s)
+    if (x.hole >= 0) ids.push_back(x.hole);
+  std::sort(ids.begin(), ids.end());
+  ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+  std::vector<int64_t> fold(static_cast<size_t>(n));
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t h = s[size_t(i)].hole;
+    const int64_t r = h < 0 ? i : int64_t(std::lower_bound(ids.begin(), ids.end(), h) - ids.begin());
+    fold[size_t(i)] = r % k;
+  }
+  for (int64_t f = 0; f < k; ++f) {
+    std::vector<Sample> train;
+    for (int64_t i = 0; i < n; ++i)
+      if (fold[size_t(i)] != f) train.push_back(s[size_t(i)]);
+    Tree tree(train, p, &vg);
+    for (int64_t i = 0; i < n; ++i) {
+      if (fold[size_t(i)] != f) continue;
+      const double* t = s[size_t(i)].loc;
+      std::vector<size_t> chosen;
+      Estimate e;
+      if (!tree.neighbors(t, -1, chosen, sdomain ? s[size_t(i)].domain : -1) || chosen.empty()) {
+        put(e, SEARCH_FAILED, &res[i]);
+        continue;
+      }
+      std::vector<Sample> sel;
+      for (size_t c : balanced(tree, t, chosen)) sel.push_back(train[c]);
+      if (p.calibration) {
+        std::vector<double> rhs;
+        for (auto& x : sel) rhs.push_back(vg.cov_points(x.loc, t));
+        calibrate(p, vg, kind, rhs, vg.total_sill(), sel);
+      }
+      put(e, krige(kind, kparam, t, sel, vg, e), &res[i]);
+    }
+  }
   return 0;
 }
 

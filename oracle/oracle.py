@@ -93,7 +93,9 @@ def lib():
                                                     ctypes.POINTER(Vario), P, P, P]),
             "orc_estimate_many": (ctypes.c_int32, [ctypes.c_int64, P, ctypes.c_int32, ctypes.c_int64, P, P, P, P,
                                                    ctypes.POINTER(Srch), ctypes.POINTER(Vario), ctypes.c_int32,
-                                                   ctypes.c_double, ctypes.c_int32, P, P, P]),
+                                                   ctypes.c_double, ctypes.c_int32, P, P, P, P, P]),
+            "orc_k_fold": (ctypes.c_int32, [ctypes.c_int64, ctypes.c_int64, P, P, P, P, P, ctypes.POINTER(Srch),
+                                            ctypes.POINTER(Vario), ctypes.c_int32, ctypes.c_double, P]),
             "orc_centroids": (None, [P, P, P, P, ctypes.c_int64, ctypes.c_int64, P]),
             "orc_sgs": (ctypes.c_int64, [ctypes.c_int64, P, P, P, ctypes.c_int64, P, P, ctypes.POINTER(Srch),
                                          ctypes.POINTER(Vario), P, P]),
@@ -310,11 +312,13 @@ def sgs(xyz, scores, nodes, z, s, vg, *, holes=None):
 
 
 def estimate_many(targets, xyz, values, s, vg, *, kind="ordinary", kparam=0.0, err=None, holes=None, loo=False,
-                  threads=0, neighbors=True, diagnostics=False):
+                  threads=0, neighbors=True, diagnostics=False, domains=None, target_domains=None):
     """estimate_many / leave_one_out_at (batch.rs:15-38, 165-190) with krige of `kind`. With `diagnostics`,
     also the per-target columns of the diagnostics table that need the samples or weights
     (crates/py/src/estimation.rs:1046-1105): negative_weight_sum, mean_distance, n_holes, n_within and
-    target_met (NaN without a calibration)."""
+    target_met (NaN without a calibration). With `domains` (the samples' codes) each target krigs from its
+    own domain, `target_domains` (a code < 0: a domain without samples, not estimated); leave-one-out takes
+    each sample's own."""
     xyz = _xyz(xyz)
     n = len(xyz)
     t = None if loo else _xyz(targets)
@@ -326,9 +330,13 @@ def estimate_many(targets, xyz, values, s, vg, *, kind="ordinary", kparam=0.0, e
     h = None if holes is None else np.ascontiguousarray(holes, dtype=np.int64)
     dg = np.empty((m, 5)) if diagnostics else None
     cs, cv = search(s), variogram(vg)
+    sd = None if domains is None else np.ascontiguousarray(domains, dtype=np.int64)
+    td = None if target_domains is None else np.ascontiguousarray(target_domains, dtype=np.int64)
+    if sd is not None and not loo and td is None:
+        raise ValueError("oracle: samples with domains need target domains")
     rc = lib().orc_estimate_many(m, _ptr(t), 1 if loo else 0, n, xyz.ctypes.data, v.ctypes.data, _ptr(e), _ptr(h),
                                  ctypes.byref(cs), ctypes.byref(cv), KINDS[kind], kparam, threads,
-                                 ctypes.cast(res, P), _ptr(nbr), _ptr(dg))
+                                 ctypes.cast(res, P), _ptr(nbr), _ptr(dg), _ptr(sd), _ptr(td))
     if rc != 0:
         raise ValueError("oracle: invalid search parameters")
     arr = np.ctypeslib.as_array(ctypes.cast(res, ctypes.POINTER(ctypes.c_byte)), shape=(ctypes.sizeof(Result) * m,))
@@ -343,6 +351,23 @@ def estimate_many(targets, xyz, values, s, vg, *, kind="ordinary", kparam=0.0, e
         for j, key in enumerate(("negative_weight_sum", "mean_distance", "n_holes", "n_within", "target_met")):
             out[key] = dg[:, j].copy()
     return out
+
+
+def k_fold(k, xyz, values, s, vg, *, kind="ordinary", kparam=0.0, err=None, holes=None, domains=None):
+    """k_fold_at over every sample (batch.rs:197-243): {value, variance, lagrange, n_used, status}."""
+    xyz = _xyz(xyz)
+    n = len(xyz)
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    e = None if err is None else np.ascontiguousarray(err, dtype=np.float64)
+    h = None if holes is None else np.ascontiguousarray(holes, dtype=np.int64)
+    sd = None if domains is None else np.ascontiguousarray(domains, dtype=np.int64)
+    res = (Result * max(n, 1))()
+    rc = lib().orc_k_fold(int(k), n, xyz.ctypes.data, v.ctypes.data, _ptr(e), _ptr(h), _ptr(sd),
+                          ctypes.byref(search(s)), ctypes.byref(variogram(vg)), KINDS[kind], kparam,
+                          ctypes.cast(res, P))
+    if rc != 0:
+        raise ValueError("oracle: invalid search parameters or k")
+    return _records(res, n)
 
 
 def _records(res, m):

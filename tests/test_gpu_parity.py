@@ -128,6 +128,19 @@ def test_predict_c2_octant_subset(oracle, precision, tol):
     assert_same_estimates(got, ref, tol)
 
 
+def test_predict_c2_model_200k_blocks(oracle):
+    """Both forms over 200,000 blocks of the 3.2M-block c2 model (every 16th cell, the whole model's
+    geometry on the device) against the oracle: FP64 at 1e-10, mixed at 1e-6, per result."""
+    w = W.c2()
+    cells = np.arange(0, w.geometry.cells(), 16)
+    targets = centroids(oracle, w)[cells]
+    ref = oracle.estimate_many(targets, w.coords, w.values, w.search, w.variogram, neighbors=False)
+    est = OrdinaryKriging(w.variogram, w.search).fit(w.coords, w.values)
+    for precision, tol in (("fp64", 1e-10), ("mixed", 1e-6)):
+        got = est.predict_full(w.geometry, precision=precision)
+        assert_same_estimates({k: v[cells] for k, v in got.items()}, ref, tol)
+
+
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 1e-6)])
 def test_predict_up_to_64_samples(oracle, precision, tol):
     w = W.c3()

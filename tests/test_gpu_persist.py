@@ -89,3 +89,22 @@ def test_runs_are_reproducible_across_contexts(precision):
     same((ca.estimate, ca.variance), (cb.estimate, cb.variance))
     big = rng.uniform(0, 100, (5000, 3)) * [1.0, 1.0, 0.3]  # Morton-ordered caller targets
     same(a.predict(big, return_variance=True), b.predict(big, return_variance=True))
+
+
+def test_estimator_with_domains_round_trips(tmp_path):
+    """Domains travel as the fitted labels in the envelope and a code column (crates/py/src/estimation.rs:
+    1110-1145); the reloaded estimator predicts each target in its domain as the saved one does."""
+    labels = np.where(coords[:, 0] < 50.0, "north", "south")
+    tl = np.where(targets[:, 0] < 50.0, "north", "south")
+    est = bt.OrdinaryKriging(model, search).fit(coords, values, domains=labels)
+    path = tmp_path / "zoned.parquet"
+    est.to_parquet(path)
+    table = pq.read_table(path)
+    assert table.column("domain").null_count == 0
+    for back in (bt.OrdinaryKriging.from_parquet(path), pickle.loads(pickle.dumps(est))):
+        same(back.predict(targets, return_variance=True, domains=tl),
+             est.predict(targets, return_variance=True, domains=tl))
+        a, b = est.cross_validate(folds=4), back.cross_validate(folds=4)
+        same((a.estimate, a.variance), (b.estimate, b.variance))
+        with pytest.raises(bt.InvalidInput, match="needs domains too"):
+            back.predict(targets)

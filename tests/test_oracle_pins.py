@@ -570,3 +570,88 @@ def test_calibration_arguments_are_checked_as_the_reference_does():
         SimpleKriging(nested(), s, mean=1.0)
     OrdinaryKriging(nested(), s)
     SimpleKriging(nested(), Search(radius=60, target_efficiency=0.5), mean=1.0)
+
+
+# ---- k-fold and hard domains (crates/estimation/src/batch.rs tests) ----------
+def batch_samples():
+    """batch.rs:256-263: 200 samples at (37 i mod 101, 53 i mod 97, 0), value sin(x / 10) + y / 50."""
+    i = np.arange(200)
+    x, y = (i * 37 % 101).astype(float), (i * 53 % 97).astype(float)
+    return np.column_stack([x, y, np.zeros(200)]), np.sin(x / 10.0) + y / 50.0
+
+
+def batch_grid():
+    """batch.rs:582-586: a 30 x 30 grid of targets 5 apart."""
+    i = np.arange(900)
+    return np.column_stack([(i % 30) * 5.0, (i // 30) * 5.0, np.zeros(900)])
+
+
+def domain_of(p):
+    """batch.rs:991-997."""
+    v = p[0] + 0.3 * p[1]
+    return 0 if v < 45.0 else (1 if v < 80.0 else 2)
+
+
+def batch_search(min_samples, radius):
+    from boitata_b200 import Search
+
+    return Search(radius=radius, max_samples=12, min_samples=min_samples)
+
+
+def spherical_40():
+    from boitata_b200 import Structure, Variogram
+
+    return Variogram([Structure("spherical", 1.0, 40.0)])
+
+
+def same_bits(a, b):
+    return all(np.array_equal(a[k].view(np.int64), b[k].view(np.int64)) for k in ("value", "variance")) and \
+        np.array_equal(a["status"], b["status"])
+
+
+def test_k_fold_with_one_sample_per_fold_is_leave_one_out(oracle):
+    # batch.rs:349-372
+    xyz, v = batch_samples()
+    s, vg = batch_search(4, 30.0), spherical_40()
+    loo = oracle.estimate_many(None, xyz, v, s, vg, loo=True, neighbors=False)
+    folds = oracle.k_fold(len(xyz), xyz, v, s, vg)
+    assert np.sum(loo["status"] == 0) > 150
+    assert same_bits(loo, folds)
+    with pytest.raises(ValueError):
+        oracle.k_fold(1, xyz, v, s, vg)
+
+
+def test_k_fold_never_splits_a_hole(oracle):
+    # batch.rs:463-489: every seventh sample untagged, the others in holes of five; every sample is estimated
+    # for k = 2, 5 and n.
+    xyz, v = batch_samples()
+    i = np.arange(len(xyz))
+    holes = np.where(i % 7 == 0, -1, 1000 - i // 5)
+    s, vg = batch_search(2, 60.0), spherical_40()
+    for k in (2, 5, len(xyz)):
+        out = oracle.k_fold(k, xyz, v, s, vg, holes=holes)
+        assert np.all(out["status"] == 0), k
+
+
+def test_hard_domains_are_separate_estimations(oracle):
+    # batch.rs:1047-1075: with hard boundaries a domain's targets (and its samples' leave-one-out) are
+    # estimated as if the other domains' samples did not exist.
+    xyz, v = batch_samples()
+    targets = batch_grid()
+    dom = np.array([domain_of(p) for p in xyz])
+    tdom = np.array([domain_of(p) for p in targets])
+    s, vg = batch_search(2, 30.0), spherical_40()
+    hard = oracle.estimate_many(targets, xyz, v, s, vg, domains=dom, target_domains=tdom, neighbors=False)
+    hard_cv = oracle.estimate_many(None, xyz, v, s, vg, loo=True, domains=dom, neighbors=False)
+    for d in range(3):
+        own = dom == d
+        at = tdom == d
+        alone = oracle.estimate_many(targets[at], xyz[own], v[own], s, vg, neighbors=False)
+        assert same_bits(alone, {k: x[at] for k, x in hard.items()})
+        cv = oracle.estimate_many(None, xyz[own], v[own], s, vg, loo=True, neighbors=False)
+        assert same_bits(cv, {k: x[own] for k, x in hard_cv.items()})
+    assert np.sum(hard["status"] == 0) > 300
+    # A target of a domain without samples is not estimated.
+    none = oracle.estimate_many(targets[:5], xyz, v, s, vg, domains=dom, target_domains=np.full(5, -1),
+                                neighbors=False)
+    assert np.all(none["status"] == 1) and np.all(np.isnan(none["value"]))
