@@ -200,6 +200,9 @@ struct btk_ctx {
   DevBuf<uint32_t> hole;
   bool has_hole = false;
 
+  // the dense LU's matrices for systems beyond 128 samples
+  DevBuf<double> lu_scratch;
+
   // domain codes of the fitted samples (btk_set_domains) and of a call's targets
   DevBuf<int32_t> dom, tdom;
   bool has_dom = false;
@@ -263,8 +266,10 @@ int check_search(btk_ctx* ctx, const btk_search* s) {
   if (s->sectors > 0 && s->octant) return fail(ctx, BTK_EINVAL, "give octant or sectors, not both");
   if (s->max_per_octant >= 0 && !s->octant) return fail(ctx, BTK_EINVAL, "max_per_octant needs octant");
   if (s->max_per_octant == 0) return fail(ctx, BTK_EINVAL, "max_per_sector must be >= 1");
-  if (s->max_samples > kMaxLU)
-    return fail(ctx, BTK_EUNSUPPORTED, "more than 128 samples per system (the dense LU's shared-memory limit)");
+  if (s->max_samples > kMaxLUGlobal)
+    return fail(ctx, BTK_EUNSUPPORTED, "more than 1024 samples per system (the dense LU's limit)");
+  if (s->calibration && s->max_samples > kMaxLU)
+    return fail(ctx, BTK_EUNSUPPORTED, "a calibrated search of more than 128 samples (its Cholesky's shared-memory limit)");
   if (s->sectors > 0 && (s->sectors < 2 || s->sectors > 360 || s->max_per_sector < 1))
     return fail(ctx, BTK_EINVAL, "sectors need 2 <= count <= 360 and max_per_sector >= 1");
   const bool balances = s->octant || s->sectors > 0;
@@ -525,6 +530,10 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
   a.nbr = ctx->nbr.p, a.count = ctx->cnt.p, a.sstatus = ctx->sst.p;
   a.m = m;
   a.value = o->value, a.variance = o->variance, a.lagrange = o->lagrange, a.n_used = o->n_used, a.status = o->status;
+  if (const size_t lu = lu_scratch_doubles(ctx->sm_count, int(srch.max_samples))) {
+    CK(ctx->lu_scratch.grow(lu));
+    a.lu_scratch = ctx->lu_scratch.p;
+  }
   if (ctx->sup_n > 0 && !loo) {  // block support; cross-validation stays at point support
     CK(launch_support_cbb(L, ctx->vgd, ctx->sup.p, ctx->sup_n, ctx->sup_cbb.p));
     a.sup = ctx->sup.p, a.sup_n = ctx->sup_n, a.sup_cbb = ctx->sup_cbb.p;

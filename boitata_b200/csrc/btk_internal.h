@@ -11,7 +11,8 @@
 namespace btk {
 
 constexpr int kMaxN = 64;       // most samples per system of the warp kernels (kernel.rs:11)
-constexpr int kMaxLU = 128;     // most samples per system of the dense LU (krige.rs:127-201)
+constexpr int kMaxLU = 128;     // most samples per system of the dense LU with its matrix in shared memory
+constexpr int kMaxLUGlobal = 1024;  // most samples per system of the dense LU (krige.rs:127-201), the matrix in global memory
 constexpr int kMaxSlots = 64;   // most list entries per search lane
 constexpr double kPivot = 1e-12;  // kernel.rs:17
 constexpr double kEps = 1e-6;     // coincident.rs:11
@@ -123,6 +124,7 @@ struct SolveDev {
   int64_t *lu, *lu_len;
   const int64_t* perm;
   int64_t nwork;
+  double* lu_scratch;  // systems beyond kMaxLU samples: lu_scratch_doubles() for the LU's matrices
   // Diagnostics pass (the LU kernel's `diag` form): per-target columns, and
   // the fitted samples' hole codes (null: every sample untagged).
   double *negw, *mdist;
@@ -273,6 +275,8 @@ cudaError_t launch_sgs_commit(const Launch& L, int64_t nwork, const int64_t* lis
 // With `diag`, the estimated systems (status OK) are solved again for their
 // weights and only a.negw / a.mdist / a.nholes are written.
 cudaError_t launch_solve_lu(const Launch& L, const SolveDev& a, int kmax, bool diag = false);
+// Doubles of global scratch launch_solve_lu needs for systems of kmax samples (0 up to kMaxLU).
+size_t lu_scratch_doubles(int sm_count, int kmax);
 
 // Objective and gradient of systems of at most `rows` (32 or 64) samples,
 // FP64 or mixed (FP32 factorisation with FP64 refinement; the systems it

@@ -4,7 +4,9 @@
 // variograms that are not stationary (a power structure, composite.rs:64-66),
 // whose bordered matrix is not positive definite.
 //
-// The system and its LU live in shared memory. The factorisation follows
+// The system and its LU live in shared memory up to 128 samples; beyond, the
+// matrix lives in a per-CTA slice of a global scratch buffer (one CTA per
+// SM), the rest of the system in shared memory. The factorisation follows
 // nalgebra 0.33's LU (lu.rs: partial pivoting on the first largest |a_ri| of
 // the column, a zero pivot column skipped, the column scaled by 1 / pivot,
 // the trailing block updated); solve applies the row swaps in order, then the
@@ -30,17 +32,19 @@ struct LuHead {
   int n, nn, dim, kind, twin, sing, nperm;
   int piv[2];        // pivot row of the column, double-buffered by column parity
   double pv[2];      // and its value
-  int cof[kMaxLU], cfirst[kMaxLU], csize[kMaxLU];
 };
 
 struct LuLayout {
-  size_t head, p, e, f, b, x, perm, a, total;
+  size_t head, p, e, f, b, x, perm, clus, a, total;
   int stride;
 };
 
 __host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
 
-__host__ __device__ inline LuLayout lu_layout(int kmax) {
+// Shared-memory layout of one system of at most kmax samples. With `global`
+// the bordered matrix lives in the CTA's slice of a global scratch buffer
+// instead (systems beyond kMaxLU samples, whose matrix does not fit).
+__host__ __device__ inline LuLayout lu_layout(int kmax, bool global = false) {
   LuLayout l;
   const int dmax = kmax + 1;
   l.stride = dmax | 1;
@@ -51,19 +55,30 @@ __host__ __device__ inline LuLayout lu_layout(int kmax) {
   l.b = l.f + sizeof(double) * kmax;
   l.x = l.b + sizeof(double) * dmax;
   l.perm = l.x + sizeof(double) * dmax;
-  l.a = align16(l.perm + sizeof(int) * 2 * dmax);
-  l.total = l.a + sizeof(double) * size_t(dmax) * l.stride;
+  l.clus = l.perm + sizeof(int) * 2 * dmax;  // cluster of each sample, first member and size of each cluster
+  l.a = align16(l.clus + sizeof(int) * 3 * kmax);
+  l.total = global ? l.a : l.a + sizeof(double) * size_t(dmax) * l.stride;
   return l;
 }
 
+// Doubles of one system's matrix in the global scratch (GA form).
+__host__ __device__ inline size_t lu_matrix_doubles(int kmax) {
+  const int dmax = kmax + 1;
+  return size_t(dmax) * size_t(dmax | 1);
+}
+
 // NT threads per system: 128 up to 64 samples, 512 beyond (one system per SM
-// then, its matrix filling most of the shared memory).
-template <bool DIAG, int NT>
+// then, its matrix filling most of the shared memory). GA: the matrix in the
+// CTA's slice of a.lu_scratch (beyond kMaxLU samples).
+template <bool DIAG, int NT, bool GA = false>
 __global__ void __launch_bounds__(NT) k_solve_lu(SolveDev a, int kmax) {
   constexpr int kThreads = NT, kWarps = NT / 32;
   extern __shared__ __align__(16) unsigned char smem[];
-  const LuLayout lay = lu_layout(kmax);
+  const LuLayout lay = lu_layout(kmax, GA);
   LuHead& H = *reinterpret_cast<LuHead*>(smem + lay.head);
+  int* cof = reinterpret_cast<int*>(smem + lay.clus);
+  int* cfirst = cof + kmax;
+  int* csize = cfirst + kmax;
   double* P = reinterpret_cast<double*>(smem + lay.p);  // [3][kmax], world
   double* E = reinterpret_cast<double*>(smem + lay.e);
   double* F = reinterpret_cast<double*>(smem + lay.f);  // f(z)
@@ -71,7 +86,8 @@ __global__ void __launch_bounds__(NT) k_solve_lu(SolveDev a, int kmax) {
   double* X = reinterpret_cast<double*>(smem + lay.x);
   int* pa = reinterpret_cast<int*>(smem + lay.perm);
   int* pb = pa + kmax + 1;
-  double* A = reinterpret_cast<double*>(smem + lay.a);
+  double* A = GA ? a.lu_scratch + size_t(blockIdx.x) * lu_matrix_doubles(kmax)
+                 : reinterpret_cast<double*>(smem + lay.a);
   const int S = lay.stride;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t nitems = a.list ? *a.list_len : (a.perm ? a.nwork : a.m);
@@ -152,25 +168,25 @@ __global__ void __launch_bounds__(NT) k_solve_lu(SolveDev a, int kmax) {
         for (int i = 0; i < n; ++i) {
           int c = -1;
           for (int q = 0; q < nc && c < 0; ++q) {
-            const int f = H.cfirst[q];
+            const int f = cfirst[q];
             if (d2_exact(P[f], P[kmax + f], P[2 * kmax + f], P[i], P[kmax + i], P[2 * kmax + i]) <= eps2) c = q;
           }
-          if (c < 0) c = nc, H.cfirst[nc] = i, H.csize[nc] = 0, ++nc;
-          H.cof[i] = c;
-          H.csize[c] += 1;
+          if (c < 0) c = nc, cfirst[nc] = i, csize[nc] = 0, ++nc;
+          cof[i] = c;
+          csize[c] += 1;
         }
         for (int c = 0; c < nc; ++c) {
-          const int f = H.cfirst[c];
+          const int f = cfirst[c];
           double x0 = P[f], x1 = P[kmax + f], x2 = P[2 * kmax + f], err = E[f], zb = F[f];
-          if (H.csize[c] > 1) {
-            const double k = double(H.csize[c]);
+          if (csize[c] > 1) {
+            const double k = double(csize[c]);
             double var = 0.0, zs = 0.0;
             for (int i = f; i < n; ++i) {
-              if (H.cof[i] != c) continue;
+              if (cof[i] != c) continue;
               var += E[i];
               zs += F[i];
               for (int j = f; j < n; ++j)
-                if (H.cof[j] == c)
+                if (cof[j] == c)
                   var += cov64(vg, lag_world(vg, P[i], P[kmax + i], P[2 * kmax + i], P[j], P[kmax + j],
                                              P[2 * kmax + j]));
             }
@@ -277,7 +293,7 @@ __global__ void __launch_bounds__(NT) k_solve_lu(SolveDev a, int kmax) {
       if (tid == 0 && !H.sing && a.negw) {  // krige.rs:70-75 over the spread weights
         double neg = -0.0;
         for (int i = 0; i < n; ++i) {
-          const double w = H.twin ? X[H.cof[i]] / double(H.csize[H.cof[i]]) : X[i];
+          const double w = H.twin ? X[cof[i]] / double(csize[cof[i]]) : X[i];
           if (w < 0.0) neg += w;
         }
         a.negw[ti] = neg;
@@ -307,20 +323,28 @@ __global__ void __launch_bounds__(NT) k_solve_lu(SolveDev a, int kmax) {
 
 }  // namespace
 
+size_t lu_scratch_doubles(int sm_count, int kmax) {
+  return kmax > kMaxLU ? size_t(sm_count) * lu_matrix_doubles(kmax) : 0;
+}
+
 cudaError_t launch_solve_lu(const Launch& L, const SolveDev& a, int kmax, bool diag) {
-  if (kmax < 1 || kmax > kMaxLU) return cudaErrorInvalidValue;
+  if (kmax < 1 || kmax > kMaxLUGlobal) return cudaErrorInvalidValue;
   if (diag && !a.status) return cudaErrorInvalidValue;
-  const size_t smem = lu_layout(kmax).total;
+  const bool global = kmax > kMaxLU;
+  if (global && !a.lu_scratch) return cudaErrorInvalidValue;
+  const size_t smem = lu_layout(kmax, global).total;
   const bool wide = kmax > 64;
   const int threads = wide ? 512 : 128;
-  auto kern = diag ? (wide ? k_solve_lu<true, 512> : k_solve_lu<true, 128>)
-                   : (wide ? k_solve_lu<false, 512> : k_solve_lu<false, 128>);
+  auto kern = global ? (diag ? k_solve_lu<true, 512, true> : k_solve_lu<false, 512, true>)
+                     : diag ? (wide ? k_solve_lu<true, 512> : k_solve_lu<true, 128>)
+                            : (wide ? k_solve_lu<false, 512> : k_solve_lu<false, 128>);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
   if (e != cudaSuccess) return e;
-  int64_t blocks = int64_t(L.sm_count) * (per_sm > 0 ? per_sm : 1);
+  // The global form: one CTA per SM, each with its own slice of the scratch.
+  int64_t blocks = int64_t(L.sm_count) * (global ? 1 : (per_sm > 0 ? per_sm : 1));
   const int64_t items = a.perm ? a.nwork : a.m;
   if (!a.list && blocks > items) blocks = items;
   if (blocks < 1) blocks = 1;

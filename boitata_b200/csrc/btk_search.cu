@@ -446,18 +446,21 @@ constexpr int kRulesK = BTK_RULES_CANDIDATES;
 // candidates per round: its candidate set grows with every simulated node,
 // and the K-nearest cut, not the selection, dominates the search.
 constexpr int kSgsK = 128, kSgsK32 = 64;  // at most 64 / at most 32 samples
-constexpr int kHoleHash = 128;  // > 2 x 64 accepted holes
+// Slots of the accepted-hole table: at least the most samples a list holds
+// (each accepted sample adds at most one hole), so a lookup always ends.
+constexpr int kHoleHash = 128;        // lists of at most 128 samples
+constexpr int kHoleHashBig = 2048;    // up to kMaxLUGlobal samples
 constexpr uint32_t kNoHole = 0xffffffffu;
 
-template <int K>
+template <int K, int HH = kHoleHash>
 struct RulesSmem {
+  static constexpr int kHash = HH;
   double cd[2 * K];
   uint32_t ci[2 * K];
   uint16_t sec[2 * K];
-  uint32_t hkey[kHoleHash];
-  int hcnt[kHoleHash];
+  uint32_t hkey[HH];
+  int hcnt[HH];
   int per_sector[360];
-  uint32_t chosen[kMaxLU];
 };
 
 // Ascending bitonic sort of (d2, index) keys 0 .. n-1 by one warp, padded to a
@@ -521,12 +524,13 @@ __device__ int longest_empty(const SearchDev& sp, const int* counts) {
 
 // Hole slot of h in the warp's table of accepted holes (the free slot where
 // it would go when absent).
-template <int K>
-__device__ __forceinline__ int hole_slot(const RulesSmem<K>& S, uint32_t h) {
-  int k = int((h * 2654435761u) >> 25);  // 7 bits
-  for (int probe = 0; probe < kHoleHash; ++probe) {
+template <class Sm>
+__device__ __forceinline__ int hole_slot(const Sm& S, uint32_t h) {
+  constexpr int HH = Sm::kHash;
+  int k = int((h * 2654435761u) >> (HH == kHoleHash ? 25 : 21)) & (HH - 1);  // 7 or 11 bits
+  for (int probe = 0; probe < HH; ++probe) {
     if (S.hkey[k] == h || S.hkey[k] == kNoHole) break;
-    k = (k + 1) & (kHoleHash - 1);
+    k = (k + 1) & (HH - 1);
   }
   return k;
 }
@@ -536,8 +540,8 @@ __device__ __forceinline__ int hole_slot(const RulesSmem<K>& S, uint32_t h) {
 // an open sector (per_sector below the cap) from a hole below its cap, goes
 // into the warp's buffer; above 2K - 32 candidates the buffer keeps its K
 // nearest. Returns the count; *dropped tells whether candidates were cut.
-template <int K>
-__device__ int rules_scan(const SearchDev& sp, const GridDev& g, RulesSmem<K>& S, const double q[3], const double t[3],
+template <int K, int HH>
+__device__ int rules_scan(const SearchDev& sp, const GridDev& g, RulesSmem<K, HH>& S, const double q[3], const double t[3],
                           uint32_t left, double after_d, uint32_t after_i, bool filter, unsigned openmask,
                           bool& dropped, int lane, uint32_t my, double& d2u, int32_t dom) {
   const double glo[3] = {g.lo[0], g.lo[1], g.lo[2]};
@@ -662,7 +666,7 @@ __device__ int rules_scan(const SearchDev& sp, const GridDev& g, RulesSmem<K>& S
   return n;
 }
 
-template <int K>
+template <int K, int HH = kHoleHash>
 __global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, const double* __restrict__ tx,
                                                       const double* __restrict__ ty, const double* __restrict__ tz,
                                                       const int64_t* __restrict__ perm, int64_t m, int loo,
@@ -670,7 +674,7 @@ __global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, c
                                                       int8_t* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
-  RulesSmem<K>& S = reinterpret_cast<RulesSmem<K>*>(smem_raw)[threadIdx.x >> 5];
+  RulesSmem<K, HH>& S = reinterpret_cast<RulesSmem<K, HH>*>(smem_raw)[threadIdx.x >> 5];
   const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
   for (int64_t w = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); w < m; w += warps) {
     const int64_t ti = perm ? perm[w] : w;
@@ -685,7 +689,7 @@ __global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, c
     const uint32_t my = sp.sgs ? sp.sgs_node0 + uint32_t(ti) : 0xffffffffu;
     const int32_t dom = sp.sdom ? sp.tdom[ti] : 0;  // the target's domain (hard boundaries)
     double d2u = INFINITY, far = 0.0;  // nearest unsimulated earlier node; farthest accepted
-    for (int i = lane; i < kHoleHash; i += 32) S.hkey[i] = kNoHole, S.hcnt[i] = 0;
+    for (int i = lane; i < HH; i += 32) S.hkey[i] = kNoHole, S.hcnt[i] = 0;
     for (int i = lane; i < 360; i += 32) S.per_sector[i] = 0;
     __syncwarp();
     // Selector state (lane 0's copy is the one that counts)
@@ -731,7 +735,7 @@ __global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, c
             ++untagged;
           }
           far = S.cd[i];
-          S.chosen[nchosen++] = idx;
+          nbr[ti * sp.max_samples + nchosen++] = idx;  // the list goes straight to its row
         }
       nchosen = __shfl_sync(kFull, nchosen, 0);
       __syncwarp();
@@ -777,7 +781,7 @@ __global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, c
       status[ti] = st;
     }
     __syncwarp();
-    for (int j = lane; j < sp.max_samples; j += 32) nbr[ti * sp.max_samples + j] = j < nchosen ? S.chosen[j] : 0xffffffffu;
+    for (int j = nchosen + lane; j < sp.max_samples; j += 32) nbr[ti * sp.max_samples + j] = 0xffffffffu;
     __syncwarp();
   }
 }
@@ -792,9 +796,16 @@ cudaError_t launch_search(const Launch& L, const SearchDev& sp, const GridDev& g
     const bool small = sp.sgs && sp.max_samples <= 64 && sp.max_per_hole < 0 && !sp.plane && sp.min_sectors < 0 &&
                        sp.max_empty_sectors < 0 && sp.min_holes < 0;
     const bool tiny = small && sp.max_samples <= 32;
-    const size_t smem =
-        (tiny ? sizeof(RulesSmem<kSgsK32>) : small ? sizeof(RulesSmem<kSgsK>) : sizeof(RulesSmem<kRulesK>)) * kWarps;
-    auto kern = tiny ? k_search_rules<kSgsK32> : small ? k_search_rules<kSgsK> : k_search_rules<kRulesK>;
+    const bool big = sp.max_samples > kMaxLU;  // more accepted holes than the small table holds
+    const size_t smem = (big    ? sizeof(RulesSmem<kRulesK, kHoleHashBig>)
+                         : tiny ? sizeof(RulesSmem<kSgsK32>)
+                         : small ? sizeof(RulesSmem<kSgsK>)
+                                 : sizeof(RulesSmem<kRulesK>)) *
+                        kWarps;
+    auto kern = big    ? k_search_rules<kRulesK, kHoleHashBig>
+                : tiny ? k_search_rules<kSgsK32>
+                : small ? k_search_rules<kSgsK>
+                        : k_search_rules<kRulesK>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;

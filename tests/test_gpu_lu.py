@@ -141,8 +141,31 @@ def test_block_kriging_through_the_lu(oracle, vg):
     assert_same_estimates(bk.predict_full(t), ref, 1e-10)
 
 
-def test_more_than_128_samples_is_refused():
+@pytest.mark.parametrize("max_samples", [129, 200, 400])
+def test_systems_beyond_128_samples_match_krige_lu(oracle, max_samples):
+    """Beyond 128 samples the LU's matrix lives in global memory (krige_lu has no upper limit): lists, and
+    OK / SK estimates with coincident pairs, against the oracle; FP64 in both precisions."""
     w = W.c1()
-    s = Search(ranges=(300.0, 300.0, 100.0), max_samples=129, min_samples=1)
-    with pytest.raises(Exception, match="128"):
+    coords, values = with_pairs(w)
+    s = Search(ranges=(400.0, 400.0, 150.0), max_samples=max_samples, min_samples=1, max_per_hole=60)
+    holes = np.arange(len(coords)) // 7
+    rng = np.random.default_rng(max_samples)
+    targets = np.vstack([centroids(oracle, w, 97), rng.uniform(-200, 1200, (60, 3)) * [1, 1, 0.2]])
+    ok = OrdinaryKriging(w.variogram, s, precision="mixed").fit(coords, values, holes=holes)
+    idx, cnt, good = ok.neighbors(targets)
+    ref = oracle.estimate_many(targets, coords, values, s, w.variogram, holes=ok._holes)
+    for t in range(len(targets)):
+        assert idx[t, : cnt[t]].tolist() == [i for i in ref["neighbors"][t] if i >= 0], t
+    assert np.count_nonzero(ref["n_used"] > 128) > len(targets) // 2
+    assert_same_estimates(ok.predict_full(targets), ref, 1e-10)
+    sk = SimpleKriging(w.variogram, s, mean=1.0).fit(coords, values, holes=holes)
+    ref = oracle.estimate_many(targets, coords, values, s, w.variogram, holes=ok._holes, kind="simple", kparam=1.0,
+                               neighbors=False)
+    assert_same_estimates(sk.predict_full(targets), ref, 1e-10)
+
+
+def test_more_than_1024_samples_is_refused():
+    w = W.c1()
+    s = Search(ranges=(300.0, 300.0, 100.0), max_samples=1025, min_samples=1)
+    with pytest.raises(Exception, match="1024"):
         OrdinaryKriging(w.variogram, s).fit(w.coords, w.values).predict_full(w.coords[:4])
