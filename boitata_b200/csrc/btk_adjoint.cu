@@ -28,9 +28,10 @@
 // the lag h = |M d| of world offset d, M = diag(1, 1/semi, 1/minor) R, with
 // the shape derivatives of crates/variogram/src/model.rs:181-312.
 //
-// One group of NW warps per system (n <= 32 NW), lane = row. Every lag comes
-// from lag_world, as in the prediction kernels, so the FP64 objective is the
-// prediction path's estimate to the bit. Two forms:
+// One group of NW warps per system (n <= 32 NW), lane = row. Every lag is
+// lag_world's (with the frame M when the variogram has an anisotropy, else
+// the plain Euclidean norm, M being orthogonal then), as in the prediction
+// kernels, so the FP64 objective is the prediction path's estimate to the bit. Two forms:
 //   - FP64: the shifted, windowed right-looking LDL^T of the prediction
 //     kernels with the forward substitutions fused in, the multipliers kept
 //     in place of the covariance triangle, and one backward sweep for x;
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(128) k_grad(GradDev a) {
     const double dt[3] = {w[0] - t[0], w[1] - t[1], w[2] - t[2]};  // lag_world(t, w)'s offset
     double pt[3];
     frame_apply(a.vg, dt, pt);
-    const double hc = norm3(pt);
+    const double hc = a.vg.has_frame ? norm3(pt) : norm3(dt);  // lag_world's h, frame or not
     const double c = have ? cov64(a.vg, hc) : 0.0;
     const double diag = have ? c0 + err : 1.0;
     const int tri = row * (row - 1) / 2;
@@ -331,7 +332,7 @@ __global__ void __launch_bounds__(128) k_grad(GradDev a) {
       const double d[3] = {S.W[p][0] - S.W[q][0], S.W[p][1] - S.W[q][1], S.W[p][2] - S.W[q][2]};
       double md[3];
       frame_apply(a.vg, d, md);
-      const double h = norm3(md);
+      const double h = a.vg.has_frame ? norm3(md) : norm3(d);
       if (h > 0.0) add_lag_terms(a, coef, h, md, d, g);
     }
     group_sum<NW, 8>(S, gid, wig, g);
