@@ -1442,10 +1442,13 @@ int objective_sums(btk_ctx* ctx, Objective which, const btk_variogram* vg, int64
   if (!v.aniso.on) v.aniso = btk_aniso{1, 0.0, 0.0, 0.0, 1.0, 1.0, 1.0};  // isotropic, as a point of theta
   GradDev a{};
   make_vgdev(v, a.vg);
-  // A variogram given without anisotropy keeps the plain Euclidean lags of the
-  // prediction path (lag_world without a frame); its frame (rotation(0, 0, 0)
-  // at unit ratios, orthogonal) still gives the angle and ratio derivatives.
-  a.vg.has_frame = vg->aniso.on ? 1 : 0;
+  // At unit ratios and zero angles (a variogram without anisotropy, as the
+  // prediction path takes it) the lags are the plain Euclidean ones of
+  // lag_world without a frame: the frame, rotation(0, 0, 0), is orthogonal
+  // there, and it still gives the angle and ratio derivatives.
+  const btk_aniso& an = v.aniso;
+  a.vg.has_frame = (an.semi == an.major && an.minor == an.major && an.azimuth == 0.0 && an.dip == 0.0 &&
+                    an.rake == 0.0) ? 0 : 1;
   aniso_derivatives(v.aniso, a.dM);
   const int ntheta = 1 + 2 * v.nstruct + 5;
   a.sx = ctx->x.p, a.sy = ctx->y.p, a.sz = ctx->z.p, a.sv = ctx->v.p, a.se = ctx->has_err ? ctx->e.p : nullptr;
