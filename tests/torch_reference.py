@@ -81,13 +81,15 @@ def mean_estimate(theta, models, coords, values, targets, nbr):
     m, k, _ = P.shape
     eye = torch.eye(k, dtype=P.dtype, device=P.device)
     D = P[:, :, None, :] - P[:, None, :, :]
-    H = torch.sqrt((D * D).sum(-1) + eye)
-    h0 = torch.sqrt((P * P).sum(-1))
+    pair = live[:, :, None] & live[:, None, :]
+    # Lags of live pairs only: padded slots share one point, and sqrt at 0 would poison the gradient.
+    d2 = torch.where(pair & (eye == 0), (D * D).sum(-1), torch.ones_like(eye))
+    H = torch.sqrt(d2)
+    h0 = torch.sqrt(torch.where(live, (P * P).sum(-1), torch.ones_like(live, dtype=P.dtype)))
 
     def cov(h):
         return sum(sills[s] * (1 - shape(models[s], h / ranges[s])) for s in range(ns))
 
-    pair = live[:, :, None] & live[:, None, :]
     C = torch.where(pair, cov(H) * (1 - eye) + eye * (nugget + sills.sum()), eye.expand(m, k, k))
     K = torch.zeros((m, k + 1, k + 1), dtype=P.dtype, device=P.device)
     K[:, :k, :k] = C
