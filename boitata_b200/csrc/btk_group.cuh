@@ -59,28 +59,6 @@ __device__ __forceinline__ void group_sum5(Sm& S, int gid, int wig, double v[5])
   group_sum<NW, 5>(S, gid, wig, v);
 }
 
-// Maxima of K <= 8 values over the group, on every lane.
-template <int NW, int K, class Sm>
-__device__ __forceinline__ void group_max_many(Sm& S, int gid, int wig, double v[K]) {
-#pragma unroll
-  for (int q = 0; q < K; ++q)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v[q] = fmax(v[q], __shfl_xor_sync(kFull, v[q], o));
-  if (NW == 1) return;
-  if ((threadIdx.x & 31) == 0)
-#pragma unroll
-    for (int q = 0; q < K; ++q) S.red[wig][q] = v[q];
-  gsync<NW>(gid);
-#pragma unroll
-  for (int q = 0; q < K; ++q) {
-    double m = S.red[0][q];
-#pragma unroll
-    for (int w = 1; w < NW; ++w) m = fmax(m, S.red[w][q]);
-    v[q] = m;
-  }
-  gsync<NW>(gid);
-}
-
 // Maximum of one value over the group, on every lane.
 template <int NW, class Sm>
 __device__ __forceinline__ double group_max(Sm& S, int gid, int wig, double v) {

@@ -1,6 +1,5 @@
 // Per-system kriging solve (K2 assembly, K3 factor-and-solve, K4 epilogue),
-// one system per warp (n <= 32) or per warp pair (n <= 64); in the mixed
-// form a warp pair takes two systems of up to 64 samples at once.
+// one system per warp (n <= 32) or per warp pair (n <= 64).
 //
 // Reference: crates/estimation/src/kernel.rs:24-123 (and the coincident
 // guard of crates/estimation/src/coincident.rs:27-111 via krige.rs:83-95).
@@ -349,281 +348,6 @@ __global__ void __launch_bounds__(128) k_solve_mixed(SolveDev a, int64_t* redo, 
   }
 }
 
-// ---- mixed form, two systems per group ------------------------------------
-// The systems of the per-system lists in pairs: a group of NW warps takes
-// systems a and b, lane = row of both, each row a float2 (a in .x, b in .y),
-// so one packed FP32 FMA (__ffma2_rn) updates a slot of both and the
-// per-step broadcasts and barriers are shared. It is the tile kernel's mixed
-// scheme (btk_tile.cu) for systems of up to 32 NW samples assembled per
-// system: each system's FP64 triangle comes from assemble(); the shifted,
-// windowed FP32 LDL^T writes each pivot column of both systems to a packed
-// triangle (column k at pair_col_off(k), its length rounded up to even for
-// 16-byte reads); a column-oriented backward sweep gives x = C~^-1 v; FP64
-// residuals from each system's triangle drive up to kRefineSteps refinement
-// steps (a forward and a backward sweep over the stored columns), each system
-// stopping on its own; the corrected forms as in k_solve_mixed.
-template <int NW>
-struct alignas(16) MixedPairSmem {
-  static constexpr int R = 32 * NW;
-  static constexpr int kPad = R;          // reads past a column's end stay inside the group's area
-  static constexpr int kLen = R * R / 2;  // sum over k of (R - k) rounded down to even
-  SolveSmem<NW> sys[2];
-  alignas(16) float2 lt[kPad + kLen + kPad];
-  alignas(16) float2 prhs[2][4];  // [buffer]: pivot, y_c, y_1, y_f of the pivot row (a, b)
-  alignas(16) float2 line[2][4];  // [buffer]: a sweep's broadcast value of the three right-hand sides and 1 / D
-  double xs[6][R];                // x of a (c, 1, f) and of b
-  double red[NW][8];
-  int ired[NW];
-};
-
-// Start of column k in the packed triangle of R rows.
-template <int R>
-__device__ __forceinline__ int pair_col_off(int k) {
-  const int m = k >> 1;
-  return 2 * R * m - 2 * m * m + ((k & 1) ? R - 2 * m : 0);
-}
-
-__device__ __forceinline__ float rcp_fast(float d) {
-  float r;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
-  return r;
-}
-
-// Pivots k0 .. k1-1 of both systems' FP32 LDL^T, forward substitution of y
-// fused in; the row kept shifted (slot 0 = the current pivot column) and the
-// W slots that can still hold live columns updated, as eliminate_rows does.
-template <int NW, int W>
-__device__ __forceinline__ void eliminate_pair(float2 (&A)[32 * NW], int k0, int k1, int row, MixedPairSmem<NW>& X,
-                                               int gid, float2 (&y)[3], float2& dme, float2& dmin) {
-  constexpr int R = 32 * NW;
-  float2* col = X.lt + X.kPad + pair_col_off<R>(k0);
-  for (int k = k0; k < k1; ++k) {
-    const int b = k & 1;
-    if (row > k) col[row - k - 1] = A[0];
-    if (row == k) {
-      reinterpret_cast<float4*>(X.prhs[b])[0] = make_float4(A[0].x, A[0].y, y[0].x, y[0].y);
-      reinterpret_cast<float4*>(X.prhs[b])[1] = make_float4(y[1].x, y[1].y, y[2].x, y[2].y);
-    }
-    gsync<NW>(gid);
-    const float4 p0 = reinterpret_cast<const float4*>(X.prhs[b])[0];
-    const float4 p1 = reinterpret_cast<const float4*>(X.prhs[b])[1];
-    dmin.x = fminf(dmin.x, p0.x), dmin.y = fminf(dmin.y, p0.y);
-    if (row == k) dme = make_float2(p0.x, p0.y);
-    const float2 nrd = make_float2(rcp_fast(-p0.x), rcp_fast(-p0.y));
-    const float2 nf = row > k ? __fmul2_rn(A[0], nrd) : make_float2(0.f, 0.f);  // -L[row][k]
-#pragma unroll
-    for (int q = 0; q < W; q += 2) {
-      const float4 c4 = *reinterpret_cast<const float4*>(&col[q]);
-      A[q] = __ffma2_rn(nf, make_float2(c4.x, c4.y), A[q + 1]);
-      A[q + 1] = q + 2 < R ? __ffma2_rn(nf, make_float2(c4.z, c4.w), A[q + 2]) : make_float2(0.f, 0.f);
-    }
-    y[0] = __ffma2_rn(nf, make_float2(p0.z, p0.w), y[0]);
-    y[1] = __ffma2_rn(nf, make_float2(p1.x, p1.y), y[1]);
-    y[2] = __ffma2_rn(nf, make_float2(p1.z, p1.w), y[2]);
-    col += (R - k) & ~1;
-  }
-}
-
-// Backward sweep L^T x = D^-1 y of both systems, column-oriented: once x_k
-// is known every row i < k takes D_i L[k][i] x_k (column i of the triangle).
-template <int NW>
-__device__ __forceinline__ void backward_pair(MixedPairSmem<NW>& X, int gid, int row, int nmax, float2 rdme,
-                                              const float2 (&y)[3], float2 (&x)[3]) {
-  constexpr int R = 32 * NW;
-  float2 acc[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-  const float2* my_col = X.lt + X.kPad + pair_col_off<R>(row) - row - 1;  // + k: D_row L[k][row]
-  x[0] = x[1] = x[2] = make_float2(0.f, 0.f);
-  gsync<NW>(gid);
-  for (int k = nmax - 1; k >= 0; --k) {
-    const int b = k & 1;
-    if (row == k) {
-#pragma unroll
-      for (int v = 0; v < 3; ++v) {
-        x[v] = make_float2((y[v].x - acc[v].x) * rdme.x, (y[v].y - acc[v].y) * rdme.y);
-        X.line[b][v] = x[v];
-      }
-    }
-    gsync<NW>(gid);
-    const float2 l = row < k ? my_col[k] : make_float2(0.f, 0.f);
-#pragma unroll
-    for (int v = 0; v < 3; ++v) acc[v] = __ffma2_rn(l, X.line[b][v], acc[v]);
-  }
-}
-
-// Forward sweep L y = r of both systems (unit lower L from the stored
-// columns D_i L[k][i]): once y_i is final, rows k > i take it.
-template <int NW>
-__device__ __forceinline__ void forward_pair(MixedPairSmem<NW>& X, int gid, int row, int nmax, float2 rdme,
-                                             float2 (&y)[3]) {
-  constexpr int R = 32 * NW;
-  gsync<NW>(gid);
-  for (int i = 0; i < nmax; ++i) {
-    const int b = i & 1;
-    if (row == i) {
-#pragma unroll
-      for (int v = 0; v < 3; ++v) X.line[b][v] = make_float2(-y[v].x * rdme.x, -y[v].y * rdme.y);  // -y_i / D_i
-    }
-    gsync<NW>(gid);
-    if (row > i) {
-      const float2 l = X.lt[X.kPad + pair_col_off<R>(i) + row - i - 1];  // D_i L[row][i]
-#pragma unroll
-      for (int v = 0; v < 3; ++v) y[v] = __ffma2_rn(l, X.line[b][v], y[v]);
-    }
-  }
-}
-
-template <int NW>
-__global__ void __launch_bounds__(32 * NW, 3) k_solve_mixed_pair(SolveDev a, int64_t* redo, int64_t* redo_len) {
-  constexpr int R = 32 * NW;
-  constexpr int Q = R / 4;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int gid = 0, row = threadIdx.x, wig = row >> 5;
-  MixedPairSmem<NW>& X = *reinterpret_cast<MixedPairSmem<NW>*>(smem_raw);
-  const int64_t nitems = a.list ? *a.list_len : a.m;
-  const int64_t npairs = (nitems + 1) / 2;
-  const double c0 = a.vg.c0;
-  for (int64_t pr = blockIdx.x; pr < npairs; pr += gridDim.x) {
-    int64_t ti[2];
-    int n[2] = {0, 0}, nn[2] = {0, 0}, kind[2] = {0, 0};
-    bool have[2] = {false, false}, live[2] = {false, false};
-    double c[2] = {0.0, 0.0}, err[2] = {0.0, 0.0}, zf[2] = {0.0, 0.0};
-    for (int s = 0; s < 2; ++s) {
-      const int64_t item = 2 * pr + s;
-      ti[s] = item < nitems ? (a.list ? a.list[item] : item) : -1;
-      gsync<NW>(gid);
-      if (ti[s] >= 0)  // uniform over the group
-        live[s] = assemble<NW>(a, X.sys[s], gid, wig, row, ti[s], n[s], nn[s], have[s], c[s], err[s], zf[s], kind[s]);
-      if (!live[s]) nn[s] = 0, have[s] = false;
-    }
-    if (!live[0] && !live[1]) continue;
-    const int nmax = max(nn[0], nn[1]);
-    const int tri = row * (row - 1) / 2;
-    const double diag0 = have[0] ? c0 + err[0] : 1.0, diag1 = have[1] ? c0 + err[1] : 1.0;
-    float2 A[R];
-#pragma unroll
-    for (int q = 0; q < R; ++q) {
-      A[q].x = q < row ? (have[0] ? float(X.sys[0].T[tri + q]) : 0.f) : (q == row ? float(diag0) : 0.f);
-      A[q].y = q < row ? (have[1] ? float(X.sys[1].T[tri + q]) : 0.f) : (q == row ? float(diag1) : 0.f);
-    }
-    float2 y[3] = {make_float2(have[0] ? float(c[0]) : 0.f, have[1] ? float(c[1]) : 0.f),
-                   make_float2(have[0] ? 1.f : 0.f, have[1] ? 1.f : 0.f),
-                   make_float2(have[0] ? float(zf[0]) : 0.f, have[1] ? float(zf[1]) : 0.f)};
-    float2 dme = make_float2(1.f, 1.f), pmin = make_float2(3.0e38f, 3.0e38f);
-    const int n1 = min(nmax, Q), n2 = min(nmax, 2 * Q), n3 = min(nmax, 3 * Q);
-    eliminate_pair<NW, R>(A, 0, n1, row, X, gid, y, dme, pmin);
-    eliminate_pair<NW, 3 * Q>(A, n1, n2, row, X, gid, y, dme, pmin);
-    eliminate_pair<NW, 2 * Q>(A, n2, n3, row, X, gid, y, dme, pmin);
-    eliminate_pair<NW, Q>(A, n3, nmax, row, X, gid, y, dme, pmin);
-    // An FP32 pivot NaN or at most n ulp(C0) leaves that system to the FP64
-    // form, which also takes the singular decision (kernel.rs:61).
-    bool weak[2] = {live[0] && !(pmin.x > float(nn[0]) * 1.1920929e-7f * float(c0)),
-                    live[1] && !(pmin.y > float(nn[1]) * 1.1920929e-7f * float(c0))};
-    const float2 rdme = make_float2(rcp_fast(dme.x), rcp_fast(dme.y));
-    float2 x[3];
-    backward_pair<NW>(X, gid, row, nmax, rdme, y, x);
-    double xv[2][3];
-#pragma unroll
-    for (int v = 0; v < 3; ++v) xv[0][v] = have[0] ? double(x[v].x) : 0.0, xv[1][v] = have[1] ? double(x[v].y) : 0.0;
-    double mx[6] = {have[0] ? fabs(c[0]) : 0.0, have[0] ? fabs(zf[0]) : 0.0, have[0] ? -double(dme.x) : -1e300,
-                    have[1] ? fabs(c[1]) : 0.0, have[1] ? fabs(zf[1]) : 0.0, have[1] ? -double(dme.y) : -1e300};
-    group_max_many<NW, 6>(X, gid, wig, mx);
-    const double cmax[2] = {fmax(mx[0], 1e-300), fmax(mx[3], 1e-300)}, zmax[2] = {fmax(mx[1], 1e-300), fmax(mx[4], 1e-300)};
-    const double dmin[2] = {-mx[2], -mx[5]};
-    double r[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}}, rho[2] = {0.0, 0.0};
-    bool done[2] = {!live[0] || weak[0], !live[1] || weak[1]}, failed[2] = {false, false};
-    for (int it = 0;; ++it) {
-#pragma unroll
-      for (int v = 0; v < 3; ++v) X.xs[v][row] = xv[0][v], X.xs[3 + v][row] = xv[1][v];
-      gsync<NW>(gid);
-      // FP64 residuals r_v = v - C x_v with C from each system's FP64 triangle.
-      double acc[2][3] = {{diag0 * xv[0][0], diag0 * xv[0][1], diag0 * xv[0][2]},
-                          {diag1 * xv[1][0], diag1 * xv[1][1], diag1 * xv[1][2]}};
-      for (int j = 0; j < nmax; ++j) {
-        if (j == row) continue;
-        const int e = j < row ? tri + j : j * (j - 1) / 2 + row;
-        const double ca = j < nn[0] && row < nn[0] ? X.sys[0].T[e] : 0.0;
-        const double cb = j < nn[1] && row < nn[1] ? X.sys[1].T[e] : 0.0;
-#pragma unroll
-        for (int v = 0; v < 3; ++v) acc[0][v] = fma(ca, X.xs[v][j], acc[0][v]), acc[1][v] = fma(cb, X.xs[3 + v][j], acc[1][v]);
-      }
-#pragma unroll
-      for (int s = 0; s < 2; ++s) {
-        const double vs[3] = {c[s], 1.0, zf[s]};
-#pragma unroll
-        for (int v = 0; v < 3; ++v) r[s][v] = have[s] ? vs[v] - acc[s][v] : 0.0;
-      }
-      double rr[2] = {fmax(fmax(fabs(r[0][0]) / cmax[0], fabs(r[0][1])), fabs(r[0][2]) / zmax[0]),
-                      fmax(fmax(fabs(r[1][0]) / cmax[1], fabs(r[1][1])), fabs(r[1][2]) / zmax[1])};
-      group_max_many<NW, 2>(X, gid, wig, rr);
-      // The corrected forms err by about rho^2 C0 / D_min: refine each system
-      // until that is at most 1e-8; one that stops converging goes to FP64.
-      bool more = false;
-#pragma unroll
-      for (int s = 0; s < 2; ++s) {
-        if (done[s]) continue;
-        const double prev = rho[s];
-        rho[s] = rr[s];
-        if (rho[s] * rho[s] * c0 / dmin[s] <= 1e-8) {
-          done[s] = true;
-        } else if (it == kRefineSteps || !(rho[s] < 1.0) || (it > 0 && !(rho[s] < 0.5 * prev))) {
-          done[s] = failed[s] = true;
-        } else {
-          more = true;
-        }
-      }
-      if (!more) break;  // uniform: rr and the flags are the group's
-      float2 u[3];
-#pragma unroll
-      for (int v = 0; v < 3; ++v) u[v] = make_float2(done[0] ? 0.f : float(r[0][v]), done[1] ? 0.f : float(r[1][v]));
-      forward_pair<NW>(X, gid, row, nmax, rdme, u);
-      float2 dx[3];
-      backward_pair<NW>(X, gid, row, nmax, rdme, u, dx);
-#pragma unroll
-      for (int v = 0; v < 3; ++v) {
-        if (have[0] && !done[0]) xv[0][v] += double(dx[v].x);
-        if (have[1] && !done[1]) xv[1][v] += double(dx[v].y);
-      }
-      gsync<NW>(gid);  // every row has read xs
-    }
-    // Corrected forms u'x_v + x_u'r_v (error second order in the residuals).
-    double f[2][5];
-#pragma unroll
-    for (int s = 0; s < 2; ++s) {
-      const double* xs = xv[s];
-      const double* rs = r[s];
-      f[s][0] = xs[0] + xs[1] * rs[0], f[s][1] = xs[1] + xs[1] * rs[1], f[s][2] = zf[s] * xs[0] + xs[2] * rs[0];
-      f[s][3] = zf[s] * xs[1] + xs[2] * rs[1], f[s][4] = c[s] * xs[0] + xs[0] * rs[0];
-      if (!have[s])
-        for (int q = 0; q < 5; ++q) f[s][q] = 0.0;
-    }
-    group_sum5<NW>(X, gid, wig, f[0]);
-    group_sum5<NW>(X, gid, wig, f[1]);
-    if (row < 2 && live[row]) {
-      const int s = row;
-      const double* v = f[s];
-      if (weak[s] || failed[s] || !(rho[s] * rho[s] * c0 / dmin[s] <= 1e-8) || !(v[1] > 0.0) || !(fabs(v[0]) < 1e30))
-        redo[atomicAdd(reinterpret_cast<unsigned long long*>(redo_len), 1ull)] = ti[s];
-      else
-        epilogue(a, kind[s], ti[s], v, n[s], 0);
-    }
-  }
-}
-
-template <int NW>
-cudaError_t run_mixed_pair(const Launch& L, const SolveDev& a, int64_t* redo, int64_t* redo_len) {
-  const size_t smem = sizeof(MixedPairSmem<NW>);
-  auto kern = k_solve_mixed_pair<NW>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  if (e != cudaSuccess) return e;
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * NW, smem) != cudaSuccess || per_sm < 1)
-    per_sm = 1;
-  if (L.tuning.solve_blocks_per_sm > 0 && L.tuning.solve_blocks_per_sm < per_sm) per_sm = L.tuning.solve_blocks_per_sm;
-  kern<<<L.sm_count * per_sm, 32 * NW, smem, L.stream>>>(a, redo, redo_len);
-  ++*L.counter;
-  return cudaGetLastError();
-}
-
 __global__ void k_bucket(int64_t m, const int32_t* count, const int8_t* sstatus, int64_t* small, int64_t* large,
                          int64_t* lens) {
   for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < m; t += int64_t(gridDim.x) * blockDim.x) {
@@ -683,7 +407,7 @@ cudaError_t launch_solve(const Launch& L, const SolveDev& a, int rows) {
 }
 
 cudaError_t launch_solve_mixed(const Launch& L, const SolveDev& a, int rows, int64_t* redo, int64_t* redo_len) {
-  return rows > 32 ? run_mixed_pair<2>(L, a, redo, redo_len) : run_mixed<1>(L, a, redo, redo_len);
+  return rows > 32 ? run_mixed<2>(L, a, redo, redo_len) : run_mixed<1>(L, a, redo, redo_len);
 }
 
 cudaError_t launch_solve_redo(const Launch& L, const SolveDev& a, int rows) {
