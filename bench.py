@@ -566,12 +566,15 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     tunings = {}
+    override = {}
 
     def use(prec):
         """Each form runs at its own tuned launch configuration (set outside the timed region)."""
-        if tunings:
-            from boitata_b200.autotune import set_tuning
+        from boitata_b200.autotune import set_tuning
 
+        if prec in override:
+            set_tuning(ctx, override[prec])
+        elif tunings:
             set_tuning(ctx, tunings[prec])
 
     def step(prec):
@@ -626,49 +629,71 @@ def main():
         torch.cuda.synchronize()
         results[prec] = host_copy(outs)
 
-    timed = {}
-    launches = {}
-    with Clocks(local) as clk:
-        for prec in (N.MIXED, N.FP64):
-            capture(prec)  # the whole step as one CUDA graph
-            for _ in range(2):
-                replay()
-            barrier()
-            torch.cuda.synchronize()
-            before = ctx.launches()
-            ms = []
-            for _ in range(args.steps):
-                flush.zero_()  # L2 (126 MB) flushed between steps, outside the timed events
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                replay()
-                e1.record(stream)
-                e1.synchronize()
-                ms.append(e0.elapsed_time(e1))
-            launches[prec] = ctx.launches() - before
-            torch.cuda.synchronize()
-            barrier()
-            total = torch.tensor([sum(ms)], dtype=torch.float64, device=dev)
-            if ws > 1:
-                import torch.distributed as dist
+    def time_graph(prec):
+        """Mean ms of args.steps replays of the step's CUDA graph (max over ranks), and the launches."""
+        capture(prec)  # the whole step as one CUDA graph
+        for _ in range(2):
+            replay()
+        barrier()
+        torch.cuda.synchronize()
+        before = ctx.launches()
+        ms = []
+        for _ in range(args.steps):
+            flush.zero_()  # L2 (126 MB) flushed between steps, outside the timed events
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            replay()
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        n = ctx.launches() - before
+        torch.cuda.synchronize()
+        barrier()
+        total = torch.tensor([sum(ms)], dtype=torch.float64, device=dev)
+        if ws > 1:
+            import torch.distributed as dist
 
-                dist.all_reduce(total, op=dist.ReduceOp.MAX)
-            timed[prec] = (total.item() / args.steps, ms)
-    clocks = clk.summary()
+            dist.all_reduce(total, op=dist.ReduceOp.MAX)
+        return total.item() / args.steps, ms, n
 
-    # Per-phase kernel times (CUDA events on the launch stream), untimed pass.
-    lib.btk_set_timing(h, 1)
-    phases = {}
-    for prec in (N.MIXED, N.FP64):
+    def solve_phase(prec, reps=3):
+        """Mean per-phase kernel ms (search, solve, FP64 re-solve) of untimed steps."""
+        lib.btk_set_timing(h, 1)
         acc = np.zeros(3)
-        for _ in range(3):
+        for _ in range(reps):
             flush.zero_()
             step(prec)
             p3 = (ctypes.c_float * 3)()
             ctx.check(lib.btk_phase_ms(h, p3), "phase timing")
             acc += np.array(p3[:])
-        phases[prec] = acc / 3
-    lib.btk_set_timing(h, 0)
+        lib.btk_set_timing(h, 0)
+        return acc / reps
+
+    timed = {}
+    launches = {}
+    with Clocks(local) as clk:
+        for prec in (N.MIXED, N.FP64):
+            ms_avg, ms, launches[prec] = time_graph(prec)
+            timed[prec] = (ms_avg, ms)
+    clocks = clk.summary()
+
+    # The mixed tile solve's two factorisations (btk_tuning.tile_tensor): the tuned one is the line's
+    # value; the other is timed the same way here.
+    from boitata_b200.autotune import get_tuning
+
+    use(N.MIXED)
+    tuned_tensor = int(get_tuning(ctx).get("tile_tensor", 0))
+    override[N.MIXED] = dict(get_tuning(ctx), tile_tensor=1 - tuned_tensor)
+    step(N.MIXED)
+    torch.cuda.synchronize()
+    alt_result = host_copy(outs)
+    with Clocks(local) as clk_alt:
+        alt_ms = time_graph(N.MIXED)[0]
+    alt_phase = solve_phase(N.MIXED)
+    del override[N.MIXED]
+
+    # Per-phase kernel times (CUDA events on the launch stream), untimed pass.
+    phases = {prec: solve_phase(prec) for prec in (N.MIXED, N.FP64)}
     peak64 = lib.btk_peak_flops(h, 1)
     peak32 = lib.btk_peak_flops(h, 0)
 
@@ -726,6 +751,20 @@ def main():
         "gpu_launches": int(launches[N.MIXED]),
         "clocks": clocks,
     }
+    forms = {tuned_tensor: (ms_mixed, phases[N.MIXED][1], mixed), 1 - tuned_tensor: (alt_ms, alt_phase[1], alt_result)}
+    line["tile_factorisation"] = {
+        "tuned": "tensor" if tuned_tensor else "unblocked",
+        "forms": {name: {"ms_per_step": forms[v][0], "blocks_per_s": ws * m / (forms[v][0] * 1e-3),
+                         "solve_ms": forms[v][1], "mixed_over_fp64": ms_fp64 / forms[v][0],
+                         "vs_fp64_max_error": float(np.nanmax(np.concatenate([
+                             rel_err(forms[v][2]["value"], v64), rel_err(forms[v][2]["variance"], s64)]))),
+                         "fp64_fallback_systems": int(np.sum((forms[v][2]["status"] & 0x10) != 0))}
+                  for v, name in ((0, "unblocked"), (1, "tensor"))},
+        "about": "mixed tile solve: 'unblocked' = FP32 right-looking LDL^T, packed FMA, two systems a warp; "
+                 "'tensor' = 8-column panels on the CUDA cores, trailing updates as split-TF32 mma.sync "
+                 "(m16n8k8, three per tile); both with the same FP64 residual test and refinement",
+        "clocks_alt": clk_alt.summary(),
+    }
 
     if not args.no_e2e:
         cent = np.empty((m, 3))
@@ -767,6 +806,8 @@ def main():
         base, ref, cells = cpu_baseline(w, args.cpu_sample)
         line["cpu_baseline"] = base
         line["oracle_error"] = {"fp64": oracle_error(fp64, ref, cells), "mixed": oracle_error(mixed, ref, cells),
+                                "mixed_" + ("unblocked" if tuned_tensor else "tensor"): oracle_error(alt_result, ref,
+                                                                                                   cells),
                                 "sample": base["sample"],
                                 "metric": "|a-b| / (1 + max(|a|, |b|)) over value, variance and lagrange against "
                                           "the FP64 oracle (crates/estimation/src/kernel.rs:178-180)",

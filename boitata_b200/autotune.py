@@ -5,11 +5,12 @@ The tunables (btk_tuning in include/boitata_b200.h):
 - the block-model tile one search warp serves (32 cells);
 - warps per search CTA (shared-memory granularity);
 - resident solve CTAs per SM;
-- the table size of the tile-shared solve (0: per-system assembly).
+- the table size of the tile-shared solve (0: per-system assembly);
+- for the mixed form, the tile solve's factorisation with its trailing updates on the tensor pipe or not.
 
 They are picked by timing the real workload. The time is the sum of the search and solve kernels, taken
 with CUDA events on the launch stream. Three stages run, each at the best of the one before: cell size x
-tile, then search CTA warps, then table size x solve CTAs per SM. Block models (autotune_geometry) and
+tile, then search CTA warps, then table size x solve CTAs per SM, then (mixed form) the tensor pipe. Block models (autotune_geometry) and
 device target arrays (autotune_device, e.g. uneven neighbour counts with per-target kinds in one launch)
 are tuned alike. The choice is cached per workload signature in a JSON file (BTK_TUNING_CACHE, or
 ~/.cache/boitata_b200/tuning.json) and applied to the context.
@@ -39,7 +40,8 @@ def get_tuning(ctx):
     t = N.TuningC()
     ctx.check(ctx._lib.btk_get_tuning(ctx.handle, ctypes.byref(t)), "tuning")
     return {"samples_per_cell": t.samples_per_cell, "tile": tuple(t.tile), "search_warps": t.search_warps,
-            "solve_blocks_per_sm": t.solve_blocks_per_sm, "tile_union": t.tile_union, "host_chunk": t.host_chunk}
+            "solve_blocks_per_sm": t.solve_blocks_per_sm, "tile_union": t.tile_union, "host_chunk": t.host_chunk,
+            "tile_tensor": t.tile_tensor}
 
 
 def set_tuning(ctx, cfg):
@@ -51,6 +53,7 @@ def set_tuning(ctx, cfg):
     t.solve_blocks_per_sm = int(cfg["solve_blocks_per_sm"])
     t.tile_union = int(cfg.get("tile_union", 64))
     t.host_chunk = int(cfg.get("host_chunk", 0))
+    t.tile_tensor = int(cfg.get("tile_tensor", 0))
     ctx.check(ctx._lib.btk_set_tuning(ctx.handle, ctypes.byref(t)), "tuning")
 
 
@@ -122,8 +125,9 @@ def time_device(estimator, m, d_xyz, d_kinds=None, *, kparam=0.0, precision="mix
     return float(np.median(times))
 
 
-def _search(ctx, base, timer, table):
-    """The three stages over the tunables, each at the best of the one before; returns (best, ms)."""
+def _search(ctx, base, timer, table, mixed=False):
+    """The stages over the tunables, each at the best of the one before; returns (best, ms). The mixed form
+    adds a fourth: the tile solve's factorisation with and without the tensor pipe."""
     best, best_ms = dict(base), float("inf")
     for ppc in SAMPLES_PER_CELL:
         for tile in TILES:
@@ -154,10 +158,18 @@ def _search(ctx, base, timer, table):
             table.append((dict(cfg), ms))
             if ms < best_ms:
                 best, best_ms = dict(cfg), ms
+    stage3 = dict(best)
+    if mixed and stage3["tile_union"] > 0:
+        cfg = dict(stage3, tile_tensor=1 - int(stage3.get("tile_tensor", 0)))
+        set_tuning(ctx, cfg)
+        ms = timer()
+        table.append((dict(cfg), ms))
+        if ms < best_ms:
+            best, best_ms = dict(cfg), ms
     return best, best_ms
 
 
-def _tune(estimator, key, timer, use_cache):
+def _tune(estimator, key, timer, use_cache, mixed=False):
     estimator._fitted()
     estimator._use_pass(0)
     ctx = estimator._ctx
@@ -175,7 +187,7 @@ def _tune(estimator, key, timer, use_cache):
         set_tuning(ctx, cfg)
         return {"best": cfg, "ms": cache[key]["ms"], "table": [], "cached": True}
     table = []
-    best, best_ms = _search(ctx, get_tuning(ctx), timer, table)
+    best, best_ms = _search(ctx, get_tuning(ctx), timer, table, mixed)
     set_tuning(ctx, best)
     if use_cache:
         cache[key] = {"best": {**best, "tile": list(best["tile"])}, "ms": best_ms}
@@ -192,7 +204,8 @@ def autotune_geometry(estimator, geometry, *, precision="mixed", steps=2, use_ca
     """Picks and applies the fastest tuning for kriging `geometry` with `estimator` (fitted, first pass).
     Returns {"best": config, "ms": time, "table": [(config, ms), ...], "cached": bool}."""
     key = signature(estimator, geometry, precision)
-    return _tune(estimator, key, lambda: time_geometry(estimator, geometry, precision, steps), use_cache)
+    return _tune(estimator, key, lambda: time_geometry(estimator, geometry, precision, steps), use_cache,
+                 precision == "mixed")
 
 
 def autotune_device(estimator, m, d_xyz, d_kinds=None, *, kparam=0.0, precision="mixed", steps=2, use_cache=True,
@@ -203,4 +216,4 @@ def autotune_device(estimator, m, d_xyz, d_kinds=None, *, kparam=0.0, precision=
         f'"tag": {json.dumps(tag)}}}'
     return _tune(estimator, key,
                  lambda: time_device(estimator, m, d_xyz, d_kinds, kparam=kparam, precision=precision, steps=steps),
-                 use_cache)
+                 use_cache, precision == "mixed")

@@ -832,6 +832,7 @@ int btk_get_tuning(const btk_ctx* ctx, btk_tuning* out) {
   out->solve_blocks_per_sm = ctx->tuning.solve_blocks_per_sm;
   out->tile_union = ctx->tuning.tile_union;
   out->host_chunk = ctx->tuning.host_chunk;
+  out->tile_tensor = ctx->tuning.tile_tensor;
   return BTK_OK;
 }
 
@@ -847,6 +848,7 @@ int btk_set_tuning(btk_ctx* ctx, const btk_tuning* t) {
   if (t->tile_union != 0 && (t->tile_union < 32 || t->tile_union > 255))
     return fail(ctx, BTK_EINVAL, "tile_union must be 0 or in 32..255");
   if (t->host_chunk < 0) return fail(ctx, BTK_EINVAL, "host_chunk must be >= 0");
+  if (t->tile_tensor != 0 && t->tile_tensor != 1) return fail(ctx, BTK_EINVAL, "tile_tensor must be 0 or 1");
   if (!(t->samples_per_cell > 0.0 && t->samples_per_cell <= 1e6))
     return fail(ctx, BTK_EINVAL, "samples_per_cell must be > 0");
   for (int a = 0; a < 3; ++a) ctx->tuning.tile[a] = t->tile[a];
@@ -854,6 +856,7 @@ int btk_set_tuning(btk_ctx* ctx, const btk_tuning* t) {
   ctx->tuning.solve_blocks_per_sm = t->solve_blocks_per_sm;
   ctx->tuning.tile_union = t->tile_union;
   ctx->tuning.host_chunk = t->host_chunk;
+  ctx->tuning.tile_tensor = t->tile_tensor;
   if (t->samples_per_cell != ctx->ppc) {
     ctx->ppc = t->samples_per_cell;
     if (ctx->fitted) {

@@ -180,6 +180,7 @@ struct Tuning {
   int tile_union = 64;           // tile-shared solve: most distinct samples per tile; 0: per-system solve
                                  // (64 lets four mixed-form CTAs share an SM; a tile above it is split)
   int host_chunk = 0;            // host-buffer calls: targets per pipelined chunk; 0: one chunk
+  int tile_tensor = 0;           // mixed tile solve: 1 = trailing updates on the tensor pipe (split TF32)
 };
 
 struct Launch {

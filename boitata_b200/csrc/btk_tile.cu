@@ -29,7 +29,11 @@
 //      column to a packed per-warp triangle in shared memory, a
 //      column-oriented backward sweep over that triangle for x = C^-1 v, FP64
 //      residuals r = v - C x from the FP64 table and the corrected forms
-//      u'x_v + x_u'r_v, as in btk_solve.cu's mixed kernel.
+//      u'x_v + x_u'r_v, as in btk_solve.cu's mixed kernel. The tensor form
+//      of the mixed solve (tuning tile_tensor) factors the same two systems
+//      blocked instead: the lower triangles in place in the packed triangle,
+//      8-column panels on the CUDA cores, the trailing updates as split-TF32
+//      mma.sync tiles (factor_tc); the sweep and the FP64 tail are shared.
 //
 // Systems the tile does not take: a failed search (outputs written here),
 // n > 32 (appended to `large`) and a sample flagged coincident at fit time
@@ -377,6 +381,144 @@ __device__ __forceinline__ float warp_maxf(float v) {
 
 __device__ __forceinline__ float2 rcp2(float2 d) { return make_float2(rcp_approx(d.x), rcp_approx(d.y)); }
 
+// Entry (i, c), i > c, of the packed lower triangle (see WarpMixed); the
+// tensor form keeps the diagonal in the front pad, lt[c].
+__device__ __forceinline__ int tri(int i, int c) { return kLtPad + col_off(c) + i - c - 1; }
+
+// x = hi + lo with hi and lo in TF32 (round to nearest): a product of two
+// such splits, hi*hi + hi*lo + lo*hi, carries about FP32's precision.
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
+  const float r = x - __uint_as_float(hi);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
+}
+
+// d += a b for a 16x8 (row) by 8x8 (col) TF32 tile, FP32 accumulation.
+// Fragments (PTX ISA, mma.m16n8k8 .tf32), g = lane / 4, t = lane % 4:
+// a0 (g, t), a1 (g + 8, t), a2 (g, t + 4), a3 (g + 8, t + 4);
+// b0 (k = t, n = g), b1 (k = t + 4, n = g);
+// d0 (g, 2t), d1 (g, 2t + 1), d2 (g + 8, 2t), d3 (g + 8, 2t + 1).
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// The FP32 LDL^T of two systems (float2: a in .x, b in .y) in blocked form
+// with the trailing updates on the tensor pipe. The lower triangles sit in
+// place in the warp's packed triangle (padded rows and columns: the
+// identity); each panel of 8 columns is factored row per lane on the CUDA
+// cores, with the forward substitution of y fused in, writing its columns
+// D_k L[i][k] back in place; the trailing lower triangle then takes
+// -W L^T (W = L D, the panel's columns) as 16x8 tiles of split-TF32 mma,
+// three per tile and system (lo*hi, hi*lo, hi*hi). On return the triangle
+// holds what the unblocked form writes, so the backward sweep is shared.
+__device__ __forceinline__ void factor_tc(const TileHead& H, const double* Ua, const double* Ub, WarpMixed& Ws,
+                                          int ta, int tb, int na, int nb, int nmax, int lane, float2 (&y)[3],
+                                          float2& dme, float2& pmin) {
+  float2* lt = Ws.lt;
+  // The columns that take pivots, every row below the diagonal; columns
+  // past nmax are never read for a system's results.
+  for (int c = 0; c < nmax; ++c) {
+    if (lane >= c) {
+      const int mca = H.map[ta][c], mcb = H.map[tb][c];
+      const float vx = (lane < na && c < na) ? float(Ua[mca]) : (lane == c ? 1.f : 0.f);
+      const float vy = (lane < nb && c < nb) ? float(Ub[mcb]) : (lane == c ? 1.f : 0.f);
+      lt[lane == c ? c : tri(lane, c)] = make_float2(vx, vy);
+    }
+  }
+  __syncwarp();
+  const int g = lane >> 2, t = lane & 3;
+  const int np = (nmax + 7) >> 3;
+  for (int p = 0; p < np; ++p) {
+    const int kb = 8 * p;
+    float2 pa[8];  // this lane's row in the panel's columns
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int c = kb + m;
+      pa[m] = lane > c ? lt[tri(lane, c)] : (lane == c ? lt[c] : make_float2(0.f, 0.f));
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int k = kb + j;
+      if (k >= nmax) break;
+      const int b = k & 1;
+      if (lane > k) lt[tri(lane, k)] = pa[j];
+      if (lane == k) {  // pivot and right-hand side, two 16-byte stores
+        reinterpret_cast<float4*>(Ws.prhs[b])[0] = make_float4(pa[j].x, pa[j].y, y[0].x, y[0].y);
+        reinterpret_cast<float4*>(Ws.prhs[b])[1] = make_float4(y[1].x, y[1].y, y[2].x, y[2].y);
+      }
+      __syncwarp();
+      const float4 p0 = reinterpret_cast<const float4*>(Ws.prhs[b])[0];
+      const float4 p1 = reinterpret_cast<const float4*>(Ws.prhs[b])[1];
+      pmin.x = fminf(pmin.x, p0.x), pmin.y = fminf(pmin.y, p0.y);
+      if (lane == k) dme = make_float2(p0.x, p0.y);
+      const float2 nrd = make_float2(rcp_approx(-p0.x), rcp_approx(-p0.y));
+      const float2 nf = lane > k ? __fmul2_rn(pa[j], nrd) : make_float2(0.f, 0.f);  // -L[lane][k]
+      // The panel's later columns: column k at rows kb + m, entries m - j - 1.
+      const float2* col = lt + kLtPad + col_off(k);
+#pragma unroll
+      for (int m = j + 1; m < 8; m += 2) {
+        const float4 c4 = *reinterpret_cast<const float4*>(&col[m - j - 1]);
+        pa[m] = __ffma2_rn(nf, make_float2(c4.x, c4.y), pa[m]);
+        if (m + 1 < 8) pa[m + 1] = __ffma2_rn(nf, make_float2(c4.z, c4.w), pa[m + 1]);
+      }
+      y[0] = __ffma2_rn(nf, make_float2(p0.z, p0.w), y[0]);
+      y[1] = __ffma2_rn(nf, make_float2(p1.x, p1.y), y[1]);
+      y[2] = __ffma2_rn(nf, make_float2(p1.z, p1.w), y[2]);
+    }
+    if (p + 1 >= np) break;
+    // A full panel (8 (p + 1) < nmax): the trailing update on the tensor pipe.
+    __syncwarp();
+    const float2 d0 = make_float2(__shfl_sync(kFull, dme.x, kb + t), __shfl_sync(kFull, dme.y, kb + t));
+    const float2 d1 = make_float2(__shfl_sync(kFull, dme.x, kb + t + 4), __shfl_sync(kFull, dme.y, kb + t + 4));
+    const float2 rd[2] = {rcp2(d0), rcp2(d1)};
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+      if (16 * mt + 15 < kb + 8) continue;  // every row of the m-tile already pivoted
+      uint32_t ah[2][4], al[2][4];          // [system][fragment]: -W[r][kb + t + 4 (e / 2)]
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int r = 16 * mt + g + 8 * (e & 1), kk = kb + t + 4 * (e >> 1);
+        const float2 w = r > kk ? lt[tri(r, kk)] : make_float2(0.f, 0.f);
+        split_tf32(-w.x, ah[0][e], al[0][e]);
+        split_tf32(-w.y, ah[1][e], al[1][e]);
+      }
+      for (int nt = p + 1; nt < np; ++nt) {
+        if (16 * mt + 15 < 8 * nt) continue;  // above the diagonal
+        uint32_t bh[2][2], bl[2][2];          // [system][fragment]: L[8 nt + g][kb + t + 4 q]
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int c = 8 * nt + g, kk = kb + t + 4 * q;
+          const float2 w = lt[tri(c, kk)];
+          split_tf32(w.x * rd[q].x, bh[0][q], bl[0][q]);
+          split_tf32(w.y * rd[q].y, bh[1][q], bl[1][q]);
+        }
+        float cx[4], cy[4];
+        int at[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int r = 16 * mt + g + 8 * (e >> 1), c = 8 * nt + 2 * t + (e & 1);
+          at[e] = r > c ? tri(r, c) : (r == c ? c : -1);
+          const float2 v = at[e] >= 0 ? lt[at[e]] : make_float2(0.f, 0.f);
+          cx[e] = v.x, cy[e] = v.y;
+        }
+        mma_tf32(cx, al[0], bh[0]);
+        mma_tf32(cx, ah[0], bl[0]);
+        mma_tf32(cx, ah[0], bh[0]);
+        mma_tf32(cy, al[1], bh[1]);
+        mma_tf32(cy, ah[1], bl[1]);
+        mma_tf32(cy, ah[1], bh[1]);
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (at[e] >= 0) lt[at[e]] = make_float2(cx[e], cy[e]);
+      }
+    }
+    __syncwarp();
+  }
+}
+
 // Pivots k0 .. k1-1 of the FP32 LDL^T of two systems at once (float2 lanes:
 // system a in .x, b in .y), forward substitution of y fused in; the row is
 // kept shifted (slot 0 = the current pivot column) and a step updates the W
@@ -412,7 +554,9 @@ __device__ __forceinline__ void eliminate2(float2 (&A)[32], int k0, int k1, int 
   }
 }
 
-// Mixed form: systems 2p (a) and 2p + 1 (b) of the tile on one warp, lane = row.
+// Mixed form: systems 2p (a) and 2p + 1 (b) of the tile on one warp, lane = row;
+// TC: the blocked factorisation with tensor-pipe trailing updates.
+template <bool TC>
 __device__ void solve_mixed(const TileDev& a, const TileHead& H, const double* P, const double* Z, const double* UU,
                             int umax, int S, WarpMixed& W, int p) {
   const SolveDev& s = a.s;
@@ -439,20 +583,24 @@ __device__ void solve_mixed(const TileDev& a, const TileHead& H, const double* P
   }
   const double* Ua = UU + ma * S;
   const double* Ub = UU + mb * S;
-  float2 A[32];
-#pragma unroll
-  for (int q = 0; q < 32; ++q) {
-    A[q].x = (ha && q < na) ? float(Ua[H.map[ta][q]]) : (q == lane ? 1.f : 0.f);
-    A[q].y = (hb && q < nb) ? float(Ub[H.map[tb][q]]) : (q == lane ? 1.f : 0.f);
-  }
   float2 y[3] = {make_float2(float(ca), float(cb)), make_float2(ha ? 1.f : 0.f, hb ? 1.f : 0.f),
                  make_float2(float(za), float(zb))};
   float2 dme = make_float2(1.f, 1.f), pmin = make_float2(3.0e38f, 3.0e38f);
-  const int n1 = min(nmax, 8), n2 = min(nmax, 16), n3 = min(nmax, 24);
-  eliminate2<32>(A, 0, n1, lane, W, y, dme, pmin);
-  eliminate2<24>(A, n1, n2, lane, W, y, dme, pmin);
-  eliminate2<16>(A, n2, n3, lane, W, y, dme, pmin);
-  eliminate2<8>(A, n3, nmax, lane, W, y, dme, pmin);
+  if constexpr (TC) {
+    factor_tc(H, Ua, Ub, W, ta, tb, na, nb, nmax, lane, y, dme, pmin);
+  } else {
+    float2 A[32];
+#pragma unroll
+    for (int q = 0; q < 32; ++q) {
+      A[q].x = (ha && q < na) ? float(Ua[H.map[ta][q]]) : (q == lane ? 1.f : 0.f);
+      A[q].y = (hb && q < nb) ? float(Ub[H.map[tb][q]]) : (q == lane ? 1.f : 0.f);
+    }
+    const int n1 = min(nmax, 8), n2 = min(nmax, 16), n3 = min(nmax, 24);
+    eliminate2<32>(A, 0, n1, lane, W, y, dme, pmin);
+    eliminate2<24>(A, n1, n2, lane, W, y, dme, pmin);
+    eliminate2<16>(A, n2, n3, lane, W, y, dme, pmin);
+    eliminate2<8>(A, n3, nmax, lane, W, y, dme, pmin);
+  }
   // An FP32 pivot that is NaN or at most n ulp(C0) is not resolved from the
   // rounding of its row: the FP64 form takes the system (and with it the
   // singular decision, kernel.rs:61).
@@ -539,8 +687,9 @@ __device__ void solve_mixed(const TileDev& a, const TileHead& H, const double* P
 // two float2 rows fit without spills), and with a 64-sample table both
 // forms' shared memory fits four times in the SM's 228 KB. The mixed form
 // at three CTAs (168 registers) took 20.1 ms at 3.2M blocks, at four 18.1.
-template <bool MIXED>
+template <int FORM>  // 0: FP64; 1: mixed; 2: mixed with the tensor-pipe factorisation
 __global__ void __launch_bounds__(kThreads, 4) k_tile(TileDev a) {
+  constexpr bool MIXED = FORM != 0;
   extern __shared__ __align__(16) unsigned char smem[];
   const Layout lay = layout(a.umax, a.stride, MIXED);
   const TileHead& H = *reinterpret_cast<const TileHead*>(smem + lay.head);
@@ -555,7 +704,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(TileDev a) {
     if (MIXED) {
       WarpMixed& W = reinterpret_cast<WarpMixed*>(smem + lay.warp)[warp];
       for (int p = warp; p < kT / 2; p += kThreads / 32)
-        if (H.go[2 * p] || H.go[2 * p + 1]) solve_mixed(a, H, P, Z, UU, a.umax, a.stride, W, p);
+        if (H.go[2 * p] || H.go[2 * p + 1]) solve_mixed<FORM == 2>(a, H, P, Z, UU, a.umax, a.stride, W, p);
     } else {
       WarpFp64& W = reinterpret_cast<WarpFp64*>(smem + lay.warp)[warp];
       for (int t = warp; t < kT; t += kThreads / 32)
@@ -578,20 +727,14 @@ __global__ void __launch_bounds__(kThreads, 4) k_tile(TileDev a) {
 
 }  // namespace
 
-cudaError_t launch_tile(const Launch& L, const TileDev& a0, bool mixed) {
-  TileDev a = a0;
-  if (a.umax < 2 || a.umax > 255) return cudaErrorInvalidValue;
-  a.stride = a.umax | 1;  // odd row stride
-  const size_t smem = layout(a.umax, a.stride, mixed).total;
-  cudaError_t e;
+namespace {
+
+template <int FORM>
+cudaError_t launch_form(const Launch& L, const TileDev& a) {
+  const size_t smem = layout(a.umax, a.stride, FORM != 0).total;
   int per_sm = 0;
-  if (mixed) {
-    e = cudaFuncSetAttribute(k_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<true>, kThreads, smem);
-  } else {
-    e = cudaFuncSetAttribute(k_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<false>, kThreads, smem);
-  }
+  cudaError_t e = cudaFuncSetAttribute(k_tile<FORM>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<FORM>, kThreads, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   if (L.tuning.solve_blocks_per_sm > 0 && L.tuning.solve_blocks_per_sm < per_sm) per_sm = L.tuning.solve_blocks_per_sm;
@@ -599,12 +742,19 @@ cudaError_t launch_tile(const Launch& L, const TileDev& a0, bool mixed) {
   int64_t blocks = int64_t(L.sm_count) * per_sm;
   if (blocks > ntiles) blocks = ntiles;
   if (blocks < 1) blocks = 1;
-  if (mixed)
-    k_tile<true><<<int(blocks), kThreads, smem, L.stream>>>(a);
-  else
-    k_tile<false><<<int(blocks), kThreads, smem, L.stream>>>(a);
+  k_tile<FORM><<<int(blocks), kThreads, smem, L.stream>>>(a);
   ++*L.counter;
   return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_tile(const Launch& L, const TileDev& a0, bool mixed) {
+  TileDev a = a0;
+  if (a.umax < 2 || a.umax > 255) return cudaErrorInvalidValue;
+  a.stride = a.umax | 1;  // odd row stride
+  if (!mixed) return launch_form<0>(L, a);
+  return L.tuning.tile_tensor ? launch_form<2>(L, a) : launch_form<1>(L, a);
 }
 
 }  // namespace btk

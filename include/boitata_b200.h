@@ -136,8 +136,11 @@ typedef struct {
  * 32), warps per search CTA, resident solve CTAs per SM (0: defaults), and
  * the most distinct samples the tile-shared solve tabulates for 16
  * consecutive targets (32..255; 0: every system assembles its own matrix),
- * and for calls with host buffers the targets per chunk of the copy/compute
- * pipeline (0: the whole call at once; at most 8 chunks). */
+ * for calls with host buffers the targets per chunk of the copy/compute
+ * pipeline (0: the whole call at once; at most 8 chunks), and for the mixed
+ * form's tile-shared solve whether the factorisation's trailing updates run
+ * on the tensor pipe (1: 8-column panels on the CUDA cores, the updates as
+ * split-TF32 mma; 0: the unblocked FP32 elimination). */
 typedef struct {
   double samples_per_cell;
   int32_t tile[3];
@@ -145,6 +148,7 @@ typedef struct {
   int32_t solve_blocks_per_sm;
   int32_t tile_union;
   int32_t host_chunk;
+  int32_t tile_tensor;
 } btk_tuning;
 
 typedef struct btk_ctx btk_ctx;

@@ -1,0 +1,96 @@
+"""The mixed form's tile solve with its trailing updates on the tensor pipe (tuning.tile_tensor = 1).
+
+The factorisation is blocked: 8-column panels on the CUDA cores, the
+trailing lower triangle updated by split-TF32 mma (btk_tile.cu factor_tc).
+Its results are held to the mixed form's bar against the oracle (1e-6 per
+result in |a - b| <= tol (1 + max(|a|, |b|)), NaN pattern, status and
+n_used equal), and they differ in the last bits from the unblocked FP32
+elimination's, which shows the other factorisation ran.
+"""
+
+import numpy as np
+import pytest
+from conftest import close
+from test_gpu_parity import assert_same_estimates, centroids
+
+from boitata_b200 import OrdinaryKriging
+from boitata_b200 import workloads as W
+from boitata_b200.autotune import get_tuning, set_tuning
+from boitata_b200.errors import InvalidInput
+
+pytestmark = pytest.mark.gpu
+
+
+def tensor(est, on=1):
+    set_tuning(est._ctx, dict(get_tuning(est._ctx), tile_tensor=on))
+    return est
+
+
+def test_tensor_form_c1_block_model(oracle):
+    w = W.c1()
+    targets = centroids(oracle, w)
+    est = tensor(OrdinaryKriging(w.variogram, w.search, precision="mixed").fit(w.coords, w.values))
+    got = est.predict_full(targets)
+    ref = oracle.estimate_many(targets, w.coords, w.values, w.search, w.variogram, neighbors=False)
+    assert_same_estimates(got, ref, 1e-6)
+    on_device = est.predict_full(w.geometry)
+    for k in ("value", "variance", "lagrange"):
+        np.testing.assert_array_equal(on_device[k], got[k])
+
+
+def test_tensor_form_c2_model_200k_blocks(oracle):
+    """200,000 blocks of the 3.2M-block c2 model (every 16th cell), whole geometry on the device."""
+    w = W.c2()
+    cells = np.arange(0, w.geometry.cells(), 16)
+    targets = centroids(oracle, w)[cells]
+    ref = oracle.estimate_many(targets, w.coords, w.values, w.search, w.variogram, neighbors=False)
+    est = OrdinaryKriging(w.variogram, w.search, precision="mixed").fit(w.coords, w.values)
+    plain = est.predict_full(w.geometry)
+    got = tensor(est).predict_full(w.geometry)
+    sel = {k: v[cells] for k, v in got.items()}
+    assert_same_estimates(sel, ref, 1e-6)
+    fin = np.isfinite(got["value"])
+    assert not np.array_equal(got["value"][fin], plain["value"][fin])
+    assert np.all(close(got["value"][fin], plain["value"][fin], 1e-6))
+    # Refinement and re-solve flags stay rare (bit 0x10: the FP64 re-solve took the system).
+    assert np.mean((got["status"][fin] & 0x10) != 0) < 0.01
+
+
+def test_tensor_form_uneven_counts_and_kinds(oracle):
+    # c3: 4-64 samples (the tile takes n <= 32), simple kriging on every 10th target in the same launch.
+    w = W.c3()
+    targets = centroids(oracle, w, 3)
+    kinds = np.where(np.arange(len(targets)) % 10 == 0, "simple", "ordinary")
+    est = tensor(OrdinaryKriging(w.variogram, w.search, precision="mixed").fit(w.coords, w.values))
+    got = est.predict_kinds(targets, kinds, mean=1.0)
+    for kind in ("ordinary", "simple"):
+        sel = kinds == kind
+        ref = oracle.estimate_many(targets[sel], w.coords, w.values, w.search, w.variogram, kind=kind, kparam=1.0,
+                                   neighbors=False)
+        assert_same_estimates({k: v[sel] for k, v in got.items()}, ref, 1e-6)
+
+
+def test_tensor_form_ill_conditioned_systems(oracle):
+    # Gaussian model with a 1e-4 nugget and near-duplicate samples: condition numbers reach ~5e5, the
+    # systems go through the refinement; every result at 1e-6 against the oracle.
+    w = W.c5(holes=160)
+    rng = np.random.default_rng(0)
+    cent = centroids(oracle, w)
+    targets = cent[rng.choice(len(cent), 2000, replace=False)]
+    ref = oracle.estimate_many(targets, w.coords, w.values, w.search, w.variogram, neighbors=False)
+    est = tensor(OrdinaryKriging(w.variogram, w.search, precision="mixed").fit(w.coords, w.values))
+    got = est.predict_full(targets)
+    fin = np.isfinite(ref["value"])
+    assert np.array_equal(fin, np.isfinite(got["value"]))
+    assert np.array_equal(got["status"] & 0x0F, ref["status"].astype(np.int8))
+    assert np.mean((got["status"][fin] & 0x10) != 0) < 0.05
+    for k in ("value", "variance", "lagrange"):
+        assert np.all(close(got[k][fin], ref[k][fin], 1e-6)), k
+
+
+def test_tensor_switch_is_checked():
+    w = W.c1()
+    est = OrdinaryKriging(w.variogram, w.search, precision="mixed").fit(w.coords[:500], w.values[:500])
+    with pytest.raises(InvalidInput, match="tile_tensor"):
+        tensor(est, 2)
+    assert get_tuning(est._ctx)["tile_tensor"] == 0
