@@ -426,6 +426,20 @@ def config_c3(args, dev, stream, flush, tune=True):
         got[name] = host_copy(outs)
         out[name] = {"blocks_per_s": m / (ms * 1e-3), "ms_per_step": ms, "gpu_launches_per_step":
                      launches / max(args.steps, 5)}
+    # The mixed form's other kernel for its systems above 32 samples, timed the same way.
+    from boitata_b200.autotune import get_tuning, set_tuning
+
+    tuned = get_tuning(ctx)
+    set_tuning(ctx, dict(tuned, mixed_large=1 - int(tuned["mixed_large"])))
+    ctx.check(lib.btk_graph_capture_device(h, m, d_xyz.data_ptr(), d_kinds.data_ptr(), N.ORDINARY, 1.0, N.MIXED,
+                                           ctypes.byref(oc)), "capture")
+    ms, _ = Replay(ctx, stream, flush).time(args.warmup, max(args.steps, 5))
+    got["mixed_alt"] = host_copy(outs)
+    out["mixed_alt"] = {"blocks_per_s": m / (ms * 1e-3), "ms_per_step": ms,
+                        "large_systems": "fp64 kernel" if not tuned["mixed_large"] else
+                        "fp32 factorisation, fp64 refinement"}
+    out["mixed"]["large_systems"] = "fp64 kernel" if tuned["mixed_large"] else "fp32 factorisation, fp64 refinement"
+    set_tuning(ctx, tuned)
     n_used = got["fp64"]["n_used"]
     ok = (got["fp64"]["status"] & 0x0F) == 0
     out["n_used"] = {"min": int(n_used[ok].min()), "max": int(n_used[ok].max()), "mean": float(n_used[ok].mean())}
@@ -437,7 +451,7 @@ def config_c3(args, dev, stream, flush, tune=True):
                                  neighbors=False)
         for k, v in r.items():
             ref.setdefault(k, np.empty(m, dtype=v.dtype))[sel] = v
-    out["oracle_error"] = {name: oracle_error(got[name], ref) for name in ("fp64", "mixed")}
+    out["oracle_error"] = {name: oracle_error(got[name], ref) for name in ("fp64", "mixed", "mixed_alt")}
     out["launch"] = "btk_graph_capture_device (btk_predict_kinds_device: Hilbert order, search, tile solve, " \
                     "per-system kernels, FP64 re-solve) replayed per step; L2 flushed between steps"
     del est
@@ -465,16 +479,29 @@ def config_c5(args, dev, stream, flush, sample=20_000):
                        "8 per octant / 64 max, radius 300 m", "blocks": m, "samples": int(len(w.coords))}
     got = {}
     steps = max(2, min(args.steps, 3))
-    for prec, name in ((N.FP64, "fp64"), (N.MIXED, "mixed")):
+    from boitata_b200.autotune import get_tuning, set_tuning
+
+    base = get_tuning(ctx)
+    # The mixed form's systems above 32 samples (nearly all here) in FP32 with FP64 refinement, or by the FP64
+    # kernel (btk_tuning.mixed_large); the mixed form is the faster of the two, as the autotuner picks.
+    variants = ((N.FP64, "fp64", base), (N.MIXED, "mixed_fp32_large", dict(base, mixed_large=0)),
+                (N.MIXED, "mixed_fp64_large", dict(base, mixed_large=1)))
+    for prec, name, tun in variants:
+        set_tuning(ctx, tun)
         ctx.check(lib.btk_graph_capture_geometry(h, ctypes.byref(gc), N.ORDINARY, 0.0, prec, ctypes.byref(oc)),
                   "capture")
         ms, _ = Replay(ctx, stream, flush).time(1, steps)
         st = outs["status"].cpu().numpy()
         got[name] = {k: v.cpu().numpy() for k, v in outs.items()}
         out[name] = {"blocks_per_s": m / (ms * 1e-3), "ms_per_step": ms}
-        if name == "mixed":
+        if prec == N.MIXED:
             fin = (st & 0x0F) == 0
             out[name]["fp64_fallback_fraction"] = float(np.mean((st[fin] & 0x10) != 0))
+    set_tuning(ctx, base)
+    pick = min(("mixed_fp32_large", "mixed_fp64_large"), key=lambda k: out[k]["ms_per_step"])
+    out["mixed"] = dict(out[pick], large_systems="fp64 kernel" if pick == "mixed_fp64_large" else
+                        "fp32 factorisation, fp64 refinement")
+    got["mixed"] = got[pick]
     out["mixed_over_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
     # The gradient of the global mean estimate with respect to the variogram (nugget, sill, range, 2 ratios,
     # 3 angles), neighbourhoods frozen at theta0, covariances recomputed in the adjoint; against one forward
@@ -498,7 +525,8 @@ def config_c5(args, dev, stream, flush, sample=20_000):
     cells = np.arange(0, m, m // sample)[:sample]
     cent = oracle.centroids(g.origin, g.size, g.count, g.rotation)[cells]
     ref = oracle.estimate_many(cent, w.coords, w.values, w.search, w.variogram, neighbors=False)
-    out["oracle_error"] = {name: oracle_error(got[name], ref, cells) for name in ("fp64", "mixed")}
+    out["oracle_error"] = {name: oracle_error(got[name], ref, cells)
+                           for name in ("fp64", "mixed_fp32_large", "mixed_fp64_large")}
     out["oracle_error"]["sample"] = f"every {m // sample}th block ({len(cells)} blocks)"
     out["oracle_error"]["note"] = ("condition numbers reach ~5e5 here, so two FP64 evaluation orders differ by up "
                                    "to ~1e-15 x cond (about 1e-10) on their own")

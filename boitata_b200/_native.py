@@ -53,7 +53,8 @@ class GeometryC(ctypes.Structure):
 class TuningC(ctypes.Structure):
     _fields_ = [("samples_per_cell", ctypes.c_double), ("tile", ctypes.c_int32 * 3), ("search_warps", ctypes.c_int32),
                 ("solve_blocks_per_sm", ctypes.c_int32), ("tile_union", ctypes.c_int32),
-                ("host_chunk", ctypes.c_int32), ("tile_tensor", ctypes.c_int32)]
+                ("host_chunk", ctypes.c_int32), ("tile_tensor", ctypes.c_int32),
+                ("mixed_large", ctypes.c_int32)]
 
 
 class OutputsC(ctypes.Structure):

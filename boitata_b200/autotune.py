@@ -6,11 +6,13 @@ The tunables (btk_tuning in include/boitata_b200.h):
 - warps per search CTA (shared-memory granularity);
 - resident solve CTAs per SM;
 - the table size of the tile-shared solve (0: per-system assembly);
-- for the mixed form, the tile solve's factorisation with its trailing updates on the tensor pipe or not.
+- for the mixed form, the tile solve's factorisation with its trailing updates on the tensor pipe or not;
+- for the mixed form, the kernel of the systems above 32 samples: FP32 with FP64 refinement, or FP64.
 
 They are picked by timing the real workload. The time is the sum of the search and solve kernels, taken
 with CUDA events on the launch stream. Three stages run, each at the best of the one before: cell size x
-tile, then search CTA warps, then table size x solve CTAs per SM, then (mixed form) the tensor pipe. Block models (autotune_geometry) and
+tile, then search CTA warps, then table size x solve CTAs per SM, then (mixed form) the tensor pipe and the
+large systems' kernel. Block models (autotune_geometry) and
 device target arrays (autotune_device, e.g. uneven neighbour counts with per-target kinds in one launch)
 are tuned alike. The choice is cached per workload signature in a JSON file (BTK_TUNING_CACHE, or
 ~/.cache/boitata_b200/tuning.json) and applied to the context.
@@ -41,7 +43,7 @@ def get_tuning(ctx):
     ctx.check(ctx._lib.btk_get_tuning(ctx.handle, ctypes.byref(t)), "tuning")
     return {"samples_per_cell": t.samples_per_cell, "tile": tuple(t.tile), "search_warps": t.search_warps,
             "solve_blocks_per_sm": t.solve_blocks_per_sm, "tile_union": t.tile_union, "host_chunk": t.host_chunk,
-            "tile_tensor": t.tile_tensor}
+            "tile_tensor": t.tile_tensor, "mixed_large": t.mixed_large}
 
 
 def set_tuning(ctx, cfg):
@@ -54,6 +56,7 @@ def set_tuning(ctx, cfg):
     t.tile_union = int(cfg.get("tile_union", 64))
     t.host_chunk = int(cfg.get("host_chunk", 0))
     t.tile_tensor = int(cfg.get("tile_tensor", 0))
+    t.mixed_large = int(cfg.get("mixed_large", 0))
     ctx.check(ctx._lib.btk_set_tuning(ctx.handle, ctypes.byref(t)), "tuning")
 
 
@@ -125,9 +128,10 @@ def time_device(estimator, m, d_xyz, d_kinds=None, *, kparam=0.0, precision="mix
     return float(np.median(times))
 
 
-def _search(ctx, base, timer, table, mixed=False):
+def _search(ctx, base, timer, table, mixed=False, large=False):
     """The stages over the tunables, each at the best of the one before; returns (best, ms). The mixed form
-    adds a fourth: the tile solve's factorisation with and without the tensor pipe."""
+    adds the tile solve's factorisation with and without the tensor pipe and, when systems can hold more
+    than 32 samples (`large`), their per-system kernel in FP32 with refinement or in FP64."""
     best, best_ms = dict(base), float("inf")
     for ppc in SAMPLES_PER_CELL:
         for tile in TILES:
@@ -166,6 +170,14 @@ def _search(ctx, base, timer, table, mixed=False):
         table.append((dict(cfg), ms))
         if ms < best_ms:
             best, best_ms = dict(cfg), ms
+    stage4 = dict(best)
+    if mixed and large:
+        cfg = dict(stage4, mixed_large=1 - int(stage4.get("mixed_large", 0)))
+        set_tuning(ctx, cfg)
+        ms = timer()
+        table.append((dict(cfg), ms))
+        if ms < best_ms:
+            best, best_ms = dict(cfg), ms
     return best, best_ms
 
 
@@ -187,7 +199,8 @@ def _tune(estimator, key, timer, use_cache, mixed=False):
         set_tuning(ctx, cfg)
         return {"best": cfg, "ms": cache[key]["ms"], "table": [], "cached": True}
     table = []
-    best, best_ms = _search(ctx, get_tuning(ctx), timer, table, mixed)
+    large = any(s.max_samples > 32 for s in estimator.searches)
+    best, best_ms = _search(ctx, get_tuning(ctx), timer, table, mixed, large)
     set_tuning(ctx, best)
     if use_cache:
         cache[key] = {"best": {**best, "tile": list(best["tile"])}, "ms": best_ms}

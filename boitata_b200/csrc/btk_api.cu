@@ -603,7 +603,10 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
     SolveDev ab = a;
     if (two || tiled) ab.list = ctx->lists.p + b * m, ab.list_len = ctx->lens.p + b;
     const int rows = b == 0 ? 32 : 64;
-    if (precision == BTK_FP64)
+    // The mixed form's systems above 32 samples take the FP64 kernel when the
+    // tuning says so: per-pivot barriers, not arithmetic, bound those
+    // kernels, so FP32 saves little there and its refinement adds sweeps.
+    if (precision == BTK_FP64 || (b == 1 && ctx->tuning.mixed_large))
       CK(launch_solve(L, ab, rows));
     else
       CK(launch_solve_mixed(L, ab, rows, ctx->redo.p + b * m, ctx->redo_len.p + b));
@@ -833,6 +836,7 @@ int btk_get_tuning(const btk_ctx* ctx, btk_tuning* out) {
   out->tile_union = ctx->tuning.tile_union;
   out->host_chunk = ctx->tuning.host_chunk;
   out->tile_tensor = ctx->tuning.tile_tensor;
+  out->mixed_large = ctx->tuning.mixed_large;
   return BTK_OK;
 }
 
@@ -849,6 +853,7 @@ int btk_set_tuning(btk_ctx* ctx, const btk_tuning* t) {
     return fail(ctx, BTK_EINVAL, "tile_union must be 0 or in 32..255");
   if (t->host_chunk < 0) return fail(ctx, BTK_EINVAL, "host_chunk must be >= 0");
   if (t->tile_tensor != 0 && t->tile_tensor != 1) return fail(ctx, BTK_EINVAL, "tile_tensor must be 0 or 1");
+  if (t->mixed_large != 0 && t->mixed_large != 1) return fail(ctx, BTK_EINVAL, "mixed_large must be 0 or 1");
   if (!(t->samples_per_cell > 0.0 && t->samples_per_cell <= 1e6))
     return fail(ctx, BTK_EINVAL, "samples_per_cell must be > 0");
   for (int a = 0; a < 3; ++a) ctx->tuning.tile[a] = t->tile[a];
@@ -857,6 +862,7 @@ int btk_set_tuning(btk_ctx* ctx, const btk_tuning* t) {
   ctx->tuning.tile_union = t->tile_union;
   ctx->tuning.host_chunk = t->host_chunk;
   ctx->tuning.tile_tensor = t->tile_tensor;
+  ctx->tuning.mixed_large = t->mixed_large;
   if (t->samples_per_cell != ctx->ppc) {
     ctx->ppc = t->samples_per_cell;
     if (ctx->fitted) {

@@ -181,6 +181,7 @@ struct Tuning {
                                  // (64 lets four mixed-form CTAs share an SM; a tile above it is split)
   int host_chunk = 0;            // host-buffer calls: targets per pipelined chunk; 0: one chunk
   int tile_tensor = 0;           // mixed tile solve: 1 = trailing updates on the tensor pipe (split TF32)
+  int mixed_large = 0;           // mixed form: 1 = systems above 32 samples by the FP64 per-system kernel
 };
 
 struct Launch {

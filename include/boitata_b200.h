@@ -140,7 +140,9 @@ typedef struct {
  * pipeline (0: the whole call at once; at most 8 chunks), and for the mixed
  * form's tile-shared solve whether the factorisation's trailing updates run
  * on the tensor pipe (1: 8-column panels on the CUDA cores, the updates as
- * split-TF32 mma; 0: the unblocked FP32 elimination). */
+ * split-TF32 mma; 0: the unblocked FP32 elimination), and for the mixed
+ * form's systems of more than 32 samples which per-system kernel solves them
+ * (0: FP32 factorisation with FP64 refinement; 1: the FP64 kernel). */
 typedef struct {
   double samples_per_cell;
   int32_t tile[3];
@@ -149,6 +151,7 @@ typedef struct {
   int32_t tile_union;
   int32_t host_chunk;
   int32_t tile_tensor;
+  int32_t mixed_large;
 } btk_tuning;
 
 typedef struct btk_ctx btk_ctx;

@@ -94,3 +94,25 @@ def test_tensor_switch_is_checked():
     with pytest.raises(InvalidInput, match="tile_tensor"):
         tensor(est, 2)
     assert get_tuning(est._ctx)["tile_tensor"] == 0
+
+
+def test_mixed_large_systems_by_the_fp64_kernel(oracle):
+    """tuning.mixed_large = 1: the mixed form's systems above 32 samples are the FP64 form's, bit for bit;
+    the rest keep the mixed tile solve; everything at 1e-6 against the oracle (c3: 4-64 samples)."""
+    w = W.c3()
+    targets = centroids(oracle, w, 3)
+    est = OrdinaryKriging(w.variogram, w.search, precision="mixed").fit(w.coords, w.values)
+    set_tuning(est._ctx, dict(get_tuning(est._ctx), mixed_large=1))
+    got = est.predict_full(targets)
+    fp64 = est.predict_full(targets, precision="fp64")
+    ref = oracle.estimate_many(targets, w.coords, w.values, w.search, w.variogram, neighbors=False)
+    assert_same_estimates(got, ref, 1e-6)
+    large = (got["n_used"] > 32) & np.isfinite(got["value"])
+    assert large.sum() > 1000
+    for k in ("value", "variance", "lagrange"):
+        np.testing.assert_array_equal(got[k][large], fp64[k][large])
+    assert not np.any(got["status"][large] & 0x10)
+    small = (got["n_used"] <= 32) & np.isfinite(got["value"])
+    assert not np.array_equal(got["value"][small], fp64["value"][small])
+    with pytest.raises(InvalidInput, match="mixed_large"):
+        set_tuning(est._ctx, dict(get_tuning(est._ctx), mixed_large=3))
