@@ -320,3 +320,32 @@ def test_ill_conditioned_systems(oracle):
         assert np.all(close(mixed[k][fin], ref[k][fin], 1e-6)), k
     np.testing.assert_array_equal(mixed["n_used"][fin], ref["n_used"][fin])
 
+
+
+def test_octants_of_samples_on_the_sector_planes(oracle):
+    """Samples within a few ulps of the three octant planes through each target, under rotated searches at
+    UTM-sized coordinates: the kernel's fast sector test (axes w - axes t against a rounding bound) must
+    hand every such sample to the reference-order evaluation, so the lists equal the oracle's."""
+    rng = np.random.default_rng(21)
+    x0, y0, z0 = 512_345.25, 6_954_321.5, 1_150.0
+    targets = np.column_stack([x0 + rng.uniform(0, 200, 40), y0 + rng.uniform(0, 200, 40),
+                               z0 + rng.uniform(-50, 50, 40)])
+    vg = Variogram([Structure("spherical", 1.0, 100.0)])
+    for rot in [(30.0, 10.0, 0.0), (0.0, 0.0, 0.0), (-65.0, 45.0, 20.0)]:
+        axes = oracle.block_frame(*rot)  # rows: the octant frame
+        pts = []
+        for t in targets:
+            for r in range(3):
+                u, v = axes[(r + 1) % 3], axes[(r + 2) % 3]
+                for _ in range(12):
+                    w = t + rng.uniform(-40, 40) * u + rng.uniform(-40, 40) * v
+                    w = w + axes[r] * rng.choice([0.0, 1e-13, -1e-13, 1e-11, -1e-11, 1e-9])
+                    for _ in range(int(rng.integers(0, 3))):
+                        a = int(rng.integers(0, 3))
+                        w[a] = np.nextafter(w[a], np.inf if rng.random() < 0.5 else -np.inf)
+                    pts.append(w)
+        coords = np.array(pts)
+        s = Search(radius=60.0, max_samples=24, min_samples=1, octant=True, max_per_sector=3, rotation=rot,
+                   ratios=(0.8, 0.5))
+        ok = OrdinaryKriging(vg, s).fit(coords, np.zeros(len(coords)))
+        assert_same_neighbors(ok, oracle, coords, s, vg, targets)
