@@ -139,8 +139,12 @@ __device__ __forceinline__ void sweep_back64(GradSmem<NW>& S, int gid, int row, 
   }
 }
 
+// Resident CTAs an SM: the FP64 form with two-warp groups held to 168
+// registers, three CTAs instead of two at 244 (the c5 mean gradient went from
+// 1.32 to 1.13 s, results bit-identical); the mixed one-warp form five (the
+// c4 mixed gradient), the others four.
 template <int NW, bool MIXED>
-__global__ void __launch_bounds__(128) k_grad(GradDev a) {
+__global__ void __launch_bounds__(128, MIXED ? (NW == 1 ? 5 : 4) : (NW == 1 ? 4 : 3)) k_grad(GradDev a) {
   constexpr int R = 32 * NW;
   constexpr int GROUPS = 128 / R;
   constexpr int Q = R / 4;
