@@ -497,7 +497,6 @@ def config_c5(args, dev, stream, flush, sample=20_000):
         if prec == N.MIXED:
             fin = (st & 0x0F) == 0
             out[name]["fp64_fallback_fraction"] = float(np.mean((st[fin] & 0x10) != 0))
-    set_tuning(ctx, base)
     pick = min(("mixed_fp32_large", "mixed_fp64_large"), key=lambda k: out[k]["ms_per_step"])
     out["mixed"] = dict(out[pick], large_systems="fp64 kernel" if pick == "mixed_fp64_large" else
                         "fp32 factorisation, fp64 refinement")
@@ -511,13 +510,19 @@ def config_c5(args, dev, stream, flush, sample=20_000):
     del outs, oc
     theta = theta_of(w.variogram)
     grad = {}
-    for precision in ("fp64", "mixed"):
-        bm = BlockMean(est, w.geometry, precision=precision)
+    # The mixed form's gradient with either kernel for systems above 32 samples; "mixed" is the one the
+    # forward picked.
+    for name, large in (("fp64", 0), ("mixed_fp32_large", 0), ("mixed_fp64_large", 1)):
+        set_tuning(ctx, dict(base, mixed_large=large))
+        bm = BlockMean(est, w.geometry, precision="fp64" if name == "fp64" else "mixed")
         times, sums = objective_times(bm, theta, 0, bm.n, 1, 3, dev)
-        grad[precision] = {"objective_ms": times[False], "objective_and_gradient_ms": times[True],
-                           "over_forward_step": times[True] / out[precision]["ms_per_step"],
-                           "mean": float(sums[0] / sums[1]), "systems": int(sums[1]),
-                           "grad": [float(x) for x in sums[2:] / sums[1]]}
+        grad[name] = {"objective_ms": times[False], "objective_and_gradient_ms": times[True],
+                      "over_forward_step": times[True] / out[name]["ms_per_step"],
+                      "mean": float(sums[0] / sums[1]), "systems": int(sums[1]),
+                      "grad": [float(x) for x in sums[2:] / sums[1]]}
+    set_tuning(ctx, base)
+    grad["mixed"] = dict(grad[pick], over_forward_step=grad[pick]["objective_and_gradient_ms"] /
+                         out["mixed"]["ms_per_step"])
     out["mean_gradient"] = grad
     out["c5_grad_ms"] = min(v["objective_and_gradient_ms"] for v in grad.values())
     out["c5_forward_ms"] = min(out["fp64"]["ms_per_step"], out["mixed"]["ms_per_step"])
@@ -827,7 +832,7 @@ def main():
 
         # The host call's copy/compute pipeline (btk_tuning.host_chunk): the chunk is picked by timing, as the
         # autotuner picks the kernels' launch shapes, then timed over the full step count.
-        trial = {hc: e2e_time(hc, 2) for hc in (0, -(-m // 4), -(-m // 8))}
+        trial = {hc: e2e_time(hc, 2) for hc in (0, -(-m // 2), -(-m // 4), -(-m // 8))}
         best_chunk = min(trial, key=trial.get)
         t_best = e2e_time(best_chunk, args.steps)
         line["e2e"] = {"value": ws * m / t_best, "unit": UNIT, "h2d_bytes_per_step": m * 24,

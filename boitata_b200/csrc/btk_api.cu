@@ -1488,7 +1488,10 @@ int objective_sums(btk_ctx* ctx, Objective which, const btk_variogram* vg, int64
   }
   Launch L = ctx->launch(nullptr);
   ctx->mark(0, L.stream);
-  CK(launch_grad(L, a, ctx->g_sums.p, ctx->search.max_samples > 32 ? 64 : 32, precision == BTK_MIXED));
+  // The mixed form's systems above 32 samples take the FP64 kernel when the
+  // tuning says so, as in the prediction path (tuning.mixed_large).
+  const int rows = ctx->search.max_samples > 32 ? 64 : 32;
+  CK(launch_grad(L, a, ctx->g_sums.p, rows, precision == BTK_MIXED && !(rows > 32 && ctx->tuning.mixed_large)));
   ctx->mark(1, L.stream);
   ctx->mark(2, L.stream);
   ctx->mark(3, L.stream);

@@ -165,6 +165,15 @@ def test_block_mean_matches_predict_and_the_references(oracle):
     m2, g2, nv2, v2 = mixed.evaluate(th, values=True)
     assert nv2 == nv and np.all(close(v2[fin], values[fin], 1e-8)) and close(m2, mean, 1e-8)
     np.testing.assert_allclose(g2, g, rtol=1e-5, atol=1e-9)
+    # tuning.mixed_large: the mixed form's systems above 32 samples by the FP64 kernel, as in prediction.
+    from boitata_b200.autotune import get_tuning, set_tuning
+
+    set_tuning(est._ctx, dict(get_tuning(est._ctx), mixed_large=1))
+    m3, g3, nv3, v3 = mixed.evaluate(th, values=True)
+    assert m3 == mean and nv3 == nv
+    np.testing.assert_array_equal(g3, g)
+    np.testing.assert_array_equal(v3, values)
+    set_tuning(est._ctx, dict(get_tuning(est._ctx), mixed_large=0))
 
 
 @pytest.mark.gpu
