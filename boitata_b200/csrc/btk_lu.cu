@@ -32,6 +32,10 @@ struct LuHead {
   int n, nn, dim, kind, twin, sing, nperm;
   int piv[2];        // pivot row of the column, double-buffered by column parity
   double pv[2];      // and its value
+  // Look-ahead: each warp's first largest |a_r,k+1| over its rows after column
+  // k's update (value, signed value, row), double-buffered by column parity.
+  double wabs[2][16], wval[2][16];
+  int wrow[2][16];
 };
 
 struct LuLayout {
@@ -70,8 +74,13 @@ __host__ __device__ inline size_t lu_matrix_doubles(int kmax) {
 // NT threads per system: 128 up to 64 samples, 512 beyond (one system per SM
 // then, its matrix filling most of the shared memory). GA: the matrix in the
 // CTA's slice of a.lu_scratch (beyond kMaxLU samples).
+// Launch bounds: given only the block size, the compiler held the 512-thread
+// form to 64 registers and spilled; a minimum of one CTA an SM (its matrix
+// fills the shared memory) leaves it about 100, without spills. The
+// 128-thread form (at most 65 columns) keeps the compiler's own choice (no
+// minimum): 64 registers, no spills.
 template <bool DIAG, int NT, bool GA = false>
-__global__ void __launch_bounds__(NT) k_solve_lu(SolveDev a, int kmax) {
+__global__ void __launch_bounds__(NT, NT > 128 ? 1 : 0) k_solve_lu(SolveDev a, int kmax) {
   constexpr int kThreads = NT, kWarps = NT / 32;
   extern __shared__ __align__(16) unsigned char smem[];
   const LuLayout lay = lu_layout(kmax, GA);
@@ -219,9 +228,101 @@ __global__ void __launch_bounds__(NT) k_solve_lu(SolveDev a, int kmax) {
       B[i] = v, X[i] = v;
     }
     __syncthreads();
-    // LU with partial pivoting (nalgebra lu.rs). Per column: warp 0 finds the
-    // first largest |a_rk| (r >= k); rows k and the pivot swap; each warp
-    // scales and updates its rows below k (row k is only read meanwhile).
+    if constexpr (NT > 128) {
+    // LU with partial pivoting (nalgebra lu.rs), the 512-thread form: per column k the first largest
+    // |a_rk| (r >= k) is the pivot; rows k and the pivot swap; each warp scales
+    // and updates its rows below k (row k is only read meanwhile). Column k's
+    // pivot comes from column k - 1's update (look-ahead): lane 0 of each warp
+    // keeps the first largest |a_r,k| over the warp's rows (ascending) as it
+    // writes them, and after the column's barrier every thread reduces the
+    // warps' candidates, larger value first and the lower row on a tie, which
+    // is the first largest over all rows. Column 0, and a column after a
+    // skipped one, take warp 0's search instead. Each lane keeps the pivot
+    // row's entries of its columns in registers for all of its warp's rows.
+    // Columns a lane caches: all of them while dim - k - 1 <= 32 kCache (dim up to 161).
+    constexpr int kCache = 5;
+    bool ahead = false;        // uniform: piv and diag hold column k's pivot
+    int piv = 0;
+    double diag = 0.0;
+    for (int k = 0; k < dim; ++k) {
+      const int b = k & 1;
+      if (!ahead) {
+        if (warp == 0) {
+          double bv = -1.0;
+          int bi = k;
+          for (int r = k + lane; r < dim; r += 32) {
+            const double v = fabs(A[r * S + k]);
+            if (v > bv) bv = v, bi = r;
+          }
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            const double v2 = __shfl_xor_sync(kFull, bv, o);
+            const int i2 = __shfl_xor_sync(kFull, bi, o);
+            if (v2 > bv || (v2 == bv && i2 < bi)) bv = v2, bi = i2;
+          }
+          if (lane == 0) H.piv[b] = bi, H.pv[b] = A[bi * S + k];
+        }
+        __syncthreads();
+        piv = H.piv[b], diag = H.pv[b];
+      }
+      ahead = false;
+      if (diag == 0.0) continue;  // uniform: a zero column is skipped
+      if (piv != k) {
+        for (int j = tid; j < dim; j += kThreads) {
+          const double tmp = A[k * S + j];
+          A[k * S + j] = A[piv * S + j];
+          A[piv * S + j] = tmp;
+        }
+        if (tid == 0) pa[H.nperm] = k, pb[H.nperm] = piv, ++H.nperm;
+        __syncthreads();
+      }
+      const double inv = 1.0 / diag;
+      double prow[kCache];
+#pragma unroll
+      for (int q = 0; q < kCache; ++q) {
+        const int c = k + 1 + lane + 32 * q;
+        prow[q] = c < dim ? A[k * S + c] : 0.0;
+      }
+      double bv = -1.0, sv = 0.0;
+      int bi = k + 1;
+      for (int r = k + 1 + warp; r < dim; r += kWarps) {
+        const double l = A[r * S + k] * inv;
+        __syncwarp();
+        if (lane == 0) A[r * S + k] = l;
+#pragma unroll
+        for (int q = 0; q < kCache; ++q) {
+          const int c = k + 1 + lane + 32 * q;
+          if (c < dim) {
+            const double v = fma(-prow[q], l, A[r * S + c]);
+            A[r * S + c] = v;
+            if (q == 0 && lane == 0 && fabs(v) > bv) bv = fabs(v), sv = v, bi = r;
+          }
+        }
+        for (int c = k + 1 + lane + 32 * kCache; c < dim; c += 32) A[r * S + c] = fma(-A[k * S + c], l, A[r * S + c]);
+      }
+      if (lane == 0) H.wabs[b][warp] = bv, H.wval[b][warp] = sv, H.wrow[b][warp] = bi;
+      __syncthreads();
+      if (k + 1 < dim) {
+        double best = -1.0, val = 0.0;
+        int row = k + 1;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+          const double v = H.wabs[b][w];
+          const int i = H.wrow[b][w];
+          if (v > best || (v == best && i < row)) best = v, val = H.wval[b][w], row = i;
+        }
+        // No row's |a| exceeded -1 (all NaN): row k + 1 with its own value, as the search gives.
+        piv = row, diag = best < 0.0 ? A[(k + 1) * S + k + 1] : val;
+        ahead = true;
+      }
+    }
+    } else {
+    // LU with partial pivoting (nalgebra lu.rs), the 128-thread form (at most
+    // 65 columns): per column, warp 0 finds the first largest |a_rk| (r >= k);
+    // rows k and the pivot swap; each warp scales and updates its rows below k
+    // (row k is only read meanwhile). The look-ahead of the 512-thread form
+    // costs more than it saves at this size (32-sample power models: 9.3
+    // against 10.6 M systems/s).
     for (int k = 0; k < dim; ++k) {
       const int b = k & 1;
       if (warp == 0) {
@@ -260,6 +361,7 @@ __global__ void __launch_bounds__(NT) k_solve_lu(SolveDev a, int kmax) {
         for (int c = k + 1 + lane; c < dim; c += 32) A[r * S + c] = fma(-A[k * S + c], l, A[r * S + c]);
       }
       __syncthreads();
+    }
     }
     // LU::solve by warp 0: row swaps, then L (unit lower) and U substitutions.
     if (warp == 0) {

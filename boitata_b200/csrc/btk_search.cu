@@ -666,8 +666,12 @@ __device__ int rules_scan(const SearchDev& sp, const GridDev& g, RulesSmem<K, HH
   return n;
 }
 
+// With the 512-candidate buffers (16.5 KB a warp) shared memory holds an SM to
+// three CTAs, so up to 170 registers cost no occupancy; given only the block
+// size the compiler kept 128 and spilled about 210 bytes a thread. The SGS
+// forms (small buffers, four CTAs by registers) keep 128.
 template <int K, int HH = kHoleHash>
-__global__ void __launch_bounds__(128) k_search_rules(SearchDev sp, GridDev g, const double* __restrict__ tx,
+__global__ void __launch_bounds__(128, K >= 512 ? 3 : 4) k_search_rules(SearchDev sp, GridDev g, const double* __restrict__ tx,
                                                       const double* __restrict__ ty, const double* __restrict__ tz,
                                                       const int64_t* __restrict__ perm, int64_t m, int loo,
                                                       uint32_t* __restrict__ nbr, int32_t* __restrict__ count,

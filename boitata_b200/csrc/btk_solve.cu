@@ -253,8 +253,11 @@ __global__ void __launch_bounds__(128) k_solve64(SolveDev a, int8_t flag) {
 // solve; each takes its residual in FP64 from the FP64 triangle.
 constexpr int kRefineSteps = 3;
 
+// Four CTAs an SM: shared memory allows no more for either group size, and
+// given only the block size the compiler held the one-warp form to 96
+// registers and spilled about 100 bytes a thread.
 template <int NW, bool kPairs = false>
-__global__ void __launch_bounds__(128) k_solve_mixed(SolveDev a, int64_t* redo, int64_t* redo_len) {
+__global__ void __launch_bounds__(128, 4) k_solve_mixed(SolveDev a, int64_t* redo, int64_t* redo_len) {
   constexpr int R = 32 * NW;
   constexpr int GROUPS = 128 / R;
   extern __shared__ __align__(16) unsigned char smem_raw[];
