@@ -212,9 +212,13 @@ __global__ void __launch_bounds__(NT, NT > 128 ? 1 : 0) k_solve_lu(SolveDev a, i
     __syncthreads();
     const int nn = H.nn, dim = H.dim;
     const double t0 = H.t[0], t1 = H.t[1], t2 = H.t[2];
-    // The bordered system (krige.rs:150-166) and its right-hand side.
-    for (int e = tid; e < dim * dim; e += kThreads) {
-      const int i = e / dim, j = e % dim;
+    // The bordered system (krige.rs:150-166) and its right-hand side: the
+    // lower triangle and the diagonal, each entry written to both halves
+    // (lag_world is symmetric to the bit).
+    for (int e = tid; e < dim * (dim + 1) / 2; e += kThreads) {
+      int i, j;
+      tri_index(e, i, j);  // (i + 1, j): the strict lower triangle of dim + 1 rows
+      i -= 1;
       double v;
       if (i < nn && j < nn)
         v = i == j ? vg.c0 + E[i]
@@ -222,6 +226,7 @@ __global__ void __launch_bounds__(NT, NT > 128 ? 1 : 0) k_solve_lu(SolveDev a, i
       else
         v = (i == nn && j == nn) ? 0.0 : 1.0;
       A[i * S + j] = v;
+      A[j * S + i] = v;
     }
     for (int i = tid; i < dim; i += kThreads) {
       const double v = i < nn ? support_cov(a, t0, t1, t2, P[i], P[kmax + i], P[2 * kmax + i]) : 1.0;
@@ -363,8 +368,70 @@ __global__ void __launch_bounds__(NT, NT > 128 ? 1 : 0) k_solve_lu(SolveDev a, i
       __syncthreads();
     }
     }
-    // LU::solve by warp 0: row swaps, then L (unit lower) and U substitutions.
-    if (warp == 0) {
+    // LU::solve: row swaps, then L (unit lower) and U substitutions.
+    if constexpr (NT > 128) {
+      // Blocked by 32 rows: warp 0 solves the diagonal block with the block's
+      // unknowns in registers (lane = row), then every thread applies the
+      // block's solved entries to one row beyond it. Each row still takes its
+      // updates one column at a time in the serial order (ascending for L,
+      // descending for U) with the same FMAs, so X is the serial solve's to
+      // the bit; the block's other warps no longer wait on warp 0.
+      if (tid == 0)
+        for (int q = 0; q < H.nperm; ++q) {
+          const double tmp = X[pa[q]];
+          X[pa[q]] = X[pb[q]];
+          X[pb[q]] = tmp;
+        }
+      __syncthreads();
+      const int nblk = (dim + 31) / 32;
+      for (int j = 0; j < nblk; ++j) {
+        const int j0 = 32 * j, j1 = min(dim, j0 + 32);
+        if (warp == 0) {
+          const int r = j0 + lane;
+          double x = r < j1 ? X[r] : 0.0;
+          for (int i = j0; i < j1; ++i) {
+            const double coeff = __shfl_sync(kFull, x, i - j0);
+            if (r > i && r < j1) x = fma(-coeff, A[r * S + i], x);
+          }
+          if (r < j1) X[r] = x;
+        }
+        __syncthreads();
+        for (int r = j1 + tid; r < dim; r += kThreads) {
+          double x = X[r];
+          for (int i = j0; i < j1; ++i) x = fma(-X[i], A[r * S + i], x);
+          X[r] = x;
+        }
+        __syncthreads();
+      }
+      for (int j = nblk - 1; j >= 0; --j) {
+        const int j0 = 32 * j, j1 = min(dim, j0 + 32);
+        if (warp == 0) {
+          const int r = j0 + lane;
+          double x = r < j1 ? X[r] : 0.0;
+          bool sing = false;
+          for (int i = j1 - 1; i >= j0; --i) {
+            const double d = A[i * S + i];
+            if (d == 0.0) {  // uniform over the warp
+              sing = true;
+              break;
+            }
+            const double coeff = __shfl_sync(kFull, x / d, i - j0);
+            if (r == i) x = coeff;
+            else if (r < i && r >= j0) x = fma(-coeff, A[r * S + i], x);
+          }
+          if (r < j1) X[r] = x;
+          if (lane == 0 && sing) H.sing = 1;
+        }
+        __syncthreads();
+        if (H.sing) break;  // uniform: every thread read it after the barrier
+        for (int r = tid; r < j0; r += kThreads) {
+          double x = X[r];
+          for (int i = j1 - 1; i >= j0; --i) x = fma(-X[i], A[r * S + i], x);
+          X[r] = x;
+        }
+        __syncthreads();
+      }
+    } else if (warp == 0) {
       if (lane == 0)
         for (int q = 0; q < H.nperm; ++q) {
           const double tmp = X[pa[q]];
