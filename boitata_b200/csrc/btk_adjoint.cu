@@ -270,6 +270,9 @@ __global__ void __launch_bounds__(128, MIXED ? (NW == 1 ? 5 : 4) : (NW == 1 ? 4 
       const double thr = kPivot * c0;
       gsync<NW>(gid);  // every row has its covariances: the triangle now takes the multipliers
       double* Lrow = S.T + tri;
+      // Uniform windows for both warps: warp 0's own (eliminate_staged) made the
+      // objective faster but the objective with its gradient slower (c5: 1.155
+      // against 1.129 s), the kernel's code being larger.
       eliminate_rows<NW, R, true>(A, 0, n1, row, S, gid, y0, y1, y2, dme, sing, thr, Lrow);
       if (!sing) eliminate_rows<NW, 3 * Q, true>(A, n1, n2, row, S, gid, y0, y1, y2, dme, sing, thr, Lrow);
       if (!sing) eliminate_rows<NW, 2 * Q, true>(A, n2, n3, row, S, gid, y0, y1, y2, dme, sing, thr, Lrow);

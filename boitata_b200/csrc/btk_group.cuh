@@ -111,6 +111,31 @@ __device__ __forceinline__ void eliminate_rows(double (&A)[32 * NW], int k0, int
   }
 }
 
+// The pivots 0 .. nn-1 in four stages of R/4 with windows of R, 3R/4, R/2 and
+// R/4 slots (the columns a step can still change in row R - 1). In a group of
+// two warps, warp 0's rows (0 .. 31) hold at most 31 - k live slots at pivot
+// k: it takes windows of 32 and 16 slots in the first two stages and none
+// after (it still meets every barrier), so it skips the updates of columns its
+// rows do not have. The live slots take the same operations either way.
+template <int NW, bool kStoreL = false, class Sm>
+__device__ __forceinline__ void eliminate_staged(double (&A)[32 * NW], int nn, int row, int wig, Sm& S, int gid,
+                                                 double& y0, double& y1, double& y2, double& dme, bool& sing,
+                                                 double thr, double* Lrow = nullptr) {
+  constexpr int R = 32 * NW, Q = R / 4;
+  const int n1 = min(nn, Q), n2 = min(nn, 2 * Q), n3 = min(nn, 3 * Q);
+  if (NW == 2 && wig == 0) {
+    eliminate_rows<NW, 32, kStoreL>(A, 0, n1, row, S, gid, y0, y1, y2, dme, sing, thr, Lrow);
+    if (!sing) eliminate_rows<NW, 16, kStoreL>(A, n1, n2, row, S, gid, y0, y1, y2, dme, sing, thr, Lrow);
+    if (!sing) eliminate_rows<NW, 0, kStoreL>(A, n2, n3, row, S, gid, y0, y1, y2, dme, sing, thr, Lrow);
+    if (!sing) eliminate_rows<NW, 0, kStoreL>(A, n3, nn, row, S, gid, y0, y1, y2, dme, sing, thr, Lrow);
+  } else {
+    eliminate_rows<NW, R, kStoreL>(A, 0, n1, row, S, gid, y0, y1, y2, dme, sing, thr, Lrow);
+    if (!sing) eliminate_rows<NW, 3 * Q, kStoreL>(A, n1, n2, row, S, gid, y0, y1, y2, dme, sing, thr, Lrow);
+    if (!sing) eliminate_rows<NW, 2 * Q, kStoreL>(A, n2, n3, row, S, gid, y0, y1, y2, dme, sing, thr, Lrow);
+    if (!sing) eliminate_rows<NW, Q, kStoreL>(A, n3, nn, row, S, gid, y0, y1, y2, dme, sing, thr, Lrow);
+  }
+}
+
 // The FP32 form of eliminate_rows: the multiplier of row i at step k goes to
 // L[i][k] for the substitutions, and a pivot at most thr or NaN leaves the
 // system to the FP64 form.

@@ -229,13 +229,7 @@ __global__ void __launch_bounds__(128) k_solve64(SolveDev a, int8_t flag) {
     double dme = 1.0;
     bool sing = false;
     const double thr = kPivot * c0;
-    // Four stages of R/4 pivots over windows of R, 3R/4, R/2 and R/4 slots.
-    constexpr int Q = R / 4;
-    const int n1 = min(nn, Q), n2 = min(nn, 2 * Q), n3 = min(nn, 3 * Q);
-    eliminate_rows<NW, R>(A, 0, n1, row, S, gid, y0, y1, y2, dme, sing, thr);
-    if (!sing) eliminate_rows<NW, 3 * Q>(A, n1, n2, row, S, gid, y0, y1, y2, dme, sing, thr);
-    if (!sing) eliminate_rows<NW, 2 * Q>(A, n2, n3, row, S, gid, y0, y1, y2, dme, sing, thr);
-    if (!sing) eliminate_rows<NW, Q>(A, n3, nn, row, S, gid, y0, y1, y2, dme, sing, thr);
+    eliminate_staged<NW>(A, nn, row, wig, S, gid, y0, y1, y2, dme, sing, thr);
     if (sing) {
       if (row == 0) write_fail(a, ti, BTK_ST_SINGULAR, 0);
       continue;
