@@ -609,8 +609,10 @@ __device__ void solve_mixed(const TileDev& a, const TileHead& H, const double* P
   __syncwarp();
   // Backward sweep L^T x = D^-1 y, column-oriented: once x_k is known every
   // row i < k takes D_i L[k][i] x_k (column i of the triangle) into acc_i,
-  // and x_i = (y_i - acc_i) / D_i.
-  const float2 rdme = rcp2(dme);
+  // and x_i = y_i / D_i - acc_i / D_i: y / D is taken once, so a step costs
+  // one packed FMA per right-hand side.
+  const float2 rdme = rcp2(dme), nrd = make_float2(-rdme.x, -rdme.y);
+  const float2 yd[3] = {__fmul2_rn(y[0], rdme), __fmul2_rn(y[1], rdme), __fmul2_rn(y[2], rdme)};
   float2 acc[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
   float2 x[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
   const float2* my_col = W.lt + kLtPad + col_off(lane) - lane - 1;  // + k: D_i L[k][i]
@@ -618,7 +620,7 @@ __device__ void solve_mixed(const TileDev& a, const TileHead& H, const double* P
     float2 z[3];
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
-      const float2 w = make_float2((y[v].x - acc[v].x) * rdme.x, (y[v].y - acc[v].y) * rdme.y);
+      const float2 w = __ffma2_rn(acc[v], nrd, yd[v]);
       z[v].x = __shfl_sync(kFull, w.x, k);
       z[v].y = __shfl_sync(kFull, w.y, k);
     }
