@@ -416,7 +416,7 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
 // holds what the unblocked form writes, so the backward sweep is shared.
 __device__ __forceinline__ void factor_tc(const TileHead& H, const double* Ua, const double* Ub, WarpMixed& Ws,
                                           int ta, int tb, int na, int nb, int nmax, int lane, float2 (&y)[3],
-                                          float2& dme, float2& pmin) {
+                                          float2& dme) {
   float2* lt = Ws.lt;
   // The columns that take pivots, every row below the diagonal; columns
   // past nmax are never read for a system's results.
@@ -452,7 +452,6 @@ __device__ __forceinline__ void factor_tc(const TileHead& H, const double* Ua, c
       __syncwarp();
       const float4 p0 = reinterpret_cast<const float4*>(Ws.prhs[b])[0];
       const float4 p1 = reinterpret_cast<const float4*>(Ws.prhs[b])[1];
-      pmin.x = fminf(pmin.x, p0.x), pmin.y = fminf(pmin.y, p0.y);
       if (lane == k) dme = make_float2(p0.x, p0.y);
       const float2 nrd = make_float2(rcp_approx(-p0.x), rcp_approx(-p0.y));
       const float2 nf = lane > k ? __fmul2_rn(pa[j], nrd) : make_float2(0.f, 0.f);  // -L[lane][k]
@@ -525,7 +524,7 @@ __device__ __forceinline__ void factor_tc(const TileHead& H, const double* Ua, c
 // slots that can still hold live columns, as in the FP64 eliminate().
 template <int W>
 __device__ __forceinline__ void eliminate2(float2 (&A)[32], int k0, int k1, int lane, WarpMixed& Ws,
-                                           float2 (&y)[3], float2& dme, float2& dmin) {
+                                           float2 (&y)[3], float2& dme) {
   float2* col = Ws.lt + kLtPad + col_off(k0);
   for (int k = k0; k < k1; ++k) {
     const int b = k & 1;
@@ -537,7 +536,6 @@ __device__ __forceinline__ void eliminate2(float2 (&A)[32], int k0, int k1, int 
     __syncwarp();
     const float4 p0 = reinterpret_cast<const float4*>(Ws.prhs[b])[0];
     const float4 p1 = reinterpret_cast<const float4*>(Ws.prhs[b])[1];
-    dmin.x = fminf(dmin.x, p0.x), dmin.y = fminf(dmin.y, p0.y);
     if (lane == k) dme = make_float2(p0.x, p0.y);
     const float2 nrd = make_float2(rcp_approx(-p0.x), rcp_approx(-p0.y));
     const float2 nf = lane > k ? __fmul2_rn(A[0], nrd) : make_float2(0.f, 0.f);  // -L[lane][k]
@@ -585,9 +583,9 @@ __device__ void solve_mixed(const TileDev& a, const TileHead& H, const double* P
   const double* Ub = UU + mb * S;
   float2 y[3] = {make_float2(float(ca), float(cb)), make_float2(ha ? 1.f : 0.f, hb ? 1.f : 0.f),
                  make_float2(float(za), float(zb))};
-  float2 dme = make_float2(1.f, 1.f), pmin = make_float2(3.0e38f, 3.0e38f);
+  float2 dme = make_float2(1.f, 1.f);
   if constexpr (TC) {
-    factor_tc(H, Ua, Ub, W, ta, tb, na, nb, nmax, lane, y, dme, pmin);
+    factor_tc(H, Ua, Ub, W, ta, tb, na, nb, nmax, lane, y, dme);
   } else {
     float2 A[32];
 #pragma unroll
@@ -596,16 +594,17 @@ __device__ void solve_mixed(const TileDev& a, const TileHead& H, const double* P
       A[q].y = (hb && q < nb) ? float(Ub[H.map[tb][q]]) : (q == lane ? 1.f : 0.f);
     }
     const int n1 = min(nmax, 8), n2 = min(nmax, 16), n3 = min(nmax, 24);
-    eliminate2<32>(A, 0, n1, lane, W, y, dme, pmin);
-    eliminate2<24>(A, n1, n2, lane, W, y, dme, pmin);
-    eliminate2<16>(A, n2, n3, lane, W, y, dme, pmin);
-    eliminate2<8>(A, n3, nmax, lane, W, y, dme, pmin);
+    eliminate2<32>(A, 0, n1, lane, W, y, dme);
+    eliminate2<24>(A, n1, n2, lane, W, y, dme);
+    eliminate2<16>(A, n2, n3, lane, W, y, dme);
+    eliminate2<8>(A, n3, nmax, lane, W, y, dme);
   }
   // An FP32 pivot that is NaN or at most n ulp(C0) is not resolved from the
   // rounding of its row: the FP64 form takes the system (and with it the
-  // singular decision, kernel.rs:61).
-  const bool weak_a = !(pmin.x > float(na) * 1.1920929e-7f * float(c0));
-  const bool weak_b = !(pmin.y > float(nb) * 1.1920929e-7f * float(c0));
+  // singular decision, kernel.rs:61). Lane k holds pivot k; the padded rows'
+  // unit pivots of the smaller system take no part.
+  const bool weak_a = __any_sync(kFull, ha && !(dme.x > float(na) * 1.1920929e-7f * float(c0)));
+  const bool weak_b = __any_sync(kFull, hb && !(dme.y > float(nb) * 1.1920929e-7f * float(c0)));
   __syncwarp();
   // Backward sweep L^T x = D^-1 y, column-oriented: once x_k is known every
   // row i < k takes D_i L[k][i] x_k (column i of the triangle) into acc_i,

@@ -116,3 +116,26 @@ def test_mixed_large_systems_by_the_fp64_kernel(oracle):
     assert not np.array_equal(got["value"][small], fp64["value"][small])
     with pytest.raises(InvalidInput, match="mixed_large"):
         set_tuning(est._ctx, dict(get_tuning(est._ctx), mixed_large=3))
+
+
+def test_mixed_tile_solve_with_a_large_sill(oracle):
+    """Grades in units whose variance is about 1e6 (c2's samples, values x 1e3, sills and nugget x 1e6):
+    the mixed tile solve tests its FP32 pivots against n ulp of C0 over each system's own pivots (not the
+    padded rows' unit pivots), so its systems are not sent to the FP64 re-solve wholesale, and every result
+    is held to 1e-6 against the oracle."""
+    from boitata_b200 import Structure, Variogram
+
+    w = W.c2()
+    vg = w.variogram
+    big = Variogram([Structure(s.model, s.sill * 1e6, s.range) for s in vg.structures], nugget=vg.nugget * 1e6,
+                    rotation=vg.rotation, ratios=vg.ratios)
+    values = w.values * 1e3
+    rng = np.random.default_rng(9)
+    targets = centroids(oracle, w)[rng.choice(w.geometry.cells(), 20000, replace=False)]
+    ref = oracle.estimate_many(targets, w.coords, values, w.search, big, neighbors=False)
+    for tensor_form in (0, 1):
+        est = tensor(OrdinaryKriging(big, w.search, precision="mixed").fit(w.coords, values), tensor_form)
+        got = est.predict_full(targets)
+        assert_same_estimates(got, ref, 1e-6)
+        fin = np.isfinite(got["value"])
+        assert np.mean((got["status"][fin] & 0x10) != 0) < 0.01, tensor_form
