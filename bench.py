@@ -42,8 +42,8 @@ sys.path.insert(0, ROOT)
 # DRAM bytes per system of k_tile<mixed> from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum over
 # the systems of the launch), valid for the tile kernel's sources whose hash is TILE_TRAFFIC_SOURCE: when they
 # change, the line reports no traffic until a new capture is made.
-TILE_DRAM_BYTES_PER_SYSTEM = (132861440 + 12633088) / 800000
-TILE_TRAFFIC_SOURCE = "f7a327c561d0ced8"
+TILE_DRAM_BYTES_PER_SYSTEM = (132830720 + 12697344) / 800000
+TILE_TRAFFIC_SOURCE = "8249380f74c2b07c"
 TILE_SOURCES = ("boitata_b200/csrc/btk_tile.cu", "boitata_b200/csrc/btk_device.cuh", "boitata_b200/csrc/btk_internal.h")
 
 
