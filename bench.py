@@ -43,6 +43,7 @@ sys.path.insert(0, ROOT)
 # the systems of the launch), valid for the tile kernel's sources whose hash is TILE_TRAFFIC_SOURCE: when they
 # change, the line reports no traffic until a new capture is made.
 TILE_DRAM_BYTES_PER_SYSTEM = (132830720 + 12697344) / 800000
+TILE_WARP_INSTRUCTIONS_PER_SYSTEM = 2754600250 / 800000  # sm__inst_executed.sum of the same capture
 TILE_TRAFFIC_SOURCE = "8249380f74c2b07c"
 TILE_SOURCES = ("boitata_b200/csrc/btk_tile.cu", "boitata_b200/csrc/btk_device.cuh", "boitata_b200/csrc/btk_internal.h")
 
@@ -741,6 +742,7 @@ def main():
     flops = float(np.sum(flops_per_system(n_used[st64 == 0], [s.model for s in w.variogram.structures])))
 
     ms_mixed, ms_fp64 = timed[N.MIXED][0], timed[N.FP64][0]
+    solve_ms = phases[N.MIXED][1]
     if TILE_TRAFFIC_SOURCE == tile_source_hash():
         traffic = TILE_DRAM_BYTES_PER_SYSTEM * m
         traffic_source = ("dram__bytes_read.sum + dram__bytes_write.sum of k_tile<mixed> per system from one ncu "
@@ -748,8 +750,19 @@ def main():
                           "of one launch (the per-target streams grow in proportion)")
     else:
         traffic, traffic_source = None, "no ncu capture of the current tile kernel sources"
+    issue_view = None
+    if traffic is not None and clocks.get("sm_mhz"):
+        # The tile solve is issue-bound: its warp instructions (same capture) against one instruction a
+        # clock per scheduler, four per SM, at the SM clock sampled during the timed region.
+        inst = TILE_WARP_INSTRUCTIONS_PER_SYSTEM * m
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        peak_issue = sms * 4 * clocks["sm_mhz"] * 1e6
+        issue_view = {"warp_instructions_per_step": inst, "achieved_per_s": inst / (solve_ms * 1e-3),
+                      "peak_per_s": peak_issue, "frac": inst / (solve_ms * 1e-3) / peak_issue,
+                      "source": "sm__inst_executed.sum of k_tile<mixed> per system from the capture named in "
+                                "traffic_source; peak: 4 warp instructions a clock per SM at the median sampled "
+                                "SM clock"}
     value = ws * m / (ms_mixed * 1e-3)
-    solve_ms = phases[N.MIXED][1]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -780,7 +793,8 @@ def main():
                      # and writes the outputs; its tables live in shared memory, so HBM is far from bound.
                      "hbm_view": None if traffic is None else {
                          "achieved_gbs": traffic / (solve_ms * 1e-3) / 1e9, "peak_gbs": hbm_peak()[0],
-                         "frac": traffic / (solve_ms * 1e-3) / 1e9 / hbm_peak()[0], "peak_source": hbm_peak()[1]}},
+                         "frac": traffic / (solve_ms * 1e-3) / 1e9 / hbm_peak()[0], "peak_source": hbm_peak()[1]},
+                     "issue_view": issue_view},
         "gpu_launches": int(launches[N.MIXED]),
         "clocks": clocks,
     }
