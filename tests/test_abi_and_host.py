@@ -164,3 +164,30 @@ def test_oracle_diagnostics_columns(oracle):
                              holes=np.array([5, 5, 6]), neighbors=False, diagnostics=True)
     assert r["n_holes"][0] == 2 and r["mean_distance"][0] == pytest.approx(4.5 / 3)
     assert r["negative_weight_sum"][0] <= 0.0
+
+
+def test_ctypes_mirrors_match_the_c_header_layouts(tmp_path):
+    """Every struct the Python layer passes through the C ABI has the size and field offsets of its
+    declaration in include/boitata_b200.h (a C probe compiled with gcc prints them)."""
+    import subprocess
+
+    pairs = {"btk_aniso": _native.Aniso, "btk_structure": _native.StructureC, "btk_variogram": _native.VariogramC,
+             "btk_search": _native.SearchC, "btk_geometry": _native.GeometryC, "btk_tuning": _native.TuningC,
+             "btk_outputs": _native.OutputsC, "btk_diagnostics": _native.DiagnosticsC}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "boitata_b200.h"', "int main(void) {"]
+    for cname, py in pairs.items():
+        lines.append(f'  printf("{cname} :sizeof %zu\\n", sizeof({cname}));')
+        for field, _ in py._fields_:
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["  return 0;", "}"]
+    src, exe = tmp_path / "probe.c", tmp_path / "probe"
+    src.write_text("\n".join(lines) + "\n")
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        cname, key, value = line.split()
+        got[(cname, key)] = int(value)
+    for cname, py in pairs.items():
+        assert got[(cname, ":sizeof")] == ctypes.sizeof(py), cname
+        for field, _ in py._fields_:
+            assert got[(cname, field)] == getattr(py, field).offset, (cname, field)
