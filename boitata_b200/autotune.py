@@ -199,7 +199,9 @@ def _tune(estimator, key, timer, use_cache, mixed=False):
         set_tuning(ctx, cfg)
         return {"best": cfg, "ms": cache[key]["ms"], "table": [], "cached": True}
     table = []
-    large = any(s.max_samples > 32 for s in estimator.searches)
+    from .estimation import held_samples
+
+    large = any(held_samples(s, len(estimator._samples[0])) > 32 for s in estimator.searches)
     best, best_ms = _search(ctx, get_tuning(ctx), timer, table, mixed, large)
     set_tuning(ctx, best)
     if use_cache:

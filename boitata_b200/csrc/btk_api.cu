@@ -257,8 +257,15 @@ int check_vg(btk_ctx* ctx, const btk_variogram* vg) {
   return BTK_OK;
 }
 
-// crates/estimation/src/search.rs:214-264, plus the options not run here.
-int check_search(btk_ctx* ctx, const btk_search* s) {
+// The samples a system can hold: max_samples, or the fitted samples when there
+// are fewer (but never below min_samples or min_holes, which keep their meaning).
+int64_t held_samples(const btk_search& s, int64_t n) {
+  return std::min(s.max_samples, std::max(n, std::max(s.min_samples, s.min_holes)));
+}
+
+// crates/estimation/src/search.rs:214-264, plus the options not run here. The
+// support limits apply to what a system can hold with n fitted samples.
+int check_search(btk_ctx* ctx, const btk_search* s, int64_t n = INT64_MAX) {
   if (!s) return fail(ctx, BTK_EINVAL, "search is required");
   if (std::isnan(s->radius) || s->radius <= 0.0 || s->max_samples <= 0 || s->min_samples < 0 ||
       s->min_samples > s->max_samples)
@@ -266,9 +273,10 @@ int check_search(btk_ctx* ctx, const btk_search* s) {
   if (s->sectors > 0 && s->octant) return fail(ctx, BTK_EINVAL, "give octant or sectors, not both");
   if (s->max_per_octant >= 0 && !s->octant) return fail(ctx, BTK_EINVAL, "max_per_octant needs octant");
   if (s->max_per_octant == 0) return fail(ctx, BTK_EINVAL, "max_per_sector must be >= 1");
-  if (s->max_samples > kMaxLUGlobal)
+  const int64_t most = held_samples(*s, n);
+  if (most > kMaxLUGlobal)
     return fail(ctx, BTK_EUNSUPPORTED, "more than 1024 samples per system (the dense LU's limit)");
-  if (s->calibration && s->max_samples > kMaxLU)
+  if (s->calibration && most > kMaxLU)
     return fail(ctx, BTK_EUNSUPPORTED, "a calibrated search of more than 128 samples (its Cholesky's shared-memory limit)");
   if (s->sectors > 0 && (s->sectors < 2 || s->sectors > 360 || s->max_per_sector < 1))
     return fail(ctx, BTK_EINVAL, "sectors need 2 <= count <= 360 and max_per_sector >= 1");
@@ -288,6 +296,24 @@ int check_search(btk_ctx* ctx, const btk_search* s) {
                !fin(a.rake)))
     return fail(ctx, BTK_EINVAL, "search anisotropy ranges must be finite and > 0, angles finite");
   return BTK_OK;
+}
+
+// The search as stored: a max_samples above what a system can hold (fewer
+// fitted samples, e.g. the reference's "all of them" idiom) becomes that
+// count, with the per-octant cap the original implies made explicit (the
+// reference derives it from max_samples, search.rs:488-512), so every target
+// selects the same samples and the tables are sized by what a system holds.
+btk_search effective_search(const btk_search& s, int64_t n, bool planar) {
+  btk_search e = s;
+  const int64_t most = held_samples(s, n);
+  if (most < s.max_samples) {
+    if (e.octant && e.max_per_octant < 0) {
+      const int64_t nsec = planar ? 4 : 8;
+      e.max_per_octant = std::min(s.max_samples / nsec + (s.max_samples % nsec ? 1 : 0), most);
+    }
+    e.max_samples = most;
+  }
+  return e;
 }
 
 void make_vgdev(const btk_variogram& vg, VgDev& d) {
@@ -335,9 +361,10 @@ void make_searchdev(btk_ctx* ctx) {
   d.plane = s.sectors > 0 ? int(s.sectors) : 0;
   d.balances = (s.octant || s.sectors > 0) ? 1 : 0;
   // More than 64 samples also take this kernel: its candidate buffer, not a
-  // per-lane heap, holds the list.
+  // per-lane heap, holds the list; so do sector caps whose lists would not fit
+  // a lane's 64 heap slots (e.g. 16 a sector over 8 octants).
   d.rules = (s.max_per_hole >= 0 || s.sectors > 0 || s.min_sectors >= 0 || s.max_empty_sectors >= 0 ||
-             s.min_holes >= 0 || s.max_samples > kMaxN) ? 1 : 0;
+             s.min_holes >= 0 || s.max_samples > kMaxN || int64_t(d.nsec) * cap > kMaxSlots) ? 1 : 0;
   d.max_per_hole = s.max_per_hole;
   d.min_sectors = int(s.min_sectors), d.max_empty_sectors = int(s.max_empty_sectors), d.min_holes = int(s.min_holes);
   d.rsec = d.plane ? d.plane : (s.octant ? d.nsec : 0);
@@ -988,7 +1015,7 @@ int btk_fit(btk_ctx* ctx, int64_t n, const double* xyz, const double* values, co
   if (n >= int64_t(0xffffffffu)) return fail(ctx, BTK_EINVAL, "too many samples");
   int rc = check_vg(ctx, vg);
   if (rc) return rc;
-  if ((rc = check_search(ctx, search))) return rc;
+  if ((rc = check_search(ctx, search, n))) return rc;
   std::vector<double> hx(n), hy(n), hz(n);
   for (int64_t i = 0; i < n; ++i) {
     hx[i] = xyz[3 * i], hy[i] = xyz[3 * i + 1], hz[i] = xyz[3 * i + 2];
@@ -1001,12 +1028,12 @@ int btk_fit(btk_ctx* ctx, int64_t n, const double* xyz, const double* values, co
   ctx->n = n;
   ctx->frozen = false;
   ctx->mean_m = 0;
-  ctx->search = *search;
   ctx->vg = *vg;
   ctx->has_err = err_var != nullptr;
   bool planar = true;  // search.rs:470-473
   for (int64_t i = 1; i < n && planar; ++i) planar = hz[i] == hz[0];
   ctx->planar = planar;
+  ctx->search = effective_search(*search, n, planar);
   ctx->spd.origin[0] = hx[0], ctx->spd.origin[1] = hy[0], ctx->spd.origin[2] = hz[0];
   make_vgdev(*vg, ctx->vgd);
   for (auto* b : {&ctx->x, &ctx->y, &ctx->z, &ctx->v, &ctx->e}) CK(b->grow(n));
@@ -1036,9 +1063,9 @@ int btk_fit(btk_ctx* ctx, int64_t n, const double* xyz, const double* values, co
 int btk_set_search(btk_ctx* ctx, const btk_search* search) {
   int rc = need_fit(ctx);
   if (rc) return rc;
-  if ((rc = check_search(ctx, search))) return rc;
+  if ((rc = check_search(ctx, search, ctx->n))) return rc;
   CK(cudaSetDevice(ctx->device));
-  ctx->search = *search;
+  ctx->search = effective_search(*search, ctx->n, ctx->planar);
   ctx->frozen = false;
   ctx->mean_m = 0;
   if ((rc = index_samples(ctx))) return rc;

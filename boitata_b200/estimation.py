@@ -46,6 +46,13 @@ def points(coords):
     return np.ascontiguousarray(a)
 
 
+def held_samples(search, n):
+    """The samples a system can hold, the width of the engine's neighbour rows: max_samples, or the n fitted
+    samples when there are fewer (never below min_samples or min_holes). btk_api.cu's held_samples."""
+    floor = max(n, search.min_samples, search.min_holes if search.min_holes is not None else -1)
+    return min(search.max_samples, floor)
+
+
 def finite(values, what, n=None):
     v = np.ascontiguousarray(np.asarray(values, dtype=np.float64))
     if v.ndim != 1:
@@ -569,7 +576,7 @@ class _Base:
         as for predict when fitted with domains."""
         self._fitted()
         self._use_pass(search_pass)
-        k = self.searches[search_pass].max_samples
+        k = held_samples(self.searches[search_pass], len(self._samples[0]))
         if loo:
             m = len(self._samples[0])
             xyz = None

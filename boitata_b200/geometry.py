@@ -45,12 +45,50 @@ class Geometry:
 
 
 class BlockModel:
-    """A regular block model: its `geometry` and the centroids of its cells."""
+    """A regular block model: its `geometry` and the centroids of its cells.
 
-    def __init__(self, geometry):
-        if not isinstance(geometry, Geometry):
-            raise InvalidInput("BlockModel needs a Geometry")
-        self.geometry = geometry
+    BlockModel(origin, size, count, *, rotation=(0, 0, 0)) as the reference's
+    constructor (crates/py/src/containers.rs:788-840: `origin` the corner of
+    the first cell, `rotation` azimuth, dip, rake in degrees), or
+    BlockModel(geometry). Masked models (`index`) are not run here.
+    """
+
+    def __init__(self, origin, size=None, count=None, *, rotation=(0.0, 0.0, 0.0), attributes=None, index=None,
+                 crs=None, length_unit=None):
+        from .errors import Unsupported
+
+        if index is not None:
+            raise Unsupported("masked block models (index) are not run by this engine")
+        if isinstance(origin, Geometry):
+            if size is not None or count is not None:
+                raise InvalidInput("give a Geometry, or origin, size and count")
+            self.geometry = origin
+        elif size is None or count is None:
+            raise InvalidInput("BlockModel needs origin, size and count, or a Geometry")
+        else:
+            self.geometry = Geometry(origin, size, count, rotation)
+        self.attributes, self.crs, self.length_unit = attributes, crs, length_unit
+
+    @property
+    def origin(self):
+        return self.geometry.origin
+
+    @property
+    def size(self):
+        return self.geometry.size
+
+    @property
+    def count(self):
+        return self.geometry.count
+
+    @property
+    def rotation(self):
+        return self.geometry.rotation
+
+    @property
+    def coords(self):
+        """Every cell's centroid, (n, 3) in cell order, computed by the engine."""
+        return self.centroids()
 
     def __len__(self):
         return self.geometry.cells()

@@ -191,3 +191,19 @@ def test_ctypes_mirrors_match_the_c_header_layouts(tmp_path):
         assert got[(cname, ":sizeof")] == ctypes.sizeof(py), cname
         for field, _ in py._fields_:
             assert got[(cname, field)] == getattr(py, field).offset, (cname, field)
+
+
+def test_block_model_takes_the_reference_constructor():
+    from boitata_b200.errors import InvalidInput, Unsupported
+
+    m = bt.BlockModel((1.0, 2.0, 3.0), (2.5, 2.5, 1.0), (4, 3, 2), rotation=(30.0, 0.0, 0.0))
+    assert (m.origin, m.size, m.count, m.rotation) == ((1.0, 2.0, 3.0), (2.5, 2.5, 1.0), (4, 3, 2), (30.0, 0.0, 0.0))
+    assert len(m) == 24 and isinstance(m.geometry, bt.Geometry)
+    g = bt.Geometry((0, 0, 0), (1, 1, 1), (2, 2, 2))
+    assert bt.BlockModel(g).geometry is g
+    with pytest.raises(InvalidInput):
+        bt.BlockModel((0, 0, 0), (1, 1, 1))
+    with pytest.raises(InvalidInput):
+        bt.BlockModel(g, (1, 1, 1), (2, 2, 2))
+    with pytest.raises(Unsupported):
+        bt.BlockModel((0, 0, 0), (1, 1, 1), (2, 2, 2), index=[0, 3])

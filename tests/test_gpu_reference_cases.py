@@ -78,3 +78,92 @@ def test_a_one_node_block_is_the_point_estimate():
     assert point["variance"][0] == pytest.approx(2 * gamma50, abs=1e-9)
     assert block["variance"][0] == pytest.approx(point["variance"][0], abs=1e-9)
     assert point["value"][0] == pytest.approx(1.0) and block["value"][0] == pytest.approx(1.0)
+
+
+@pytest.mark.parametrize("octant", [False, True])
+def test_max_samples_beyond_the_data_takes_them_all(oracle, octant):
+    """max_samples far above the 40 samples (the reference's 'take them all' idiom): every target takes all
+    40; with octants and a max_samples of 100, the per-octant cap the reference derives from it (13) still
+    limits each octant, list for list as the oracle's tree."""
+    r = np.random.default_rng(3)
+    xyz = r.uniform(0, 100, (40, 3))
+    vg = bt.Variogram([("spherical", 1.0, 40.0)])
+    z = r.normal(size=40)
+    every = bt.Search(radius=500, max_samples=1 << 40, octant=octant)
+    d = bt.OrdinaryKriging(vg, every).fit(xyz, z).predict(xyz[:5] + 1.0, diagnostics=True)
+    assert np.all(np.asarray(d["n_samples"]) == 40)
+    capped = bt.Search(radius=500, max_samples=100, octant=octant)
+    ok = bt.OrdinaryKriging(vg, capped).fit(xyz, z)
+    targets = r.uniform(-20, 120, (60, 3))
+    idx, cnt, good = ok.neighbors(targets)
+    tree = oracle.Tree(xyz, capped, vg)
+    for t, target in enumerate(targets):
+        want_ok, want = tree.neighbors(target)
+        assert idx[t, : cnt[t]].tolist() == want and bool(good[t]) == want_ok, t
+    ref = oracle.estimate_many(targets, xyz, z, capped, vg, neighbors=False)
+    np.testing.assert_allclose(ok.predict(targets), ref["value"], rtol=1e-10, atol=1e-10)
+
+
+def test_ranges_select_the_same_neighbours_as_radius_and_ratios():
+    r = np.random.default_rng(5)
+    xyz, z, at = r.uniform(0, 100, (300, 3)), r.normal(size=300), r.uniform(10, 90, (80, 3))
+    vg = bt.Variogram([("spherical", 1.0, 40.0)])
+    by_ratios = bt.Search(radius=60, rotation=(30, 10, 0), ratios=(0.5, 0.25), max_samples=12, octant=True)
+    by_ranges = bt.Search(ranges=(60, 30, 15), rotation=(30, 10, 0), max_samples=12, octant=True)
+    a, b = (bt.OrdinaryKriging(vg, s).fit(xyz, z).predict(at, diagnostics=True) for s in (by_ratios, by_ranges))
+    for key in ("value", "n_samples", "mean_distance"):
+        np.testing.assert_array_equal(a[key], b[key])
+
+
+@pytest.mark.parametrize("precision,tol", FORMS)
+def test_block_kriging_of_a_constant_is_the_constant(precision, tol):
+    xy, _, vg, s = scattered()
+    bk = bt.BlockKriging(vg, s, size=(10, 10), precision=precision).fit(xy, np.full(len(xy), 3.0))
+    np.testing.assert_allclose(bk.predict([[50.0, 50.0], [5.0, 95.0]]), 3.0, atol=tol)
+
+
+def test_indicator_kriging_gives_probabilities():
+    xy, z, vg, s = scattered()
+    ik = bt.IndicatorKriging(vg, s, threshold=float(np.median(z))).fit(xy, z)
+    p = ik.predict(np.random.default_rng(4).uniform(0, 100, (50, 2)))
+    assert np.all((p >= -1e-9) & (p <= 1 + 1e-9))
+
+
+def test_near_duplicates_share_their_weight_whatever_the_neighbourhood_size():
+    # 64 samples take the warp kernels, 65 the dense LU: both merge the pair 1e-9 m apart.
+    lattice = np.array([[x, y] for x in range(0, 100, 11) for y in range(0, 100, 11)], float)
+    xy = np.vstack([[[50.5, 50.5], [50.5 + 1e-9, 50.5]], lattice])
+    z = np.r_[1.0, 5.0, np.sin(lattice[:, 0] / 17.0) + 3.0]
+    vg = bt.Variogram([("spherical", 1.0, 50.0)])
+    out = [bt.OrdinaryKriging(vg, bt.Search(radius=1e3, max_samples=n)).fit(xy, z).predict([[52.0, 51.0]])[0]
+           for n in (64, 65)]
+    assert np.all(np.isfinite(out))
+
+
+def test_measurement_error_blends_a_datum_with_its_neighbours():
+    # With error variance e at datum 0, its estimate there is the LOO estimate moved towards the datum by
+    # k = var_loo / (var_loo + e); zero error variances change nothing.
+    xy, z, vg, _ = scattered()
+    xy, z = xy[:20], z[:20]
+    wide = bt.Search(radius=500, max_samples=50)
+    plain = bt.OrdinaryKriging(vg, wide).fit(xy, z)
+    zero = bt.OrdinaryKriging(vg, wide).fit(xy, z, error_variance=np.zeros(20))
+    grid = np.random.default_rng(6).uniform(0, 100, (50, 2))
+    np.testing.assert_array_equal(plain.predict(grid), zero.predict(grid))
+    loo = plain.cross_validate()
+    e = np.where(np.arange(20) == 0, 0.2, 0.0)
+    noisy = bt.OrdinaryKriging(vg, wide).fit(xy, z, error_variance=e)
+    k = loo.variance[0] / (loo.variance[0] + 0.2)
+    assert noisy.predict(xy[:1])[0] == pytest.approx(loo.estimate[0] + k * (z[0] - loo.estimate[0]), abs=1e-9)
+
+
+def test_block_kriging_follows_a_rotated_model():
+    # A block model rotated 90 degrees with 50 x 5 blocks krigs as 5 x 50 blocks at the same centres.
+    r = np.random.default_rng(0)
+    xy, z = r.uniform(0, 100, (40, 2)), r.normal(size=40)
+    s = bt.Search(radius=500, max_samples=40)
+    vg = bt.Variogram([("spherical", 1.0, 20.0)])
+    model = bt.BlockModel((0, 0, 0), (50, 5, 1), (1, 1, 1), rotation=(90, 0, 0))
+    rotated = bt.BlockKriging(vg, s, (50, 5, 1)).fit(xy, z).predict(model)
+    plain = bt.BlockKriging(vg, s, (5, 50, 1)).fit(xy, z).predict(model.coords[:, :2])
+    assert rotated == pytest.approx(plain)

@@ -129,3 +129,16 @@ def test_plane_sectors_at_their_boundaries(oracle, P, rotation):
     vg = Variogram([Structure("spherical", 1.0, 200.0)], nugget=0.1)
     est = OrdinaryKriging(vg, s).fit(X, rng.uniform(0, 1, len(X)))
     assert_same_neighbors(est, oracle, X, s, vg, T, None)
+
+
+@pytest.mark.parametrize("per_octant,most", [(16, 32), (40, 64)])
+def test_octant_caps_beyond_a_lanes_heap(oracle, per_octant, most):
+    """Octant caps whose eight lists exceed a search lane's 64 heap slots (16 or 40 a sector) run in the
+    rules kernel: lists equal the oracle's tree, estimates to 1e-10."""
+    w, _ = drill_holes()
+    s = Search(radius=250.0, octant=True, max_per_sector=per_octant, max_samples=most)
+    est = OrdinaryKriging(w.variogram, s).fit(w.coords, w.values)
+    targets = targets_in(w, 300, 7)
+    assert_same_neighbors(est, oracle, w.coords, s, w.variogram, targets, None)
+    ref = oracle.estimate_many(targets, w.coords, w.values, s, w.variogram, neighbors=False)
+    assert_same_estimates(est.predict_full(targets), ref, 1e-10)
