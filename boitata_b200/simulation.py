@@ -25,7 +25,7 @@ import numpy as np
 
 from . import _native as N
 from .errors import InvalidInput, Unsupported
-from .estimation import finite, hole_codes, points
+from .estimation import distinct, finite, hole_codes, points
 from .geometry import BlockModel, Geometry
 from .search import Search
 from .transforms import normal_score
@@ -100,6 +100,13 @@ class SGS:
         w = None if weights is None else finite(weights, "weights", n)
         if holes is not None and len(holes) != n:
             raise InvalidInput(f"holes: expected {n} values, got {len(holes)}")
+        # Samples sharing a location keep the first, with a warning naming them (crates/py/src/simulation.rs
+        # `located`, args.rs:318-376), before the normal-score transform.
+        keep = distinct(locs, None if holes is None else list(holes))
+        if len(keep) < n:
+            locs, vals = locs[keep], vals[keep]
+            w = None if w is None else w[keep]
+            holes = None if holes is None else [list(holes)[i] for i in keep]
         scores, table = normal_score(vals, w)
         codes = None if holes is None else hole_codes(list(holes))
         self._data = (np.ascontiguousarray(locs), np.ascontiguousarray(vals), scores, table, codes)

@@ -167,3 +167,100 @@ def test_block_kriging_follows_a_rotated_model():
     rotated = bt.BlockKriging(vg, s, (50, 5, 1)).fit(xy, z).predict(model)
     plain = bt.BlockKriging(vg, s, (5, 50, 1)).fit(xy, z).predict(model.coords[:, :2])
     assert rotated == pytest.approx(plain)
+
+
+def test_cross_validation_summary():
+    xy, z, vg, s = scattered()
+    cv = bt.OrdinaryKriging(vg, s).fit(xy, z).cross_validate()
+    assert cv.estimate.shape == z.shape
+    assert abs(cv.mean_error) < 0.1 and cv.correlation > 0.8
+    assert np.isfinite(cv.standardized_squared_error)
+
+
+@pytest.mark.parametrize("rule", [
+    bt.Search(radius=50, max_samples=4, octant=True, max_per_sector=1),
+    bt.Search(radius=50, max_samples=6, sectors=6, max_per_sector=1, max_empty_sectors=2),
+    bt.Search(radius=50, max_samples=6, max_per_hole=2, min_holes=3),
+], ids=["octant", "sectors", "holes"])
+def test_cross_validation_searches_as_if_the_sample_were_absent(rule):
+    xy, z, vg, _ = scattered()
+    holes = [f"DH{i // 5}" for i in range(len(xy))]
+    cv = bt.OrdinaryKriging(vg, rule).fit(xy, z, holes=holes).cross_validate()
+    for i in range(0, len(xy), 7):
+        rest = np.arange(len(xy)) != i
+        alone = bt.OrdinaryKriging(vg, rule).fit(xy[rest], z[rest], holes=list(np.array(holes)[rest]))
+        np.testing.assert_allclose(cv.estimate[i], alone.predict(xy[i:i + 1])[0], rtol=1e-9, atol=1e-12)
+
+
+def test_shared_locations_keep_the_first_and_name_their_holes():
+    xy = np.array([[0.0, 0.0], [10.0, 0.0], [0.0, 0.0], [0.0, 10.0]])
+    v = np.array([1.0, 2.0, 5.0, 3.0])
+    vg, s = bt.Variogram([("spherical", 1.0, 30.0)]), bt.Search(radius=50, max_samples=8)
+    with pytest.warns(UserWarning, match="holes DH1, DH3 at"):
+        ok = bt.OrdinaryKriging(vg, s).fit(xy, v, holes=["DH1", "DH2", "DH3", "DH4"])
+    np.testing.assert_array_equal(ok.cross_validate().actual, [1.0, 2.0, 3.0])
+    assert np.isfinite(ok.predict([[2.0, 2.0]])).all()
+    with pytest.warns(UserWarning, match="rows 0, 2"):
+        sgs = bt.SGS(vg, s).fit(xy, v)
+    assert np.isfinite(sgs.simulate([[2.0, 2.0], [5.0, 5.0]], n=2, seed=1).mean).all()
+
+
+def test_neighbourhood_diagnostics():
+    xy, z, vg, _ = scattered()
+    holes = np.arange(len(z)) // 3
+    ok = bt.OrdinaryKriging(vg, bt.Search(radius=30, max_samples=8)).fit(xy, z, holes=holes)
+    d = ok.predict(np.random.default_rng(8).uniform(0, 100, (200, 2)), diagnostics=True)
+    assert {"n_holes", "mean_distance", "negative_weight_sum", "lagrange", "max_samples_reached"} <= set(
+        d.column_names)
+    assert np.all((d["n_holes"] >= 1) & (d["n_holes"] <= d["n_samples"]))
+    assert np.all((d["mean_distance"] > 0) & (d["mean_distance"] <= 30))
+    assert np.all(d["negative_weight_sum"] <= 0) and np.any(d["negative_weight_sum"] < 0)
+    assert np.isfinite(d["lagrange"]).all()
+    np.testing.assert_array_equal(d["max_samples_reached"], d["n_samples"] == 8)
+    np.testing.assert_array_equal(d["support_variance"], 1.0)
+    cov = d["support_variance"] - d["variance"] - d["lagrange"]
+    np.testing.assert_allclose(cov / d["estimate_variance"], d["slope"], rtol=1e-12)
+
+
+def test_plane_sectors_cap_each_sector():
+    r = np.random.default_rng(7)
+    xyz, z = r.uniform(0, 100, (400, 3)), r.normal(size=400)
+    vg = bt.Variogram([("spherical", 1.0, 40.0)])
+    s = bt.Search(radius=60, max_samples=48, sectors=4, max_per_sector=3, rotation=(30, 0, 0), ratios=(0.5, 0.2))
+    d = bt.OrdinaryKriging(vg, s).fit(xyz, z).predict(r.uniform(20, 80, (50, 3)), diagnostics=True)
+    assert np.all(np.asarray(d["n_samples"]) <= 12)
+
+
+def test_min_sectors_leaves_a_one_sided_target_to_the_next_pass():
+    g = np.random.default_rng(5)
+    east = np.column_stack([g.uniform(10, 60, 200), g.uniform(-25, 25, 200)])
+    holes = np.arange(200) // 5
+    flat = np.full(200, 3.0)
+    vg = bt.Variogram([("spherical", 1.0, 40.0)])
+    outside, inside = np.array([[-10.0, 0.0]]), np.array([[35.0, 0.0]])
+    one_sided, fallback = bt.Search(radius=100, octant=True, min_sectors=3), bt.Search(radius=100)
+    for s in (one_sided, bt.Search(radius=100, octant=True, max_empty_sectors=1)):
+        ok = bt.OrdinaryKriging(vg, [s, fallback]).fit(east, flat, holes=holes)
+        assert ok.predict(outside, diagnostics=True)["pass"][0] == 2.0
+        assert ok.predict(inside, diagnostics=True)["pass"][0] == 1.0
+    assert np.isnan(bt.OrdinaryKriging(vg, one_sided).fit(east, flat).predict(outside)[0])
+    rules = bt.Search(radius=100, octant=True, max_per_sector=3, min_sectors=4, max_empty_sectors=1, min_holes=4)
+    d = bt.OrdinaryKriging(vg, rules).fit(east, flat, holes=holes).predict(g.uniform(15, 55, (40, 2)),
+                                                                          diagnostics=True)
+    done = np.isfinite(d["value"])
+    assert done.any()
+    np.testing.assert_allclose(d["value"][done], 3.0, atol=1e-10)
+    assert (d["n_holes"][done] >= 4).all() and (d["n_samples"][done] <= 12).all()
+
+
+def test_min_holes_needs_that_many_holes():
+    xy, z, vg, _ = scattered()
+    holes = np.arange(150) // 50
+    at = np.random.default_rng(9).uniform(0, 100, (60, 2))
+    for need, estimated in ((3, True), (4, False)):
+        s = bt.Search(radius=500, max_samples=150, min_holes=need)
+        d = bt.OrdinaryKriging(vg, s).fit(xy, z, holes=holes).predict(at, diagnostics=True)
+        assert np.isfinite(d["value"]).all() == estimated
+    few = bt.Search(radius=500, max_samples=4, max_per_hole=1, min_holes=3)
+    d = bt.OrdinaryKriging(vg, few).fit(xy, z, holes=holes).predict(at, diagnostics=True)
+    assert np.isfinite(d["value"]).all() and (d["n_holes"] >= 3).all()
