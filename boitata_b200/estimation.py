@@ -201,13 +201,26 @@ class CrossValidation:
         return float(np.nanmean(self.error ** 2))
 
     @property
+    def rmse(self):
+        return float(np.sqrt(self.mean_squared_error))
+
+    @property
     def standardized_squared_error(self):
+        """Mean of error^2 / variance over the estimated samples (near 1 for a calibrated variance)."""
         return float(np.nanmean(self.error ** 2 / self.variance))
 
     @property
     def correlation(self):
         ok = np.isfinite(self.estimate)
         return float(np.corrcoef(self.actual[ok], self.estimate[ok])[0, 1])
+
+    @property
+    def slope(self):
+        """Least-squares slope of the actual values on the estimates; below 1 shows conditional bias."""
+        ok = np.isfinite(self.estimate)
+        e, a = self.estimate[ok], self.actual[ok]
+        de = e - e.mean()
+        return float(np.dot(de, a - a.mean()) / np.dot(de, de))
 
 
 class _Base:
@@ -218,11 +231,7 @@ class _Base:
             raise InvalidInput("kriging needs a variogram")
         if not isinstance(variogram, Variogram):
             raise InvalidInput("variogram must be a Variogram")
-        searches = list(search) if isinstance(search, (list, tuple)) else [search]
-        if not searches or not all(isinstance(s, Search) for s in searches):
-            raise InvalidInput("search must be a Search or a sequence of Search (passes)")
-        if self._kind == N.SIMPLE and any(s.target_slope is not None for s in searches):
-            raise InvalidInput("simple kriging has a slope of regression of 1; calibrate it with target_efficiency")
+        searches = self._searches(search)
         if self._kind == N.SIMPLE and not variogram.is_stationary():
             raise InvalidInput("simple kriging needs a variogram with a sill: every structure must be stationary "
                                "(not power); use ordinary kriging")
@@ -236,6 +245,31 @@ class _Base:
         self._ctx = None
         self._pass = None
         self._samples = None
+
+    def _searches(self, search):
+        """`search` (a Search or passes) as the list of passes, checked for this estimator."""
+        searches = list(search) if isinstance(search, (list, tuple)) else [search]
+        if not searches or not all(isinstance(s, Search) for s in searches):
+            raise InvalidInput("search must be a Search or a sequence of Search (passes)")
+        if self._kind == N.SIMPLE and any(s.target_slope is not None for s in searches):
+            raise InvalidInput("simple kriging has a slope of regression of 1; calibrate it with target_efficiency")
+        return searches
+
+    def with_search(self, search):
+        """A copy with `search` (a Search or passes) in place of the searches, keeping the variogram, the
+        precision and the fitted samples, holes, error variances and domains
+        (crates/py/src/estimation.rs:1742-1756). The copy indexes the samples for its searches on a context
+        of its own."""
+        import copy
+
+        searches = self._searches(search)
+        out = copy.copy(self)
+        out.searches = searches
+        out._ctx, out._pass = None, None
+        if out._samples is not None:
+            out._ctx = N.Context(out._device)
+            out._use_pass(0)
+        return out
 
     # -- fit --------------------------------------------------------------
     def fit(self, coords, values, *, holes=None, error_variance=None, domains=None):

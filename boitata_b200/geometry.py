@@ -66,7 +66,9 @@ class BlockModel:
         elif size is None or count is None:
             raise InvalidInput("BlockModel needs origin, size and count, or a Geometry")
         else:
-            self.geometry = Geometry(origin, size, count, rotation)
+            # Two values stand for x and y: z takes origin 0, size 1, count 1 (containers.rs:804-806).
+            pad = lambda v, fill: tuple(v) + (fill,) if len(tuple(v)) == 2 else tuple(v)  # noqa: E731
+            self.geometry = Geometry(pad(origin, 0.0), pad(size, 1.0), pad(count, 1), rotation)
         self.attributes, self.crs, self.length_unit = attributes, crs, length_unit
 
     @property

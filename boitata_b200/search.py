@@ -60,8 +60,8 @@ class Search:
         if max_per_sector is not None and self.sectors is None and not self.octant:
             raise InvalidInput("max_per_sector needs octant or sectors")
         self.max_per_octant = max_per_sector if (self.octant and self.sectors is None) else None
-        self.max_per_sector = (max_per_sector if max_per_sector is not None else
-                               -(-self.max_samples // max(self.sectors, 1))) if self.sectors is not None else None
+        self._sector_cap = (max_per_sector if max_per_sector is not None else
+                            -(-self.max_samples // max(self.sectors, 1))) if self.sectors is not None else None
         if rotation is None and ratios is None:
             self.rotation = self.ratios = None
             self.anisotropy = None
@@ -80,7 +80,7 @@ class Search:
         if self.sectors is not None:
             if self.octant:
                 raise bad("give octant or sectors, not both")
-            if not (2 <= self.sectors <= 360) or self.max_per_sector == 0:
+            if not (2 <= self.sectors <= 360) or self._sector_cap == 0:
                 raise bad("sectors need 2 <= count <= 360 and max_per_sector >= 1")
             count = ring = self.sectors
         elif self.octant:
@@ -103,22 +103,65 @@ class Search:
     def balances(self):
         return self.octant or self.sectors is not None
 
+    @property
+    def max_per_sector(self):
+        """Cap per plane sector, or per octant when given with octant (crates/py/src/estimation.rs:599-606)."""
+        return self._sector_cap if self.sectors is not None else self.max_per_octant
+
+    @property
     def ranges(self):
+        """(major, semi, minor) of the ellipsoid; None without an anisotropy of its own."""
         if self.anisotropy is None:
             return None
         return (self.radius, self.radius * self.anisotropy[4], self.radius * self.anisotropy[5])
 
     def scaled(self, factor, min_samples=None, max_samples=None):
-        """A pass with the ellipsoid scaled by `factor` (estimation.rs:276-307)."""
+        """A pass with the ellipsoid scaled by `factor`, and `min_samples` / `max_samples` in place of its own
+        (estimation.rs:276-307): plane sectors left at their default cap follow the new max_samples."""
+        factor = float(factor)
+        if not (math.isfinite(factor) and factor > 0):
+            raise InvalidInput("factors must be finite and > 0")
         out = Search.__new__(Search)
         out.__dict__.update(self.__dict__)
-        out.radius = self.radius * float(factor)
+        out.radius = self.radius * factor
         if min_samples is not None:
-            out.min_samples = int(min_samples)
+            out.min_samples = _count(min_samples, "min_samples")
         if max_samples is not None:
-            out.max_samples = int(max_samples)
+            out.max_samples = _count(max_samples, "max_samples")
+            if self.sectors is not None and self._sector_cap == -(-self.max_samples // self.sectors):
+                out._sector_cap = -(-out.max_samples // self.sectors)
         out._check()
         return out
+
+    @staticmethod
+    def passes(base, factors=(1.0, 2.0, 3.0), *, min_samples=None, max_samples=None):
+        """Passes of `base` with its ellipsoid widened by each factor, and one min_samples / max_samples per
+        pass in place of the base's (crates/py/src/estimation.rs:511-557)."""
+        factors = list(factors)
+        if not factors:
+            raise InvalidInput("passes need at least one factor")
+        for given, what in ((min_samples, "min_samples"), (max_samples, "max_samples")):
+            if given is not None and len(given) != len(factors):
+                raise InvalidInput(f"{what}: expected {len(factors)} values, got {len(given)}")
+        return [base.scaled(f, None if min_samples is None else min_samples[i],
+                            None if max_samples is None else max_samples[i]) for i, f in enumerate(factors)]
+
+    def to_json(self):
+        """{"type": "Search", "format": 1, <the search's serde fields>} (crates/py/src/estimation.rs:401-412,
+        crates/py/src/persist.rs:20-33)."""
+        import json
+
+        from .persist import FORMAT, search_json
+
+        return json.dumps({"type": "Search", "format": FORMAT, **search_json(self)}, separators=(",", ":"),
+                          allow_nan=False)
+
+    @staticmethod
+    def from_json(text):
+        """Reads to_json output; InvalidInput on another class's JSON or a newer format (persist.rs:35-51)."""
+        from .persist import _open, search_from
+
+        return search_from(_open("Search", text))
 
     def to_c(self):
         s = N.SearchC()
@@ -127,7 +170,7 @@ class Search:
         s.max_per_hole = none if self.max_per_hole is None else self.max_per_hole
         s.octant = 1 if self.octant else 0
         s.sectors = 0 if self.sectors is None else self.sectors
-        s.max_per_sector = 0 if self.max_per_sector is None else self.max_per_sector
+        s.max_per_sector = 0 if self._sector_cap is None else self._sector_cap
         s.max_per_octant = none if self.max_per_octant is None else self.max_per_octant
         s.min_sectors = none if self.min_sectors is None else self.min_sectors
         s.max_empty_sectors = none if self.max_empty_sectors is None else self.max_empty_sectors

@@ -207,3 +207,70 @@ def test_block_model_takes_the_reference_constructor():
         bt.BlockModel(g, (1, 1, 1), (2, 2, 2))
     with pytest.raises(Unsupported):
         bt.BlockModel((0, 0, 0), (1, 1, 1), (2, 2, 2), index=[0, 3])
+    flat = bt.BlockModel(origin=(5.0, 5.0), size=(10, 10), count=(20, 20))
+    assert (flat.origin, flat.size, flat.count, len(flat)) == ((5.0, 5.0, 0.0), (10.0, 10.0, 1.0), (20, 20, 1), 400)
+
+
+def test_search_passes_scale_the_ellipsoid():
+    """Search.passes / scaled (crates/py/src/estimation.rs:276-307, 511-557): the ellipsoid widened by each
+    factor, rotation and rules kept, plane sectors at their default cap follow a new max_samples."""
+    base = bt.Search(ranges=(40, 20, 10), rotation=(45, 0, 0), max_samples=12, sectors=4, min_holes=2)
+    passes = bt.Search.passes(base)
+    assert [p.ranges for p in passes] == [(40, 20, 10), (80, 40, 20), (120, 60, 30)]
+    assert all((p.rotation, p.sectors, p.min_holes, p.max_samples) == ((45, 0, 0), 4, 2, 12) for p in passes)
+    custom = bt.Search.passes(base, (1, 1.5), min_samples=(4, 2), max_samples=(12, 24))
+    assert [(p.radius, p.min_samples, p.max_samples, p.max_per_sector) for p in custom] == [
+        (40, 4, 12, 3), (60, 2, 24, 6)]
+    kept = bt.Search.passes(bt.Search(radius=40, sectors=4, max_per_sector=2), (1, 2), max_samples=(16, 32))
+    assert [p.max_per_sector for p in kept] == [2, 2]
+    for bad in ({"factors": ()}, {"factors": (1, -2)}, {"factors": (1, float("inf"))}, {"max_samples": (8,)},
+                {"min_samples": (20, 20, 20)}):
+        with pytest.raises(bt.InvalidInput):
+            bt.Search.passes(base, **bad)
+    s = bt.Search(radius=50, octant=True, max_per_hole=3, rotation=(30, 10, 5), ratios=(0.5, 0.2))
+    assert (s.octant, s.max_per_hole, s.rotation, s.ratios) == (True, 3, (30, 10, 5), (0.5, 0.2))
+    plain = bt.Search(radius=50)
+    assert not plain.octant
+    assert plain.max_per_hole is plain.rotation is plain.ratios is plain.ranges is None
+
+
+def test_sector_and_hole_rules_are_checked_and_kept():
+    """The rules round-trip through Search.to_json / from_json (crates/py/src/estimation.rs:401-412) and
+    the constructor rejects what search.rs:214-264 rejects."""
+    s = bt.Search(radius=50, octant=True, max_per_sector=2, min_sectors=3, max_empty_sectors=1, min_holes=2)
+    assert (s.max_per_sector, s.min_sectors, s.max_empty_sectors, s.min_holes) == (2, 3, 1, 2)
+    back = bt.Search.from_json(s.to_json())
+    assert (back.max_per_sector, back.min_sectors, back.max_empty_sectors, back.min_holes) == (2, 3, 1, 2)
+    assert s.to_json().startswith('{"type":"Search","format":1,"min_samples":1,"max_samples":16,"radius":50.0')
+    plain = bt.Search.from_json(bt.Search(radius=50, octant=True).to_json())
+    assert plain.max_per_sector is plain.min_sectors is plain.max_empty_sectors is plain.min_holes is None
+    aniso = bt.Search(ranges=(40, 20, 10), rotation=(45, 10, 5), sectors=4, max_samples=12, target_slope=0.9)
+    again = bt.Search.from_json(aniso.to_json())
+    assert (again.ranges, again.rotation, again.sectors, again.max_per_sector, again.target_slope) == (
+        (40, 20, 10), (45, 10, 5), 4, 3, 0.9)
+    with pytest.raises(bt.InvalidInput, match="expected a Search"):
+        bt.Search.from_json('{"type":"Variogram","format":1}')
+    with pytest.raises(bt.InvalidInput, match="newer"):
+        bt.Search.from_json(s.to_json().replace('"format":1', '"format":2'))
+    for bad in ({"min_sectors": 2}, {"max_empty_sectors": 1}, {"octant": True, "min_sectors": 9},
+                {"octant": True, "min_sectors": 0}, {"octant": True, "max_empty_sectors": 4},
+                {"sectors": 6, "min_sectors": 7}, {"sectors": 6, "max_empty_sectors": 6},
+                {"octant": True, "max_per_sector": 0}, {"min_holes": 0}, {"min_holes": 17}):
+        with pytest.raises(bt.InvalidInput):
+            bt.Search(radius=50, **bad)
+
+
+def test_cross_validation_summary_statistics():
+    """CrossValidation's rmse, slope and standardized error (python/boitata/estimation.py:110-145) over the
+    estimated samples only."""
+    from boitata_b200.estimation import CrossValidation
+
+    r = np.random.default_rng(0)
+    actual = r.normal(size=50)
+    est = 0.7 * actual + 0.3 * r.normal(size=50)
+    est[3] = np.nan
+    cv = CrossValidation(actual, est, np.full(50, 0.25))
+    ok = ~np.isnan(est)
+    assert cv.rmse == pytest.approx(np.sqrt(np.mean((est[ok] - actual[ok]) ** 2)), rel=1e-14)
+    assert cv.slope == pytest.approx(np.polyfit(est[ok], actual[ok], 1)[0], rel=1e-12)
+    assert cv.standardized_squared_error == pytest.approx(np.mean((est[ok] - actual[ok]) ** 2) / 0.25, rel=1e-14)

@@ -264,3 +264,111 @@ def test_min_holes_needs_that_many_holes():
     few = bt.Search(radius=500, max_samples=4, max_per_hole=1, min_holes=3)
     d = bt.OrdinaryKriging(vg, few).fit(xy, z, holes=holes).predict(at, diagnostics=True)
     assert np.isfinite(d["value"]).all() and (d["n_holes"] >= 3).all()
+
+
+def test_passes_reach_further_targets():
+    """Search.passes of a 10 m search that needs 3 samples: targets beyond the first pass's reach take the
+    second (the pass column of the diagnostics)."""
+    xy, z, vg, _ = scattered()
+    grid = np.random.default_rng(12).uniform(-50, 150, (200, 2))
+    ok = bt.OrdinaryKriging(vg, bt.Search.passes(bt.Search(radius=10, min_samples=3))).fit(xy, z)
+    d = ok.predict(grid, diagnostics=True)
+    assert {1.0, 2.0} <= set(np.asarray(d["pass"]).tolist())
+    by_hand = bt.OrdinaryKriging(vg, [bt.Search(radius=r, min_samples=3) for r in (10, 20, 30)]).fit(xy, z)
+    np.testing.assert_array_equal(ok.predict(grid), by_hand.predict(grid))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_with_search_keeps_the_samples(precision):
+    """with_search (crates/py/src/estimation.rs:1742-1756): the same passes give the same predictions and
+    k-fold estimates; another search gives others; the estimator's type, holes and error variances stay."""
+    xy, z, vg, s = scattered()
+    passes = [s, bt.Search(radius=200, max_samples=4)]
+    holes = np.arange(len(z)) // 5
+    ok = bt.OrdinaryKriging(vg, passes, precision=precision).fit(xy, z, holes=holes)
+    targets = np.random.default_rng(13).uniform(-50, 150, (300, 2))
+    same = ok.with_search(passes)
+    assert type(same) is bt.OrdinaryKriging and same.precision == precision
+    np.testing.assert_array_equal(same.predict(targets), ok.predict(targets))
+    np.testing.assert_array_equal(same.cross_validate(folds=5).estimate, ok.cross_validate(folds=5).estimate)
+    other = ok.with_search(bt.Search(radius=50, max_samples=4)).predict(targets)
+    assert not np.array_equal(other, ok.predict(targets), equal_nan=True)
+    np.testing.assert_array_equal(ok.predict(targets), same.predict(targets))
+    one = bt.Search(radius=500, max_samples=150, min_holes=30)
+    d = ok.with_search(one).predict(targets[:20], diagnostics=True)
+    assert (d["n_holes"] == 30).all()
+    sk = bt.SimpleKriging(vg, s, mean=0.5, precision=precision).fit(xy, z, error_variance=np.full(len(z), 0.1))
+    again = sk.with_search(s)
+    assert type(again) is bt.SimpleKriging
+    np.testing.assert_array_equal(again.predict(targets), sk.predict(targets))
+    with pytest.raises(bt.InvalidInput):
+        sk.with_search(bt.Search(radius=50, target_slope=0.9))
+
+
+def test_block_model_in_the_plane():
+    """BlockModel(origin=(5, 5), size=(10, 10), count=(20, 20)) (the reference's 2-D form, containers.rs:808-811:
+    origin z 0, size z 1, one layer): 400 centroids at 10, 20, ..., 200 (origin is the corner), x fastest, on
+    the z = 0.5 plane; estimated on the plane of the 2-D data."""
+    b = bt.BlockModel(origin=(5.0, 5.0), size=(10, 10), count=(20, 20))
+    c = np.asarray(b.coords)
+    assert c.shape == (400, 3)
+    np.testing.assert_array_equal(c[:, 0], np.tile(np.arange(20) * 10.0 + 10.0, 20))
+    np.testing.assert_array_equal(c[:, 1], np.repeat(np.arange(20) * 10.0 + 10.0, 20))
+    np.testing.assert_array_equal(c[:, 2], 0.5)
+    xy, z, vg, s = scattered()
+    ok = bt.OrdinaryKriging(vg, s).fit(xy, z)
+    # A one-layer model's centroids take the elevation of 2-D data (crates/py/src/estimation.rs:960-992).
+    np.testing.assert_array_equal(ok.predict(b), ok.predict(c[:, :2]))
+    assert not np.array_equal(ok.predict(b), ok.predict(c), equal_nan=True)
+
+
+def test_search_passes_fill_what_earlier_passes_left():
+    """A target the tight pass leaves unestimated takes the wide pass's estimate, bit for bit
+    (estimation.py:337-355 over the passes)."""
+    xy, z, vg, _ = scattered()
+    grid = np.column_stack([np.repeat(np.arange(0, 150, 5.0), 30), np.tile(np.arange(0, 150, 5.0), 30)])
+    tight, wide = bt.Search(radius=10, min_samples=4), bt.Search(radius=80, min_samples=2)
+    first = bt.OrdinaryKriging(vg, tight).fit(xy, z).predict(grid)
+    second = bt.OrdinaryKriging(vg, wide).fit(xy, z).predict(grid)
+    ok = bt.OrdinaryKriging(vg, [tight, wide]).fit(xy, z)
+    d = ok.predict(grid, diagnostics=True)
+    np.testing.assert_array_equal(d["pass"], np.where(np.isfinite(first), 1.0, np.where(np.isfinite(second), 2.0,
+                                                                                          np.nan)))
+    np.testing.assert_array_equal(d["value"], np.where(np.isfinite(first), first, second))
+    assert {1.0, 2.0} <= set(np.asarray(d["pass"])[np.isfinite(d["pass"])].tolist())
+    assert np.isfinite(ok.cross_validate().estimate).all()
+    with pytest.raises(bt.InvalidInput):
+        bt.OrdinaryKriging(vg, [])
+
+
+def test_k_fold_keeps_holes_whole():
+    """cross_validate(folds=4) with 5 samples a hole: each fold is the estimate of an estimator fitted
+    without that fold's holes, bit for bit; five folds are worse than leave-one-out."""
+    xy, z, vg, s = scattered()
+    holes = np.arange(len(z)) // 5
+    cv = bt.OrdinaryKriging(vg, s).fit(xy, z, holes=holes).cross_validate(folds=4)
+    expected = np.empty(len(z))
+    for fold in range(4):
+        test = holes % 4 == fold
+        expected[test] = bt.OrdinaryKriging(vg, s).fit(xy[~test], z[~test]).predict(xy[test])
+    np.testing.assert_array_equal(cv.estimate, expected)
+    ok = bt.OrdinaryKriging(vg, s).fit(xy, z)
+    np.testing.assert_array_equal(ok.cross_validate(folds=len(z)).estimate, ok.cross_validate().estimate)
+    five = ok.cross_validate(folds=5)
+    assert np.isfinite(five.estimate).all() and five.rmse > ok.cross_validate().rmse
+
+
+def test_a_shared_contact_location_keeps_each_domains_sample():
+    """Two samples at one location in two domains: each domain keeps its own, so a target there takes the
+    sample of its domain (hard boundaries; the reference's test of this uses an infinite soft distance)."""
+    xy, z, vg, _ = scattered()
+    zone = np.where(xy[:, 0] < 50, "MS", "SM")
+    both = np.vstack([xy, [[50.0, 50.0], [50.0, 50.0]]])
+    labels = np.r_[zone, ["SM", "MS"]]
+    data = np.r_[z, 5.0, -5.0]
+    ok = bt.OrdinaryKriging(vg, bt.Search(radius=30)).fit(both, data, domains=labels)
+    at = ok.predict([[50.0, 50.0]] * 2, domains=["MS", "SM"])
+    np.testing.assert_allclose(at, [-5.0, 5.0], atol=1e-8)
+    near = ok.predict([[50.5, 50.0]] * 2, domains=["MS", "SM"], diagnostics=True)
+    assert np.isfinite(near["value"]).all() and near["value"][0] < near["value"][1]
+    assert np.isfinite(ok.cross_validate().estimate[-2:]).all()
