@@ -8,10 +8,10 @@ variance run as hand-written sm_100a CUDA kernels behind the C ABI of
 include/boitata_b200.h.
 """
 
-from .errors import InvalidInput, Unsupported
+from .errors import BoitataError, InvalidInput, MissingColumn, Unsupported
 from .persist import FileError
 from .estimation import BlockKriging, CrossValidation, IndicatorKriging, OrdinaryKriging, SimpleKriging
-from .geometry import BlockModel, Geometry
+from .geometry import BlockModel, Geometry, PointSet
 from .search import Search
 from .simulation import SGS, Simulation
 from .table import Table
@@ -20,12 +20,15 @@ from .variogram import Structure, Variogram
 __all__ = [
     "BlockKriging",
     "BlockModel",
+    "BoitataError",
     "CrossValidation",
     "FileError",
     "Geometry",
     "IndicatorKriging",
     "InvalidInput",
+    "MissingColumn",
     "OrdinaryKriging",
+    "PointSet",
     "SGS",
     "Search",
     "Simulation",

@@ -24,7 +24,7 @@ import numpy as np
 
 from . import _native as N
 from .errors import InvalidInput, Unsupported
-from .geometry import BlockModel, Geometry
+from .geometry import BlockModel, Geometry, PointSet
 from .search import Search
 from .table import Table
 from .variogram import Variogram
@@ -44,6 +44,24 @@ def points(coords):
     if a.shape[1] == 2:
         a = np.column_stack([a, np.zeros(len(a))])
     return np.ascontiguousarray(a)
+
+
+def column(data, arg, what):
+    """`arg`, or the column of the container `data` it names (python/boitata/_columns.py:13-27)."""
+    if not isinstance(arg, str):
+        return arg
+    if not isinstance(data, (PointSet, BlockModel)):
+        raise InvalidInput(f'{what} names column "{arg}"; that needs a container')
+    return data[arg]
+
+
+def domains_of(data, domains, domain_column):
+    """The domains given, or the container's column `domain_column` (estimation.py:675-678)."""
+    if domain_column is None:
+        return domains
+    if domains is not None:
+        raise InvalidInput("give one of domains or domain_column")
+    return column(data, str(domain_column), "domain_column")
 
 
 def held_samples(search, n):
@@ -272,11 +290,23 @@ class _Base:
         return out
 
     # -- fit --------------------------------------------------------------
-    def fit(self, coords, values, *, holes=None, error_variance=None, domains=None):
+    def fit(self, coords, values, *, holes=None, error_variance=None, domains=None, domain_column=None):
         """Stores the samples; samples sharing a location keep the first one, with a warning. With
         `domains` (one label per sample: strings, finite numbers or booleans) a target is estimated from
         the samples of its own domain only (hard boundaries), shared locations are dropped within a domain
-        only, and predict needs the targets' domains too (python/boitata/estimation.py:226-250)."""
+        only, and predict needs the targets' domains too (python/boitata/estimation.py:226-250).
+        `coords` may be a PointSet or BlockModel whose columns `values`, `holes`, `error_variance` and
+        `domain_column` name."""
+        values = column(coords, values, "values")
+        holes = column(coords, holes, "holes")
+        error_variance = column(coords, error_variance, "error_variance")
+        domains = domains_of(coords, domains, domain_column)
+        if isinstance(coords, Geometry):
+            coords = BlockModel(coords)
+        if isinstance(coords, BlockModel):
+            coords = coords.centroids(self._ctx)
+        elif isinstance(coords, PointSet):
+            coords = coords.coords
         locs = points(coords)
         n = len(locs)
         vals = finite(values, "values", n)
@@ -408,7 +438,7 @@ class _Base:
         z = locs[0, 2]
         return z if math.isfinite(z) and np.all(locs[:, 2] == z) else None
 
-    def predict_full(self, targets, *, precision=None, diagnostics=False, domains=None):
+    def predict_full(self, targets, *, precision=None, diagnostics=False, domains=None, domain_column=None):
         """Every output of the engine: value, variance, lagrange, n_used, status and pass (1-based, 0 unfilled);
         with `diagnostics`, also negative_weight_sum, mean_distance and n_holes of the samples used.
         `domains`: the targets' domain labels (one per target, or one for all) when fitted with domains."""
@@ -416,6 +446,7 @@ class _Base:
         precision = precision or self.precision
         if precision not in PRECISIONS:
             raise InvalidInput(f"precision must be one of {sorted(PRECISIONS)}")
+        domains = domains_of(targets, domains, domain_column)
         if isinstance(targets, Geometry):
             targets = BlockModel(targets)
         if isinstance(targets, BlockModel):
@@ -423,6 +454,8 @@ class _Base:
             z = self._level(targets)
             if z is not None:
                 xyz[:, 2] = z
+        elif isinstance(targets, PointSet):
+            xyz = targets.coords
         else:
             xyz = points(targets)
         codes = target_codes(getattr(self, "_domain_labels", None), domains, len(xyz))
@@ -455,13 +488,16 @@ class _Base:
             remaining = np.nonzero(~np.isfinite(res["value"]))[0]
         return res
 
-    def predict(self, targets, *, return_variance=False, diagnostics=False, precision=None, domains=None):
+    def predict(self, targets, *, return_variance=False, diagnostics=False, precision=None, domains=None,
+                domain_column=None):
         """Estimates at targets; NaN where the search found too few samples (estimation.py:273-335).
 
-        targets : (n, 2|3) array, Geometry or BlockModel (centroids made on the device).
+        targets : (n, 2|3) array, PointSet, Geometry or BlockModel (centroids made on the device).
         domains : the targets' domain labels (one per target, or one for all), when fitted with domains; a
             target of a domain without samples is NaN.
+        domain_column : the column of `targets` (a PointSet or BlockModel) holding their domains.
         """
+        domains = domains_of(targets, domains, domain_column)
         if diagnostics:
             return self._diagnostics(targets, precision, domains)
         res = self.predict_full(targets, precision=precision, domains=domains)

@@ -44,7 +44,78 @@ class Geometry:
         return f"Geometry(origin={self.origin}, size={self.size}, count={self.count}, rotation={self.rotation})"
 
 
-class BlockModel:
+class _Columns:
+    """Named attribute columns of a container, one value a row (containers.rs:75-210: attributes,
+    `container[name]`, with_column)."""
+
+    def _set_columns(self, attributes, rows):
+        cols = {}
+        if attributes is not None:
+            names = list(attributes.column_names) if hasattr(attributes, "column_names") else list(attributes)
+            for name in names:
+                a = np.asarray(attributes[name])
+                if a.ndim != 1 or len(a) != rows:
+                    raise InvalidInput(f'column "{name}": expected {rows} values, got shape {a.shape}')
+                cols[str(name)] = a
+        self.attributes = cols
+
+    @property
+    def column_names(self):
+        return list(self.attributes)
+
+    def __contains__(self, name):
+        return name in self.attributes
+
+    def __getitem__(self, name):
+        try:
+            return self.attributes[name]
+        except KeyError:
+            import difflib
+
+            from .errors import MissingColumn
+
+            close = difflib.get_close_matches(str(name), self.column_names, n=1)
+            hint = f' (did you mean "{close[0]}"?)' if close else ""
+            raise MissingColumn(f'no column "{name}"{hint}; columns: {", ".join(self.column_names)}') from None
+
+    def with_column(self, name, values):
+        """A copy with the column `name` added or replaced."""
+        import copy
+
+        out = copy.copy(self)
+        out.attributes = dict(self.attributes)
+        a = np.asarray(values)
+        if a.ndim != 1 or len(a) != len(self):
+            raise InvalidInput(f'column "{name}": expected {len(self)} values, got shape {a.shape}')
+        out.attributes[str(name)] = a
+        return out
+
+
+class PointSet(_Columns):
+    """Points with attribute columns: PointSet(coords, attributes=None, *, crs=None, length_unit=None) as the
+    reference's (crates/py/src/containers.rs:75-100); `coords` (n, 2) or (n, 3), 2-D points on z = 0."""
+
+    def __init__(self, coords, attributes=None, *, crs=None, length_unit=None):
+        a = np.asarray(coords, dtype=np.float64)
+        if a.ndim != 2 or a.shape[1] not in (2, 3):
+            raise InvalidInput("coordinates must be a 2-D array of shape (n, 2) or (n, 3)")
+        if not np.all(np.isfinite(a)):
+            raise InvalidInput("coordinates must be finite")
+        if a.shape[1] == 2:
+            a = np.column_stack([a, np.zeros(len(a))])
+        self._coords = np.ascontiguousarray(a)
+        self._set_columns(attributes, len(a))
+        self.crs, self.length_unit = crs, length_unit
+
+    @property
+    def coords(self):
+        return self._coords
+
+    def __len__(self):
+        return len(self._coords)
+
+
+class BlockModel(_Columns):
     """A regular block model: its `geometry` and the centroids of its cells.
 
     BlockModel(origin, size, count, *, rotation=(0, 0, 0)) as the reference's
@@ -69,7 +140,8 @@ class BlockModel:
             # Two values stand for x and y: z takes origin 0, size 1, count 1 (containers.rs:804-806).
             pad = lambda v, fill: tuple(v) + (fill,) if len(tuple(v)) == 2 else tuple(v)  # noqa: E731
             self.geometry = Geometry(pad(origin, 0.0), pad(size, 1.0), pad(count, 1), rotation)
-        self.attributes, self.crs, self.length_unit = attributes, crs, length_unit
+        self._set_columns(attributes, self.geometry.cells())
+        self.crs, self.length_unit = crs, length_unit
 
     @property
     def origin(self):

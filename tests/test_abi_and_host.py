@@ -274,3 +274,40 @@ def test_cross_validation_summary_statistics():
     assert cv.rmse == pytest.approx(np.sqrt(np.mean((est[ok] - actual[ok]) ** 2)), rel=1e-14)
     assert cv.slope == pytest.approx(np.polyfit(est[ok], actual[ok], 1)[0], rel=1e-12)
     assert cv.standardized_squared_error == pytest.approx(np.mean((est[ok] - actual[ok]) ** 2) / 0.25, rel=1e-14)
+
+
+def test_point_sets_and_named_columns():
+    """PointSet / BlockModel attribute columns (crates/py/src/containers.rs:75-210) and the estimators'
+    column arguments (python/boitata/estimation.py:226-330, _columns.py:13-27), checked before any device
+    work."""
+    r = np.random.default_rng(3)
+    xy = r.uniform(0, 100, (150, 2))
+    zone = np.where(xy[:, 0] < 50, "W", "E")
+    samples = bt.PointSet(xy, {"grade": np.sin(xy[:, 0] / 15), "zone": zone})
+    assert len(samples) == 150 and samples.coords.shape == (150, 3) and not samples.coords[:, 2].any()
+    assert samples.column_names == ["grade", "zone"] and "zone" in samples
+    np.testing.assert_array_equal(samples["zone"], zone)
+    w = samples.with_column("w", np.linspace(1, 2, 150))
+    assert w.column_names == ["grade", "zone", "w"] and samples.column_names == ["grade", "zone"]
+    with pytest.raises(bt.MissingColumn, match='did you mean "grade"'):
+        samples["grades"]
+    with pytest.raises(KeyError):
+        samples["rock"]
+    with pytest.raises(bt.InvalidInput, match="expected 150"):
+        samples.with_column("short", np.zeros(3))
+    with pytest.raises(bt.InvalidInput, match="expected 150"):
+        bt.PointSet(xy, {"bad": np.zeros(4)})
+    blocks = bt.BlockModel(origin=(0, 0), size=(10, 10), count=(10, 10), attributes={"zone": np.arange(100) % 2})
+    assert blocks.column_names == ["zone"] and blocks.with_column("ok", np.ones(100))["ok"].shape == (100,)
+    ok = bt.OrdinaryKriging(bt.Variogram([("spherical", 1.0, 40.0)]), bt.Search(radius=50))
+    with pytest.raises(bt.InvalidInput, match="one of domains or domain_column"):
+        ok.fit(samples, "grade", domains=zone, domain_column="zone")
+    with pytest.raises(bt.InvalidInput, match="needs a container"):
+        ok.fit(xy, "grade")
+    with pytest.raises(bt.MissingColumn):
+        ok.fit(samples, "gold")
+    with pytest.raises(bt.InvalidInput, match="one of domains or domain_column"):
+        ok.predict(samples, domains=zone, domain_column="zone")
+    with pytest.raises(bt.MissingColumn):
+        ok.predict(samples, domain_column="rock")
+    assert issubclass(bt.InvalidInput, bt.BoitataError) and issubclass(bt.MissingColumn, bt.BoitataError)

@@ -372,3 +372,35 @@ def test_a_shared_contact_location_keeps_each_domains_sample():
     near = ok.predict([[50.5, 50.0]] * 2, domains=["MS", "SM"], diagnostics=True)
     assert np.isfinite(near["value"]).all() and near["value"][0] < near["value"][1]
     assert np.isfinite(ok.cross_validate().estimate[-2:]).all()
+
+
+def test_column_names_match_arrays():
+    """fit(PointSet, "grade", holes="hole", domain_column="zone") and predict(BlockModel,
+    domain_column="zone") give the estimates of the same arrays, bit for bit; a PointSet target at the
+    data returns the data."""
+    xy, z, vg, s = scattered()
+    holes = np.arange(len(z)) // 3
+    zone = np.where(xy[:, 0] < 50, 1, 2)
+    samples = bt.PointSet(xy, {"grade": z, "hole": holes, "zone": zone})
+    grid = bt.BlockModel(origin=(0, 0), size=(10, 10), count=(10, 10))
+    blocks = grid.with_column("zone", np.where(np.asarray(grid.coords)[:, 0] < 50, 1, 2))
+    ok = bt.OrdinaryKriging(vg, s)
+    arrays = ok.fit(xy, z, holes=holes, domains=zone).predict(grid, domains=blocks["zone"])
+    names = ok.fit(samples, "grade", holes="hole", domain_column="zone").predict(blocks, domain_column="zone")
+    np.testing.assert_array_equal(names, arrays)
+    assert np.isfinite(arrays).all()
+    plain = bt.OrdinaryKriging(vg, s).fit(samples, "grade")
+    est = plain.predict(grid)
+    assert est.shape == (100,)
+    np.testing.assert_array_equal(grid.with_column("ok", est)["ok"], est)
+    np.testing.assert_allclose(plain.predict(bt.PointSet(xy[:3])), z[:3], atol=1e-8)
+    d = plain.predict(bt.PointSet(xy[:3]), diagnostics=True)
+    np.testing.assert_allclose(d["slope"], 1.0)
+
+
+def test_simple_kriging_needs_a_sill_and_ordinary_takes_the_power_model():
+    xy, z, _, _ = scattered()
+    power = bt.Variogram([("power", 1.0, 1.5)])
+    with pytest.raises(bt.InvalidInput, match="simple kriging needs a variogram with a sill"):
+        bt.SimpleKriging(power, bt.Search(radius=1000), mean=1.0)
+    assert np.isfinite(bt.OrdinaryKriging(power, bt.Search(radius=1000)).fit(xy, z).predict([[50.0, 50.0]])[0])
