@@ -82,19 +82,48 @@ def finite(values, what, n=None):
     return v
 
 
+def _hole_text(v):
+    """A hole label as the reference keys it (crates/py/src/args.rs:14-45): the text of a string, boolean
+    ("true" / "false") or finite number (integral values without a decimal point, so 1, 1.0 and "1" are one
+    hole); None for None and NaN."""
+    if v is None:
+        return None
+    if isinstance(v, str):
+        return v
+    if isinstance(v, (bool, np.bool_)):
+        return "true" if v else "false"
+    if isinstance(v, (int, np.integer)):
+        return str(int(v))
+    try:
+        f = float(v)
+    except (TypeError, ValueError):
+        f = math.inf
+    if math.isnan(f):
+        return None
+    if not math.isfinite(f):
+        raise InvalidInput("holes must be a 1-D sequence of labels: strings, finite numbers or booleans, None or "
+                           "NaN for none")
+    return str(int(f)) if f == math.floor(f) and abs(f) < 9e15 else repr(f)
+
+
 def hole_codes(labels):
-    """Integer codes of hole labels (crates/py/src/args.rs:276-292): one per distinct label, in order of
+    """Integer codes of hole labels (crates/py/src/args.rs:257-292): one per distinct label text, in order of
     first appearance, and a fresh one for each row without a label (None or NaN), which then counts as a
     hole of its own."""
-    codes, out = {}, np.empty(len(labels), dtype=np.int64)
+    if isinstance(labels, str):
+        raise InvalidInput("holes must be a sequence of labels")
+    items = labels.to_pylist() if hasattr(labels, "to_pylist") else np.asarray(labels).tolist()
+    if not isinstance(items, list) or any(isinstance(v, list) for v in items):
+        raise InvalidInput("holes must be a 1-D sequence of labels: strings, finite numbers or booleans, None or "
+                           "NaN for none")
+    codes, out = {}, np.empty(len(items), dtype=np.int64)
     nxt = 0
-    for i, v in enumerate(labels):
-        missing = v is None or (isinstance(v, float) and math.isnan(v))
-        if missing:
+    for i, v in enumerate(items):
+        key = _hole_text(v)
+        if key is None:
             out[i] = nxt
             nxt += 1
             continue
-        key = str(v)
         if key not in codes:
             codes[key] = nxt
             nxt += 1

@@ -175,6 +175,11 @@ def method_json(est):
     return {"Kriging": "Ordinary"}
 
 
+def envelope_of(name, fields):
+    """persist.rs:20-33: {"type": name, "format": 1, <fields>...}, compact, non-finite floats as strings."""
+    return json.dumps({"type": name, "format": FORMAT, **fields}, separators=(",", ":"), allow_nan=False)
+
+
 def envelope(est):
     """persist.rs:20-33 and :85-92: type and format first, then fitted, then the estimator's fields."""
     fields = {"type": type(est).__name__, "format": FORMAT, "fitted": est._samples is not None,

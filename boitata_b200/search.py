@@ -149,12 +149,9 @@ class Search:
     def to_json(self):
         """{"type": "Search", "format": 1, <the search's serde fields>} (crates/py/src/estimation.rs:401-412,
         crates/py/src/persist.rs:20-33)."""
-        import json
+        from .persist import envelope_of, search_json
 
-        from .persist import FORMAT, search_json
-
-        return json.dumps({"type": "Search", "format": FORMAT, **search_json(self)}, separators=(",", ":"),
-                          allow_nan=False)
+        return envelope_of("Search", search_json(self))
 
     @staticmethod
     def from_json(text):

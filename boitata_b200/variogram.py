@@ -46,6 +46,19 @@ class Structure:
     def exponent(self):
         return self._param if self.model == "power" else None
 
+    def to_json(self):
+        """{"type": "Structure", "format": 1, "model": ..., "sill": ..., "range": ...} (variogram.rs:196-208)."""
+        from .persist import envelope_of, variogram_json
+
+        return envelope_of("Structure", variogram_json(Variogram([self]))["structures"][0])
+
+    @staticmethod
+    def from_json(text):
+        from .persist import _open, variogram_from
+
+        d = _open("Structure", text)
+        return variogram_from({"nugget": 0.0, "structures": [d], "anisotropy": None}).structures[0]
+
     def __repr__(self):
         return f"Structure({self.model!r}, {self.sill}, {self.range})"
 
@@ -124,6 +137,20 @@ class Variogram:
         return Variogram(st, nugget=self.nugget if nugget is None else nugget,
                          rotation=self.rotation if rotation is None else rotation,
                          ratios=self.ratios if ratios is None else ratios)
+
+    def to_json(self):
+        """{"type": "Variogram", "format": 1, "nugget": ..., "structures": [...], "anisotropy": ...}
+        (variogram.rs:569-579, composite.rs:12-18)."""
+        from .persist import envelope_of, variogram_json
+
+        return envelope_of("Variogram", variogram_json(self))
+
+    @staticmethod
+    def from_json(text):
+        """Reads to_json output; InvalidInput on another class's JSON or a newer format."""
+        from .persist import _open, variogram_from
+
+        return variogram_from(_open("Variogram", text))
 
     def __repr__(self):
         return (f"Variogram({self.structures!r}, nugget={self.nugget}, rotation={self.rotation}, "

@@ -311,3 +311,21 @@ def test_point_sets_and_named_columns():
     with pytest.raises(bt.MissingColumn):
         ok.predict(samples, domain_column="rock")
     assert issubclass(bt.InvalidInput, bt.BoitataError) and issubclass(bt.MissingColumn, bt.BoitataError)
+
+
+def test_hole_labels_are_keyed_as_the_reference_keys_them():
+    """crates/py/src/args.rs:14-45, 257-292: labels keyed by their text (1, 1.0 and "1" are one hole; True and
+    "true" too), None and NaN each a hole of their own, infinite labels rejected before any device work."""
+    from boitata_b200.estimation import hole_codes
+
+    np.testing.assert_array_equal(hole_codes([1, 1.0, "1", True, "true", None, np.nan, 2.5, "a"]),
+                                  [0, 0, 0, 1, 1, 2, 3, 4, 5])
+    np.testing.assert_array_equal(hole_codes(np.array([None] * 4, dtype=object)), [0, 1, 2, 3])
+    np.testing.assert_array_equal(hole_codes(np.full(3, np.nan)), [0, 1, 2])
+    for bad in ([np.inf, 1.0], [[1, 2], [3, 4]], "DH1"):
+        with pytest.raises(bt.InvalidInput, match="sequence of labels"):
+            hole_codes(bad)
+    xy = np.random.default_rng(3).uniform(0, 100, (150, 2))
+    ok = bt.OrdinaryKriging(bt.Variogram([("spherical", 1.0, 40.0)]), bt.Search(radius=50))
+    with pytest.raises(bt.InvalidInput, match="holes must be a 1-D sequence of labels"):
+        ok.fit(xy, xy[:, 0], holes=np.full(150, np.inf))

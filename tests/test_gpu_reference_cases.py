@@ -404,3 +404,17 @@ def test_simple_kriging_needs_a_sill_and_ordinary_takes_the_power_model():
     with pytest.raises(bt.InvalidInput, match="simple kriging needs a variogram with a sill"):
         bt.SimpleKriging(power, bt.Search(radius=1000), mean=1.0)
     assert np.isfinite(bt.OrdinaryKriging(power, bt.Search(radius=1000)).fit(xy, z).predict([[50.0, 50.0]])[0])
+
+
+@pytest.mark.parametrize("missing", [None, np.nan])
+def test_missing_hole_ids_count_as_their_own_hole(missing):
+    """Untagged samples (None or NaN hole ids) are holes of their own: a min_holes search gives the
+    estimates of the estimator fitted without holes."""
+    xy, z, vg, _ = scattered()
+    holes = np.array([missing] * len(z), dtype=object)
+    targets = xy[:3] + 1.0
+    est = bt.OrdinaryKriging(vg, bt.Search(radius=200, max_samples=12, min_holes=2))
+    out = est.fit(xy, z, holes=holes).predict(targets)
+    np.testing.assert_array_equal(out, est.fit(xy, z).predict(targets))
+    tagged = est.fit(xy, z, holes=np.r_[np.arange(len(z) - 1), np.nan]).predict(targets)
+    np.testing.assert_array_equal(tagged, out)

@@ -99,3 +99,26 @@ def test_nonfinite_floats_are_strings():
     with pytest.raises(bt.InvalidInput):
         persist._unnum("x", "r")
     assert np.isnan(persist._unnum("NaN", "r"))
+
+
+def test_parameters_round_trip_through_json_and_pickle():
+    """Variogram, Structure and Search to_json / from_json (crates/py/src/variogram.rs:196-208, 569-579,
+    estimation.rs:401-412) and pickle give the same JSON back; an infinite radius survives; the envelope's
+    type and format are checked (python/tests/test_persist.py:121-135 of the reference)."""
+    import pickle
+
+    objs = [bt.Variogram([("spherical", 0.7, 50.0), bt.Structure("matern", 0.2, 30.0, order=2.5)], nugget=0.1,
+                         rotation=(30.0, 10.0, 0.0), ratios=(0.5, 0.2)),
+            bt.Structure("exponential", 1.0, 30.0), bt.Structure("power", 1.0, 1.0, exponent=1.5),
+            bt.Search(np.inf, rotation=(10.0, 0.0, 0.0), ratios=(0.5, 0.5)),
+            bt.Search(30.0, sectors=6, max_per_sector=2, min_holes=2, target_efficiency=0.5)]
+    for obj in objs:
+        for back in (type(obj).from_json(obj.to_json()), pickle.loads(pickle.dumps(obj))):
+            assert type(back) is type(obj) and back.to_json() == obj.to_json()
+    assert bt.Search.from_json(bt.Search(np.inf).to_json()).radius == np.inf
+    text = objs[0].to_json()
+    assert text.startswith('{"type":"Variogram","format":1,"nugget":0.1,"structures":[{"model":"Spherical"')
+    with pytest.raises(bt.InvalidInput, match="expected a Search"):
+        bt.Search.from_json(text)
+    with pytest.raises(bt.InvalidInput, match=r"^format 2 is newer"):
+        bt.Variogram.from_json(text.replace('"format":1', '"format":2'))
