@@ -11,6 +11,7 @@ include/boitata_b200.h.
 from .errors import BoitataError, InvalidInput, MissingColumn, Unsupported
 from .persist import FileError
 from .estimation import BlockKriging, CrossValidation, IndicatorKriging, OrdinaryKriging, SimpleKriging
+from .calibrate import calibrate_search, global_bias
 from .geometry import BlockModel, Geometry, PointSet
 from .search import Search
 from .simulation import SGS, Simulation
@@ -37,5 +38,7 @@ __all__ = [
     "Table",
     "Unsupported",
     "Variogram",
+    "calibrate_search",
+    "global_bias",
 ]
 __version__ = "0.1.0"

@@ -497,6 +497,10 @@ class _Base:
 
     def _passes(self, xyz, precision, diagnostics=False, codes=None):
         m = len(xyz)
+        if m == 0:  # no targets: empty columns of every output
+            res = self._run(xyz, precision, diagnostics)
+            res["pass"] = np.zeros(0, dtype=np.int32)
+            return res
         res = None
         remaining = np.arange(m)
         for p in range(len(self.searches)):

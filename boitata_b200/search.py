@@ -115,9 +115,10 @@ class Search:
             return None
         return (self.radius, self.radius * self.anisotropy[4], self.radius * self.anisotropy[5])
 
-    def scaled(self, factor, min_samples=None, max_samples=None):
-        """A pass with the ellipsoid scaled by `factor`, and `min_samples` / `max_samples` in place of its own
-        (estimation.rs:276-307): plane sectors left at their default cap follow the new max_samples."""
+    def _varied(self, factor, min_samples, max_samples, min_holes):
+        """A copy with the ellipsoid scaled by `factor`, `min_samples` / `max_samples` in place of its own when
+        given, and `min_holes` in place of its own, checked once all are set (crates/py/src/estimation.rs:276-307):
+        plane sectors left at their default cap follow the new max_samples."""
         factor = float(factor)
         if not (math.isfinite(factor) and factor > 0):
             raise InvalidInput("factors must be finite and > 0")
@@ -130,8 +131,19 @@ class Search:
             out.max_samples = _count(max_samples, "max_samples")
             if self.sectors is not None and self._sector_cap == -(-self.max_samples // self.sectors):
                 out._sector_cap = -(-out.max_samples // self.sectors)
+        out.min_holes = _count(min_holes, "min_holes")
         out._check()
         return out
+
+    def scaled(self, factor, min_samples=None, max_samples=None):
+        """A pass with the ellipsoid scaled by `factor`, and `min_samples` / `max_samples` in place of its own
+        (estimation.rs:276-307): plane sectors left at their default cap follow the new max_samples."""
+        return self._varied(factor, min_samples, max_samples, self.min_holes)
+
+    def _vary(self, factor, max_samples, min_holes):
+        """A copy with the ellipsoid scaled by `factor`, and `max_samples` and `min_holes` (None: no hole rule)
+        in place of its own; for calibrate_search (crates/py/src/estimation.rs:560-564)."""
+        return self._varied(factor, None, max_samples, min_holes)
 
     @staticmethod
     def passes(base, factors=(1.0, 2.0, 3.0), *, min_samples=None, max_samples=None):
