@@ -12,6 +12,7 @@ from .errors import BoitataError, InvalidInput, MissingColumn, Unsupported
 from .persist import FileError
 from .estimation import BlockKriging, CrossValidation, IndicatorKriging, OrdinaryKriging, SimpleKriging
 from .calibrate import calibrate_search, global_bias
+from .declustering import Declustering, weight_declustering
 from .geometry import BlockModel, Geometry, PointSet
 from .search import Search
 from .simulation import SGS, Simulation
@@ -23,6 +24,7 @@ __all__ = [
     "BlockModel",
     "BoitataError",
     "CrossValidation",
+    "Declustering",
     "FileError",
     "Geometry",
     "IndicatorKriging",
@@ -40,5 +42,6 @@ __all__ = [
     "Variogram",
     "calibrate_search",
     "global_bias",
+    "weight_declustering",
 ]
 __version__ = "0.1.0"

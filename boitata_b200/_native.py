@@ -97,6 +97,8 @@ SIGNATURES = {
                                       ctypes.POINTER(OutputsC), P]),
     "btk_predict_ex_device": (ctypes.c_int, [P, ctypes.c_int64, P, P, P, ctypes.c_int32, ctypes.c_double,
                                              ctypes.c_int32, ctypes.POINTER(OutputsC), P]),
+    "btk_predict_weights": (ctypes.c_int, [P, ctypes.c_int64, P, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, P,
+                                           ctypes.POINTER(OutputsC), P, P]),
     "btk_centroids": (ctypes.c_int, [P, ctypes.POINTER(GeometryC), ctypes.c_int64, ctypes.c_int64, P]),
     "btk_launch_count": (ctypes.c_int64, [P]),
     "btk_set_support": (ctypes.c_int, [P, P, P, P]),

@@ -155,6 +155,7 @@ struct btk_ctx {
 
   // per-call scratch, grown on demand
   DevBuf<double> txyz, aos;
+  DevBuf<double> wts;  // btk_predict_weights: [target][max_samples] kriging weights
   DevBuf<int64_t> perm, lists, lens, redo, redo_len;
   DevBuf<uint32_t> nbr;
   DevBuf<int32_t> cnt, o_nused;
@@ -508,13 +509,13 @@ int check_domains(btk_ctx* ctx, const int32_t* tdom, bool loo) {
 int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const double* ty, const double* tz,
              const int64_t* perm, int64_t nwork, int loo, int32_t kind, double kparam, int32_t precision,
              const btk_outputs* o, const int8_t* kinds = nullptr, const btk_diagnostics* dg = nullptr,
-             const int32_t* tdom = nullptr) {
+             const int32_t* tdom = nullptr, double* wout = nullptr) {
   if (int rc = check_domains(ctx, tdom, loo != 0)) return rc;
   if (kind < BTK_ORDINARY || kind > BTK_INDICATOR) return fail(ctx, BTK_EINVAL, "unknown kriging kind");
   if (precision != BTK_FP64 && precision != BTK_MIXED) return fail(ctx, BTK_EINVAL, "unknown precision");
   if (kind == BTK_SIMPLE && !std::isfinite(kparam)) return fail(ctx, BTK_EINVAL, "simple kriging needs a finite mean");
   if (!o || !o->value) return fail(ctx, BTK_EINVAL, "outputs need a value array");
-  if (dg && !o->status) return fail(ctx, BTK_EINVAL, "diagnostics need the status output");
+  if ((dg || wout) && !o->status) return fail(ctx, BTK_EINVAL, "diagnostics and weights need the status output");
   const btk_search& srch = ctx->search;
   if (srch.calibration == 1 && kind == BTK_SIMPLE && !kinds)
     return fail(ctx, BTK_EINVAL, "simple kriging has a slope of regression of 1; calibrate it with target_efficiency");
@@ -577,14 +578,18 @@ int run_path(btk_ctx* ctx, cudaStream_t s, int64_t m, const double* tx, const do
     CK(launch_calibrate(L, ac, ctx->spd, cd, int(srch.max_samples)));
   }
   // The diagnostics pass over every work slot, after the solve has set each status.
+  // With `wout`, the same pass writes each estimated system's weights.
   auto diagnose = [&]() -> int {
-    if (!dg) return BTK_OK;
+    if (!dg && !wout) return BTK_OK;
     SolveDev ad = a;
     ad.perm = perm, ad.nwork = perm ? nwork : m;
-    ad.negw = dg->negative_weight_sum, ad.mdist = dg->mean_distance, ad.nholes = dg->n_holes;
-    ad.hole = ctx->has_hole ? ctx->hole.p : nullptr;
+    if (dg) {
+      ad.negw = dg->negative_weight_sum, ad.mdist = dg->mean_distance, ad.nholes = dg->n_holes;
+      ad.hole = ctx->has_hole ? ctx->hole.p : nullptr;
+    }
+    ad.wout = wout;
     CK(launch_solve_lu(L, ad, int(ctx->search.max_samples), true));
-    if (dg->target_met) {
+    if (dg && dg->target_met) {
       if (srch.calibration)
         CK(cudaMemcpyAsync(dg->target_met, ctx->met.p, size_t(m), cudaMemcpyDeviceToDevice, L.stream));
       else
@@ -1255,6 +1260,47 @@ int btk_predict_ex(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kin
   return predict_host(ctx, m, xyz, kinds, kinds ? BTK_ORDINARY : kind, kparam, precision, out, diag, domains);
 }
 
+int btk_predict_weights(btk_ctx* ctx, int64_t m, const double* xyz, int32_t kind, double kparam, int32_t precision,
+                        const int32_t* domains, const btk_outputs* out, int64_t* idx, double* weights) {
+  int rc = need_fit(ctx);
+  if (rc) return rc;
+  if (!out || !out->value || !out->status) return fail(ctx, BTK_EINVAL, "weights need the value and status outputs");
+  if (m < 0 || (m > 0 && (!xyz || !idx || !weights)))
+    return fail(ctx, BTK_EINVAL, "targets, idx and weights are required");
+  if ((rc = check_domains(ctx, domains, false))) return rc;
+  if (m == 0) return BTK_OK;
+  CK(cudaSetDevice(ctx->device));
+  if ((rc = upload_targets(ctx, m, xyz))) return rc;
+  const size_t k = size_t(ctx->search.max_samples), mk = size_t(m) * k;
+  CK(ctx->wts.grow(mk));
+  if (domains) {
+    CK(ctx->tdom.grow(size_t(m)));
+    CK(cudaMemcpyAsync(ctx->tdom.p, domains, size_t(m) * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  btk_outputs d{};
+  if ((rc = host_outputs(ctx, m, out, &d))) return rc;
+  const double* t = ctx->txyz.p;
+  if ((rc = run_path(ctx, ctx->stream, m, t, t + m, t + 2 * m, nullptr, m, 0, kind, kparam, precision, &d, nullptr,
+                     nullptr, domains ? ctx->tdom.p : nullptr, ctx->wts.p)))
+    return rc;
+  std::vector<uint32_t> nb(mk);
+  std::vector<int32_t> cnt(static_cast<size_t>(m));
+  CK(cudaMemcpyAsync(nb.data(), ctx->nbr.p, mk * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(cnt.data(), ctx->cnt.p, size_t(m) * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(weights, ctx->wts.p, mk * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if ((rc = copy_out(ctx, m, &d, out))) return rc;  // synchronises the stream
+  for (int64_t t0 = 0; t0 < m; ++t0) {
+    const bool est = (out->status[t0] & 0x0F) == BTK_ST_OK;
+    const size_t n = est ? size_t(std::max(cnt[t0], 0)) : 0;
+    for (size_t r = 0; r < k; ++r) {
+      const size_t e = size_t(t0) * k + r;
+      const bool used = r < n;
+      idx[e] = used ? int64_t(nb[e]) : -1;
+      if (!used) weights[e] = 0.0;
+    }
+  }
+  return BTK_OK;
+}
 int btk_predict_ex_device(btk_ctx* ctx, int64_t m, const double* d_xyz, const int8_t* d_kinds,
                           const int32_t* d_domains, int32_t kind, double kparam, int32_t precision,
                           const btk_outputs* d_out, void* stream) {

@@ -130,6 +130,10 @@ struct SolveDev {
   double *negw, *mdist;
   int32_t* nholes;
   const uint32_t* hole;
+  // The same pass's kriging weights, [target][max_samples] in list order and
+  // spread over coincident clusters as the estimate spreads them (null: not
+  // wanted); rows of targets it does not estimate are left as they are.
+  double* wout;
 };
 
 // Tile-shared solve (btk_tile.cu): the systems of kTileTargets consecutive

@@ -467,6 +467,9 @@ __global__ void __launch_bounds__(NT, NT > 128 ? 1 : 0) k_solve_lu(SolveDev a, i
         }
         a.negw[ti] = neg;
       }
+      if (!H.sing && a.wout)  // Estimate::weights, one per sample of the list (batch.rs:76-95)
+        for (int i = tid; i < n; i += NT)
+          a.wout[ti * a.max_samples + i] = H.twin ? X[cof[i]] / double(csize[cof[i]]) : X[i];
       continue;
     }
     if (tid == 0) {

@@ -478,18 +478,25 @@ class _Base:
         domains = domains_of(targets, domains, domain_column)
         if isinstance(targets, Geometry):
             targets = BlockModel(targets)
+        xyz = self._locate(targets)
+        codes = target_codes(getattr(self, "_domain_labels", None), domains, len(xyz))
+        with self._support(targets):
+            return self._passes(xyz, precision, diagnostics, codes)
+
+    def _locate(self, targets):
+        """(m, 3) target points: a BlockModel's centroids (made on the device; a single layer turned only in
+        azimuth at the elevation of 2-D data), a PointSet's coordinates, or an array's."""
+        if isinstance(targets, Geometry):
+            targets = BlockModel(targets)
         if isinstance(targets, BlockModel):
             xyz = targets.centroids(self._ctx)
             z = self._level(targets)
             if z is not None:
                 xyz[:, 2] = z
-        elif isinstance(targets, PointSet):
-            xyz = targets.coords
-        else:
-            xyz = points(targets)
-        codes = target_codes(getattr(self, "_domain_labels", None), domains, len(xyz))
-        with self._support(targets):
-            return self._passes(xyz, precision, diagnostics, codes)
+            return xyz
+        if isinstance(targets, PointSet):
+            return targets.coords
+        return points(targets)
 
     def _support(self, targets):
         """Context manager setting the engine's target support for one prediction (point support here)."""

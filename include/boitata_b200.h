@@ -273,6 +273,17 @@ int btk_set_domains(btk_ctx* ctx, const int32_t* codes);
 int btk_predict_ex(btk_ctx* ctx, int64_t m, const double* xyz, const int8_t* kinds, const int32_t* domains,
                    int32_t kind, double kparam, int32_t precision, const btk_outputs* out,
                    const btk_diagnostics* diag);
+/* Kriging weights (weights_many, crates/estimation/src/batch.rs:76-95, as
+ * the estimator's weight declustering calls it, crates/py/src/estimation.rs:
+ * 1509-1585): btk_predict_ex's outputs at m host targets (out->value and
+ * out->status required; `domains` as btk_predict_ex), and for each target
+ * estimated its list (idx, m x max_samples, -1 past the samples used) and
+ * the weight of each listed sample (weights, m x max_samples, 0 past them;
+ * spread over coincident clusters as the estimate spreads them). Rows of
+ * targets not estimated are -1 and 0. The weights come from the dense-LU
+ * diagnostics pass in FP64, whatever `precision` the estimates take. */
+int btk_predict_weights(btk_ctx* ctx, int64_t m, const double* xyz, int32_t kind, double kparam, int32_t precision,
+                        const int32_t* domains, const btk_outputs* out, int64_t* idx, double* weights);
 /* The same with device arrays (d_xyz as btk_predict_device), queued on `stream`. */
 int btk_predict_ex_device(btk_ctx* ctx, int64_t m, const double* d_xyz, const int8_t* d_kinds,
                           const int32_t* d_domains, int32_t kind, double kparam, int32_t precision,

@@ -98,3 +98,10 @@ def test_block_kriging_rejects_bad_support(options, match):
     vg, s = bt.Variogram([("spherical", 1.0, 40.0)]), bt.Search(radius=50)
     with pytest.raises(bt.InvalidInput, match=match):
         bt.BlockKriging(vg, s, **{"size": (10, 10), **options})
+
+
+def test_weight_declustering_needs_a_kriging_estimator():
+    with pytest.raises(bt.InvalidInput, match="linear in the data"):
+        bt.weight_declustering(np.zeros((3, 2)), np.zeros(3), np.zeros((2, 2)), estimator=object())
+    d = bt.Declustering(weights=np.ones(2), mean=1.0, cell_size=float("nan"))
+    assert d.mean == 1.0 and np.isnan(d.cell_size)

@@ -292,16 +292,18 @@ def cond_tolerance(w, ref, t, floor):
     return max(floor, 2e-15 * np.linalg.cond(cov))
 
 
-def test_ill_conditioned_systems(oracle):
-    # c5 in small: clustered holes, 10 % of samples copied 0.01 m away, Gaussian model with a 1e-4 nugget,
-    # 64 neighbours. Condition numbers reach ~5e5, so two FP64 evaluation orders differ by up to ~1e-15
-    # times the condition number: each FP64 system is held to max(1e-10, 2e-15 cond). The mixed form
-    # refines these systems iteratively from their FP32 factors: fewer than 5 % may fall back to FP64, and
-    # every result is held to 1e-6 against the oracle.
-    w = W.c5(holes=160)
+@pytest.mark.parametrize("holes,blocks", [(160, 2000), (1600, 20000)])
+def test_ill_conditioned_systems(oracle, holes, blocks):
+    # c5: clustered holes, 10 % of samples copied 0.01 m away, Gaussian model with a 1e-4 nugget, 64
+    # neighbours; at 160 holes (20,000 samples) and at its full 1,600 holes (220,000 samples), with 20,000
+    # blocks of the 10.24M-block model. Condition numbers reach ~5e5, so two FP64 evaluation orders differ by
+    # up to ~1e-15 times the condition number: each FP64 system is held to max(1e-10, 2e-15 cond). The
+    # mixed form refines these systems iteratively from their FP32 factors: fewer than 5 % may fall back to
+    # FP64, and every result is held to 1e-6 against the oracle.
+    w = W.c5(holes=holes)
     rng = np.random.default_rng(0)
-    cent = centroids(oracle, w)
-    targets = cent[rng.choice(len(cent), 2000, replace=False)]
+    cells = np.sort(rng.choice(w.geometry.cells(), blocks, replace=False))
+    targets = oracle.centroids(w.geometry.origin, w.geometry.size, w.geometry.count, w.geometry.rotation)[cells]
     ref = oracle.estimate_many(targets, w.coords, w.values, w.search, w.variogram)
     fp64 = OrdinaryKriging(w.variogram, w.search).fit(w.coords, w.values)
     assert_same_neighbors(fp64, oracle, w.coords, w.search, w.variogram, targets[:300])
