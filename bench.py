@@ -42,9 +42,9 @@ sys.path.insert(0, ROOT)
 # DRAM bytes per system of k_tile<mixed> from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum over
 # the systems of the launch), valid for the tile kernel's sources whose hash is TILE_TRAFFIC_SOURCE: when they
 # change, the line reports no traffic until a new capture is made.
-TILE_DRAM_BYTES_PER_SYSTEM = (132830720 + 12697344) / 800000
-TILE_WARP_INSTRUCTIONS_PER_SYSTEM = 2754600250 / 800000  # sm__inst_executed.sum of the same capture
-TILE_TRAFFIC_SOURCE = "8249380f74c2b07c"
+TILE_DRAM_BYTES_PER_SYSTEM = (132878336 + 12759808) / 800000
+TILE_WARP_INSTRUCTIONS_PER_SYSTEM = 2754602618 / 800000  # sm__inst_executed.sum of the same capture
+TILE_TRAFFIC_SOURCE = "c862de9d82734b4b"
 TILE_SOURCES = ("boitata_b200/csrc/btk_tile.cu", "boitata_b200/csrc/btk_device.cuh", "boitata_b200/csrc/btk_internal.h")
 
 

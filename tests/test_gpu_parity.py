@@ -284,18 +284,20 @@ def test_ordinary_and_simple_kriging_in_one_launch(oracle, precision, tol):
 
 
 def cond_tolerance(oracle, w, ref, targets, t, floor):
-    """The tolerance of target t's FP64 estimate: max(floor, eps cond sum|w_i z_i| / (1 + |v|)). The GPU and the
-    host evaluate the covariances with different exp implementations, which may differ in the last bit; a
-    perturbation of one ulp in the entries of a system of condition number cond moves its estimate v = w'z by
-    up to about eps cond sum|w_i z_i|, and cancellation makes that sum large against |v| (a c5 system of
-    condition 3e5 with sum|w_i z_i| = 163 and v = -0.05 moved by up to 1.0e-9 under random one-ulp
-    perturbations, solved in extended precision)."""
+    """The tolerance of target t's FP64 estimate: max(floor, eps cond |w|_2 |z|_2 / (1 + |v|)). The GPU and the
+    host evaluate the covariances with different exp implementations, whose results may differ in the last bit,
+    and each side's solve is backward stable to about that size. For entrywise relative perturbations of at
+    most eps of a covariance matrix C with nonnegative entries, |dC|_2 <= eps |C|_2, so the weights move by at
+    most eps cond(C) |w|_2 to first order and the estimate v = w'z by eps cond |w|_2 |z|_2. Two c5 systems
+    checked in extended precision: condition 6.1e5, the oracle 6.2e-10 from the exact solve and the GPU 1e-11
+    (bound 4.3e-9); condition 3.2e5 with v = -0.05, the GPU 1.6e-9 and the oracle 1e-10 from it (bound
+    5.9e-8; one-ulp random perturbations of its entries moved v by up to 1.0e-9)."""
     nb = [i for i in ref["neighbors"][t] if i >= 0]
     d = np.sqrt(((w.coords[nb][:, None] - w.coords[nb][None]) ** 2).sum(-1))
     cov = np.where(d > 0, np.exp(-3 * (d / 200.0) ** 2), 1.0 + 1e-4)
     _, _, wt = oracle.krige("ordinary", targets[t], w.coords[nb], w.values[nb], w.variogram)
-    spread = np.abs(wt * w.values[nb]).sum()
-    return max(floor, np.finfo(float).eps * np.linalg.cond(cov) * spread / (1.0 + abs(ref["value"][t])))
+    size = np.linalg.norm(wt) * np.linalg.norm(w.values[nb])
+    return max(floor, np.finfo(float).eps * np.linalg.cond(cov) * size / (1.0 + abs(ref["value"][t])))
 
 
 @pytest.mark.parametrize("holes,blocks", [(160, 2000), (1600, 20000)])
