@@ -1273,6 +1273,7 @@ int btk_predict_weights(btk_ctx* ctx, int64_t m, const double* xyz, int32_t kind
   if ((rc = upload_targets(ctx, m, xyz))) return rc;
   const size_t k = size_t(ctx->search.max_samples), mk = size_t(m) * k;
   CK(ctx->wts.grow(mk));
+  CK(cudaMemsetAsync(ctx->wts.p, 0, mk * sizeof(double), ctx->stream));  // no row keeps an earlier call's weights
   if (domains) {
     CK(ctx->tdom.grow(size_t(m)));
     CK(cudaMemcpyAsync(ctx->tdom.p, domains, size_t(m) * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
