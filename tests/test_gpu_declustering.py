@@ -137,3 +137,50 @@ def test_weights_entry_point_lists_and_errors(oracle):
         assert np.dot(w[j, : len(lst)], z[lst]) == pytest.approx(value[j], abs=1e-10)
     with pytest.raises(bt.InvalidInput, match="no target was estimated"):
         bt.weight_declustering(xy, z, [[900.0, 900.0]], estimator=bt.OrdinaryKriging(MODEL, SEARCH))
+
+
+def weights_at(est, t):
+    """btk_predict_weights at targets t (m x 3): (status, idx, weights)."""
+    import ctypes
+
+    m, k = len(t), est.searches[0].max_samples
+    value, status = np.full(m, np.nan), np.zeros(m, dtype=np.int8)
+    idx, w = np.zeros((m, k), dtype=np.int64), np.zeros((m, k))
+    o = N.OutputsC(value.ctypes.data, None, None, None, status.ctypes.data)
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    ctx = est._ctx
+    ctx.check(ctx._lib.btk_predict_weights(ctx.handle, m, t.ctypes.data, est._kind, est._kparam, N.FP64, None,
+                                           ctypes.byref(o), idx.ctypes.data, w.ctypes.data), "weights")
+    return status, idx, w
+
+
+def test_weights_of_coincident_clusters_and_blocks(oracle):
+    """Per-system weights against the oracle's krige (krige.rs:83-95: the coincident guard merges samples
+    within 1e-6 m and spreads the cluster's weight evenly) and block_krige (block.rs:120-198)."""
+    rng = np.random.default_rng(12)
+    xy = rng.uniform(0, 100, (120, 2))
+    xy = np.vstack([xy, xy[:15] + [3e-7, 0.0]])  # near-duplicates: kept at fit, merged by the guard
+    z = np.sin(xy[:, 0] / 15) + xy[:, 1] / 50
+    locs = np.column_stack([xy, np.zeros(len(xy))])
+    t = np.column_stack([rng.uniform(0, 100, (300, 2)), np.zeros(300)])
+    est = bt.OrdinaryKriging(MODEL, SEARCH).fit(xy, z)
+    status, idx, w = weights_at(est, t)
+    merged = 0
+    for j in range(len(t)):
+        lst = idx[j][idx[j] >= 0].tolist()
+        st, _, ref = oracle.krige("ordinary", t[j], locs[lst], z[lst], MODEL)
+        assert (status[j] == N.ST_OK) == (st == 0)
+        if st == 0:
+            np.testing.assert_allclose(w[j, : len(lst)], ref, rtol=0, atol=1e-10 * (1 + np.abs(ref).max()))
+            merged += any(i >= 120 for i in lst)
+    assert merged > 20  # the guard's path was taken
+    blk = bt.BlockKriging(MODEL, SEARCH, size=(10, 10), discretization=(3, 3, 1)).fit(xy[:120], z[:120])
+    with blk._support(None):
+        status, idx, w = weights_at(blk, t)
+    off = oracle.block_offsets((10.0, 10.0, 1.0), (3, 3, 1))
+    for j in range(len(t)):
+        lst = idx[j][idx[j] >= 0].tolist()
+        st, _, ref = oracle.block_krige(t[j], off, locs[lst], z[lst], MODEL)
+        assert (status[j] == N.ST_OK) == (st == 0)
+        if st == 0:
+            np.testing.assert_allclose(w[j, : len(lst)], ref, rtol=0, atol=1e-10 * (1 + np.abs(ref).max()))
