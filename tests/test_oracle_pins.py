@@ -655,3 +655,24 @@ def test_hard_domains_are_separate_estimations(oracle):
     none = oracle.estimate_many(targets[:5], xyz, v, s, vg, domains=dom, target_domains=np.full(5, -1),
                                 neighbors=False)
     assert np.all(none["status"] == 1) and np.all(np.isnan(none["value"]))
+
+
+@pytest.mark.parametrize("rules", [{}, {"max_per_hole": 4}, {"max_per_hole": 4, "octant": True}],
+                         ids=["plain", "per_hole", "per_hole_octant"])
+def test_search_scale_tree_matches_brute_force(oracle, rules):
+    """tests/search_scale.rs:73-127 on a subset: the oracle's tree equals the test's brute force among
+    504,100 drill-hole composites at lattice targets (exact ties), including the three targets that once
+    lost a neighbour."""
+    from search_scale_case import brute, composites, targets
+
+    locs, vals, holes = composites()
+    t = targets()
+    sub = np.r_[np.arange(0, len(t) - 3, 311), len(t) - 3, len(t) - 2, len(t) - 1]
+    s = Search(radius=200.0, min_samples=4, max_samples=32, **rules)
+    ref = oracle.estimate_many(t[sub], locs, vals, s, Variogram([("spherical", 1.0, 100.0)]), holes=holes)
+    for j, k in enumerate(sub):
+        b = brute(t[k], locs, holes, 200.0, 32, 4, **rules)
+        assert (b is None) == (ref["status"][j] == 1), k
+        if b is not None:
+            got = ref["neighbors"][j]
+            assert got[got >= 0].tolist() == b, k
