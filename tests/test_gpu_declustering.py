@@ -184,3 +184,26 @@ def test_weights_of_coincident_clusters_and_blocks(oracle):
         assert (status[j] == N.ST_OK) == (st == 0)
         if st == 0:
             np.testing.assert_allclose(w[j, : len(lst)], ref, rtol=0, atol=1e-10 * (1 + np.abs(ref).max()))
+
+
+def test_lowers_clustered_samples_and_the_bias():
+    """batch.rs:1293-1306: a 10 x 10 grid at 10 m plus 60 samples on a spiral where the field is high; over
+    targets covering the square, the clustered samples weigh less than half the grid's and the declustered
+    mean lies within a quarter of the naive mean's bias from the field's true mean."""
+    field = lambda x, y: np.sin(x / 15.0) + y / 40.0  # noqa: E731
+    i = np.arange(100)
+    grid = np.column_stack([(i % 10) * 10.0 + 5.0, (i // 10) * 10.0 + 5.0])
+    k = np.arange(60)
+    a, r = k * 2.4, 1.0 + np.sqrt(k) * 1.5
+    spiral = np.column_stack([23.0 + r * np.cos(a), 85.0 + r * np.sin(a)])
+    xy = np.vstack([grid, spiral])
+    z = field(xy[:, 0], xy[:, 1])
+    c = np.arange(10_000)
+    cover = np.column_stack([(c % 100) + 0.5, (c // 100) + 0.5])
+    truth = field(cover[:, 0], cover[:, 1]).mean()
+    naive = z.mean()
+    vg = bt.Variogram([("spherical", 1.0, 40.0)])
+    d = bt.weight_declustering(xy, z, cover, estimator=bt.OrdinaryKriging(vg, bt.Search(radius=50, max_samples=16)))
+    assert abs(d.weights.sum() - 160.0) < 1e-9
+    assert d.weights[100:].mean() < 0.5 * d.weights[:100].mean()
+    assert abs(d.mean - truth) < 0.25 * abs(naive - truth)
