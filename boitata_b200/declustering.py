@@ -84,11 +84,11 @@ def weight_declustering(coords, values, targets, *, estimator):
     if not isinstance(estimator, _Base):
         raise InvalidInput("weight declustering needs an estimator linear in the data (a kriging estimator)")
     vals = np.asarray(column(coords, values, "values"), dtype=np.float64)
+    locs = _sample_points(coords, None)
     est = copy.copy(estimator)
     est._ctx = est._pass = est._samples = None
     est._holes = est._domains = est._domain_labels = None
-    est.fit(coords, vals)
-    locs = _sample_points(coords, est._ctx)
+    est.fit(locs, vals)  # samples sharing a location keep the first, with a warning
     kept = est._samples[0]
     n_all, n_kept = len(locs), len(kept)
 
