@@ -293,8 +293,9 @@ def loo_gradient(args, dev, ws=1, rank=0):
 
 def callers(dev):
     """The paths around the headline one, each timed once warm (wall clock around the host call, inputs on
-    the host): the dense LU of 128-sample and power-model systems and a calibrated search over c1's 50,000
-    blocks, and one sequential Gaussian simulation of 400,000 nodes conditioned on c2's 50,000 composites."""
+    the host): the dense LU of 128-sample and power-model systems, a calibrated search and weight declustering
+    over c1's 50,000 blocks, and one sequential Gaussian simulation of 400,000 nodes conditioned on c2's 50,000
+    composites."""
     import torch
 
     import boitata_b200 as bt
@@ -324,6 +325,17 @@ def callers(dev):
             ts.append(time.perf_counter() - t0)
         out[name] = {"blocks_per_s": g.cells() / float(np.median(ts)), "blocks": g.cells(),
                      "workload": "c1 samples and block model, " + name.replace("_", " ")}
+    # Weight declustering: the kriging weights each c1 sample receives over the 50,000 blocks (search,
+    # solve and the FP64 weights pass on the device, the target-order sum on the host).
+    est = bt.OrdinaryKriging(w.variogram, w.search)
+    bt.weight_declustering(w.coords, w.values, g, estimator=est)
+    ts = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        bt.weight_declustering(w.coords, w.values, g, estimator=est)
+        ts.append(time.perf_counter() - t0)
+    out["weight_declustering"] = {"blocks_per_s": g.cells() / float(np.median(ts)), "blocks": g.cells(),
+                                  "workload": "c1 samples and block model, OK weights summed per sample"}
     w2 = workloads.c2()
     scores, _ = normal_score(w2.values)
     sim_grid = bt.Geometry((0.0, 0.0, 0.0), (5.0, 5.0, 6.25), (100, 100, 40))

@@ -13,6 +13,7 @@ sums them in, so a call is reproducible to the bit.
 
 import copy
 import ctypes
+import threading
 from dataclasses import dataclass
 
 import numpy as np
@@ -31,6 +32,20 @@ class Declustering:
     weights: np.ndarray
     mean: float
     cell_size: float
+
+
+_LOCAL = threading.local()
+
+
+def _context(device):
+    """A context of this thread for declustering calls on `device`, kept between calls: each call fits its
+    samples on it again, and its device buffers, grown by earlier calls, are reused instead of allocated."""
+    cache = getattr(_LOCAL, "contexts", None)
+    if cache is None:
+        cache = _LOCAL.contexts = {}
+    if device not in cache:
+        cache[device] = N.Context(device)
+    return cache[device]
 
 
 def _seq_sum(x):
@@ -86,8 +101,9 @@ def weight_declustering(coords, values, targets, *, estimator):
     vals = np.asarray(column(coords, values, "values"), dtype=np.float64)
     locs = _sample_points(coords, None)
     est = copy.copy(estimator)
-    est._ctx = est._pass = est._samples = None
+    est._pass = est._samples = None
     est._holes = est._domains = est._domain_labels = None
+    est._ctx = _context(est._device)
     est.fit(locs, vals)  # samples sharing a location keep the first, with a warning
     kept = est._samples[0]
     n_all, n_kept = len(locs), len(kept)
@@ -109,9 +125,9 @@ def weight_declustering(coords, values, targets, *, estimator):
             remaining = remaining[~got]
     t_all = np.concatenate(tidx) if tidx else np.zeros(0, dtype=np.int64)
     order = np.argsort(t_all, kind="stable")  # target order; each target's list stays in its order
-    sums = np.zeros(n_kept)
-    if len(order):
-        np.add.at(sums, np.concatenate(sidx)[order], np.concatenate(wts)[order])
+    # bincount adds each bin's weights in input order, from 0.0: the reference's sum, term for term
+    sums = (np.bincount(np.concatenate(sidx)[order], weights=np.concatenate(wts)[order], minlength=n_kept)
+            if len(order) else np.zeros(n_kept))
     total = _seq_sum(sums)
     if not total > 0.0:
         raise InvalidInput("no target was estimated")
